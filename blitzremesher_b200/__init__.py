@@ -1,0 +1,346 @@
+"""B200-native candidate-audit engine for BlitzRemesher.
+
+Python mirror of the C ABI in ``include/blitz_audit.h``. The compute path is
+the CUDA library ``libblitz_b200.so``; there is no CPU fallback: loading fails
+loudly if the library is missing and every audit call reports
+``BLITZ_UNAVAILABLE`` without a GPU.
+
+Names follow the reference: ``evaluate`` mirrors ``blitz::evaluate``
+(src/evaluate.cpp:353) and ``AuditSession.candidates`` mirrors the four-gate
+gate of src/neural/generate.cpp:365-388 applied to GpuActionState trials.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+from pathlib import Path
+from typing import Optional, Sequence
+
+import numpy as np
+
+from . import synthetic  # noqa: F401
+
+HERE = Path(__file__).resolve().parent
+LIB_PATH = HERE / "libblitz_b200.so"
+
+BLITZ_OK, BLITZ_INVALID_ARGUMENT, BLITZ_OUT_OF_MEMORY, BLITZ_INTERNAL_ERROR = 0, 1, 2, 3
+BLITZ_CANCELLED, BLITZ_BUDGET_LIMITED, BLITZ_UNAVAILABLE = 4, 5, 6
+ABI_VERSION = 5
+
+
+class BlitzError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"blitz status {status}: {message}")
+        self.status = status
+
+
+class Stream(C.Structure):
+    _fields_ = [("data", C.c_void_p), ("count", C.c_size_t), ("stride", C.c_size_t)]
+
+
+class BlitzMesh(C.Structure):
+    _fields_ = [("struct_size", C.c_uint32), ("abi_version", C.c_uint32), ("positions", Stream),
+                ("normals", Stream), ("uv", Stream), ("colors", Stream), ("tangents", Stream),
+                ("indices", C.c_void_p), ("index_count", C.c_size_t), ("materials", C.c_void_p),
+                ("material_count", C.c_size_t), ("double_sided", C.c_void_p), ("double_sided_count", C.c_size_t)]
+
+
+class NeuralOptionsV2(C.Structure):
+    _fields_ = [("struct_size", C.c_uint32), ("version", C.c_uint32), ("device", C.c_int32),
+                ("memory_mib", C.c_uint32), ("action_trials", C.c_uint32), ("ranking_seed", C.c_uint32),
+                ("exact_position_bps", C.c_uint16), ("action_batch", C.c_uint8), ("origin", C.c_uint8),
+                ("ranking", C.c_uint8), ("confirmation", C.c_uint8), ("raster_backend", C.c_uint8),
+                ("vertex_storage", C.c_uint8), ("preserve_uv", C.c_uint8), ("overdraw_tiebreak", C.c_uint8),
+                ("cache_rasters", C.c_uint8), ("mask_only_coverage", C.c_uint8), ("direct_targets", C.c_uint8),
+                ("view_batch", C.c_uint8), ("candidate_batch", C.c_uint8), ("reserved", C.c_uint8 * 3)]
+
+
+class NeuralInfo(C.Structure):
+    _fields_ = [("struct_size", C.c_uint32), ("encode_ns", C.c_uint64), ("inference_ns", C.c_uint64),
+                ("decode_ns", C.c_uint64), ("gpu_audit_ns", C.c_uint64), ("reference_audit_ns", C.c_uint64),
+                ("decoded", C.c_uint64), ("legal_collapses", C.c_uint64), ("rejected_collapses", C.c_uint64),
+                ("reference_rejections", C.c_uint64), ("fallback_levels", C.c_uint32)]
+
+
+class EvalSettings(C.Structure):
+    _fields_ = [("struct_size", C.c_uint32), ("profile", C.c_uint8), ("supersample", C.c_uint8),
+                ("max_supersample", C.c_uint8), ("force_two_sided", C.c_uint8), ("conservative_screen", C.c_uint8),
+                ("reserved", C.c_uint8 * 1), ("views_orthographic", C.c_uint16), ("views_perspective", C.c_uint16),
+                ("views_seed", C.c_uint32), ("screen_size", C.c_double), ("limit", C.c_double),
+                ("max_changed_area", C.c_double)]
+
+
+class Measurement(C.Structure):
+    _fields_ = [("error", C.c_double), ("coverage", C.c_double), ("coverage_upper", C.c_double),
+                ("changed_area", C.c_double), ("normal_degrees", C.c_double), ("worst_view", C.c_uint32),
+                ("changed_area_worst_view", C.c_uint32), ("views_evaluated", C.c_uint32),
+                ("supersample", C.c_uint8), ("complete", C.c_uint8), ("passed", C.c_uint8),
+                ("resource_limited", C.c_uint8), ("cancelled", C.c_uint8), ("reserved", C.c_uint8 * 3)]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+
+
+class Collapse(C.Structure):
+    _fields_ = [("from_", C.c_uint32), ("to", C.c_uint32), ("placement", C.c_uint32), ("position", C.c_float * 3)]
+
+
+class Verdict(C.Structure):
+    _fields_ = [("accepted", C.c_uint8), ("failed_gate", C.c_uint8), ("exact_path", C.c_uint8),
+                ("reserved", C.c_uint8), ("removed", C.c_uint32)]
+
+
+COLLAPSE_DTYPE = np.dtype([("from", "<u4"), ("to", "<u4"), ("placement", "<u4"), ("position", "<f4", (3,))])
+VERDICT_DTYPE = np.dtype([("accepted", "u1"), ("failed_gate", "u1"), ("exact_path", "u1"), ("reserved", "u1"),
+                          ("removed", "<u4")])
+MEASUREMENT_DTYPE = np.dtype([("error", "<f8"), ("coverage", "<f8"), ("coverage_upper", "<f8"),
+                              ("changed_area", "<f8"), ("normal_degrees", "<f8"), ("worst_view", "<u4"),
+                              ("changed_area_worst_view", "<u4"), ("views_evaluated", "<u4"),
+                              ("supersample", "u1"), ("complete", "u1"), ("passed", "u1"),
+                              ("resource_limited", "u1"), ("cancelled", "u1"), ("reserved", "u1", (3,))],
+                             align=True)
+assert COLLAPSE_DTYPE.itemsize == C.sizeof(Collapse)
+assert VERDICT_DTYPE.itemsize == C.sizeof(Verdict)
+assert MEASUREMENT_DTYPE.itemsize == C.sizeof(Measurement)
+
+_lib = None
+
+EXPORTS = {
+    "blitz_abi_version": ([], C.c_uint32),
+    "blitz_neural_options_v2_init": ([C.POINTER(NeuralOptionsV2), C.c_size_t], C.c_int),
+    "blitz_eval_settings_init": ([C.POINTER(EvalSettings), C.c_size_t], C.c_int),
+    "blitz_audit_session_create": ([C.POINTER(BlitzMesh), C.POINTER(NeuralOptionsV2), C.POINTER(C.c_void_p),
+                                    C.c_char_p, C.c_size_t], C.c_int),
+    "blitz_audit_session_destroy": ([C.c_void_p], None),
+    "blitz_audit_bind_reference": ([C.c_void_p, C.POINTER(BlitzMesh), C.c_char_p, C.c_size_t], C.c_int),
+    "blitz_audit_evaluate": ([C.c_void_p, C.POINTER(BlitzMesh), C.POINTER(BlitzMesh), C.POINTER(EvalSettings),
+                              C.POINTER(Measurement), C.c_char_p, C.c_size_t], C.c_int),
+    "blitz_audit_actions": ([C.c_void_p, C.c_void_p, C.c_size_t, C.POINTER(C.c_size_t), C.c_char_p, C.c_size_t],
+                            C.c_int),
+    "blitz_audit_raster": ([C.c_void_p, C.POINTER(BlitzMesh), C.c_double, C.c_uint8, C.c_uint16, C.c_uint16,
+                            C.c_uint32, C.c_uint32, C.c_uint8, C.c_void_p, C.c_size_t, C.POINTER(C.c_uint32),
+                            C.POINTER(C.c_uint8), C.c_char_p, C.c_size_t], C.c_int),
+    "blitz_audit_candidates": ([C.c_void_p, C.c_void_p, C.c_size_t, C.POINTER(EvalSettings), C.c_void_p,
+                                C.c_void_p, C.c_char_p, C.c_size_t], C.c_int),
+    "blitz_audit_candidates_device": ([C.c_void_p, C.c_void_p, C.c_size_t, C.POINTER(EvalSettings), C.c_void_p,
+                                       C.c_void_p, C.c_void_p, C.c_char_p, C.c_size_t], C.c_int),
+    "blitz_audit_session_info": ([C.c_void_p, C.POINTER(NeuralInfo)], C.c_int),
+    "blitz_audit_profile_enable": ([C.c_void_p, C.c_int], C.c_int),
+    "blitz_audit_profile_read": ([C.c_void_p, C.c_void_p], C.c_int),
+}
+
+
+class AuditProfile(C.Structure):
+    _fields_ = [("struct_size", C.c_uint32), ("enabled", C.c_uint32), ("launches", C.c_uint64),
+                ("audit_launches", C.c_uint64), ("audit_ms", C.c_double), ("prepare_ms", C.c_double),
+                ("verdict_ms", C.c_double), ("units", C.c_uint64), ("region_samples", C.c_uint64),
+                ("changed_samples", C.c_uint64), ("record_bytes", C.c_uint64)]
+
+
+def library_path() -> Path:
+    return LIB_PATH
+
+
+def load() -> C.CDLL:
+    """Loads the CUDA library (building it if sources are newer). Raises if absent."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    from . import build as _build
+
+    if _build.needs_build():
+        try:
+            _build.build()
+        except Exception as exc:  # pragma: no cover - explicit failure, never a fallback
+            if not LIB_PATH.exists():
+                raise RuntimeError(f"libblitz_b200.so is missing and could not be built: {exc}") from exc
+    if not LIB_PATH.exists():
+        raise RuntimeError("libblitz_b200.so is missing; run blitzremesher_b200/build.py")
+    lib = C.CDLL(str(LIB_PATH))
+    for name, (args, res) in EXPORTS.items():
+        fn = getattr(lib, name)
+        fn.argtypes = args
+        fn.restype = res
+    _lib = lib
+    return lib
+
+
+class _MeshHold:
+    """Keeps numpy arrays alive while a BlitzMesh borrows them."""
+
+    def __init__(self, mesh):
+        self.pos = np.ascontiguousarray(mesh.positions, dtype=np.float32)
+        self.idx = np.ascontiguousarray(mesh.indices, dtype=np.uint32).reshape(-1)
+        self.uv = None if mesh.uv is None else np.ascontiguousarray(mesh.uv, dtype=np.float32)
+        self.mat = None if mesh.materials is None else np.ascontiguousarray(mesh.materials, dtype=np.uint16)
+        self.ds = None if mesh.double_sided is None else np.ascontiguousarray(mesh.double_sided, dtype=np.uint8)
+        m = BlitzMesh()
+        m.struct_size = C.sizeof(BlitzMesh)
+        m.abi_version = ABI_VERSION
+        m.positions = Stream(self.pos.ctypes.data, self.pos.shape[0], 12)
+        if self.uv is not None:
+            m.uv = Stream(self.uv.ctypes.data, self.uv.shape[0], 8)
+        m.indices = self.idx.ctypes.data
+        m.index_count = self.idx.size
+        if self.mat is not None:
+            m.materials, m.material_count = self.mat.ctypes.data, self.mat.size
+        if self.ds is not None:
+            m.double_sided, m.double_sided_count = self.ds.ctypes.data, self.ds.size
+        self.c = m
+
+
+def eval_settings(screen: float, limit: float, views: Sequence[int] = (32, 0, 0xB1172026), supersample: int = 8,
+                  max_supersample: int = 8, max_changed_area: float = 1.0, force_two_sided: bool = False,
+                  conservative_screen: bool = False) -> EvalSettings:
+    s = EvalSettings()
+    load().blitz_eval_settings_init(C.byref(s), C.sizeof(s))
+    s.screen_size, s.limit, s.max_changed_area = screen, limit, max_changed_area
+    s.views_orthographic, s.views_perspective, s.views_seed = int(views[0]), int(views[1]), int(views[2])
+    s.supersample, s.max_supersample = supersample, max_supersample
+    s.force_two_sided, s.conservative_screen = int(force_two_sided), int(conservative_screen)
+    return s
+
+
+def neural_options(**kw) -> NeuralOptionsV2:
+    o = NeuralOptionsV2()
+    load().blitz_neural_options_v2_init(C.byref(o), C.sizeof(o))
+    for k, v in kw.items():
+        setattr(o, k, v)
+    return o
+
+
+def _check(status: int, err) -> None:
+    if status != BLITZ_OK:
+        raise BlitzError(status, err.value.decode(errors="replace"))
+
+
+class AuditSession:
+    """Owns the device-resident source, previous LOD, state topology and plans."""
+
+    def __init__(self, source, options: Optional[NeuralOptionsV2] = None):
+        self.lib = load()
+        self._source = _MeshHold(source)
+        self.handle = C.c_void_p()
+        err = C.create_string_buffer(512)
+        opts = C.byref(options) if options is not None else None
+        _check(self.lib.blitz_audit_session_create(C.byref(self._source.c), opts, C.byref(self.handle), err, 512), err)
+        self._previous = None
+
+    def close(self) -> None:
+        if self.handle:
+            self.lib.blitz_audit_session_destroy(self.handle)
+            self.handle = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def bind_reference(self, previous=None) -> None:
+        err = C.create_string_buffer(512)
+        self._previous = None if previous is None else _MeshHold(previous)
+        ptr = None if previous is None else C.byref(self._previous.c)
+        _check(self.lib.blitz_audit_bind_reference(self.handle, ptr, err, 512), err)
+
+    def evaluate(self, reference, candidate, settings: EvalSettings) -> Measurement:
+        r, c = _MeshHold(reference), _MeshHold(candidate)
+        out = Measurement()
+        err = C.create_string_buffer(512)
+        _check(self.lib.blitz_audit_evaluate(self.handle, C.byref(r.c), C.byref(c.c), C.byref(settings),
+                                             C.byref(out), err, 512), err)
+        return out
+
+    def rasterize(self, mesh, screen: float, supersample: int, views: Sequence[int], view: int,
+                  force_two_sided: bool = False):
+        """Packed coverage mask (u64 words), clipped flag and raster side."""
+        h = _MeshHold(mesh)
+        size = int(np.ceil(screen + 8)) * supersample
+        words = np.zeros((size * size + 63) // 64, dtype=np.uint64)
+        out_size, clipped = C.c_uint32(), C.c_uint8()
+        err = C.create_string_buffer(512)
+        _check(self.lib.blitz_audit_raster(self.handle, C.byref(h.c), screen, supersample, int(views[0]),
+                                           int(views[1]), int(views[2]), view, int(force_two_sided),
+                                           words.ctypes.data, words.size, C.byref(out_size), C.byref(clipped),
+                                           err, 512), err)
+        return words, bool(clipped.value), int(out_size.value)
+
+    def actions(self) -> np.ndarray:
+        count = C.c_size_t()
+        err = C.create_string_buffer(512)
+        _check(self.lib.blitz_audit_actions(self.handle, None, 0, C.byref(count), err, 512), err)
+        out = np.zeros(count.value, dtype=COLLAPSE_DTYPE)
+        _check(self.lib.blitz_audit_actions(self.handle, out.ctypes.data, out.size, C.byref(count), err, 512), err)
+        return out
+
+    def candidates(self, collapses: np.ndarray, gates: Sequence[EvalSettings], measurements: bool = False):
+        collapses = np.ascontiguousarray(collapses, dtype=COLLAPSE_DTYPE)
+        n = collapses.size
+        verdicts = np.zeros(n, dtype=VERDICT_DTYPE)
+        meas = np.zeros((n, 4), dtype=MEASUREMENT_DTYPE) if measurements else None
+        g = (EvalSettings * 4)(*gates)
+        err = C.create_string_buffer(512)
+        _check(self.lib.blitz_audit_candidates(self.handle, collapses.ctypes.data, n, g, verdicts.ctypes.data,
+                                               None if meas is None else meas.ctypes.data, err, 512), err)
+        return (verdicts, meas) if measurements else verdicts
+
+    def candidates_device(self, collapses_ptr: int, n: int, gates: Sequence[EvalSettings], verdicts_ptr: int,
+                          measurements_ptr: int = 0, stream: int = 0) -> None:
+        g = (EvalSettings * 4)(*gates)
+        err = C.create_string_buffer(512)
+        _check(self.lib.blitz_audit_candidates_device(self.handle, collapses_ptr, n, g, verdicts_ptr,
+                                                      measurements_ptr or None, stream or None, err, 512), err)
+
+    def profile(self, enable: Optional[bool] = None) -> dict:
+        """Enables/disables kernel profiling (resetting counters) or reads it."""
+        if enable is not None:
+            assert self.lib.blitz_audit_profile_enable(self.handle, int(enable)) == BLITZ_OK
+        p = AuditProfile()
+        p.struct_size = C.sizeof(AuditProfile)
+        assert self.lib.blitz_audit_profile_read(self.handle, C.byref(p)) == BLITZ_OK
+        return {k: getattr(p, k) for k, _ in p._fields_ if k != "struct_size"}
+
+    def info(self) -> dict:
+        i = NeuralInfo()
+        i.struct_size = C.sizeof(NeuralInfo)
+        assert self.lib.blitz_audit_session_info(self.handle, C.byref(i)) == BLITZ_OK
+        return {k: getattr(i, k) for k, _ in i._fields_ if k != "struct_size"}
+
+
+def evaluate(reference, candidate, settings: EvalSettings, session: Optional[AuditSession] = None) -> Measurement:
+    """blitz::evaluate on the GPU. The session supplies bounds (of its source)."""
+    own = session is None
+    s = session or AuditSession(reference)
+    try:
+        return s.evaluate(reference, candidate, settings)
+    finally:
+        if own:
+            s.close()
+
+
+def midpoint_collapses(actions: np.ndarray) -> np.ndarray:
+    out = np.zeros(actions.size, dtype=COLLAPSE_DTYPE)
+    out["from"], out["to"] = actions["from"], actions["to"]
+    return out
+
+
+def four_gates(search: EvalSettings, audit: EvalSettings, source_limit: float, transition_limit: float):
+    """Gate settings in the reference order: source@search, previous@search,
+    source@audit, previous@audit (generate.cpp:365-388); the search gates use
+    max_changed_area = 1 (chain.cpp:187)."""
+    gates = []
+    for base, is_audit in ((search, False), (audit, True)):
+        for limit in (source_limit, transition_limit):
+            g = EvalSettings()
+            C.memmove(C.byref(g), C.byref(base), C.sizeof(EvalSettings))
+            g.limit = limit
+            if not is_audit:
+                g.max_changed_area = 1.0
+            gates.append(g)
+    return gates

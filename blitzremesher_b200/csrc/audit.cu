@@ -1,0 +1,394 @@
+// Incremental candidate audit and four-gate verdicts.
+//
+// A collapse changes coverage only where the faces of faces(from) U faces(to)
+// land, before or after. For every (candidate, view) one warp rasterizes those
+// faces (old and new) over their joint bounding box, derives the candidate's
+// per-sample face count from the resident state counts (count - old + new),
+// builds the coverage words with __ballot_sync, updates the XOR/OR popcounts
+// against the resident reference mask, and measures the exact squared
+// distance of every changed sample by a row scan over coverage words. The
+// result equals a full re-raster of the candidate (evaluate.cpp:125-209)
+// sample for sample.
+#include "kernels.cuh"
+
+namespace b200 {
+namespace {
+
+constexpr int kAuditWarps = 8;
+constexpr int kRegionWords = 4;  // region width <= 128 samples after 32-alignment
+constexpr int kRegionRows = 128; // region height
+constexpr int kQueue = 512;      // changed samples per (candidate, view)
+
+struct WarpScratch {
+    FaceSetup faces[2 * kMaxAffected];
+    uint32_t region[kRegionRows * kRegionWords];
+    uint32_t queue[kQueue];
+};
+
+__device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31; }
+
+__device__ __forceinline__ uint32_t size_mask(uint32_t size, uint32_t chunk) {
+    uint32_t rem = size - chunk * 32;
+    return rem >= 32 ? 0xffffffffu : ((1u << rem) - 1u);
+}
+// Columns [32*chunk, 32*chunk+32) of `row` from a linear bit stream (one
+// padding word at the end of every mask keeps the second load in bounds).
+__device__ __forceinline__ uint32_t chunk_global(const uint32_t* bits, uint32_t size, uint32_t row, uint32_t chunk) {
+    size_t b = size_t(row) * size + size_t(chunk) * 32;
+    uint32_t sh = uint32_t(b & 31);
+    size_t w = b >> 5;
+    uint32_t v = bits[w];
+    if (sh) v = (v >> sh) | (bits[w + 1] << (32 - sh));
+    return v & size_mask(size, chunk);
+}
+
+struct CandMask {
+    const uint32_t* state; // state coverage outside the region
+    const uint32_t* region;
+    uint32_t size, y0, y1, c0, words;
+    __device__ uint32_t chunk(uint32_t row, uint32_t c) const {
+        if (row >= y0 && row <= y1 && c >= c0 && c < c0 + words)
+            return region[(row - y0) * words + (c - c0)] & size_mask(size, c);
+        return chunk_global(state, size, row, c);
+    }
+};
+struct RefMask {
+    const uint32_t* bits;
+    uint32_t size;
+    __device__ uint32_t chunk(uint32_t row, uint32_t c) const { return chunk_global(bits, size, row, c); }
+};
+
+// Smallest |dx| <= maxdx with a covered sample at (x+dx, row); kNone if none.
+template <class M> __device__ uint32_t nearest_in_row(const M& mask, uint32_t row, uint32_t x, uint32_t maxdx) {
+    uint32_t cx = x >> 5, bx = x & 31, best = kNone;
+    uint32_t w = mask.chunk(row, cx);
+    uint32_t left = w & (bx == 31 ? 0xffffffffu : ((2u << bx) - 1u));
+    uint32_t right = w & (0xffffffffu << bx);
+    if (left) best = bx - (31 - __clz(left));
+    if (right) {
+        uint32_t d = (__ffs(right) - 1) - bx;
+        best = d < best ? d : best;
+    }
+    if (best == 0) return 0;
+    // Left chunks.
+    for (uint32_t c = cx; c-- > 0;) {
+        uint32_t nearest = x - (c * 32 + 31);
+        if (nearest > maxdx || nearest >= best) break;
+        uint32_t v = mask.chunk(row, c);
+        if (v) {
+            uint32_t d = x - (c * 32 + (31 - __clz(v)));
+            best = d < best ? d : best;
+            break;
+        }
+    }
+    uint32_t chunks = (mask.size + 31) >> 5;
+    for (uint32_t c = cx + 1; c < chunks; ++c) {
+        uint32_t nearest = c * 32 - x;
+        if (nearest > maxdx || nearest >= best) break;
+        uint32_t v = mask.chunk(row, c);
+        if (v) {
+            uint32_t d = c * 32 + (__ffs(v) - 1) - x;
+            best = d < best ? d : best;
+            break;
+        }
+    }
+    return best <= maxdx ? best : kNone;
+}
+
+// Exact squared Euclidean distance from (x, y) to the nearest covered sample.
+template <class M> __device__ uint32_t nearest_d2(const M& mask, uint32_t x, uint32_t y) {
+    const uint32_t size = mask.size;
+    uint32_t best = kNone;
+    for (uint32_t dy = 0;; ++dy) {
+        uint64_t dy2 = uint64_t(dy) * dy;
+        if (best != kNone && dy2 >= best) break;
+        bool any = false;
+        for (int side = 0; side < (dy ? 2 : 1); ++side) {
+            int64_t row = side ? int64_t(y) + dy : int64_t(y) - dy;
+            if (row < 0 || row >= int64_t(size)) continue;
+            any = true;
+            uint32_t maxdx = best == kNone ? size : uint32_t(sqrtf(float(best - dy2))) + 1;
+            uint32_t dx = nearest_in_row(mask, uint32_t(row), x, maxdx);
+            if (dx != kNone) {
+                uint64_t d = uint64_t(dx) * dx + dy2;
+                if (d < best) best = uint32_t(d);
+            }
+        }
+        if (!any) break;
+    }
+    return best;
+}
+
+__device__ __forceinline__ Proj project_pt(const PlanDev& plan, const Camera& cam, float x, float y, float z) {
+    return project(x, y, z, plan.center, cam, plan.ss, plan.size);
+}
+
+__device__ void audit_view(const CandidateRecord& rec, const PlanDev& plan, uint32_t v, WarpScratch& ws,
+                           ViewRecord* out, unsigned long long* stats) {
+    const uint32_t lane = lane_id();
+    const PlanView pv = plan.views[v];
+    const Camera cam = plan.cameras[v];
+    const uint32_t size = plan.size;
+    const uint32_t K = rec.count;
+    // Face setups: old faces at [0, K), candidate faces at [32, 32 + K).
+    bool old_ok = false, new_ok = false, old_clip = false, new_clip = false;
+    if (lane < K) {
+        const AffectedFace& af = rec.faces[lane];
+        Proj po[3], pn[3];
+        Proj pp = project_pt(plan, cam, rec.placement[0], rec.placement[1], rec.placement[2]);
+        for (int j = 0; j < 3; ++j) {
+            po[j] = project_pt(plan, cam, af.p[3 * j], af.p[3 * j + 1], af.p[3 * j + 2]);
+            pn[j] = (af.moved >> j) & 1 ? pp : po[j];
+        }
+        bool two = plan.force_two || af.two;
+        FaceSetup so = setup_face(po[0], po[1], po[2], cam.perspective != 0, two, size);
+        ws.faces[lane] = so;
+        old_ok = so.status == kFaceOk;
+        old_clip = so.status == kFaceClipZ || so.status == kFaceClipBox;
+        if (af.kept) {
+            FaceSetup sn = setup_face(pn[0], pn[1], pn[2], cam.perspective != 0, two, size);
+            ws.faces[32 + lane] = sn;
+            new_ok = sn.status == kFaceOk;
+            new_clip = sn.status == kFaceClipZ || sn.status == kFaceClipBox;
+        }
+    }
+    const uint32_t ok_old = __ballot_sync(0xffffffffu, old_ok), ok_new = __ballot_sync(0xffffffffu, new_ok);
+    const int clip_delta = __popc(__ballot_sync(0xffffffffu, new_clip)) - __popc(__ballot_sync(0xffffffffu, old_clip));
+    int x0 = 1 << 30, y0 = 1 << 30, x1 = -1, y1 = -1;
+    if (old_ok) {
+        const FaceSetup& s = ws.faces[lane];
+        x0 = min(x0, s.x0), x1 = max(x1, s.x1), y0 = min(y0, s.y0), y1 = max(y1, s.y1);
+    }
+    if (new_ok) {
+        const FaceSetup& s = ws.faces[32 + lane];
+        x0 = min(x0, s.x0), x1 = max(x1, s.x1), y0 = min(y0, s.y0), y1 = max(y1, s.y1);
+    }
+    for (int o = 16; o; o >>= 1) {
+        x0 = min(x0, __shfl_xor_sync(0xffffffffu, x0, o));
+        y0 = min(y0, __shfl_xor_sync(0xffffffffu, y0, o));
+        x1 = max(x1, __shfl_xor_sync(0xffffffffu, x1, o));
+        y1 = max(y1, __shfl_xor_sync(0xffffffffu, y1, o));
+    }
+    __syncwarp();
+    ViewRecord r;
+    r.pad = 0;
+    r.flags = pv.clipped_ref ? kRecClippedRef : 0;
+    r.ca = pv.cov_ref > 0;
+    if (int64_t(pv.clip_state) + clip_delta > 0 || !plan.state_is_ref) {
+        // A clipped candidate keeps the CPU's partial-raster values; a state
+        // that differs from the reference needs the full distance field.
+        r.flags |= kRecFallback | (int64_t(pv.clip_state) + clip_delta > 0 ? kRecClippedCand : 0);
+        r.max_d2 = 0, r.changed = 0, r.total = 0, r.cb = 0;
+        if (lane == 0) out[v] = r;
+        return;
+    }
+    int dchg = 0, dtot = 0, dcov = 0;
+    uint32_t qn = 0;
+    bool fallback = false;
+    CandMask cmask;
+    cmask.state = pv.state_bits;
+    cmask.region = ws.region;
+    cmask.size = size;
+    if (x1 >= 0) {
+        const int wx0 = x0 & ~31;
+        const int words = ((x1 - wx0) >> 5) + 1, rows = y1 - y0 + 1;
+        cmask.y0 = uint32_t(y0), cmask.y1 = uint32_t(y1), cmask.c0 = uint32_t(wx0 >> 5), cmask.words = uint32_t(words);
+        if (words > kRegionWords || rows > kRegionRows) {
+            fallback = true;
+        } else {
+            for (int y = y0; y <= y1; ++y)
+                for (int w = 0; w < words; ++w) {
+                    const int x = wx0 + 32 * w + int(lane);
+                    const bool inside = x < int(size);
+                    int delta = 0;
+                    if (inside) {
+                        for (uint32_t m = ok_old; m; m &= m - 1) {
+                            const FaceSetup& s = ws.faces[__ffs(m) - 1];
+                            if (x >= s.x0 && x <= s.x1 && y >= s.y0 && y <= s.y1 && face_covers(s, x, y)) --delta;
+                        }
+                        for (uint32_t m = ok_new; m; m &= m - 1) {
+                            const FaceSetup& s = ws.faces[32 + __ffs(m) - 1];
+                            if (x >= s.x0 && x <= s.x1 && y >= s.y0 && y <= s.y1 && face_covers(s, x, y)) ++delta;
+                        }
+                    }
+                    const size_t i = size_t(y) * size + size_t(x);
+                    const int pc = inside ? int(pv.state_count[i]) : 0;
+                    const int cc = pc + delta;
+                    const bool rbit = inside && ((pv.ref_bits[i >> 5] >> (i & 31)) & 1u);
+                    const uint32_t Cw = __ballot_sync(0xffffffffu, cc > 0);
+                    const uint32_t Pw = __ballot_sync(0xffffffffu, pc > 0);
+                    const uint32_t Rw = __ballot_sync(0xffffffffu, rbit);
+                    if (__ballot_sync(0xffffffffu, cc < 0)) fallback = true;
+                    dchg += __popc(Cw ^ Rw) - __popc(Pw ^ Rw);
+                    dtot += __popc(Cw | Rw) - __popc(Pw | Rw);
+                    dcov += __popc(Cw) - __popc(Pw);
+                    if (lane == 0) ws.region[(y - y0) * words + w] = Cw;
+                    const uint32_t xm = Cw ^ Rw;
+                    if (xm) {
+                        const uint32_t pos = qn + __popc(xm & ((1u << lane) - 1u));
+                        if (((xm >> lane) & 1u) && pos < kQueue)
+                            ws.queue[pos] = uint32_t(x) | (uint32_t(y) << 15) | (uint32_t(cc > 0) << 30);
+                        qn += __popc(xm);
+                    }
+                }
+            if (qn > kQueue) fallback = true;
+        }
+    }
+    __syncwarp();
+    r.changed = uint32_t(int64_t(pv.changed) + dchg);
+    r.total = uint32_t(int64_t(pv.total) + dtot);
+    const int64_t cov_c = int64_t(pv.cov_state) + dcov;
+    r.cb = cov_c > 0;
+    uint32_t best = 0;
+    if (!fallback && r.changed && r.ca && r.cb) {
+        RefMask rmask{pv.ref_bits, size};
+        for (uint32_t k = lane; k < qn; k += 32) {
+            const uint32_t e = ws.queue[k];
+            const uint32_t x = e & 0x7fffu, y = (e >> 15) & 0x7fffu;
+            // Candidate-only sample: nearest reference sample; reference-only
+            // sample: nearest candidate sample.
+            const uint32_t d = (e >> 30) & 1u ? nearest_d2(rmask, x, y) : nearest_d2(cmask, x, y);
+            best = d > best ? d : best;
+        }
+        for (int o = 16; o; o >>= 1) {
+            const uint32_t y = __shfl_xor_sync(0xffffffffu, best, o);
+            best = y > best ? y : best;
+        }
+    }
+    r.max_d2 = best;
+    if (fallback) r.flags |= kRecFallback;
+    if (best >= kExactLimit) r.flags |= kRecLarge;
+    if (lane == 0) {
+        out[v] = r;
+        if (stats) {
+            const uint64_t samples = x1 >= 0 ? uint64_t(y1 - y0 + 1) * uint64_t((((x1 - (x0 & ~31)) >> 5) + 1) * 32) : 0;
+            atomicAdd(stats, 1ull);
+            atomicAdd(stats + 1, (unsigned long long)samples);
+            atomicAdd(stats + 2, (unsigned long long)qn);
+        }
+    }
+    __syncwarp();
+}
+
+__global__ void __launch_bounds__(kAuditWarps * 32) k_audit(const CandidateRecord* recs, uint32_t n, PlanDev plan,
+                                                             ViewRecord* out, unsigned long long* stats) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    CandidateRecord& rec = *reinterpret_cast<CandidateRecord*>(smem);
+    WarpScratch* scratch = reinterpret_cast<WarpScratch*>(smem + ((sizeof(CandidateRecord) + 15) & ~size_t(15)));
+    const uint32_t warp = threadIdx.x >> 5;
+    for (uint32_t c = blockIdx.x; c < n; c += gridDim.x) {
+        const uint32_t* src = reinterpret_cast<const uint32_t*>(recs + c);
+        uint32_t* dst = reinterpret_cast<uint32_t*>(&rec);
+        for (uint32_t i = threadIdx.x; i < sizeof(CandidateRecord) / 4; i += blockDim.x) dst[i] = src[i];
+        __syncthreads();
+        ViewRecord* row = out + size_t(c) * plan.nviews;
+        if (!rec.valid || !rec.fast) {
+            for (uint32_t v = threadIdx.x; v < plan.nviews; v += blockDim.x) {
+                ViewRecord r{};
+                r.flags = rec.valid ? kRecFallback : 0;
+                row[v] = r;
+            }
+        } else {
+            for (uint32_t v = warp; v < plan.nviews; v += kAuditWarps)
+                audit_view(rec, plan, v, scratch[warp], row, stats);
+        }
+        __syncthreads();
+    }
+}
+
+struct VerdictOut {
+    uint8_t accepted, failed_gate, exact_path, resume_gate;
+    uint32_t removed;
+};
+
+__global__ void k_verdicts(const ViewRecord* const* plan_records, const uint32_t* plan_views, const uint32_t* plan_ss,
+                           const GateDev* gates, const CandidateRecord* recs, uint32_t n, VerdictOut* verdicts,
+                           Measurement* measurements, uint32_t* exact_count) {
+    uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= n) return;
+    const CandidateRecord& rec = recs[c];
+    VerdictOut v{0, 0, 0, 0, rec.removed};
+    Measurement* meas = measurements ? measurements + size_t(c) * 4 : nullptr;
+    if (meas)
+        for (int g = 0; g < 4; ++g) meas[g] = default_measurement();
+    if (!rec.valid) {
+        v.failed_gate = rec.failed;
+        verdicts[c] = v;
+        return;
+    }
+    bool accepted = true;
+    for (int g = 0; g < 4 && accepted; ++g) {
+        const GateDev gd = gates[g];
+        const uint32_t views = plan_views[gd.plan], ss = plan_ss[gd.plan];
+        const ViewRecord* rows = plan_records[gd.plan] + size_t(c) * views;
+        Measurement m = default_measurement();
+        m.supersample = gd.settings.supersample;
+        bool exact = false;
+        for (uint32_t vi = 0; vi < views; ++vi) {
+            const ViewRecord r = rows[vi];
+            if (r.flags & (kRecFallback | kRecLarge)) {
+                exact = true;
+                break;
+            }
+            Measurement cur = default_measurement();
+            cur.worst_view = vi;
+            finish_view(cur, r, gd.settings, ss, double(r.max_d2));
+            if (!refinement_done(cur, gd.settings, ss)) {
+                exact = true;
+                break;
+            }
+            if (!aggregate_view(m, cur, vi)) break;
+        }
+        if (exact) {
+            v.exact_path = 1;
+            v.resume_gate = uint8_t(g);
+            v.failed_gate = 0xff;
+            atomicAdd(exact_count, 1u);
+            accepted = false;
+            break;
+        }
+        if (meas) meas[g] = m;
+        if (!measurement_accepted(m)) {
+            v.failed_gate = uint8_t(g + 1);
+            accepted = false;
+        }
+    }
+    v.accepted = accepted;
+    verdicts[c] = v;
+}
+} // namespace
+
+size_t audit_smem_bytes() {
+    return ((sizeof(CandidateRecord) + 15) & ~size_t(15)) + kAuditWarps * sizeof(WarpScratch);
+}
+
+void launch_audit(const CandidateRecord* records, uint32_t n, const PlanDev& plan, ViewRecord* out,
+                  unsigned long long* stats, cudaStream_t s) {
+    if (!n) return;
+    static bool configured = false;
+    size_t smem = audit_smem_bytes();
+    if (!configured) {
+        cudaFuncSetAttribute(k_audit, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+        configured = true;
+    }
+    int sms = 148;
+    int dev = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_audit, kAuditWarps * 32, smem);
+    if (per_sm < 1) per_sm = 1;
+    uint32_t grid = uint32_t(sms * per_sm);
+    if (grid > n) grid = n;
+    k_audit<<<grid, kAuditWarps * 32, smem, s>>>(records, n, plan, out, stats);
+}
+
+void launch_verdicts(const ViewRecord* const* plan_records, const uint32_t* plan_views, const uint32_t* plan_ss,
+                     const GateDev* gates, const CandidateRecord* records, uint32_t n, void* verdicts,
+                     void* measurements, uint32_t* exact_count, cudaStream_t s) {
+    if (!n) return;
+    k_verdicts<<<(n + 127) / 128, 128, 0, s>>>(plan_records, plan_views, plan_ss, gates, records, n,
+                                               static_cast<VerdictOut*>(verdicts),
+                                               static_cast<Measurement*>(measurements), exact_count);
+}
+
+} // namespace b200

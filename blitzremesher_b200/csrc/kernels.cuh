@@ -1,0 +1,129 @@
+// Device data layouts and kernel launchers of the candidate-audit engine.
+#pragma once
+#include "common.cuh"
+#include <cuda_runtime.h>
+
+namespace b200 {
+
+// Borrowed device view of one mesh state (FP32 master streams).
+struct DevMesh {
+    const float* pos;     // 3 per vertex slot
+    const uint32_t* idx;  // 3 per face
+    const uint16_t* mat;  // per face or null
+    const uint8_t* sided; // per material or null
+    const float* uv;      // 2 per vertex slot or null
+    uint32_t nv, nf, nsided, pad;
+};
+
+// Topology on geometric classes (a class is named by its smallest slot).
+struct DevTopology {
+    const uint32_t* geometry;     // slot -> class root
+    const uint32_t* canonical;    // slot -> attribute chart root
+    const uint32_t* face_offsets; // class -> range in faces (nv+1)
+    const uint32_t* faces;        // face per class corner, ascending per class
+    const uint32_t* nbr_offsets;  // class -> range in neighbors (nv+1)
+    const uint32_t* neighbors;    // sorted unique neighbour classes
+    const uint8_t* nbr_count;     // face-edge multiplicity, capped at 3
+    const uint8_t* boundary;      // class flags
+    const uint8_t* invalid;
+    const uint32_t* slot_offsets; // class -> range in slots (nv+1)
+    const uint32_t* slots;        // vertex slots per class, ascending
+};
+
+// One directed collapse edit (action_gpu.cu:129-132).
+struct Edit {
+    uint32_t from, to, source[2], target[2];
+    uint8_t wedges, removed, valid, pad;
+};
+
+constexpr int kMaxAffected = 32; // faces in faces(from) U faces(to) handled on the fast path
+
+// A candidate's affected faces: old corner positions, which corners move to the
+// placement, whether the face survives, and the face's two-sided flag.
+struct AffectedFace {
+    float p[9];     // old corner positions
+    uint8_t moved;  // bit j: corner j lands on the placement
+    uint8_t kept;   // survives the collapse
+    uint8_t two;    // two-sided material
+    uint8_t pad;
+};
+struct CandidateRecord {
+    float placement[3];
+    uint32_t count;   // affected faces (<= kMaxAffected when fast)
+    uint8_t valid;    // legal + placement valid
+    uint8_t fast;     // handled by the incremental path
+    uint8_t removed;  // faces removed
+    uint8_t failed;   // 5 illegal, 6 invalid placement
+    uint32_t from, to;
+    AffectedFace faces[kMaxAffected];
+};
+
+// One audit plan: a reference, a camera set, a screen size and a sampling.
+struct PlanView {
+    const uint32_t* ref_bits;   // reference mask, CPU semantics (u64 layout as u32 words)
+    const uint32_t* state_bits; // current state: count > 0
+    const uint8_t* state_count; // current state: covering faces per sample
+    uint32_t changed, total;    // state vs reference
+    uint32_t cov_ref, cov_state;
+    uint32_t clip_state;        // clipped faces of the state
+    uint32_t clipped_ref;       // reference raster clipped
+};
+struct PlanDev {
+    const Camera* cameras;
+    const PlanView* views;
+    float center[3];
+    uint32_t nviews, ss, size;
+    uint32_t force_two;
+    uint32_t state_is_ref; // state masks equal the reference masks
+};
+
+// ---- launchers (kernels.cu) ----
+void launch_weld(const DevMesh& m, uint32_t* table, uint32_t capacity, bool with_uv, uint32_t* out,
+                 cudaStream_t s);
+void launch_exclusive_scan(const uint32_t* in, uint32_t* out, uint32_t n, uint32_t* scratch, cudaStream_t s);
+size_t scan_scratch_words(uint32_t n);
+void launch_topology(const DevMesh& m, uint32_t* geometry, uint32_t* face_offsets, uint32_t* faces,
+                     uint32_t* cursor, uint32_t* entry_offsets, uint32_t* entries, uint32_t* nbr_offsets,
+                     uint32_t* neighbors, uint8_t* nbr_count, uint8_t* boundary, uint8_t* invalid,
+                     uint8_t* visited, uint32_t* slot_offsets, uint32_t* slots, uint32_t* scan_scratch,
+                     uint32_t* host_counts, cudaStream_t s);
+void launch_enumerate(const DevMesh& m, const DevTopology& t, uint32_t* edge_base, uint8_t* valid,
+                      Edit* slots, uint32_t* offsets, Edit* out, uint32_t* scan_scratch, uint32_t total_nbrs,
+                      bool preserve_uv, cudaStream_t s);
+void launch_flat_faces(const DevMesh& m, uint32_t* flat_count, cudaStream_t s);
+void launch_position_table(const DevMesh& m, const DevTopology& t, uint32_t* table, uint32_t capacity,
+                           cudaStream_t s);
+void launch_prepare(const DevMesh& m, const DevTopology& t, const DevMesh& original, const DevTopology& ot,
+                    const void* collapses, uint32_t n, const uint32_t* table, uint32_t capacity,
+                    const uint32_t* flat_total, bool preserve_uv, CandidateRecord* out, cudaStream_t s);
+void launch_raster(const DevMesh& m, const Camera* cam, const float* center, uint32_t ss, uint32_t size,
+                   bool force_two, bool cpu_semantics, uint32_t* bits, uint8_t* counts, uint32_t* state,
+                   cudaStream_t s);
+void launch_popcounts(const uint32_t* a, const uint32_t* b, uint32_t words, unsigned long long* out,
+                      cudaStream_t s);
+void launch_distance(const uint32_t* from, const uint32_t* to, uint32_t size, uint32_t* g, uint32_t* d2,
+                     int32_t* stack_v, long long* stack_num, long long* stack_den, uint32_t* out_max,
+                     cudaStream_t s);
+void launch_audit(const CandidateRecord* records, uint32_t n, const PlanDev& plan, ViewRecord* out,
+                  unsigned long long* stats, cudaStream_t s);
+struct GateDev {
+    GateSettings settings;
+    uint32_t plan;
+};
+void launch_verdicts(const ViewRecord* const* plan_records, const uint32_t* plan_views,
+                     const uint32_t* plan_ss, const GateDev* gates, const CandidateRecord* records,
+                     uint32_t n, void* verdicts, void* measurements, uint32_t* exact_count, cudaStream_t s);
+size_t audit_smem_bytes();
+
+// Full trial mesh of one collapse (exact path): indices compacted in face order,
+// positions with every slot of class `to` at the placement.
+struct TrialInfo {
+    Edit edit;
+    float placement[3];
+    uint32_t ok;
+};
+void launch_trial(const DevMesh& m, const DevTopology& t, const void* collapse, TrialInfo* info, uint32_t* keep,
+                  uint32_t* offsets, uint32_t* out_idx, uint16_t* out_mat, float* out_pos, uint32_t* scan_scratch,
+                  cudaStream_t s);
+
+} // namespace b200

@@ -1,0 +1,242 @@
+// Full-raster path: coverage masks and sample counts of whole meshes, mask
+// popcounts, and the exact squared distance transform used when a view is
+// audited without the incremental path.
+//
+// Coverage semantics follow evaluate.cpp:125-189 (FP64 conservative test at
+// sample centres, culling, clipping with the CPU's stop-at-first-clipped-face
+// rule). Distances follow evaluate.cpp:33-70 and 196-209: the CPU float field
+// equals the exact integer squared distance below 2^24; above it the float
+// rounding of the two separable passes is reproduced.
+#include "kernels.cuh"
+
+namespace b200 {
+namespace {
+constexpr int kThreads = 256;
+inline uint32_t blocks_for(uint64_t n, int threads = kThreads) { return uint32_t((n + threads - 1) / threads); }
+
+struct RasterArgs {
+    DevMesh m;
+    Camera cam;
+    float center[3];
+    uint32_t ss, size, force_two, cpu_semantics;
+};
+
+__device__ FaceSetup face_setup(const RasterArgs& a, uint32_t f) {
+    Proj p[3];
+    for (int j = 0; j < 3; ++j) {
+        uint32_t v = a.m.idx[3 * f + j];
+        p[j] = project(a.m.pos[3 * v], a.m.pos[3 * v + 1], a.m.pos[3 * v + 2], a.center, a.cam, a.ss, a.size);
+    }
+    bool two = a.force_two;
+    if (!two && a.m.sided) {
+        uint16_t mat = a.m.mat ? a.m.mat[f] : 0;
+        two = mat < a.m.nsided && a.m.sided[mat];
+    }
+    return setup_face(p[0], p[1], p[2], a.cam.perspective != 0, two, a.size);
+}
+
+__global__ void k_state_init(uint32_t* state) {
+    if (threadIdx.x < 4) state[threadIdx.x] = threadIdx.x == 0 ? kNone : 0u;
+}
+
+// state[0]: first box-clipped face (min index), state[1]: any clip,
+// state[2]: clipped face count, state[3]: count overflow.
+__global__ void k_raster_clip(RasterArgs a, uint32_t* state) {
+    uint32_t f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= a.m.nf) return;
+    FaceSetup s = face_setup(a, f);
+    if (s.status == kFaceClipBox) atomicMin(state, f);
+    if (s.status == kFaceClipBox || s.status == kFaceClipZ) {
+        state[1] = 1;
+        atomicAdd(state + 2, 1u);
+    }
+}
+
+__device__ __forceinline__ void count_sample(uint8_t* counts, size_t i, uint32_t* state) {
+    uint32_t* w = reinterpret_cast<uint32_t*>(counts) + (i >> 2);
+    uint32_t shift = 8 * uint32_t(i & 3);
+    uint32_t old = atomicAdd(w, 1u << shift);
+    if (((old >> shift) & 0xffu) == 0xffu) state[3] = 1;
+}
+
+// One thread per face over its bounding box. bits: coverage (u64 LE layout as
+// u32 words); counts: covering faces per sample (u8, packed in u32 words).
+__global__ void k_raster_fill(RasterArgs a, uint32_t* bits, uint8_t* counts, uint32_t* state) {
+    uint32_t f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= a.m.nf) return;
+    if (a.cpu_semantics && f > state[0]) return;
+    FaceSetup s = face_setup(a, f);
+    if (s.status != kFaceOk) return;
+    for (int y = s.y0; y <= s.y1; ++y)
+        for (int x = s.x0; x <= s.x1; ++x) {
+            if (!face_covers(s, x, y)) continue;
+            size_t i = size_t(y) * a.size + x;
+            if (bits) atomicOr(bits + (i >> 5), 1u << (i & 31));
+            if (counts) count_sample(counts, i, state);
+        }
+}
+
+__global__ void k_popcounts(const uint32_t* a, const uint32_t* b, uint32_t words, unsigned long long* out) {
+    unsigned long long changed = 0, total = 0, ca = 0, cb = 0;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < words; i += gridDim.x * blockDim.x) {
+        uint32_t x = a[i], y = b[i];
+        changed += __popc(x ^ y);
+        total += __popc(x | y);
+        ca += __popc(x);
+        cb += __popc(y);
+    }
+    for (int o = 16; o; o >>= 1) {
+        changed += __shfl_down_sync(0xffffffffu, changed, o);
+        total += __shfl_down_sync(0xffffffffu, total, o);
+        ca += __shfl_down_sync(0xffffffffu, ca, o);
+        cb += __shfl_down_sync(0xffffffffu, cb, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        if (changed) atomicAdd(out, changed);
+        if (total) atomicAdd(out + 1, total);
+        if (ca) atomicAdd(out + 2, ca);
+        if (cb) atomicAdd(out + 3, cb);
+    }
+}
+
+__device__ __forceinline__ bool bit_at(const uint32_t* bits, size_t i) { return (bits[i >> 5] >> (i & 31)) & 1u; }
+
+// Horizontal distance to the nearest covered sample of each row (INF if none).
+__global__ void k_row_nearest(const uint32_t* to, uint32_t size, uint32_t* g) {
+    uint32_t y = blockIdx.x * blockDim.x + threadIdx.x;
+    if (y >= size) return;
+    size_t row = size_t(y) * size;
+    uint32_t last = kNone;
+    for (uint32_t x = 0; x < size; ++x) {
+        if (bit_at(to, row + x)) last = x;
+        g[row + x] = last == kNone ? kNone : x - last;
+    }
+    last = kNone;
+    for (uint32_t x = size; x-- > 0;) {
+        if (bit_at(to, row + x)) last = x;
+        if (last != kNone && last - x < g[row + x]) g[row + x] = last - x;
+    }
+}
+
+// Lower envelope of the parabolas (y-q)^2 + g(x,q)^2 over rows q with a site
+// (Felzenszwalb–Huttenlocher), in exact integer arithmetic: intersections are
+// kept as fractions and compared by cross-multiplication.
+__global__ void k_column_envelope(const uint32_t* g, uint32_t size, uint32_t* d2, int32_t* sv, long long* snum,
+                                  long long* sden) {
+    uint32_t x = blockIdx.x * blockDim.x + threadIdx.x;
+    if (x >= size) return;
+    int32_t* v = sv + size_t(x) * size;
+    long long* zn = snum + size_t(x) * size;
+    long long* zd = sden + size_t(x) * size;
+    int k = -1;
+    for (uint32_t q = 0; q < size; ++q) {
+        uint32_t gq = g[size_t(q) * size + x];
+        if (gq == kNone) continue;
+        long long fq = (long long)gq * gq + (long long)q * q;
+        if (k < 0) {
+            k = 0;
+            v[0] = int32_t(q);
+            continue;
+        }
+        long long num, den;
+        for (;;) {
+            int p = v[k];
+            uint32_t gp = g[size_t(p) * size + x];
+            long long fp = (long long)gp * gp + (long long)p * p;
+            num = fq - fp;
+            den = 2ll * ((long long)q - p);
+            // s > z[k]  <=>  num/den > zn[k]/zd[k]
+            if (k == 0 || num * zd[k] > zn[k] * den) break;
+            --k;
+        }
+        ++k;
+        v[k] = int32_t(q);
+        zn[k] = num;
+        zd[k] = den;
+    }
+    if (k < 0) {
+        for (uint32_t y = 0; y < size; ++y) d2[size_t(y) * size + x] = kNone;
+        return;
+    }
+    int top = k;
+    k = 0;
+    for (uint32_t y = 0; y < size; ++y) {
+        while (k < top && zn[k + 1] < (long long)y * zd[k + 1]) ++k;
+        long long dy = (long long)y - v[k];
+        uint32_t gq = g[size_t(v[k]) * size + x];
+        d2[size_t(y) * size + x] = uint32_t(dy * dy + (long long)gq * gq);
+    }
+}
+
+// CPU float value of the field where the exact distance reaches 2^24: the
+// row pass rounds g^2 to float, the column pass rounds (dy^2 + f) to float.
+__device__ float cpu_field_value(const uint32_t* g, uint32_t size, uint32_t x, uint32_t y) {
+    float best = INFINITY;
+    for (uint32_t q = 0; q < size; ++q) {
+        uint32_t gq = g[size_t(q) * size + x];
+        if (gq == kNone) continue;
+        float f = __uint2float_rn(gq * gq);
+        double dy = double(y) - double(q);
+        float val = __double2float_rn(dy * dy + double(f));
+        best = val < best ? val : best;
+    }
+    return best;
+}
+
+// Max over samples covered by `from` and not by `to` of the field of `to`, as
+// float bit patterns (non-negative floats order like their bits).
+__global__ void k_directed_max(const uint32_t* from, const uint32_t* to, const uint32_t* d2, const uint32_t* g,
+                               uint32_t size, uint32_t* out) {
+    size_t n = size_t(size) * size;
+    uint32_t best = 0;
+    for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x) {
+        if (!bit_at(from, i) || bit_at(to, i)) continue;
+        uint32_t d = d2[i];
+        float val = d < kExactLimit ? float(d) : cpu_field_value(g, size, uint32_t(i % size), uint32_t(i / size));
+        uint32_t b = __float_as_uint(val);
+        best = b > best ? b : best;
+    }
+    for (int o = 16; o; o >>= 1) {
+        uint32_t y = __shfl_down_sync(0xffffffffu, best, o);
+        best = y > best ? y : best;
+    }
+    if ((threadIdx.x & 31) == 0 && best) atomicMax(out, best);
+}
+} // namespace
+
+void launch_raster(const DevMesh& m, const Camera* cam, const float* center, uint32_t ss, uint32_t size,
+                   bool force_two, bool cpu_semantics, uint32_t* bits, uint8_t* counts, uint32_t* state,
+                   cudaStream_t s) {
+    RasterArgs a;
+    a.m = m;
+    a.cam = *cam;
+    a.center[0] = center[0], a.center[1] = center[1], a.center[2] = center[2];
+    a.ss = ss, a.size = size, a.force_two = force_two, a.cpu_semantics = cpu_semantics;
+    k_state_init<<<1, 32, 0, s>>>(state);
+    if (!m.nf) return;
+    k_raster_clip<<<blocks_for(m.nf), kThreads, 0, s>>>(a, state);
+    k_raster_fill<<<blocks_for(m.nf, 128), 128, 0, s>>>(a, bits, counts, state);
+}
+
+void launch_popcounts(const uint32_t* a, const uint32_t* b, uint32_t words, unsigned long long* out,
+                      cudaStream_t s) {
+    cudaMemsetAsync(out, 0, 4 * sizeof(unsigned long long), s);
+    uint32_t grid = blocks_for(words);
+    if (grid > 1184) grid = 1184;
+    if (!grid) grid = 1;
+    k_popcounts<<<grid, kThreads, 0, s>>>(a, b, words, out);
+}
+
+// Field of `to`, max over from \ to (as float bits) into out_max.
+void launch_distance(const uint32_t* from, const uint32_t* to, uint32_t size, uint32_t* g, uint32_t* d2,
+                     int32_t* stack_v, long long* stack_num, long long* stack_den, uint32_t* out_max,
+                     cudaStream_t s) {
+    k_row_nearest<<<blocks_for(size, 64), 64, 0, s>>>(to, size, g);
+    k_column_envelope<<<blocks_for(size, 64), 64, 0, s>>>(g, size, d2, stack_v, stack_num, stack_den);
+    size_t n = size_t(size) * size;
+    uint32_t grid = uint32_t((n + kThreads - 1) / kThreads);
+    if (grid > 148 * 16) grid = 148 * 16;
+    k_directed_max<<<grid, kThreads, 0, s>>>(from, to, d2, g, size, out_max);
+}
+
+} // namespace b200

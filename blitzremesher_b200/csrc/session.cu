@@ -1,0 +1,1081 @@
+// Host runtime and C ABI of the B200 candidate-audit engine.
+//
+// A session owns the source (LOD0), the bound previous LOD, the current state
+// with its collapse topology, the audit plans (cameras + resident reference
+// masks and state counts per view) and all scratch. Every buffer is allocated
+// through the session pool, which enforces blitz_neural_options_v2::memory_mib.
+#include "../../include/blitz_audit.h"
+#include "kernels.cuh"
+
+#include <algorithm>
+#include <chrono>
+#include <cstdio>
+#include <map>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <tuple>
+#include <vector>
+
+namespace b200 {
+
+struct Failure : std::runtime_error {
+    blitz_status status;
+    Failure(blitz_status s, const std::string& m) : std::runtime_error(m), status(s) {}
+};
+
+#define B200_CUDA(x)                                                                                              \
+    do {                                                                                                         \
+        cudaError_t e_ = (x);                                                                                    \
+        if (e_ != cudaSuccess)                                                                                   \
+            throw Failure(e_ == cudaErrorMemoryAllocation ? BLITZ_OUT_OF_MEMORY : BLITZ_INTERNAL_ERROR,          \
+                          std::string("CUDA: ") + cudaGetErrorString(e_) + " at " #x);                           \
+    } while (0)
+
+// ---------------------------------------------------------------------------
+// Device memory with a byte budget.
+struct Pool {
+    size_t limit = 0, used = 0, peak = 0, allocations = 0;
+    void* get(size_t bytes) {
+        if (!bytes) return nullptr;
+        if (used + bytes > limit)
+            throw Failure(BLITZ_OUT_OF_MEMORY, "audit workspace exceeds memory_mib budget");
+        void* p = nullptr;
+        cudaError_t e = cudaMalloc(&p, bytes);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            throw Failure(BLITZ_OUT_OF_MEMORY, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+        }
+        used += bytes;
+        peak = std::max(peak, used);
+        ++allocations;
+        return p;
+    }
+    void put(void* p, size_t bytes) {
+        if (p) {
+            cudaFree(p);
+            used -= bytes;
+        }
+    }
+};
+
+template <class T> struct Buf {
+    Pool* pool = nullptr;
+    T* p = nullptr;
+    size_t n = 0;
+    Buf() = default;
+    Buf(Pool& pl, size_t count) : pool(&pl), p(static_cast<T*>(pl.get(count * sizeof(T)))), n(count) {}
+    Buf(const Buf&) = delete;
+    Buf& operator=(const Buf&) = delete;
+    Buf(Buf&& o) noexcept : pool(o.pool), p(o.p), n(o.n) { o.p = nullptr, o.n = 0; }
+    Buf& operator=(Buf&& o) noexcept {
+        if (this != &o) {
+            release();
+            pool = o.pool, p = o.p, n = o.n;
+            o.p = nullptr, o.n = 0;
+        }
+        return *this;
+    }
+    ~Buf() { release(); }
+    void release() {
+        if (pool && p) pool->put(p, n * sizeof(T));
+        p = nullptr, n = 0;
+    }
+    void ensure(Pool& pl, size_t count) {
+        if (n < count) {
+            release();
+            *this = Buf(pl, count);
+        }
+    }
+};
+
+// ---------------------------------------------------------------------------
+// Host mesh copied out of a borrowed blitz_mesh (streams may be strided).
+struct HostMesh {
+    std::vector<float> pos, normals, uv;
+    std::vector<uint8_t> colors;
+    std::vector<uint32_t> idx;
+    std::vector<uint16_t> mat;
+    std::vector<uint8_t> sided;
+    uint32_t nv() const { return uint32_t(pos.size() / 3); }
+    uint32_t nf() const { return uint32_t(idx.size() / 3); }
+};
+
+template <class T>
+static void copy_stream(const blitz_stream& s, size_t n, size_t comps, std::vector<T>& out, const char* name) {
+    if (!s.count) return;
+    if (!s.data || s.count != n || s.stride < comps * sizeof(T))
+        throw Failure(BLITZ_INVALID_ARGUMENT, std::string("invalid ") + name + " stream");
+    out.resize(n * comps);
+    const unsigned char* b = static_cast<const unsigned char*>(s.data);
+    for (size_t i = 0; i < n; ++i) std::memcpy(out.data() + i * comps, b + i * s.stride, comps * sizeof(T));
+}
+
+// Descriptor checks of c_api.cpp and validate(MeshView) (mesh.cpp:29-42).
+static HostMesh import_mesh(const blitz_mesh* m) {
+    if (!m || m->struct_size != sizeof(blitz_mesh) || m->abi_version != BLITZ_ABI_VERSION)
+        throw Failure(BLITZ_INVALID_ARGUMENT, "invalid mesh descriptor");
+    HostMesh h;
+    size_t n = m->positions.count;
+    if (!n || n >= UINT32_MAX || !m->indices || !m->index_count || m->index_count % 3 || m->index_count >= UINT32_MAX)
+        throw Failure(BLITZ_INVALID_ARGUMENT, "mesh requires nonempty triangle indices and 32-bit representable counts");
+    copy_stream<float>(m->positions, n, 3, h.pos, "position");
+    copy_stream<float>(m->normals, n, 3, h.normals, "normal");
+    copy_stream<float>(m->uv, n, 2, h.uv, "uv");
+    copy_stream<uint8_t>(m->colors, n, 4, h.colors, "color");
+    h.idx.assign(m->indices, m->indices + m->index_count);
+    size_t nf = m->index_count / 3;
+    if (m->material_count) {
+        if (!m->materials || m->material_count != nf)
+            throw Failure(BLITZ_INVALID_ARGUMENT, "material count differs from triangle count");
+        h.mat.assign(m->materials, m->materials + nf);
+    }
+    if (m->double_sided_count) {
+        if (!m->double_sided) throw Failure(BLITZ_INVALID_ARGUMENT, "invalid double-sided flags");
+        h.sided.assign(m->double_sided, m->double_sided + m->double_sided_count);
+    }
+    for (uint32_t i : h.idx)
+        if (i >= n) throw Failure(BLITZ_INVALID_ARGUMENT, "index outside vertex stream");
+    for (float f : h.pos)
+        if (!std::isfinite(f)) throw Failure(BLITZ_INVALID_ARGUMENT, "nonfinite position or normal");
+    for (float f : h.normals)
+        if (!std::isfinite(f)) throw Failure(BLITZ_INVALID_ARGUMENT, "nonfinite position or normal");
+    for (float f : h.uv)
+        if (!std::isfinite(f)) throw Failure(BLITZ_INVALID_ARGUMENT, "nonfinite UV");
+    return h;
+}
+
+struct Bounds {
+    float center[3];
+    double radius;
+};
+// mesh.cpp:12-20
+static Bounds bounds_of(const HostMesh& m) {
+    Bounds b{};
+    float lo[3] = {m.pos[0], m.pos[1], m.pos[2]}, hi[3] = {lo[0], lo[1], lo[2]};
+    for (uint32_t i = 1; i < m.nv(); ++i)
+        for (int k = 0; k < 3; ++k) lo[k] = std::min(lo[k], m.pos[3 * i + k]), hi[k] = std::max(hi[k], m.pos[3 * i + k]);
+    for (int k = 0; k < 3; ++k) b.center[k] = float((double(lo[k]) + hi[k]) * .5);
+    for (uint32_t i = 0; i < m.nv(); ++i) {
+        double x = double(m.pos[3 * i]) - b.center[0], y = double(m.pos[3 * i + 1]) - b.center[1],
+               z = double(m.pos[3 * i + 2]) - b.center[2];
+        b.radius = std::max(b.radius, std::sqrt(x * x + y * y + z * z));
+    }
+    return b;
+}
+
+// Cameras on the host with the platform libm, as the reference
+// (evaluate.cpp:16-20, 108-124): Fibonacci sphere, seed rotation, ortho first.
+struct F3 {
+    float x, y, z;
+};
+static double dotd(F3 a, F3 b) { return double(a.x) * b.x + double(a.y) * b.y + double(a.z) * b.z; }
+static F3 crossf(F3 a, F3 b) { return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x}; }
+static F3 normalizedf(F3 a) {
+    double l = std::sqrt(dotd(a, a));
+    if (!(l > 0)) return {0, 0, 0};
+    double s = 1 / l;
+    return {float(a.x * s), float(a.y * s), float(a.z * s)};
+}
+static F3 rotatef(F3 v, uint32_t seed) {
+    double a = (seed % 65521) * .000731, b = ((seed >> 8) % 32749) * .000913;
+    double x = v.x * std::cos(a) - v.y * std::sin(a), y = v.x * std::sin(a) + v.y * std::cos(a);
+    return {float(x), float(y * std::cos(b) - v.z * std::sin(b)), float(y * std::sin(b) + v.z * std::cos(b))};
+}
+static std::vector<Camera> make_cameras(const Bounds& b, double screen, uint16_t ortho, uint16_t persp, uint32_t seed) {
+    constexpr double pi = 3.14159265358979323846;
+    std::vector<Camera> out;
+    for (int projection = 0; projection < 2; ++projection) {
+        unsigned count = projection ? persp : ortho;
+        for (unsigned i = 0; i < count; ++i) {
+            double z = 1 - 2 * (i + .5) / count, r = std::sqrt(std::max(0.0, 1 - z * z)),
+                   angle = i * pi * (3 - std::sqrt(5.0));
+            F3 fwd = normalizedf(rotatef({float(r * std::cos(angle)), float(z), float(r * std::sin(angle))},
+                                         seed + projection * 104729u));
+            F3 hint = std::abs(fwd.y) > .99 ? F3{1, 0, 0} : F3{0, 1, 0};
+            F3 right = normalizedf(crossf(hint, fwd)), up = normalizedf(crossf(fwd, right));
+            double height = std::max(1024.0, 2 * screen), focal = height / (2 * std::tan(pi / 6));
+            double distance = b.radius * std::sqrt(1 + std::pow(2 * focal / screen, 2));
+            Camera c{};
+            c.right[0] = right.x, c.right[1] = right.y, c.right[2] = right.z;
+            c.up[0] = up.x, c.up[1] = up.y, c.up[2] = up.z;
+            c.forward[0] = fwd.x, c.forward[1] = fwd.y, c.forward[2] = fwd.z;
+            c.distance = distance, c.focal = focal, c.scale = screen / (b.radius * 2), c.perspective = projection;
+            out.push_back(c);
+        }
+    }
+    return out;
+}
+
+// evaluation_settings.hpp:10-23 (coverage profile).
+static GateSettings gate_of(const blitz_eval_settings* s, const Bounds& b) {
+    if (!s || s->struct_size != sizeof(blitz_eval_settings))
+        throw Failure(BLITZ_INVALID_ARGUMENT, "invalid evaluation settings descriptor");
+    if (s->profile != 0) throw Failure(BLITZ_UNAVAILABLE, "only the coverage profile is implemented");
+    bool center_ok = std::isfinite(b.center[0]) && std::isfinite(b.center[1]) && std::isfinite(b.center[2]);
+    if (!(s->screen_size > 0) || !std::isfinite(s->screen_size) || s->screen_size > 16384 || !(b.radius > 0) ||
+        !std::isfinite(b.radius) || !center_ok || !(s->limit >= 0) || !std::isfinite(s->limit) || !s->supersample ||
+        s->max_supersample < s->supersample || s->max_supersample > 32 || !std::isfinite(s->max_changed_area) ||
+        s->max_changed_area < 0 || s->max_changed_area > 1)
+        throw Failure(BLITZ_INVALID_ARGUMENT, "invalid evaluation settings");
+    if (!s->views_orthographic && !s->views_perspective)
+        throw Failure(BLITZ_INVALID_ARGUMENT, "at least one camera required");
+    GateSettings g{};
+    g.screen_size = s->screen_size, g.limit = s->limit, g.max_changed_area = s->max_changed_area;
+    g.views = uint32_t(s->views_orthographic) + s->views_perspective;
+    g.supersample = s->supersample, g.max_supersample = s->max_supersample;
+    g.conservative_screen = s->conservative_screen;
+    return g;
+}
+
+// ---------------------------------------------------------------------------
+struct DeviceMesh {
+    Buf<float> pos, uv;
+    Buf<uint32_t> idx;
+    Buf<uint16_t> mat;
+    Buf<uint8_t> sided;
+    DevMesh view{};
+    void upload(Pool& pool, const HostMesh& h, cudaStream_t s) {
+        pos = Buf<float>(pool, h.pos.size());
+        idx = Buf<uint32_t>(pool, h.idx.size());
+        B200_CUDA(cudaMemcpyAsync(pos.p, h.pos.data(), h.pos.size() * 4, cudaMemcpyHostToDevice, s));
+        B200_CUDA(cudaMemcpyAsync(idx.p, h.idx.data(), h.idx.size() * 4, cudaMemcpyHostToDevice, s));
+        if (!h.uv.empty()) {
+            uv = Buf<float>(pool, h.uv.size());
+            B200_CUDA(cudaMemcpyAsync(uv.p, h.uv.data(), h.uv.size() * 4, cudaMemcpyHostToDevice, s));
+        }
+        if (!h.mat.empty()) {
+            mat = Buf<uint16_t>(pool, h.mat.size());
+            B200_CUDA(cudaMemcpyAsync(mat.p, h.mat.data(), h.mat.size() * 2, cudaMemcpyHostToDevice, s));
+        }
+        if (!h.sided.empty()) {
+            sided = Buf<uint8_t>(pool, h.sided.size());
+            B200_CUDA(cudaMemcpyAsync(sided.p, h.sided.data(), h.sided.size(), cudaMemcpyHostToDevice, s));
+        }
+        view = DevMesh{pos.p, idx.p, mat.p, sided.p, uv.p, h.nv(), h.nf(), uint32_t(h.sided.size()), 0};
+    }
+};
+
+static bool same_data(const HostMesh& a, const HostMesh& b) {
+    return a.pos == b.pos && a.idx == b.idx && a.mat == b.mat && a.sided == b.sided && a.normals == b.normals &&
+           a.colors == b.colors && a.uv == b.uv;
+}
+// evaluate.cpp:77-82 — positions, normals, colours, indices, materials, sides.
+static bool identical(const HostMesh& a, const HostMesh& b) {
+    return a.pos == b.pos && a.normals == b.normals && a.colors == b.colors && a.idx == b.idx && a.mat == b.mat &&
+           a.sided == b.sided;
+}
+
+struct Topology {
+    Buf<uint32_t> geometry, canonical, face_offsets, faces, cursor, entries, nbr_offsets, neighbors, slot_offsets,
+        slots, scan, table;
+    Buf<uint8_t> nbr_count, boundary, invalid, visited;
+    Buf<uint32_t> edge_base, offsets, flat;
+    Buf<uint8_t> valid;
+    Buf<Edit> edit_slots, edits;
+    Buf<uint32_t> positions; // live position table
+    uint32_t table_cap = 0, pos_cap = 0, total_nbrs = 0, actions = 0;
+    DevTopology view{};
+};
+
+static uint32_t pow2_at_least(uint64_t n) {
+    uint64_t c = 2;
+    while (c < n) c *= 2;
+    if (c > (1ull << 31)) throw Failure(BLITZ_OUT_OF_MEMORY, "hash table exceeds u32");
+    return uint32_t(c);
+}
+
+struct PlanKey {
+    int reference;
+    uint16_t ortho, persp;
+    uint32_t seed;
+    double screen;
+    uint32_t ss, force_two;
+    bool operator<(const PlanKey& o) const {
+        return std::tie(reference, ortho, persp, seed, screen, ss, force_two) <
+               std::tie(o.reference, o.ortho, o.persp, o.seed, o.screen, o.ss, o.force_two);
+    }
+};
+
+struct Plan {
+    PlanKey key{};
+    uint32_t size = 0, views = 0, words = 0;
+    bool resource_limited = false;
+    Buf<Camera> cameras;
+    Buf<uint32_t> ref_bits, state_bits;
+    Buf<uint8_t> state_count;
+    Buf<PlanView> dviews;
+    std::vector<PlanView> hviews;
+    bool state_is_ref = true;
+    Buf<ViewRecord> records;
+    PlanDev dev{};
+};
+
+struct Scratch {
+    Buf<uint32_t> a, c, g, d2, maxes, state;
+    Buf<int32_t> sv;
+    Buf<long long> sn, sd;
+    Buf<unsigned long long> pop;
+    uint32_t size = 0;
+};
+
+struct Session {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    Pool pool;
+    blitz_neural_options_v2 options{};
+    HostMesh source_h, previous_h;
+    bool previous_is_source = true;
+    DeviceMesh source, previous, state;
+    Bounds bounds{};
+    Topology topo;
+    std::map<PlanKey, std::unique_ptr<Plan>> plans;
+    Scratch scratch;
+    Buf<CandidateRecord> records;
+    Buf<uint8_t> verdict_dev;
+    Buf<Measurement> meas_dev;
+    Buf<blitz_collapse> collapse_dev;
+    Buf<uint32_t> exact_count;
+    Buf<const ViewRecord*> record_table;
+    Buf<uint32_t> plan_views, plan_ss;
+    Buf<GateDev> gate_table;
+    // exact path
+    DeviceMesh trial;
+    Buf<uint32_t> trial_keep, trial_offsets;
+    Buf<TrialInfo> trial_info;
+    blitz_neural_info info{};
+    uint64_t internal_errors = 0;
+    // profiling
+    bool profiling = false;
+    blitz_audit_profile profile{};
+    Buf<unsigned long long> stats;
+    cudaEvent_t ev[6] = {};
+
+    ~Session() {
+        plans.clear();
+        for (auto& e : ev)
+            if (e) cudaEventDestroy(e);
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
+struct DeviceScope {
+    int previous = 0;
+    explicit DeviceScope(int id) {
+        B200_CUDA(cudaGetDevice(&previous));
+        B200_CUDA(cudaSetDevice(id));
+    }
+    ~DeviceScope() { cudaSetDevice(previous); }
+};
+
+static void build_topology(Session& S) {
+    Topology& t = S.topo;
+    const DevMesh& m = S.state.view;
+    const uint32_t n = m.nv, nf = m.nf;
+    Pool& P = S.pool;
+    cudaStream_t st = S.stream;
+    t.table_cap = pow2_at_least(2ull * n);
+    t.geometry = Buf<uint32_t>(P, n);
+    t.table = Buf<uint32_t>(P, t.table_cap);
+    launch_weld(m, t.table.p, t.table_cap, false, t.geometry.p, st);
+    t.face_offsets = Buf<uint32_t>(P, n + 1);
+    t.faces = Buf<uint32_t>(P, 3ull * nf);
+    t.cursor = Buf<uint32_t>(P, 2ull * (n + 1));
+    t.entries = Buf<uint32_t>(P, 6ull * nf);
+    t.nbr_offsets = Buf<uint32_t>(P, n + 1);
+    t.neighbors = Buf<uint32_t>(P, 6ull * nf);
+    t.nbr_count = Buf<uint8_t>(P, 6ull * nf);
+    t.boundary = Buf<uint8_t>(P, n);
+    t.invalid = Buf<uint8_t>(P, n);
+    t.visited = Buf<uint8_t>(P, 6ull * nf);
+    t.slot_offsets = Buf<uint32_t>(P, n + 1);
+    t.slots = Buf<uint32_t>(P, n);
+    size_t scan_words = std::max(scan_scratch_words(n + 1), scan_scratch_words(uint32_t(6ull * nf + 1)));
+    t.scan = Buf<uint32_t>(P, scan_words + 64);
+    launch_topology(m, t.geometry.p, t.face_offsets.p, t.faces.p, t.cursor.p, nullptr, t.entries.p, t.nbr_offsets.p,
+                    t.neighbors.p, t.nbr_count.p, t.boundary.p, t.invalid.p, t.visited.p, t.slot_offsets.p,
+                    t.slots.p, t.scan.p, nullptr, st);
+    B200_CUDA(cudaMemcpyAsync(&t.total_nbrs, t.nbr_offsets.p + n, 4, cudaMemcpyDeviceToHost, st));
+    B200_CUDA(cudaStreamSynchronize(st));
+    t.view = DevTopology{t.geometry.p, t.geometry.p, t.face_offsets.p, t.faces.p, t.nbr_offsets.p, t.neighbors.p,
+                         t.nbr_count.p, t.boundary.p, t.invalid.p, t.slot_offsets.p, t.slots.p};
+    // Legal actions in enumeration order.
+    t.edge_base = Buf<uint32_t>(P, n + 1);
+    t.valid = Buf<uint8_t>(P, t.total_nbrs + 1);
+    t.edit_slots = Buf<Edit>(P, t.total_nbrs + 1);
+    t.offsets = Buf<uint32_t>(P, t.total_nbrs + 1);
+    t.edits = Buf<Edit>(P, t.total_nbrs + 1);
+    launch_enumerate(m, t.view, t.edge_base.p, t.valid.p, t.edit_slots.p, t.offsets.p, t.edits.p, t.scan.p,
+                     t.total_nbrs, false, st);
+    B200_CUDA(cudaMemcpyAsync(&t.actions, t.offsets.p + t.total_nbrs, 4, cudaMemcpyDeviceToHost, st));
+    // Validation support: flat faces and live positions.
+    t.flat = Buf<uint32_t>(P, 1);
+    launch_flat_faces(m, t.flat.p, st);
+    t.pos_cap = pow2_at_least(4ull * n);
+    t.positions = Buf<uint32_t>(P, t.pos_cap);
+    launch_position_table(m, t.view, t.positions.p, t.pos_cap, st);
+    B200_CUDA(cudaStreamSynchronize(st));
+    B200_CUDA(cudaGetLastError());
+}
+
+static uint32_t mask_words(uint32_t size) {
+    uint64_t samples = uint64_t(size) * size;
+    return uint32_t(((samples + 63) / 64) * 2 + 2); // u64 layout plus one padding word pair
+}
+
+// Rasterizes a device mesh for one view; returns {any clip, first box clip, clipped faces, overflow}.
+static void raster(Session& S, const DevMesh& m, const Camera* cam_dev, uint32_t ss, uint32_t size, bool force_two,
+                   bool cpu_semantics, uint32_t* bits, uint8_t* counts, uint32_t* state_dev) {
+    launch_raster(m, cam_dev, S.bounds.center, ss, size, force_two, cpu_semantics, bits, counts, state_dev, S.stream);
+}
+
+static Plan& plan_for(Session& S, const PlanKey& key) {
+    auto it = S.plans.find(key);
+    if (it != S.plans.end()) return *it->second;
+    auto plan = std::make_unique<Plan>();
+    Plan& p = *plan;
+    p.key = key;
+    p.size = raster_size(key.screen, key.ss);
+    p.views = uint32_t(key.ortho) + key.persp;
+    if (uint64_t(p.size) * p.size > kMaxSamples) {
+        p.resource_limited = true;
+        return *(S.plans[key] = std::move(plan));
+    }
+    p.words = mask_words(p.size);
+    auto cams = make_cameras(S.bounds, key.screen, key.ortho, key.persp, key.seed);
+    p.cameras = Buf<Camera>(S.pool, cams.size());
+    B200_CUDA(cudaMemcpyAsync(p.cameras.p, cams.data(), cams.size() * sizeof(Camera), cudaMemcpyHostToDevice, S.stream));
+    const DeviceMesh& ref = key.reference == 0 || S.previous_is_source ? S.source : S.previous;
+    const HostMesh& ref_h = key.reference == 0 || S.previous_is_source ? S.source_h : S.previous_h;
+    bool state_same_mesh = same_data(ref_h, S.source_h) && true; // state is the source in this build
+    const size_t samples = size_t(p.size) * p.size;
+    p.ref_bits = Buf<uint32_t>(S.pool, size_t(p.words) * p.views);
+    p.state_count = Buf<uint8_t>(S.pool, ((samples + 3) & ~size_t(3)) * p.views);
+    B200_CUDA(cudaMemsetAsync(p.ref_bits.p, 0, size_t(p.words) * p.views * 4, S.stream));
+    B200_CUDA(cudaMemsetAsync(p.state_count.p, 0, ((samples + 3) & ~size_t(3)) * p.views, S.stream));
+    Buf<uint32_t> state(S.pool, 8 * size_t(p.views));
+    std::vector<uint32_t> hstate(8 * size_t(p.views));
+    // Reference masks (CPU semantics) and state counts.
+    for (uint32_t v = 0; v < p.views; ++v) {
+        uint32_t* rb = p.ref_bits.p + size_t(v) * p.words;
+        uint8_t* sc = p.state_count.p + ((samples + 3) & ~size_t(3)) * v;
+        raster(S, ref.view, p.cameras.p + v, key.ss, p.size, key.force_two, true, rb, nullptr, state.p + 8 * v);
+        raster(S, S.state.view, p.cameras.p + v, key.ss, p.size, key.force_two, false, nullptr, sc, state.p + 8 * v + 4);
+    }
+    B200_CUDA(cudaMemcpyAsync(hstate.data(), state.p, hstate.size() * 4, cudaMemcpyDeviceToHost, S.stream));
+    B200_CUDA(cudaStreamSynchronize(S.stream));
+    bool box_clip = false;
+    for (uint32_t v = 0; v < p.views; ++v) {
+        if (hstate[8 * v + 4 + 3]) throw Failure(BLITZ_OUT_OF_MEMORY, "more than 255 faces cover one sample");
+        box_clip |= hstate[8 * v] != kNone;
+    }
+    p.state_is_ref = state_same_mesh && !box_clip;
+    if (p.state_is_ref) {
+        p.state_bits = Buf<uint32_t>(); // shares ref bits
+    } else {
+        p.state_bits = Buf<uint32_t>(S.pool, size_t(p.words) * p.views);
+        B200_CUDA(cudaMemsetAsync(p.state_bits.p, 0, size_t(p.words) * p.views * 4, S.stream));
+        for (uint32_t v = 0; v < p.views; ++v)
+            raster(S, S.state.view, p.cameras.p + v, key.ss, p.size, key.force_two, false,
+                   p.state_bits.p + size_t(v) * p.words, nullptr, state.p + 8 * v + 4);
+    }
+    Buf<unsigned long long> pop(S.pool, 4 * size_t(p.views));
+    for (uint32_t v = 0; v < p.views; ++v) {
+        const uint32_t* sb = (p.state_is_ref ? p.ref_bits.p : p.state_bits.p) + size_t(v) * p.words;
+        launch_popcounts(p.ref_bits.p + size_t(v) * p.words, sb, p.words, pop.p + 4 * v, S.stream);
+    }
+    std::vector<unsigned long long> hpop(4 * size_t(p.views));
+    B200_CUDA(cudaMemcpyAsync(hpop.data(), pop.p, hpop.size() * 8, cudaMemcpyDeviceToHost, S.stream));
+    B200_CUDA(cudaMemcpyAsync(hstate.data(), state.p, hstate.size() * 4, cudaMemcpyDeviceToHost, S.stream));
+    B200_CUDA(cudaStreamSynchronize(S.stream));
+    p.hviews.resize(p.views);
+    for (uint32_t v = 0; v < p.views; ++v) {
+        PlanView& pv = p.hviews[v];
+        pv.ref_bits = p.ref_bits.p + size_t(v) * p.words;
+        pv.state_bits = (p.state_is_ref ? p.ref_bits.p : p.state_bits.p) + size_t(v) * p.words;
+        pv.state_count = p.state_count.p + ((samples + 3) & ~size_t(3)) * v;
+        pv.changed = uint32_t(hpop[4 * v]);
+        pv.total = uint32_t(hpop[4 * v + 1]);
+        pv.cov_ref = uint32_t(hpop[4 * v + 2]);
+        pv.cov_state = uint32_t(hpop[4 * v + 3]);
+        pv.clipped_ref = hstate[8 * v + 1];
+        pv.clip_state = hstate[8 * v + 4 + 2];
+    }
+    p.dviews = Buf<PlanView>(S.pool, p.views);
+    B200_CUDA(cudaMemcpyAsync(p.dviews.p, p.hviews.data(), p.views * sizeof(PlanView), cudaMemcpyHostToDevice, S.stream));
+    p.dev.cameras = p.cameras.p;
+    p.dev.views = p.dviews.p;
+    for (int k = 0; k < 3; ++k) p.dev.center[k] = S.bounds.center[k];
+    p.dev.nviews = p.views, p.dev.ss = key.ss, p.dev.size = p.size, p.dev.force_two = key.force_two;
+    p.dev.state_is_ref = p.state_is_ref;
+    B200_CUDA(cudaStreamSynchronize(S.stream));
+    return *(S.plans[key] = std::move(plan));
+}
+
+static void ensure_scratch(Session& S, uint32_t size) {
+    Scratch& x = S.scratch;
+    if (x.size >= size && x.a.p) return;
+    size_t samples = size_t(size) * size;
+    uint32_t words = mask_words(size);
+    x.a = Buf<uint32_t>(S.pool, words);
+    x.c = Buf<uint32_t>(S.pool, words);
+    x.g = Buf<uint32_t>(S.pool, samples);
+    x.d2 = Buf<uint32_t>(S.pool, samples);
+    x.sv = Buf<int32_t>(S.pool, samples);
+    x.sn = Buf<long long>(S.pool, samples);
+    x.sd = Buf<long long>(S.pool, samples);
+    x.maxes = Buf<uint32_t>(S.pool, 2);
+    x.state = Buf<uint32_t>(S.pool, 8);
+    x.pop = Buf<unsigned long long>(S.pool, 4);
+    x.size = size;
+}
+
+// One view at one sampling through the full-raster path.
+static void full_view(Session& S, const DevMesh& ref, const DevMesh& cand, const Camera* cam_dev, uint32_t ss,
+                      uint32_t size, bool force_two, ViewRecord& rec, double& max_d2) {
+    ensure_scratch(S, size);
+    Scratch& x = S.scratch;
+    uint32_t words = mask_words(size);
+    cudaStream_t st = S.stream;
+    B200_CUDA(cudaMemsetAsync(x.a.p, 0, size_t(words) * 4, st));
+    B200_CUDA(cudaMemsetAsync(x.c.p, 0, size_t(words) * 4, st));
+    raster(S, ref, cam_dev, ss, size, force_two, true, x.a.p, nullptr, x.state.p);
+    raster(S, cand, cam_dev, ss, size, force_two, true, x.c.p, nullptr, x.state.p + 4);
+    launch_popcounts(x.a.p, x.c.p, words, x.pop.p, st);
+    unsigned long long pop[4];
+    uint32_t state[8];
+    B200_CUDA(cudaMemcpyAsync(pop, x.pop.p, sizeof(pop), cudaMemcpyDeviceToHost, st));
+    B200_CUDA(cudaMemcpyAsync(state, x.state.p, sizeof(state), cudaMemcpyDeviceToHost, st));
+    B200_CUDA(cudaStreamSynchronize(st));
+    rec = ViewRecord{};
+    rec.changed = uint32_t(pop[0]);
+    rec.total = uint32_t(pop[1]);
+    rec.ca = pop[2] > 0;
+    rec.cb = pop[3] > 0;
+    rec.flags = (state[1] ? kRecClippedRef : 0) | (state[5] ? kRecClippedCand : 0);
+    max_d2 = 0;
+    if (rec.changed && rec.ca && rec.cb) {
+        B200_CUDA(cudaMemsetAsync(x.maxes.p, 0, 8, st));
+        launch_distance(x.a.p, x.c.p, size, x.g.p, x.d2.p, x.sv.p, x.sn.p, x.sd.p, x.maxes.p, st);
+        launch_distance(x.c.p, x.a.p, size, x.g.p, x.d2.p, x.sv.p, x.sn.p, x.sd.p, x.maxes.p + 1, st);
+        uint32_t m[2];
+        B200_CUDA(cudaMemcpyAsync(m, x.maxes.p, 8, cudaMemcpyDeviceToHost, st));
+        B200_CUDA(cudaStreamSynchronize(st));
+        float fa, fc;
+        std::memcpy(&fa, &m[0], 4);
+        std::memcpy(&fc, &m[1], 4);
+        max_d2 = std::max(double(fa), double(fc));
+    }
+}
+
+// evaluate_impl (evaluate.cpp:312-352) over the full-raster path, starting at
+// view `first_view` with a default result (the exact path resumes whole gates).
+static Measurement evaluate_full(Session& S, const DevMesh& ref, const DevMesh& cand, const blitz_eval_settings* es,
+                                 const GateSettings& g) {
+    Measurement result = default_measurement();
+    result.supersample = g.supersample;
+    auto cams = make_cameras(S.bounds, g.screen_size, es->views_orthographic, es->views_perspective, es->views_seed);
+    Buf<Camera> dcams(S.pool, cams.size());
+    B200_CUDA(cudaMemcpyAsync(dcams.p, cams.data(), cams.size() * sizeof(Camera), cudaMemcpyHostToDevice, S.stream));
+    for (uint32_t v = 0; v < cams.size(); ++v) {
+        Measurement cur = default_measurement();
+        cur.worst_view = v;
+        for (uint32_t ss = g.supersample;; ss = std::min<uint32_t>(g.max_supersample, ss * 2)) {
+            uint32_t size = raster_size(g.screen_size, ss);
+            if (uint64_t(size) * size > kMaxSamples) {
+                result.complete = 0;
+                result.passed = 0;
+                result.resource_limited = 1;
+                result.error = INFINITY;
+                return result;
+            }
+            ViewRecord rec;
+            double max_d2;
+            full_view(S, ref, cand, dcams.p + v, ss, size, es->force_two_sided, rec, max_d2);
+            finish_view(cur, rec, g, ss, max_d2);
+            if (refinement_done(cur, g, ss)) break;
+        }
+        if (!aggregate_view(result, cur, v)) return result;
+    }
+    return result;
+}
+
+struct GateRef {
+    const blitz_eval_settings* es;
+    GateSettings g;
+    int reference;
+};
+
+// Candidate whose verdict needs the full-raster path from gate `first`.
+static void exact_candidate(Session& S, const blitz_collapse& col, const GateRef* gates, int first,
+                            blitz_candidate_verdict& v, Measurement* meas) {
+    const DevMesh& m = S.state.view;
+    Topology& t = S.topo;
+    if (!S.trial.pos.p) {
+        S.trial.pos = Buf<float>(S.pool, 3ull * m.nv);
+        S.trial.idx = Buf<uint32_t>(S.pool, 3ull * m.nf);
+        if (m.mat) S.trial.mat = Buf<uint16_t>(S.pool, m.nf);
+        S.trial_keep = Buf<uint32_t>(S.pool, m.nf + 1);
+        S.trial_offsets = Buf<uint32_t>(S.pool, m.nf + 1);
+        S.trial_info = Buf<TrialInfo>(S.pool, 1);
+    }
+    Buf<blitz_collapse> one(S.pool, 1);
+    B200_CUDA(cudaMemcpyAsync(one.p, &col, sizeof(col), cudaMemcpyHostToDevice, S.stream));
+    launch_trial(m, t.view, one.p, S.trial_info.p, S.trial_keep.p, S.trial_offsets.p, S.trial.idx.p, S.trial.mat.p,
+                 S.trial.pos.p, t.scan.p, S.stream);
+    uint32_t faces = 0;
+    B200_CUDA(cudaMemcpyAsync(&faces, S.trial_offsets.p + m.nf, 4, cudaMemcpyDeviceToHost, S.stream));
+    B200_CUDA(cudaStreamSynchronize(S.stream));
+    DevMesh cand = m;
+    cand.pos = S.trial.pos.p;
+    cand.idx = S.trial.idx.p;
+    cand.mat = m.mat ? S.trial.mat.p : nullptr;
+    cand.nf = faces;
+    v.exact_path = 1;
+    v.failed_gate = 0;
+    v.accepted = 0;
+    for (int gi = first; gi < 4; ++gi) {
+        const DevMesh& ref = gates[gi].reference == 0 || S.previous_is_source ? S.source.view : S.previous.view;
+        Measurement r = evaluate_full(S, ref, cand, gates[gi].es, gates[gi].g);
+        if (meas) meas[gi] = r;
+        if (!measurement_accepted(r)) {
+            v.failed_gate = uint8_t(gi + 1);
+            return;
+        }
+    }
+    v.accepted = 1;
+}
+
+static void audit_candidates(Session& S, const blitz_collapse* cands_dev, const blitz_collapse* cands_host, size_t n,
+                             const blitz_eval_settings gates_in[4], blitz_candidate_verdict* out_dev,
+                             Measurement* meas_dev, cudaStream_t st) {
+    if (n > UINT32_MAX / 2) throw Failure(BLITZ_INVALID_ARGUMENT, "too many candidates");
+    GateRef gates[4];
+    std::vector<PlanKey> keys;
+    uint32_t plan_of[4];
+    for (int g = 0; g < 4; ++g) {
+        gates[g].es = &gates_in[g];
+        gates[g].g = gate_of(&gates_in[g], S.bounds);
+        gates[g].g.max_supersample = uint8_t(
+            bounded_refinement(gates[g].g.screen_size, gates[g].g.supersample, gates[g].g.max_supersample));
+        gates[g].reference = g % 2;
+        PlanKey k{(g % 2) && !S.previous_is_source ? 1 : 0, gates_in[g].views_orthographic,
+                  gates_in[g].views_perspective, gates_in[g].views_seed, gates_in[g].screen_size,
+                  gates_in[g].supersample, gates_in[g].force_two_sided};
+        auto it = std::find_if(keys.begin(), keys.end(), [&](const PlanKey& o) { return !(o < k) && !(k < o); });
+        plan_of[g] = uint32_t(it - keys.begin());
+        if (it == keys.end()) keys.push_back(k);
+    }
+    (void)cands_host;
+    const uint32_t nn = uint32_t(n);
+    Topology& t = S.topo;
+    S.records.ensure(S.pool, nn);
+    std::vector<Plan*> plans;
+    for (auto& k : keys) plans.push_back(&plan_for(S, k));
+    const bool prof = S.profiling && nn;
+    if (prof) {
+        S.stats.ensure(S.pool, 4);
+        B200_CUDA(cudaMemsetAsync(S.stats.p, 0, 32, st));
+        B200_CUDA(cudaEventRecord(S.ev[0], st));
+    }
+    launch_prepare(S.state.view, t.view, S.state.view, t.view, cands_dev, nn, t.positions.p, t.pos_cap, t.flat.p,
+                   S.options.preserve_uv != 0, S.records.p, st);
+    if (prof) B200_CUDA(cudaEventRecord(S.ev[1], st));
+    S.profile.launches += nn ? 1 : 0;
+    std::vector<const ViewRecord*> table(plans.size());
+    std::vector<uint32_t> pviews(plans.size()), pss(plans.size());
+    for (size_t i = 0; i < plans.size(); ++i) {
+        Plan& p = *plans[i];
+        if (p.resource_limited) throw Failure(BLITZ_BUDGET_LIMITED, "raster exceeds per-view sample budget");
+        p.records.ensure(S.pool, size_t(nn) * p.views);
+        launch_audit(S.records.p, nn, p.dev, p.records.p, prof ? S.stats.p : nullptr, st);
+        if (nn) S.profile.launches += 1, S.profile.audit_launches += 1;
+        table[i] = p.records.p;
+        pviews[i] = p.views;
+        pss[i] = p.key.ss;
+    }
+    if (prof) B200_CUDA(cudaEventRecord(S.ev[4], st));
+    S.record_table.ensure(S.pool, 4);
+    S.plan_views.ensure(S.pool, 4);
+    S.plan_ss.ensure(S.pool, 4);
+    S.gate_table.ensure(S.pool, 4);
+    S.exact_count.ensure(S.pool, 1);
+    GateDev gd[4];
+    for (int g = 0; g < 4; ++g) gd[g] = GateDev{gates[g].g, plan_of[g]};
+    B200_CUDA(cudaMemcpyAsync(S.record_table.p, table.data(), table.size() * sizeof(void*), cudaMemcpyHostToDevice, st));
+    B200_CUDA(cudaMemcpyAsync(S.plan_views.p, pviews.data(), pviews.size() * 4, cudaMemcpyHostToDevice, st));
+    B200_CUDA(cudaMemcpyAsync(S.plan_ss.p, pss.data(), pss.size() * 4, cudaMemcpyHostToDevice, st));
+    B200_CUDA(cudaMemcpyAsync(S.gate_table.p, gd, sizeof(gd), cudaMemcpyHostToDevice, st));
+    B200_CUDA(cudaMemsetAsync(S.exact_count.p, 0, 4, st));
+    if (prof) B200_CUDA(cudaEventRecord(S.ev[2], st));
+    launch_verdicts(S.record_table.p, S.plan_views.p, S.plan_ss.p, S.gate_table.p, S.records.p, nn, out_dev, meas_dev,
+                    S.exact_count.p, st);
+    if (nn) S.profile.launches += 1;
+    if (prof) B200_CUDA(cudaEventRecord(S.ev[3], st));
+    uint32_t exact = 0;
+    B200_CUDA(cudaMemcpyAsync(&exact, S.exact_count.p, 4, cudaMemcpyDeviceToHost, st));
+    B200_CUDA(cudaStreamSynchronize(st));
+    B200_CUDA(cudaGetLastError());
+    if (prof) {
+        float a = 0, b = 0, c = 0;
+        B200_CUDA(cudaEventElapsedTime(&a, S.ev[0], S.ev[1]));
+        B200_CUDA(cudaEventElapsedTime(&b, S.ev[1], S.ev[4]));
+        B200_CUDA(cudaEventElapsedTime(&c, S.ev[2], S.ev[3]));
+        unsigned long long h[4];
+        B200_CUDA(cudaMemcpy(h, S.stats.p, sizeof(h), cudaMemcpyDeviceToHost));
+        S.profile.prepare_ms += a;
+        S.profile.audit_ms += b;
+        S.profile.verdict_ms += c;
+        S.profile.units += h[0];
+        S.profile.region_samples += h[1];
+        S.profile.changed_samples += h[2];
+        S.profile.record_bytes += uint64_t(nn) * sizeof(CandidateRecord) * plans.size();
+    }
+    if (exact) {
+        std::vector<blitz_candidate_verdict> hv(nn);
+        B200_CUDA(cudaMemcpyAsync(hv.data(), out_dev, nn * sizeof(blitz_candidate_verdict), cudaMemcpyDeviceToHost, st));
+        std::vector<blitz_collapse> hc(nn);
+        B200_CUDA(cudaMemcpyAsync(hc.data(), cands_dev, nn * sizeof(blitz_collapse), cudaMemcpyDeviceToHost, st));
+        B200_CUDA(cudaStreamSynchronize(st));
+        cudaStream_t saved = S.stream;
+        S.stream = st;
+        for (uint32_t c = 0; c < nn; ++c) {
+            if (!hv[c].exact_path) continue;
+            int first = hv[c].reserved; // resume gate
+            Measurement m4[4];
+            if (meas_dev) {
+                B200_CUDA(cudaMemcpyAsync(m4, meas_dev + size_t(c) * 4, sizeof(m4), cudaMemcpyDeviceToHost, st));
+                B200_CUDA(cudaStreamSynchronize(st));
+            }
+            exact_candidate(S, hc[c], gates, first, hv[c], meas_dev ? m4 : nullptr);
+            hv[c].reserved = 0;
+            B200_CUDA(cudaMemcpyAsync(out_dev + c, &hv[c], sizeof(hv[c]), cudaMemcpyHostToDevice, st));
+            if (meas_dev)
+                B200_CUDA(cudaMemcpyAsync(meas_dev + size_t(c) * 4, m4, sizeof(m4), cudaMemcpyHostToDevice, st));
+            B200_CUDA(cudaStreamSynchronize(st));
+        }
+        S.stream = saved;
+    }
+    S.info.decoded += nn;
+}
+
+} // namespace b200
+
+// ---------------------------------------------------------------------------
+// C ABI
+using namespace b200;
+
+struct blitz_audit_session {
+    Session s;
+};
+
+namespace {
+void message(char* out, size_t n, const char* text) {
+    if (out && n) {
+        size_t k = std::min(n - 1, std::strlen(text));
+        std::memcpy(out, text, k);
+        out[k] = 0;
+    }
+}
+template <class F> blitz_status guarded(char* error, size_t cap, F f) {
+    message(error, cap, "");
+    try {
+        f();
+        return BLITZ_OK;
+    } catch (const Failure& e) {
+        message(error, cap, e.what());
+        return e.status;
+    } catch (const std::bad_alloc&) {
+        message(error, cap, "host allocation failed");
+        return BLITZ_OUT_OF_MEMORY;
+    } catch (const std::exception& e) {
+        message(error, cap, e.what());
+        return BLITZ_INTERNAL_ERROR;
+    } catch (...) {
+        message(error, cap, "unknown failure");
+        return BLITZ_INTERNAL_ERROR;
+    }
+}
+uint64_t now_ns() {
+    return uint64_t(std::chrono::duration_cast<std::chrono::nanoseconds>(
+                        std::chrono::steady_clock::now().time_since_epoch())
+                        .count());
+}
+} // namespace
+
+extern "C" {
+
+uint32_t blitz_abi_version(void) { return BLITZ_ABI_VERSION; }
+
+blitz_status blitz_neural_options_v2_init(blitz_neural_options_v2* out, size_t n) {
+    if (!out || n != sizeof(*out)) return BLITZ_INVALID_ARGUMENT;
+    *out = blitz_neural_options_v2{};
+    out->struct_size = sizeof(*out);
+    out->version = 2;
+    out->device = 0;
+    out->memory_mib = 6144;
+    out->action_trials = 64;
+    out->ranking_seed = 0xB1172026u;
+    out->exact_position_bps = 500;
+    out->action_batch = 32;
+    out->origin = 0;
+    out->ranking = 0;
+    out->confirmation = 1;
+    out->raster_backend = 0;
+    out->vertex_storage = 3;
+    out->preserve_uv = 1;
+    out->overdraw_tiebreak = 1;
+    out->cache_rasters = 1;
+    out->mask_only_coverage = 1;
+    out->direct_targets = 1;
+    out->view_batch = 4;
+    out->candidate_batch = 1;
+    return BLITZ_OK;
+}
+
+blitz_status blitz_eval_settings_init(blitz_eval_settings* out, size_t n) {
+    if (!out || n != sizeof(*out)) return BLITZ_INVALID_ARGUMENT;
+    *out = blitz_eval_settings{};
+    out->struct_size = sizeof(*out);
+    out->profile = 0;
+    out->supersample = 8;
+    out->max_supersample = 32;
+    out->views_orthographic = 642;
+    out->views_perspective = 64;
+    out->views_seed = 0xB1172026u;
+    out->screen_size = 512;
+    out->limit = 2;
+    out->max_changed_area = 1;
+    return BLITZ_OK;
+}
+
+blitz_status blitz_audit_session_create(const blitz_mesh* source, const blitz_neural_options_v2* options,
+                                        blitz_audit_session** out, char* error, size_t cap) {
+    if (out) *out = nullptr;
+    return guarded(error, cap, [&] {
+        if (!out) throw Failure(BLITZ_INVALID_ARGUMENT, "null session destination");
+        blitz_neural_options_v2 o;
+        blitz_neural_options_v2_init(&o, sizeof(o));
+        if (options) {
+            if (options->struct_size != sizeof(*options) || options->version != 2 || options->reserved[0] ||
+                options->reserved[1] || options->reserved[2] || options->preserve_uv > 1)
+                throw Failure(BLITZ_INVALID_ARGUMENT, "invalid neural v2 descriptor");
+            if (options->raster_backend != 0) throw Failure(BLITZ_UNAVAILABLE, "only the CUDA raster backend exists");
+            o = *options;
+        }
+        if (o.memory_mib < 128) throw Failure(BLITZ_INVALID_ARGUMENT, "memory_mib below 128");
+        int count = 0;
+        if (cudaGetDeviceCount(&count) != cudaSuccess || count <= o.device || o.device < 0) {
+            cudaGetLastError();
+            throw Failure(BLITZ_UNAVAILABLE, "no CUDA device for the audit session");
+        }
+        HostMesh h = import_mesh(source);
+        Bounds b = bounds_of(h);
+        if (!(b.radius > 0) || !std::isfinite(b.radius))
+            throw Failure(BLITZ_INVALID_ARGUMENT, "zero or invalid source extent");
+        auto session = std::make_unique<blitz_audit_session>();
+        Session& S = session->s;
+        S.device = o.device;
+        S.options = o;
+        S.pool.limit = size_t(o.memory_mib) << 20;
+        DeviceScope scope(S.device);
+        B200_CUDA(cudaStreamCreateWithFlags(&S.stream, cudaStreamNonBlocking));
+        S.source_h = std::move(h);
+        S.bounds = b;
+        S.source.upload(S.pool, S.source_h, S.stream);
+        S.state.upload(S.pool, S.source_h, S.stream);
+        build_topology(S);
+        *out = session.release();
+    });
+}
+
+void blitz_audit_session_destroy(blitz_audit_session* s) {
+    if (!s) return;
+    int previous = 0;
+    cudaGetDevice(&previous);
+    cudaSetDevice(s->s.device);
+    delete s;
+    cudaSetDevice(previous);
+}
+
+blitz_status blitz_audit_bind_reference(blitz_audit_session* s, const blitz_mesh* previous, char* error, size_t cap) {
+    return guarded(error, cap, [&] {
+        if (!s) throw Failure(BLITZ_INVALID_ARGUMENT, "null session");
+        Session& S = s->s;
+        DeviceScope scope(S.device);
+        if (!previous) {
+            S.previous_is_source = true;
+            S.previous = DeviceMesh{};
+            S.previous_h = HostMesh{};
+        } else {
+            HostMesh h = import_mesh(previous);
+            if (same_data(h, S.source_h)) {
+                S.previous_is_source = true;
+                S.previous = DeviceMesh{};
+                S.previous_h = HostMesh{};
+            } else {
+                S.previous_h = std::move(h);
+                S.previous.upload(S.pool, S.previous_h, S.stream);
+                S.previous_is_source = false;
+            }
+        }
+        // Plans against the previous reference are stale.
+        for (auto it = S.plans.begin(); it != S.plans.end();)
+            it = it->first.reference == 1 ? S.plans.erase(it) : std::next(it);
+        B200_CUDA(cudaStreamSynchronize(S.stream));
+    });
+}
+
+blitz_status blitz_audit_evaluate(blitz_audit_session* s, const blitz_mesh* reference, const blitz_mesh* candidate,
+                                  const blitz_eval_settings* settings, blitz_measurement* out, char* error,
+                                  size_t cap) {
+    return guarded(error, cap, [&] {
+        if (!s || !out) throw Failure(BLITZ_INVALID_ARGUMENT, "null session or output");
+        Session& S = s->s;
+        DeviceScope scope(S.device);
+        uint64_t t0 = now_ns();
+        GateSettings g = gate_of(settings, S.bounds);
+        HostMesh ref = import_mesh(reference), cand = import_mesh(candidate);
+        Measurement result = default_measurement();
+        result.supersample = g.supersample;
+        if (!identical(ref, cand)) {
+            DeviceMesh dr, dc;
+            dr.upload(S.pool, ref, S.stream);
+            dc.upload(S.pool, cand, S.stream);
+            result = evaluate_full(S, dr.view, dc.view, settings, g);
+            B200_CUDA(cudaStreamSynchronize(S.stream));
+        }
+        std::memcpy(out, &result, sizeof(*out));
+        S.info.gpu_audit_ns += now_ns() - t0;
+    });
+}
+
+blitz_status blitz_audit_raster(blitz_audit_session* s, const blitz_mesh* mesh, double screen, uint8_t ss,
+                                uint16_t ortho, uint16_t persp, uint32_t seed, uint32_t view, uint8_t force_two,
+                                uint64_t* words, size_t word_capacity, uint32_t* size_out, uint8_t* clipped,
+                                char* error, size_t cap) {
+    return guarded(error, cap, [&] {
+        if (!s || !words || !size_out || !clipped) throw Failure(BLITZ_INVALID_ARGUMENT, "null argument");
+        Session& S = s->s;
+        DeviceScope scope(S.device);
+        if (!ss || !std::isfinite(screen) || screen <= 0 || screen > 16384)
+            throw Failure(BLITZ_INVALID_ARGUMENT, "invalid raster extent");
+        if (view >= uint32_t(ortho) + persp) throw Failure(BLITZ_INVALID_ARGUMENT, "view outside camera set");
+        uint32_t size = raster_size(screen, ss);
+        if (uint64_t(size) * size > kMaxSamples) throw Failure(BLITZ_BUDGET_LIMITED, "raster exceeds per-view memory budget");
+        size_t n = (size_t(size) * size + 63) / 64;
+        if (word_capacity < n) throw Failure(BLITZ_INVALID_ARGUMENT, "word buffer too small");
+        HostMesh h = import_mesh(mesh);
+        DeviceMesh d;
+        d.upload(S.pool, h, S.stream);
+        auto cams = make_cameras(S.bounds, screen, ortho, persp, seed);
+        Buf<Camera> cam(S.pool, 1);
+        B200_CUDA(cudaMemcpyAsync(cam.p, &cams[view], sizeof(Camera), cudaMemcpyHostToDevice, S.stream));
+        Buf<uint32_t> bits(S.pool, mask_words(size));
+        Buf<uint32_t> state(S.pool, 4);
+        B200_CUDA(cudaMemsetAsync(bits.p, 0, bits.n * 4, S.stream));
+        raster(S, d.view, cam.p, ss, size, force_two, true, bits.p, nullptr, state.p);
+        uint32_t st[4];
+        B200_CUDA(cudaMemcpyAsync(words, bits.p, n * 8, cudaMemcpyDeviceToHost, S.stream));
+        B200_CUDA(cudaMemcpyAsync(st, state.p, sizeof(st), cudaMemcpyDeviceToHost, S.stream));
+        B200_CUDA(cudaStreamSynchronize(S.stream));
+        *size_out = size;
+        *clipped = st[1] != 0;
+    });
+}
+
+blitz_status blitz_audit_actions(blitz_audit_session* s, blitz_collapse* out, size_t capacity, size_t* count,
+                                 char* error, size_t cap) {
+    return guarded(error, cap, [&] {
+        if (!s || !count || (capacity && !out)) throw Failure(BLITZ_INVALID_ARGUMENT, "null argument");
+        Session& S = s->s;
+        DeviceScope scope(S.device);
+        *count = S.topo.actions;
+        size_t k = std::min<size_t>(capacity, S.topo.actions);
+        if (!k) return;
+        std::vector<Edit> edits(k);
+        B200_CUDA(cudaMemcpyAsync(edits.data(), S.topo.edits.p, k * sizeof(Edit), cudaMemcpyDeviceToHost, S.stream));
+        B200_CUDA(cudaStreamSynchronize(S.stream));
+        for (size_t i = 0; i < k; ++i) out[i] = blitz_collapse{edits[i].from, edits[i].to, 0, {0, 0, 0}};
+    });
+}
+
+blitz_status blitz_audit_candidates_device(blitz_audit_session* s, const blitz_collapse* candidates_device, size_t n,
+                                           const blitz_eval_settings gates[4], blitz_candidate_verdict* out_device,
+                                           blitz_measurement* measurements_device, void* stream, char* error,
+                                           size_t cap) {
+    return guarded(error, cap, [&] {
+        if (!s || !gates || (n && (!candidates_device || !out_device)))
+            throw Failure(BLITZ_INVALID_ARGUMENT, "null argument");
+        Session& S = s->s;
+        DeviceScope scope(S.device);
+        if (S.options.preserve_uv && !S.source_h.uv.empty())
+            throw Failure(BLITZ_UNAVAILABLE, "uv transport on the candidate path is not implemented");
+        uint64_t t0 = now_ns();
+        cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : S.stream;
+        audit_candidates(S, candidates_device, nullptr, n, gates, out_device,
+                         reinterpret_cast<Measurement*>(measurements_device), st);
+        S.info.gpu_audit_ns += now_ns() - t0;
+    });
+}
+
+blitz_status blitz_audit_candidates(blitz_audit_session* s, const blitz_collapse* candidates, size_t n,
+                                    const blitz_eval_settings gates[4], blitz_candidate_verdict* out,
+                                    blitz_measurement* measurements, char* error, size_t cap) {
+    return guarded(error, cap, [&] {
+        if (!s || !gates || (n && (!candidates || !out))) throw Failure(BLITZ_INVALID_ARGUMENT, "null argument");
+        Session& S = s->s;
+        DeviceScope scope(S.device);
+        if (S.options.preserve_uv && !S.source_h.uv.empty())
+            throw Failure(BLITZ_UNAVAILABLE, "uv transport on the candidate path is not implemented");
+        uint64_t t0 = now_ns();
+        S.collapse_dev.ensure(S.pool, std::max<size_t>(n, 1));
+        S.verdict_dev.ensure(S.pool, std::max<size_t>(n, 1) * sizeof(blitz_candidate_verdict));
+        if (measurements) S.meas_dev.ensure(S.pool, std::max<size_t>(n, 1) * 4);
+        if (n)
+            B200_CUDA(cudaMemcpyAsync(S.collapse_dev.p, candidates, n * sizeof(blitz_collapse), cudaMemcpyHostToDevice,
+                                      S.stream));
+        auto* vd = reinterpret_cast<blitz_candidate_verdict*>(S.verdict_dev.p);
+        audit_candidates(S, S.collapse_dev.p, candidates, n, gates, vd, measurements ? S.meas_dev.p : nullptr, S.stream);
+        if (n) {
+            B200_CUDA(cudaMemcpyAsync(out, vd, n * sizeof(*out), cudaMemcpyDeviceToHost, S.stream));
+            if (measurements)
+                B200_CUDA(cudaMemcpyAsync(measurements, S.meas_dev.p, n * 4 * sizeof(blitz_measurement),
+                                          cudaMemcpyDeviceToHost, S.stream));
+        }
+        B200_CUDA(cudaStreamSynchronize(S.stream));
+        for (size_t i = 0; i < n; ++i) out[i].accepted ? ++S.info.legal_collapses : ++S.info.rejected_collapses;
+        S.info.gpu_audit_ns += now_ns() - t0;
+    });
+}
+
+blitz_status blitz_audit_profile_enable(blitz_audit_session* s, int enable) {
+    return guarded(nullptr, 0, [&] {
+        if (!s) throw Failure(BLITZ_INVALID_ARGUMENT, "null session");
+        Session& S = s->s;
+        DeviceScope scope(S.device);
+        if (enable && !S.ev[0])
+            for (auto& e : S.ev) B200_CUDA(cudaEventCreate(&e));
+        S.profiling = enable != 0;
+        S.profile = blitz_audit_profile{};
+    });
+}
+
+blitz_status blitz_audit_profile_read(const blitz_audit_session* s, blitz_audit_profile* out) {
+    if (!s || !out || out->struct_size != sizeof(*out)) return BLITZ_INVALID_ARGUMENT;
+    blitz_audit_profile p = s->s.profile;
+    p.struct_size = sizeof(p);
+    p.enabled = s->s.profiling;
+    *out = p;
+    return BLITZ_OK;
+}
+
+blitz_status blitz_audit_session_info(const blitz_audit_session* s, blitz_neural_info* out) {
+    if (!s || !out || out->struct_size != sizeof(*out)) return BLITZ_INVALID_ARGUMENT;
+    blitz_neural_info i = s->s.info;
+    i.struct_size = sizeof(i);
+    *out = i;
+    return BLITZ_OK;
+}
+
+} // extern "C"

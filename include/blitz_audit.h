@@ -1,0 +1,212 @@
+/* blitz_audit.h — C ABI of the B200 candidate-audit engine.
+ *
+ * Drop-in boundary for BlitzRemesher's audit call. The ABI-5 descriptors
+ * (blitz_status, blitz_stream, blitz_mesh) and the neural v2 options and
+ * diagnostics (blitz_neural_options_v2, blitz_neural_info) keep the exact
+ * layouts of BlitzRemesher's include/blitz/blitz.h, so a client that already
+ * fills them passes the same structs here. The audit entry points are new: the
+ * reference has no C function for its audit (it is internal C++,
+ * src/neural/evaluate.cu AuditCuda::evaluate/certify and
+ * src/neural/action_gpu.cu GpuActionState::execute); each declaration below
+ * names the internal call it replaces.
+ *
+ * Conventions (as blitz.h): every call returns a blitz_status; C++ exceptions
+ * never cross; an optional caller buffer receives a NUL-terminated message;
+ * struct_size / abi_version are validated; source streams are borrowed and
+ * never freed or mutated; a missing GPU yields BLITZ_UNAVAILABLE. A session is
+ * used by one thread at a time; it preserves the caller's current CUDA device.
+ */
+#ifndef BLITZ_AUDIT_H
+#define BLITZ_AUDIT_H
+#include <stddef.h>
+#include <stdint.h>
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#ifndef BLITZ_REMESHER_H
+#define BLITZ_ABI_VERSION 5u
+/* blitz.h:9-17 */
+typedef enum blitz_status {
+    BLITZ_OK = 0,
+    BLITZ_INVALID_ARGUMENT = 1,
+    BLITZ_OUT_OF_MEMORY = 2,
+    BLITZ_INTERNAL_ERROR = 3,
+    BLITZ_CANCELLED = 4,
+    BLITZ_BUDGET_LIMITED = 5,
+    BLITZ_UNAVAILABLE = 6
+} blitz_status;
+/* blitz.h:18-21 */
+typedef struct blitz_stream {
+    const void* data;
+    size_t count, stride;
+} blitz_stream;
+/* blitz.h:28-37 */
+typedef struct blitz_mesh {
+    uint32_t struct_size, abi_version;
+    blitz_stream positions, normals, uv, colors, tangents;
+    const uint32_t* indices;
+    size_t index_count;
+    const uint16_t* materials;
+    size_t material_count;
+    const uint8_t* double_sided;
+    size_t double_sided_count;
+} blitz_mesh;
+/* blitz.h:127-141 */
+typedef struct blitz_neural_options_v2 {
+    uint32_t struct_size, version;
+    int32_t device;
+    uint32_t memory_mib, action_trials, ranking_seed;
+    uint16_t exact_position_bps;
+    uint8_t action_batch, origin;
+    uint8_t ranking;
+    uint8_t confirmation;
+    uint8_t raster_backend; /* 0 = CUDA (the only backend here) */
+    uint8_t vertex_storage; /* FP32 master streams only */
+    uint8_t preserve_uv;
+    uint8_t overdraw_tiebreak, cache_rasters, mask_only_coverage, direct_targets;
+    uint8_t view_batch, candidate_batch;
+    uint8_t reserved[3];
+} blitz_neural_options_v2;
+/* blitz.h:150-155 */
+typedef struct blitz_neural_info {
+    uint32_t struct_size;
+    uint64_t encode_ns, inference_ns, decode_ns, gpu_audit_ns, reference_audit_ns;
+    uint64_t decoded, legal_collapses, rejected_collapses, reference_rejections;
+    uint32_t fallback_levels;
+} blitz_neural_info;
+uint32_t blitz_abi_version(void);
+/* c_api.cpp:228-245 — defaults of blitz::NeuralOptions. */
+blitz_status blitz_neural_options_v2_init(blitz_neural_options_v2*, size_t);
+#endif
+
+/* POD mirror of blitz::EvalSettings for the coverage profile
+ * (include/blitz/evaluate.hpp:24-33; ViewSet evaluate.hpp:8). */
+typedef struct blitz_eval_settings {
+    uint32_t struct_size;
+    uint8_t profile;          /* 0 = coverage; normals/attributes: BLITZ_UNAVAILABLE */
+    uint8_t supersample;      /* 1..32 */
+    uint8_t max_supersample;  /* supersample..32 */
+    uint8_t force_two_sided;
+    uint8_t conservative_screen;
+    uint8_t reserved[1];
+    uint16_t views_orthographic, views_perspective;
+    uint32_t views_seed;
+    double screen_size, limit, max_changed_area;
+} blitz_eval_settings;
+
+/* POD mirror of blitz::Measurement (include/blitz/evaluate.hpp:34-39). */
+typedef struct blitz_measurement {
+    double error, coverage, coverage_upper, changed_area, normal_degrees;
+    uint32_t worst_view, changed_area_worst_view, views_evaluated;
+    uint8_t supersample, complete, passed, resource_limited, cancelled;
+    uint8_t reserved[3];
+} blitz_measurement;
+
+/* One proposed directed edge contraction relative to the session's current
+ * state: geometric class `from` contracts into class `to` (class = smallest
+ * vertex slot at the same position), written at `position` or at the edge
+ * midpoint. Mirrors neural::Action + Placement (action.hpp:11-14,
+ * placement.hpp:6-20). */
+typedef struct blitz_collapse {
+    uint32_t from, to;
+    uint32_t placement; /* 0 = midpoint of the two class roots, 1 = explicit */
+    float position[3];
+} blitz_collapse;
+
+/* Four-gate result for one collapse (generate.cpp:365-388). */
+typedef struct blitz_candidate_verdict {
+    uint8_t accepted;    /* all four gates passed */
+    uint8_t failed_gate; /* 0 accepted; 1..4 source-search, previous-search,
+                            source-audit, previous-audit; 5 illegal; 6 invalid placement */
+    uint8_t exact_path;  /* 1 when a view needed the full-raster path */
+    uint8_t reserved;
+    uint32_t removed;    /* faces the collapse removes */
+} blitz_candidate_verdict;
+
+typedef struct blitz_audit_session blitz_audit_session;
+
+blitz_status blitz_eval_settings_init(blitz_eval_settings*, size_t);
+
+/* Uploads the source (LOD0) and builds the local-collapse topology of the
+ * session's current state (initially the source). Replaces the construction
+ * of neural::AuditCuda (evaluate.cu:2179-2212) and GpuActionState
+ * (action_gpu.cu:1459-1569). `options` may be NULL (defaults). */
+blitz_status blitz_audit_session_create(const blitz_mesh* source, const blitz_neural_options_v2* options,
+                                        blitz_audit_session** out, char* error, size_t error_capacity);
+void blitz_audit_session_destroy(blitz_audit_session*);
+
+/* Binds the previous emitted LOD as the adjacent reference
+ * (AuditCuda::bind_reference, generate.cpp:313). NULL binds the source. */
+blitz_status blitz_audit_bind_reference(blitz_audit_session*, const blitz_mesh* previous, char* error,
+                                        size_t error_capacity);
+
+/* Full audit of an arbitrary candidate against an arbitrary reference with the
+ * session's bounds: the twin of blitz::evaluate (evaluate.cpp:353) and
+ * AuditCuda::evaluate (evaluate.cu:2261-2341), coverage profile. */
+blitz_status blitz_audit_evaluate(blitz_audit_session*, const blitz_mesh* reference,
+                                  const blitz_mesh* candidate, const blitz_eval_settings* settings,
+                                  blitz_measurement* out, char* error, size_t error_capacity);
+
+/* Packed coverage mask of `mesh` in camera `view` of the camera set
+ * (ortho, persp, seed) at `screen` x `supersample`, with the session's bounds:
+ * the twin of blitz::detail::rasterize_coverage (evaluate.cpp:193-195).
+ * `words` receives ceil(size*size/64) little-endian u64 words (bit i%64 of
+ * word i/64 is sample i = y*size+x; tail bits zero); `*size` the raster side. */
+blitz_status blitz_audit_raster(blitz_audit_session*, const blitz_mesh* mesh, double screen, uint8_t supersample,
+                                uint16_t views_orthographic, uint16_t views_perspective, uint32_t views_seed,
+                                uint32_t view, uint8_t force_two_sided, uint64_t* words, size_t word_capacity,
+                                uint32_t* size, uint8_t* clipped, char* error, size_t error_capacity);
+
+/* Legal directed collapses of the current state, in the reference's
+ * enumeration order (action_gpu.cu:626-643 enumerate + DeviceSelect::Flagged).
+ * Writes min(count, capacity) collapses with midpoint placement; *count
+ * receives the total. */
+blitz_status blitz_audit_actions(blitz_audit_session*, blitz_collapse* out, size_t capacity, size_t* count,
+                                 char* error, size_t error_capacity);
+
+/* Batched four-gate audit of `n` collapses of the current state: each is
+ * applied with its placement, rasterized over the gates' views and compared
+ * with the source (gates 1, 3) and the bound previous LOD (gates 2, 4).
+ * Replaces the gate lambda of generate.cpp:365-388 over
+ * GpuActionState::trial + AuditCuda::certify. Host buffers; `measurements`
+ * may be NULL, else it receives 4 per collapse (gates not reached stay
+ * zero-initialised defaults). */
+blitz_status blitz_audit_candidates(blitz_audit_session*, const blitz_collapse* candidates, size_t n,
+                                    const blitz_eval_settings gates[4], blitz_candidate_verdict* out,
+                                    blitz_measurement* measurements, char* error, size_t error_capacity);
+
+/* Same as blitz_audit_candidates with device-resident candidate and verdict
+ * arrays, enqueued on `stream` (a cudaStream_t; NULL = the session stream).
+ * Synchronises before returning. */
+blitz_status blitz_audit_candidates_device(blitz_audit_session*, const blitz_collapse* candidates_device,
+                                           size_t n, const blitz_eval_settings gates[4],
+                                           blitz_candidate_verdict* out_device,
+                                           blitz_measurement* measurements_device, void* stream,
+                                           char* error, size_t error_capacity);
+
+/* Device-side profile of the session's own kernels (no reference
+ * counterpart; the reference exposes NVTX ranges, timeline.hpp:6-19). When
+ * enabled, every candidate call times its kernels with CUDA events on the
+ * launching stream and counts the samples the audit kernel touched. */
+typedef struct blitz_audit_profile {
+    uint32_t struct_size, enabled;
+    uint64_t launches;         /* kernels launched by candidate calls */
+    uint64_t audit_launches;   /* incremental audit kernel launches */
+    double audit_ms, prepare_ms, verdict_ms; /* summed device time */
+    uint64_t units;            /* (candidate, view) pairs audited */
+    uint64_t region_samples;   /* samples rasterized by the audit kernel */
+    uint64_t changed_samples;  /* samples whose distance was searched */
+    uint64_t record_bytes;     /* candidate records read by the audit kernel */
+} blitz_audit_profile;
+blitz_status blitz_audit_profile_enable(blitz_audit_session*, int enable);
+blitz_status blitz_audit_profile_read(const blitz_audit_session*, blitz_audit_profile*);
+
+/* Session diagnostics in the reference's counter block (blitz.h:150-155):
+ * gpu_audit_ns, legal_collapses, rejected_collapses, decoded (audited). */
+blitz_status blitz_audit_session_info(const blitz_audit_session*, blitz_neural_info*);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

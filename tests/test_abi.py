@@ -1,0 +1,123 @@
+"""CPU checks of the C ABI: the library loads, exports every declared symbol,
+keeps the reference's descriptor layouts, and refuses to run without a GPU."""
+import ctypes as C
+import re
+import subprocess
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import blitzremesher_b200 as br
+
+ROOT = Path(__file__).resolve().parents[1]
+HEADER = ROOT / "include" / "blitz_audit.h"
+REFERENCE_HEADER = Path("/root/reference/include/blitz/blitz.h")
+
+
+def declared_functions():
+    text = HEADER.read_text()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(blitz_\w+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol():
+    lib = br.load()
+    names = declared_functions()
+    assert "blitz_audit_candidates" in names and "blitz_audit_evaluate" in names
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+    out = subprocess.run(["nm", "-D", "--defined-only", str(br.library_path())], capture_output=True, text=True,
+                         check=True).stdout
+    exported = set(re.findall(r"\bT (blitz_\w+)", out))
+    assert set(names) <= exported
+
+
+def _c_layout(source: str, include: Path, tmp_path: Path) -> dict:
+    prog = tmp_path / "layout.c"
+    prog.write_text(source)
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-std=c11", f"-I{include}", str(prog), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout
+    return dict(line.split("=") for line in out.split())
+
+
+LAYOUT_SRC = r"""
+#include <stdio.h>
+#include <stddef.h>
+#include "%s"
+#define S(t) printf(#t "=%%zu\n", sizeof(t));
+#define O(t, f) printf(#t "." #f "=%%zu\n", offsetof(t, f));
+int main(void) {
+  S(blitz_mesh) S(blitz_neural_options_v2) S(blitz_neural_info) S(blitz_stream)
+  O(blitz_mesh, indices) O(blitz_mesh, double_sided_count)
+  O(blitz_neural_options_v2, exact_position_bps) O(blitz_neural_options_v2, reserved)
+  O(blitz_neural_info, fallback_levels)
+  %s
+  return 0;
+}
+"""
+
+
+def test_descriptor_layouts_match_python(tmp_path):
+    extra = "S(blitz_eval_settings) S(blitz_measurement) S(blitz_collapse) S(blitz_candidate_verdict)"
+    lay = _c_layout(LAYOUT_SRC % ("blitz_audit.h", extra), ROOT / "include", tmp_path)
+    assert int(lay["blitz_mesh"]) == C.sizeof(br.BlitzMesh)
+    assert int(lay["blitz_neural_options_v2"]) == C.sizeof(br.NeuralOptionsV2)
+    assert int(lay["blitz_neural_info"]) == C.sizeof(br.NeuralInfo)
+    assert int(lay["blitz_eval_settings"]) == C.sizeof(br.EvalSettings)
+    assert int(lay["blitz_measurement"]) == C.sizeof(br.Measurement) == br.MEASUREMENT_DTYPE.itemsize
+    assert int(lay["blitz_collapse"]) == C.sizeof(br.Collapse) == br.COLLAPSE_DTYPE.itemsize
+    assert int(lay["blitz_candidate_verdict"]) == C.sizeof(br.Verdict) == br.VERDICT_DTYPE.itemsize
+
+
+@pytest.mark.skipif(not REFERENCE_HEADER.exists(), reason="reference headers absent")
+def test_abi5_descriptors_identical_to_reference(tmp_path):
+    ours = _c_layout(LAYOUT_SRC % ("blitz_audit.h", ""), ROOT / "include", tmp_path)
+    (tmp_path / "ref").mkdir()
+    theirs = _c_layout(LAYOUT_SRC % ("blitz/blitz.h", ""), REFERENCE_HEADER.parents[1], tmp_path / "ref")
+    assert ours == theirs
+
+
+def test_version_and_defaults():
+    lib = br.load()
+    assert lib.blitz_abi_version() == 5
+    o = br.neural_options()
+    assert o.struct_size == C.sizeof(br.NeuralOptionsV2) and o.version == 2 and o.memory_mib == 6144
+    assert o.preserve_uv == 1 and o.action_batch == 32
+    bad = br.NeuralOptionsV2()
+    assert lib.blitz_neural_options_v2_init(C.byref(bad), 3) == br.BLITZ_INVALID_ARGUMENT
+    s = br.eval_settings(24.0, 1.0)
+    assert s.struct_size == C.sizeof(br.EvalSettings) and s.profile == 0
+
+
+def test_session_rejects_invalid_descriptors():
+    lib = br.load()
+    mesh = br.synthetic.noisy_icosphere(1, 1)
+    h = br._MeshHold(mesh)
+    h.c.abi_version = 4
+    handle = C.c_void_p()
+    err = C.create_string_buffer(256)
+    st = lib.blitz_audit_session_create(C.byref(h.c), None, C.byref(handle), err, 256)
+    assert st in (br.BLITZ_INVALID_ARGUMENT, br.BLITZ_UNAVAILABLE)
+    assert not handle.value
+
+
+def test_no_gpu_means_unavailable():
+    import torch
+
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    with pytest.raises(br.BlitzError) as exc:
+        br.AuditSession(br.synthetic.noisy_icosphere(1, 1))
+    assert exc.value.status == br.BLITZ_UNAVAILABLE
+
+
+def test_synthetic_mesh_shapes():
+    m = br.synthetic.config1_mesh()
+    assert m.face_count == 20480 and m.vertex_count == 10242
+    assert m.positions.dtype == np.float32 and m.indices.dtype == np.uint32
+    r = np.linalg.norm(m.positions.astype(np.float64), axis=1)
+    assert r.min() >= 0.98 - 1e-6 and r.max() <= 1.02 + 1e-6
+    again = br.synthetic.config1_mesh()
+    assert np.array_equal(m.positions, again.positions)
