@@ -149,7 +149,7 @@ struct GateSettings {
 };
 
 BH Measurement default_measurement() {
-    Measurement m;
+    Measurement m{};
     m.error = m.coverage = m.coverage_upper = m.changed_area = m.normal_degrees = 0;
     m.worst_view = m.changed_area_worst_view = m.views_evaluated = 0;
     m.supersample = 0;

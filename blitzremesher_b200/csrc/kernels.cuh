@@ -96,7 +96,7 @@ void launch_position_table(const DevMesh& m, const DevTopology& t, uint32_t* tab
 void launch_prepare(const DevMesh& m, const DevTopology& t, const DevMesh& original, const DevTopology& ot,
                     const void* collapses, uint32_t n, const uint32_t* table, uint32_t capacity,
                     const uint32_t* flat_total, bool preserve_uv, CandidateRecord* out, cudaStream_t s);
-void launch_raster(const DevMesh& m, const Camera* cam, const float* center, uint32_t ss, uint32_t size,
+void launch_raster(const DevMesh& m, const Camera* cam_host, const float* center, uint32_t ss, uint32_t size,
                    bool force_two, bool cpu_semantics, uint32_t* bits, uint8_t* counts, uint32_t* state,
                    cudaStream_t s);
 void launch_popcounts(const uint32_t* a, const uint32_t* b, uint32_t words, unsigned long long* out,

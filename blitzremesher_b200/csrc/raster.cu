@@ -204,12 +204,12 @@ __global__ void k_directed_max(const uint32_t* from, const uint32_t* to, const u
 }
 } // namespace
 
-void launch_raster(const DevMesh& m, const Camera* cam, const float* center, uint32_t ss, uint32_t size,
+void launch_raster(const DevMesh& m, const Camera* cam_host, const float* center, uint32_t ss, uint32_t size,
                    bool force_two, bool cpu_semantics, uint32_t* bits, uint8_t* counts, uint32_t* state,
                    cudaStream_t s) {
     RasterArgs a;
     a.m = m;
-    a.cam = *cam;
+    a.cam = *cam_host;
     a.center[0] = center[0], a.center[1] = center[1], a.center[2] = center[2];
     a.ss = ss, a.size = size, a.force_two = force_two, a.cpu_semantics = cpu_semantics;
     k_state_init<<<1, 32, 0, s>>>(state);

@@ -424,9 +424,9 @@ static uint32_t mask_words(uint32_t size) {
 }
 
 // Rasterizes a device mesh for one view; returns {any clip, first box clip, clipped faces, overflow}.
-static void raster(Session& S, const DevMesh& m, const Camera* cam_dev, uint32_t ss, uint32_t size, bool force_two,
+static void raster(Session& S, const DevMesh& m, const Camera* cam_host, uint32_t ss, uint32_t size, bool force_two,
                    bool cpu_semantics, uint32_t* bits, uint8_t* counts, uint32_t* state_dev) {
-    launch_raster(m, cam_dev, S.bounds.center, ss, size, force_two, cpu_semantics, bits, counts, state_dev, S.stream);
+    launch_raster(m, cam_host, S.bounds.center, ss, size, force_two, cpu_semantics, bits, counts, state_dev, S.stream);
 }
 
 static Plan& plan_for(Session& S, const PlanKey& key) {
@@ -459,8 +459,8 @@ static Plan& plan_for(Session& S, const PlanKey& key) {
     for (uint32_t v = 0; v < p.views; ++v) {
         uint32_t* rb = p.ref_bits.p + size_t(v) * p.words;
         uint8_t* sc = p.state_count.p + ((samples + 3) & ~size_t(3)) * v;
-        raster(S, ref.view, p.cameras.p + v, key.ss, p.size, key.force_two, true, rb, nullptr, state.p + 8 * v);
-        raster(S, S.state.view, p.cameras.p + v, key.ss, p.size, key.force_two, false, nullptr, sc, state.p + 8 * v + 4);
+        raster(S, ref.view, &cams[v], key.ss, p.size, key.force_two, true, rb, nullptr, state.p + 8 * v);
+        raster(S, S.state.view, &cams[v], key.ss, p.size, key.force_two, false, nullptr, sc, state.p + 8 * v + 4);
     }
     B200_CUDA(cudaMemcpyAsync(hstate.data(), state.p, hstate.size() * 4, cudaMemcpyDeviceToHost, S.stream));
     B200_CUDA(cudaStreamSynchronize(S.stream));
@@ -476,7 +476,7 @@ static Plan& plan_for(Session& S, const PlanKey& key) {
         p.state_bits = Buf<uint32_t>(S.pool, size_t(p.words) * p.views);
         B200_CUDA(cudaMemsetAsync(p.state_bits.p, 0, size_t(p.words) * p.views * 4, S.stream));
         for (uint32_t v = 0; v < p.views; ++v)
-            raster(S, S.state.view, p.cameras.p + v, key.ss, p.size, key.force_two, false,
+            raster(S, S.state.view, &cams[v], key.ss, p.size, key.force_two, false,
                    p.state_bits.p + size_t(v) * p.words, nullptr, state.p + 8 * v + 4);
     }
     Buf<unsigned long long> pop(S.pool, 4 * size_t(p.views));
@@ -531,7 +531,7 @@ static void ensure_scratch(Session& S, uint32_t size) {
 }
 
 // One view at one sampling through the full-raster path.
-static void full_view(Session& S, const DevMesh& ref, const DevMesh& cand, const Camera* cam_dev, uint32_t ss,
+static void full_view(Session& S, const DevMesh& ref, const DevMesh& cand, const Camera* cam_host, uint32_t ss,
                       uint32_t size, bool force_two, ViewRecord& rec, double& max_d2) {
     ensure_scratch(S, size);
     Scratch& x = S.scratch;
@@ -539,8 +539,8 @@ static void full_view(Session& S, const DevMesh& ref, const DevMesh& cand, const
     cudaStream_t st = S.stream;
     B200_CUDA(cudaMemsetAsync(x.a.p, 0, size_t(words) * 4, st));
     B200_CUDA(cudaMemsetAsync(x.c.p, 0, size_t(words) * 4, st));
-    raster(S, ref, cam_dev, ss, size, force_two, true, x.a.p, nullptr, x.state.p);
-    raster(S, cand, cam_dev, ss, size, force_two, true, x.c.p, nullptr, x.state.p + 4);
+    raster(S, ref, cam_host, ss, size, force_two, true, x.a.p, nullptr, x.state.p);
+    raster(S, cand, cam_host, ss, size, force_two, true, x.c.p, nullptr, x.state.p + 4);
     launch_popcounts(x.a.p, x.c.p, words, x.pop.p, st);
     unsigned long long pop[4];
     uint32_t state[8];
@@ -591,7 +591,7 @@ static Measurement evaluate_full(Session& S, const DevMesh& ref, const DevMesh& 
             }
             ViewRecord rec;
             double max_d2;
-            full_view(S, ref, cand, dcams.p + v, ss, size, es->force_two_sided, rec, max_d2);
+            full_view(S, ref, cand, &cams[v], ss, size, es->force_two_sided, rec, max_d2);
             finish_view(cur, rec, g, ss, max_d2);
             if (refinement_done(cur, g, ss)) break;
         }
@@ -974,7 +974,7 @@ blitz_status blitz_audit_raster(blitz_audit_session* s, const blitz_mesh* mesh, 
         Buf<uint32_t> bits(S.pool, mask_words(size));
         Buf<uint32_t> state(S.pool, 4);
         B200_CUDA(cudaMemsetAsync(bits.p, 0, bits.n * 4, S.stream));
-        raster(S, d.view, cam.p, ss, size, force_two, true, bits.p, nullptr, state.p);
+        raster(S, d.view, &cams[view], ss, size, force_two, true, bits.p, nullptr, state.p);
         uint32_t st[4];
         B200_CUDA(cudaMemcpyAsync(words, bits.p, n * 8, cudaMemcpyDeviceToHost, S.stream));
         B200_CUDA(cudaMemcpyAsync(st, state.p, sizeof(st), cudaMemcpyDeviceToHost, S.stream));

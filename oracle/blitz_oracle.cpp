@@ -995,7 +995,12 @@ int64_t bo_trial_midpoint(const bo_mesh* m, const bo_edit* e, int preserve_uv, u
     int64_t faces = -1;
     int status = guarded([&] {
         auto t = build_topology(*m, preserve_uv != 0);
-        Trial tr = make_trial(*m, t, *m, t, *e, preserve_uv != 0);
+        bo_edit edit{};
+        edit.from = e->from, edit.to = e->to;
+        if (edit.from >= m->vertex_count || edit.to >= m->vertex_count || edit.from == edit.to ||
+            !has_neighbor(t, edit.from, edit.to) || !legal(*m, t, edit, true, preserve_uv != 0))
+            throw std::invalid_argument("illegal collapse");
+        Trial tr = make_trial(*m, t, *m, t, edit, preserve_uv != 0);
         std::copy(tr.indices.begin(), tr.indices.end(), indices);
         std::copy(tr.positions.begin(), tr.positions.end(), positions);
         if (uv && m->uv) std::copy(tr.uv.begin(), tr.uv.end(), uv);
@@ -1014,7 +1019,16 @@ int bo_audit_candidate(const bo_mesh* parent, const bo_edit* e, const bo_mesh* s
     return guarded([&] {
         *out = bo_verdict{};
         auto t = build_topology(*parent, preserve_uv != 0);
-        Trial tr = make_trial(*parent, t, *parent, t, *e, preserve_uv != 0);
+        // The edit's wedges come from legality (action_gpu.cu:487-643), as in
+        // the reference executor; only from/to are taken from the caller.
+        bo_edit edit{};
+        edit.from = e->from, edit.to = e->to;
+        if (edit.from >= parent->vertex_count || edit.to >= parent->vertex_count || edit.from == edit.to ||
+            !has_neighbor(t, edit.from, edit.to) || !legal(*parent, t, edit, true, preserve_uv != 0)) {
+            out->failed_gate = 5;
+            return;
+        }
+        Trial tr = make_trial(*parent, t, *parent, t, edit, preserve_uv != 0);
         out->placement_valid = tr.valid;
         if (!tr.valid) {
             out->failed_gate = 6;

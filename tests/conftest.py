@@ -8,6 +8,26 @@ sys.path.insert(0, str(ROOT))
 GOLDEN = ROOT / "tests" / "golden"
 
 
+FIELDS = ["error", "coverage", "coverage_upper", "changed_area", "normal_degrees", "worst_view",
+          "changed_area_worst_view", "views_evaluated", "supersample", "complete", "passed", "resource_limited",
+          "cancelled"]
+
+
+def measurement_fields(m) -> tuple:
+    """Every Measurement field, doubles as bit patterns (padding excluded)."""
+    import struct
+
+    if hasattr(m, "dtype"):  # numpy record
+        get = lambda k: m[k].item()  # noqa: E731
+    else:
+        get = lambda k: getattr(m, k)  # noqa: E731
+    out = []
+    for k in FIELDS:
+        v = get(k)
+        out.append(struct.pack("<d", v) if k in FIELDS[:5] else int(v))
+    return tuple(out)
+
+
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA device (B200)")
 
