@@ -22,7 +22,7 @@ FLAGS = [
     "-O3", "-lineinfo", "--fmad=false", "-std=c++17",
     "-Xcompiler", "-fPIC,-ffp-contract=off,-fno-fast-math",
     "-Xptxas", "-v",
-]
+] + os.environ.get("NVCC_EXTRA", "").split()
 
 
 def needs_build() -> bool:

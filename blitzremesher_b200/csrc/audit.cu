@@ -1,26 +1,32 @@
 // Incremental candidate audit and four-gate verdicts.
 //
 // A collapse changes coverage only where the faces of faces(from) U faces(to)
-// land, before or after. For every (candidate, view) one warp rasterizes those
-// faces (old and new) over their joint bounding box, derives the candidate's
-// per-sample face count from the resident state counts (count - old + new),
-// builds the coverage words with __ballot_sync, updates the XOR/OR popcounts
-// against the resident reference mask, and measures the exact squared
-// distance of every changed sample by a row scan over coverage words. The
-// result equals a full re-raster of the candidate (evaluate.cpp:125-209)
-// sample for sample.
+// land, before or after. One warp audits one (candidate, view) unit, pulled
+// from a global work queue: it projects the candidate's distinct local
+// vertices (plus the placement), sets up the old and the new faces, rasterizes
+// them over their joint bounding box to derive the candidate's per-sample face
+// count from the resident state counts (count - old + new), builds coverage
+// words with __ballot_sync, updates the XOR/OR popcounts against the resident
+// reference mask, and measures the exact squared distance of every changed
+// sample by a row scan over coverage words. The result equals a full
+// re-raster of the candidate (evaluate.cpp:125-209) sample for sample.
 #include "kernels.cuh"
 
 namespace b200 {
 namespace {
 
 constexpr int kAuditWarps = 8;
+#ifndef B200_AUDIT_MIN_BLOCKS
+#define B200_AUDIT_MIN_BLOCKS 3 // resident blocks per SM the register budget targets
+#endif
 constexpr int kRegionWords = 4;  // region width <= 128 samples after 32-alignment
 constexpr int kRegionRows = 128; // region height
-constexpr int kQueue = 512;      // changed samples per (candidate, view)
+constexpr int kQueue = 256;      // changed samples per (candidate, view)
+constexpr int kMaxOk = 48;       // rasterized (uncluded, unclipped) old + new faces
 
 struct WarpScratch {
-    FaceSetup faces[2 * kMaxAffected];
+    double vx[32], vy[32], vz[32]; // projected local vertices; 31 = placement
+    FaceSetup faces[kMaxOk];       // old faces carry pad = -1, new faces pad = +1
     uint32_t region[kRegionRows * kRegionWords];
     uint32_t queue[kQueue];
 };
@@ -70,7 +76,6 @@ template <class M> __device__ uint32_t nearest_in_row(const M& mask, uint32_t ro
         best = d < best ? d : best;
     }
     if (best == 0) return 0;
-    // Left chunks.
     for (uint32_t c = cx; c-- > 0;) {
         uint32_t nearest = x - (c * 32 + 31);
         if (nearest > maxdx || nearest >= best) break;
@@ -119,49 +124,96 @@ template <class M> __device__ uint32_t nearest_d2(const M& mask, uint32_t x, uin
     return best;
 }
 
-__device__ __forceinline__ Proj project_pt(const PlanDev& plan, const Camera& cam, float x, float y, float z) {
-    return project(x, y, z, plan.center, cam, plan.ss, plan.size);
+__device__ __forceinline__ void record_write(ViewRecord* out, const ViewRecord& r) {
+    if (lane_id() == 0) *out = r;
 }
 
-__device__ void audit_view(const CandidateRecord& rec, const PlanDev& plan, uint32_t v, WarpScratch& ws,
-                           ViewRecord* out, unsigned long long* stats) {
+__device__ void audit_unit(const CandidateRecord* __restrict__ rec, const PlanDev& plan, uint32_t v,
+                           WarpScratch& ws, ViewRecord* out, unsigned long long* stats) {
     const uint32_t lane = lane_id();
     const PlanView pv = plan.views[v];
-    const Camera cam = plan.cameras[v];
     const uint32_t size = plan.size;
-    const uint32_t K = rec.count;
-    // Face setups: old faces at [0, K), candidate faces at [32, 32 + K).
-    bool old_ok = false, new_ok = false, old_clip = false, new_clip = false;
-    if (lane < K) {
-        const AffectedFace& af = rec.faces[lane];
-        Proj po[3], pn[3];
-        Proj pp = project_pt(plan, cam, rec.placement[0], rec.placement[1], rec.placement[2]);
-        for (int j = 0; j < 3; ++j) {
-            po[j] = project_pt(plan, cam, af.p[3 * j], af.p[3 * j + 1], af.p[3 * j + 2]);
-            pn[j] = (af.moved >> j) & 1 ? pp : po[j];
-        }
-        bool two = plan.force_two || af.two;
-        FaceSetup so = setup_face(po[0], po[1], po[2], cam.perspective != 0, two, size);
-        ws.faces[lane] = so;
-        old_ok = so.status == kFaceOk;
-        old_clip = so.status == kFaceClipZ || so.status == kFaceClipBox;
-        if (af.kept) {
-            FaceSetup sn = setup_face(pn[0], pn[1], pn[2], cam.perspective != 0, two, size);
-            ws.faces[32 + lane] = sn;
-            new_ok = sn.status == kFaceOk;
-            new_clip = sn.status == kFaceClipZ || sn.status == kFaceClipBox;
-        }
+    ViewRecord r;
+    r.pad = 0;
+    r.flags = pv.clipped_ref ? kRecClippedRef : 0;
+    r.ca = pv.cov_ref > 0;
+    r.max_d2 = 0, r.changed = 0, r.total = 0, r.cb = 0;
+    if (!plan.state_is_ref) {
+        // A state that differs from the reference needs the full distance field.
+        r.flags |= kRecFallback;
+        record_write(out, r);
+        return;
     }
-    const uint32_t ok_old = __ballot_sync(0xffffffffu, old_ok), ok_new = __ballot_sync(0xffffffffu, new_ok);
-    const int clip_delta = __popc(__ballot_sync(0xffffffffu, new_clip)) - __popc(__ballot_sync(0xffffffffu, old_clip));
+    const Camera cam = plan.cameras[v];
+    const uint32_t nverts = rec->nverts, nfaces = rec->nfaces;
+    // Project the local vertices and the placement once.
+    if (lane < nverts || lane == kPlacementLocal) {
+        float px, py, pz;
+        if (lane == kPlacementLocal) px = rec->placement[0], py = rec->placement[1], pz = rec->placement[2];
+        else px = rec->verts[3 * lane], py = rec->verts[3 * lane + 1], pz = rec->verts[3 * lane + 2];
+        Proj p = project(px, py, pz, plan.center, cam, plan.ss, size);
+        ws.vx[lane] = p.x, ws.vy[lane] = p.y, ws.vz[lane] = p.z;
+    }
+    __syncwarp();
+    // Face setups, old faces first, then the candidate's faces; the rasterized
+    // ones are compacted into ws.faces (old carry -1, new +1).
+    const uint32_t below = (1u << lane) - 1u;
+    const uint8_t fl = lane < nfaces ? rec->flags[lane] : 0;
+    const bool two = plan.force_two || (fl & kFaceTwo);
     int x0 = 1 << 30, y0 = 1 << 30, x1 = -1, y1 = -1;
-    if (old_ok) {
-        const FaceSetup& s = ws.faces[lane];
-        x0 = min(x0, s.x0), x1 = max(x1, s.x1), y0 = min(y0, s.y0), y1 = max(y1, s.y1);
+    uint32_t n_old, nok;
+    int clip_delta;
+    {
+        bool ok = false, clip = false;
+        FaceSetup s;
+        if (lane < nfaces) {
+            Proj a[3];
+            for (int j = 0; j < 3; ++j) {
+                uint32_t k = rec->old_face[3 * lane + j];
+                a[j] = Proj{ws.vx[k], ws.vy[k], ws.vz[k]};
+            }
+            s = setup_face(a[0], a[1], a[2], cam.perspective != 0, two, size);
+            ok = s.status == kFaceOk;
+            clip = s.status == kFaceClipZ || s.status == kFaceClipBox;
+        }
+        const uint32_t m = __ballot_sync(0xffffffffu, ok);
+        n_old = __popc(m);
+        clip_delta = -__popc(__ballot_sync(0xffffffffu, clip));
+        const uint32_t slot = __popc(m & below);
+        if (ok && slot < uint32_t(kMaxOk)) {
+            s.pad = -1;
+            ws.faces[slot] = s;
+            x0 = s.x0, x1 = s.x1, y0 = s.y0, y1 = s.y1;
+        }
     }
-    if (new_ok) {
-        const FaceSetup& s = ws.faces[32 + lane];
-        x0 = min(x0, s.x0), x1 = max(x1, s.x1), y0 = min(y0, s.y0), y1 = max(y1, s.y1);
+    {
+        bool ok = false, clip = false;
+        FaceSetup s;
+        if (lane < nfaces && (fl & kFaceKept)) {
+            Proj a[3];
+            for (int j = 0; j < 3; ++j) {
+                uint32_t k = rec->new_face[3 * lane + j];
+                a[j] = Proj{ws.vx[k], ws.vy[k], ws.vz[k]};
+            }
+            s = setup_face(a[0], a[1], a[2], cam.perspective != 0, two, size);
+            ok = s.status == kFaceOk;
+            clip = s.status == kFaceClipZ || s.status == kFaceClipBox;
+        }
+        const uint32_t m = __ballot_sync(0xffffffffu, ok);
+        nok = n_old + __popc(m);
+        clip_delta += __popc(__ballot_sync(0xffffffffu, clip));
+        const uint32_t slot = n_old + __popc(m & below);
+        if (ok && slot < uint32_t(kMaxOk)) {
+            s.pad = 1;
+            ws.faces[slot] = s;
+            x0 = min(x0, s.x0), x1 = max(x1, s.x1), y0 = min(y0, s.y0), y1 = max(y1, s.y1);
+        }
+    }
+    if (int64_t(pv.clip_state) + clip_delta > 0 || nok > uint32_t(kMaxOk)) {
+        // A clipped candidate keeps the CPU's partial-raster values.
+        r.flags |= kRecFallback | (int64_t(pv.clip_state) + clip_delta > 0 ? kRecClippedCand : 0);
+        record_write(out, r);
+        return;
     }
     for (int o = 16; o; o >>= 1) {
         x0 = min(x0, __shfl_xor_sync(0xffffffffu, x0, o));
@@ -170,18 +222,6 @@ __device__ void audit_view(const CandidateRecord& rec, const PlanDev& plan, uint
         y1 = max(y1, __shfl_xor_sync(0xffffffffu, y1, o));
     }
     __syncwarp();
-    ViewRecord r;
-    r.pad = 0;
-    r.flags = pv.clipped_ref ? kRecClippedRef : 0;
-    r.ca = pv.cov_ref > 0;
-    if (int64_t(pv.clip_state) + clip_delta > 0 || !plan.state_is_ref) {
-        // A clipped candidate keeps the CPU's partial-raster values; a state
-        // that differs from the reference needs the full distance field.
-        r.flags |= kRecFallback | (int64_t(pv.clip_state) + clip_delta > 0 ? kRecClippedCand : 0);
-        r.max_d2 = 0, r.changed = 0, r.total = 0, r.cb = 0;
-        if (lane == 0) out[v] = r;
-        return;
-    }
     int dchg = 0, dtot = 0, dcov = 0;
     uint32_t qn = 0;
     bool fallback = false;
@@ -189,6 +229,7 @@ __device__ void audit_view(const CandidateRecord& rec, const PlanDev& plan, uint
     cmask.state = pv.state_bits;
     cmask.region = ws.region;
     cmask.size = size;
+    uint64_t samples = 0;
     if (x1 >= 0) {
         const int wx0 = x0 & ~31;
         const int words = ((x1 - wx0) >> 5) + 1, rows = y1 - y0 + 1;
@@ -196,22 +237,30 @@ __device__ void audit_view(const CandidateRecord& rec, const PlanDev& plan, uint
         if (words > kRegionWords || rows > kRegionRows) {
             fallback = true;
         } else {
-            for (int y = y0; y <= y1; ++y)
+            samples = uint64_t(rows) * words * 32;
+            // Row span of the faces this lane owns in the compacted list.
+            const bool has0 = lane < nok, has1 = lane + 32 < nok;
+            const int r00 = has0 ? ws.faces[lane].y0 : 1, r01 = has0 ? ws.faces[lane].y1 : 0;
+            const int r10 = has1 ? ws.faces[lane + 32].y0 : 1, r11 = has1 ? ws.faces[lane + 32].y1 : 0;
+            for (int y = y0; y <= y1; ++y) {
+                const uint32_t row0 = __ballot_sync(0xffffffffu, y >= r00 && y <= r01);
+                const uint32_t row1 = __ballot_sync(0xffffffffu, y >= r10 && y <= r11);
+                const size_t row_base = size_t(y) * size;
                 for (int w = 0; w < words; ++w) {
                     const int x = wx0 + 32 * w + int(lane);
                     const bool inside = x < int(size);
                     int delta = 0;
                     if (inside) {
-                        for (uint32_t m = ok_old; m; m &= m - 1) {
+                        for (uint32_t m = row0; m; m &= m - 1) {
                             const FaceSetup& s = ws.faces[__ffs(m) - 1];
-                            if (x >= s.x0 && x <= s.x1 && y >= s.y0 && y <= s.y1 && face_covers(s, x, y)) --delta;
+                            if (x >= s.x0 && x <= s.x1 && face_covers(s, x, y)) delta += s.pad;
                         }
-                        for (uint32_t m = ok_new; m; m &= m - 1) {
+                        for (uint32_t m = row1; m; m &= m - 1) {
                             const FaceSetup& s = ws.faces[32 + __ffs(m) - 1];
-                            if (x >= s.x0 && x <= s.x1 && y >= s.y0 && y <= s.y1 && face_covers(s, x, y)) ++delta;
+                            if (x >= s.x0 && x <= s.x1 && face_covers(s, x, y)) delta += s.pad;
                         }
                     }
-                    const size_t i = size_t(y) * size + size_t(x);
+                    const size_t i = row_base + size_t(x);
                     const int pc = inside ? int(pv.state_count[i]) : 0;
                     const int cc = pc + delta;
                     const bool rbit = inside && ((pv.ref_bits[i >> 5] >> (i & 31)) & 1u);
@@ -219,26 +268,28 @@ __device__ void audit_view(const CandidateRecord& rec, const PlanDev& plan, uint
                     const uint32_t Pw = __ballot_sync(0xffffffffu, pc > 0);
                     const uint32_t Rw = __ballot_sync(0xffffffffu, rbit);
                     if (__ballot_sync(0xffffffffu, cc < 0)) fallback = true;
-                    dchg += __popc(Cw ^ Rw) - __popc(Pw ^ Rw);
-                    dtot += __popc(Cw | Rw) - __popc(Pw | Rw);
-                    dcov += __popc(Cw) - __popc(Pw);
+                    if (Cw != Pw) {
+                        dchg += __popc(Cw ^ Rw) - __popc(Pw ^ Rw);
+                        dtot += __popc(Cw | Rw) - __popc(Pw | Rw);
+                        dcov += __popc(Cw) - __popc(Pw);
+                    }
                     if (lane == 0) ws.region[(y - y0) * words + w] = Cw;
                     const uint32_t xm = Cw ^ Rw;
                     if (xm) {
-                        const uint32_t pos = qn + __popc(xm & ((1u << lane) - 1u));
+                        const uint32_t pos = qn + __popc(xm & below);
                         if (((xm >> lane) & 1u) && pos < kQueue)
                             ws.queue[pos] = uint32_t(x) | (uint32_t(y) << 15) | (uint32_t(cc > 0) << 30);
                         qn += __popc(xm);
                     }
                 }
-            if (qn > kQueue) fallback = true;
+            }
+            if (qn > uint32_t(kQueue)) fallback = true;
         }
     }
     __syncwarp();
     r.changed = uint32_t(int64_t(pv.changed) + dchg);
     r.total = uint32_t(int64_t(pv.total) + dtot);
-    const int64_t cov_c = int64_t(pv.cov_state) + dcov;
-    r.cb = cov_c > 0;
+    r.cb = int64_t(pv.cov_state) + dcov > 0;
     uint32_t best = 0;
     if (!fallback && r.changed && r.ca && r.cb) {
         RefMask rmask{pv.ref_bits, size};
@@ -259,9 +310,8 @@ __device__ void audit_view(const CandidateRecord& rec, const PlanDev& plan, uint
     if (fallback) r.flags |= kRecFallback;
     if (best >= kExactLimit) r.flags |= kRecLarge;
     if (lane == 0) {
-        out[v] = r;
+        *out = r;
         if (stats) {
-            const uint64_t samples = x1 >= 0 ? uint64_t(y1 - y0 + 1) * uint64_t((((x1 - (x0 & ~31)) >> 5) + 1) * 32) : 0;
             atomicAdd(stats, 1ull);
             atomicAdd(stats + 1, (unsigned long long)samples);
             atomicAdd(stats + 2, (unsigned long long)qn);
@@ -270,29 +320,29 @@ __device__ void audit_view(const CandidateRecord& rec, const PlanDev& plan, uint
     __syncwarp();
 }
 
-__global__ void __launch_bounds__(kAuditWarps * 32) k_audit(const CandidateRecord* recs, uint32_t n, PlanDev plan,
-                                                             ViewRecord* out, unsigned long long* stats) {
+// Persistent warps pull (candidate, view) units, candidate-major, from `queue`.
+__global__ void __launch_bounds__(kAuditWarps * 32, B200_AUDIT_MIN_BLOCKS) k_audit(const CandidateRecord* __restrict__ recs, uint32_t n,
+                                                             PlanDev plan, ViewRecord* out,
+                                                             unsigned long long* stats, uint32_t* queue) {
     extern __shared__ __align__(16) unsigned char smem[];
-    CandidateRecord& rec = *reinterpret_cast<CandidateRecord*>(smem);
-    WarpScratch* scratch = reinterpret_cast<WarpScratch*>(smem + ((sizeof(CandidateRecord) + 15) & ~size_t(15)));
-    const uint32_t warp = threadIdx.x >> 5;
-    for (uint32_t c = blockIdx.x; c < n; c += gridDim.x) {
-        const uint32_t* src = reinterpret_cast<const uint32_t*>(recs + c);
-        uint32_t* dst = reinterpret_cast<uint32_t*>(&rec);
-        for (uint32_t i = threadIdx.x; i < sizeof(CandidateRecord) / 4; i += blockDim.x) dst[i] = src[i];
-        __syncthreads();
-        ViewRecord* row = out + size_t(c) * plan.nviews;
-        if (!rec.valid || !rec.fast) {
-            for (uint32_t v = threadIdx.x; v < plan.nviews; v += blockDim.x) {
-                ViewRecord r{};
-                r.flags = rec.valid ? kRecFallback : 0;
-                row[v] = r;
-            }
-        } else {
-            for (uint32_t v = warp; v < plan.nviews; v += kAuditWarps)
-                audit_view(rec, plan, v, scratch[warp], row, stats);
+    WarpScratch& ws = reinterpret_cast<WarpScratch*>(smem)[threadIdx.x >> 5];
+    const uint32_t lane = lane_id();
+    const uint64_t total = uint64_t(n) * plan.nviews;
+    for (;;) {
+        uint32_t u = 0;
+        if (lane == 0) u = atomicAdd(queue, 1u);
+        u = __shfl_sync(0xffffffffu, u, 0);
+        if (u >= total) break;
+        const uint32_t c = u / plan.nviews, v = u - c * plan.nviews;
+        const CandidateRecord* rec = recs + c;
+        ViewRecord* slot = out + u;
+        if (!rec->valid || !rec->fast) {
+            ViewRecord r{};
+            r.flags = rec->valid ? kRecFallback : 0;
+            record_write(slot, r);
+            continue;
         }
-        __syncthreads();
+        audit_unit(rec, plan, v, ws, slot, stats);
     }
 }
 
@@ -358,28 +408,28 @@ __global__ void k_verdicts(const ViewRecord* const* plan_records, const uint32_t
 }
 } // namespace
 
-size_t audit_smem_bytes() {
-    return ((sizeof(CandidateRecord) + 15) & ~size_t(15)) + kAuditWarps * sizeof(WarpScratch);
-}
+size_t audit_smem_bytes() { return kAuditWarps * sizeof(WarpScratch); }
 
 void launch_audit(const CandidateRecord* records, uint32_t n, const PlanDev& plan, ViewRecord* out,
-                  unsigned long long* stats, cudaStream_t s) {
+                  unsigned long long* stats, uint32_t* queue, cudaStream_t s) {
     if (!n) return;
-    static bool configured = false;
-    size_t smem = audit_smem_bytes();
-    if (!configured) {
+    static int configured_smem = 0;
+    const size_t smem = audit_smem_bytes();
+    if (configured_smem != int(smem)) {
         cudaFuncSetAttribute(k_audit, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-        configured = true;
+        configured_smem = int(smem);
     }
-    int sms = 148;
-    int dev = 0;
+    int sms = 148, dev = 0;
     if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     int per_sm = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_audit, kAuditWarps * 32, smem);
     if (per_sm < 1) per_sm = 1;
-    uint32_t grid = uint32_t(sms * per_sm);
-    if (grid > n) grid = n;
-    k_audit<<<grid, kAuditWarps * 32, smem, s>>>(records, n, plan, out, stats);
+    uint64_t units = uint64_t(n) * plan.nviews;
+    uint64_t grid = uint64_t(sms) * per_sm;
+    uint64_t needed = (units + kAuditWarps - 1) / kAuditWarps;
+    if (grid > needed) grid = needed;
+    cudaMemsetAsync(queue, 0, 4, s);
+    k_audit<<<uint32_t(grid), kAuditWarps * 32, smem, s>>>(records, n, plan, out, stats, queue);
 }
 
 void launch_verdicts(const ViewRecord* const* plan_records, const uint32_t* plan_views, const uint32_t* plan_ss,

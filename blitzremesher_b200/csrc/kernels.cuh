@@ -37,26 +37,28 @@ struct Edit {
 };
 
 constexpr int kMaxAffected = 32; // faces in faces(from) U faces(to) handled on the fast path
+constexpr int kMaxLocal = 31;    // distinct vertex slots of those faces; local index 31 = placement
+constexpr uint8_t kPlacementLocal = 31;
 
-// A candidate's affected faces: old corner positions, which corners move to the
-// placement, whether the face survives, and the face's two-sided flag.
-struct AffectedFace {
-    float p[9];     // old corner positions
-    uint8_t moved;  // bit j: corner j lands on the placement
-    uint8_t kept;   // survives the collapse
-    uint8_t two;    // two-sided material
-    uint8_t pad;
-};
+// A candidate's neighbourhood: the distinct vertex slots of faces(from) U
+// faces(to) with their current positions, each affected face as local corner
+// indices before and after the collapse (moved corners point at the
+// placement), whether it survives and whether its material is two-sided.
 struct CandidateRecord {
     float placement[3];
-    uint32_t count;   // affected faces (<= kMaxAffected when fast)
-    uint8_t valid;    // legal + placement valid
-    uint8_t fast;     // handled by the incremental path
-    uint8_t removed;  // faces removed
-    uint8_t failed;   // 5 illegal, 6 invalid placement
     uint32_t from, to;
-    AffectedFace faces[kMaxAffected];
+    uint8_t nverts, nfaces; // local vertices, affected faces
+    uint8_t valid;          // legal + placement valid
+    uint8_t fast;           // handled by the incremental path
+    uint8_t removed;        // faces removed
+    uint8_t failed;         // 5 illegal, 6 invalid placement
+    uint8_t pad[2];
+    float verts[kMaxLocal * 3];
+    uint8_t old_face[kMaxAffected * 3];
+    uint8_t new_face[kMaxAffected * 3];
+    uint8_t flags[kMaxAffected]; // bit0 kept, bit1 two-sided
 };
+constexpr uint8_t kFaceKept = 1, kFaceTwo = 2;
 
 // One audit plan: a reference, a camera set, a screen size and a sampling.
 struct PlanView {
@@ -105,7 +107,7 @@ void launch_distance(const uint32_t* from, const uint32_t* to, uint32_t size, ui
                      int32_t* stack_v, long long* stack_num, long long* stack_den, uint32_t* out_max,
                      cudaStream_t s);
 void launch_audit(const CandidateRecord* records, uint32_t n, const PlanDev& plan, ViewRecord* out,
-                  unsigned long long* stats, cudaStream_t s);
+                  unsigned long long* stats, uint32_t* queue, cudaStream_t s);
 struct GateDev {
     GateSettings settings;
     uint32_t plan;
