@@ -125,6 +125,8 @@ EXPORTS = {
     "blitz_audit_candidates_device": ([C.c_void_p, C.c_void_p, C.c_size_t, C.POINTER(EvalSettings), C.c_void_p,
                                        C.c_void_p, C.c_void_p, C.c_char_p, C.c_size_t], C.c_int),
     "blitz_audit_session_info": ([C.c_void_p, C.POINTER(NeuralInfo)], C.c_int),
+    "blitz_audit_coverage_distance": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint8,
+                                       C.c_int, C.POINTER(C.c_double), C.c_char_p, C.c_size_t], C.c_int),
     "blitz_audit_profile_enable": ([C.c_void_p, C.c_int], C.c_int),
     "blitz_audit_profile_read": ([C.c_void_p, C.c_void_p], C.c_int),
 }
@@ -270,6 +272,16 @@ class AuditSession:
                                            words.ctypes.data, words.size, C.byref(out_size), C.byref(clipped),
                                            err, 512), err)
         return words, bool(clipped.value), int(out_size.value)
+
+    def coverage_distance(self, a, b, width: int, height: int, supersample: int) -> float:
+        """Coverage distance of two packed host masks (u64 words)."""
+        a = np.ascontiguousarray(a, dtype=np.uint64)
+        b = np.ascontiguousarray(b, dtype=np.uint64)
+        out = C.c_double()
+        err = C.create_string_buffer(512)
+        _check(self.lib.blitz_audit_coverage_distance(self.handle, a.ctypes.data, b.ctypes.data, width, height,
+                                                      supersample, 0, C.byref(out), err, 512), err)
+        return out.value
 
     def actions(self) -> np.ndarray:
         count = C.c_size_t()

@@ -103,8 +103,8 @@ void launch_raster(const DevMesh& m, const Camera* cam_host, const float* center
                    cudaStream_t s);
 void launch_popcounts(const uint32_t* a, const uint32_t* b, uint32_t words, unsigned long long* out,
                       cudaStream_t s);
-void launch_distance(const uint32_t* from, const uint32_t* to, uint32_t size, uint32_t* g, uint32_t* d2,
-                     int32_t* stack_v, long long* stack_num, long long* stack_den, uint32_t* out_max,
+void launch_distance(const uint32_t* from, const uint32_t* to, uint32_t width, uint32_t height, uint32_t* g,
+                     uint32_t* d2, int32_t* stack_v, long long* stack_num, long long* stack_den, uint32_t* out_max,
                      cudaStream_t s);
 void launch_audit(const CandidateRecord* records, uint32_t n, const PlanDev& plan, ViewRecord* out,
                   unsigned long long* stats, uint32_t* queue, cudaStream_t s);

@@ -102,17 +102,17 @@ __global__ void k_popcounts(const uint32_t* a, const uint32_t* b, uint32_t words
 __device__ __forceinline__ bool bit_at(const uint32_t* bits, size_t i) { return (bits[i >> 5] >> (i & 31)) & 1u; }
 
 // Horizontal distance to the nearest covered sample of each row (INF if none).
-__global__ void k_row_nearest(const uint32_t* to, uint32_t size, uint32_t* g) {
+__global__ void k_row_nearest(const uint32_t* to, uint32_t width, uint32_t height, uint32_t* g) {
     uint32_t y = blockIdx.x * blockDim.x + threadIdx.x;
-    if (y >= size) return;
-    size_t row = size_t(y) * size;
+    if (y >= height) return;
+    size_t row = size_t(y) * width;
     uint32_t last = kNone;
-    for (uint32_t x = 0; x < size; ++x) {
+    for (uint32_t x = 0; x < width; ++x) {
         if (bit_at(to, row + x)) last = x;
         g[row + x] = last == kNone ? kNone : x - last;
     }
     last = kNone;
-    for (uint32_t x = size; x-- > 0;) {
+    for (uint32_t x = width; x-- > 0;) {
         if (bit_at(to, row + x)) last = x;
         if (last != kNone && last - x < g[row + x]) g[row + x] = last - x;
     }
@@ -121,15 +121,16 @@ __global__ void k_row_nearest(const uint32_t* to, uint32_t size, uint32_t* g) {
 // Lower envelope of the parabolas (y-q)^2 + g(x,q)^2 over rows q with a site
 // (Felzenszwalb–Huttenlocher), in exact integer arithmetic: intersections are
 // kept as fractions and compared by cross-multiplication.
-__global__ void k_column_envelope(const uint32_t* g, uint32_t size, uint32_t* d2, int32_t* sv, long long* snum,
-                                  long long* sden) {
+__global__ void k_column_envelope(const uint32_t* g, uint32_t width, uint32_t height, uint32_t* d2, int32_t* sv,
+                                  long long* snum, long long* sden) {
     uint32_t x = blockIdx.x * blockDim.x + threadIdx.x;
-    if (x >= size) return;
-    int32_t* v = sv + size_t(x) * size;
-    long long* zn = snum + size_t(x) * size;
-    long long* zd = sden + size_t(x) * size;
+    if (x >= width) return;
+    const uint32_t size = width; // row stride of g and d2
+    int32_t* v = sv + size_t(x) * height;
+    long long* zn = snum + size_t(x) * height;
+    long long* zd = sden + size_t(x) * height;
     int k = -1;
-    for (uint32_t q = 0; q < size; ++q) {
+    for (uint32_t q = 0; q < height; ++q) {
         uint32_t gq = g[size_t(q) * size + x];
         if (gq == kNone) continue;
         long long fq = (long long)gq * gq + (long long)q * q;
@@ -155,12 +156,12 @@ __global__ void k_column_envelope(const uint32_t* g, uint32_t size, uint32_t* d2
         zd[k] = den;
     }
     if (k < 0) {
-        for (uint32_t y = 0; y < size; ++y) d2[size_t(y) * size + x] = kNone;
+        for (uint32_t y = 0; y < height; ++y) d2[size_t(y) * size + x] = kNone;
         return;
     }
     int top = k;
     k = 0;
-    for (uint32_t y = 0; y < size; ++y) {
+    for (uint32_t y = 0; y < height; ++y) {
         while (k < top && zn[k + 1] < (long long)y * zd[k + 1]) ++k;
         long long dy = (long long)y - v[k];
         uint32_t gq = g[size_t(v[k]) * size + x];
@@ -170,10 +171,10 @@ __global__ void k_column_envelope(const uint32_t* g, uint32_t size, uint32_t* d2
 
 // CPU float value of the field where the exact distance reaches 2^24: the
 // row pass rounds g^2 to float, the column pass rounds (dy^2 + f) to float.
-__device__ float cpu_field_value(const uint32_t* g, uint32_t size, uint32_t x, uint32_t y) {
+__device__ float cpu_field_value(const uint32_t* g, uint32_t width, uint32_t height, uint32_t x, uint32_t y) {
     float best = INFINITY;
-    for (uint32_t q = 0; q < size; ++q) {
-        uint32_t gq = g[size_t(q) * size + x];
+    for (uint32_t q = 0; q < height; ++q) {
+        uint32_t gq = g[size_t(q) * width + x];
         if (gq == kNone) continue;
         float f = __uint2float_rn(gq * gq);
         double dy = double(y) - double(q);
@@ -186,13 +187,14 @@ __device__ float cpu_field_value(const uint32_t* g, uint32_t size, uint32_t x, u
 // Max over samples covered by `from` and not by `to` of the field of `to`, as
 // float bit patterns (non-negative floats order like their bits).
 __global__ void k_directed_max(const uint32_t* from, const uint32_t* to, const uint32_t* d2, const uint32_t* g,
-                               uint32_t size, uint32_t* out) {
-    size_t n = size_t(size) * size;
+                               uint32_t width, uint32_t height, uint32_t* out) {
+    size_t n = size_t(width) * height;
     uint32_t best = 0;
     for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x) {
         if (!bit_at(from, i) || bit_at(to, i)) continue;
         uint32_t d = d2[i];
-        float val = d < kExactLimit ? float(d) : cpu_field_value(g, size, uint32_t(i % size), uint32_t(i / size));
+        float val = d < kExactLimit ? float(d)
+                                    : cpu_field_value(g, width, height, uint32_t(i % width), uint32_t(i / width));
         uint32_t b = __float_as_uint(val);
         best = b > best ? b : best;
     }
@@ -228,15 +230,15 @@ void launch_popcounts(const uint32_t* a, const uint32_t* b, uint32_t words, unsi
 }
 
 // Field of `to`, max over from \ to (as float bits) into out_max.
-void launch_distance(const uint32_t* from, const uint32_t* to, uint32_t size, uint32_t* g, uint32_t* d2,
-                     int32_t* stack_v, long long* stack_num, long long* stack_den, uint32_t* out_max,
+void launch_distance(const uint32_t* from, const uint32_t* to, uint32_t width, uint32_t height, uint32_t* g,
+                     uint32_t* d2, int32_t* stack_v, long long* stack_num, long long* stack_den, uint32_t* out_max,
                      cudaStream_t s) {
-    k_row_nearest<<<blocks_for(size, 64), 64, 0, s>>>(to, size, g);
-    k_column_envelope<<<blocks_for(size, 64), 64, 0, s>>>(g, size, d2, stack_v, stack_num, stack_den);
-    size_t n = size_t(size) * size;
+    k_row_nearest<<<blocks_for(height, 64), 64, 0, s>>>(to, width, height, g);
+    k_column_envelope<<<blocks_for(width, 64), 64, 0, s>>>(g, width, height, d2, stack_v, stack_num, stack_den);
+    size_t n = size_t(width) * height;
     uint32_t grid = uint32_t((n + kThreads - 1) / kThreads);
     if (grid > 148 * 16) grid = 148 * 16;
-    k_directed_max<<<grid, kThreads, 0, s>>>(from, to, d2, g, size, out_max);
+    k_directed_max<<<grid, kThreads, 0, s>>>(from, to, d2, g, width, height, out_max);
 }
 
 } // namespace b200

@@ -316,7 +316,7 @@ struct Scratch {
     Buf<int32_t> sv;
     Buf<long long> sn, sd;
     Buf<unsigned long long> pop;
-    uint32_t size = 0;
+    size_t samples = 0;
 };
 
 struct Session {
@@ -512,11 +512,13 @@ static Plan& plan_for(Session& S, const PlanKey& key) {
     return *(S.plans[key] = std::move(plan));
 }
 
-static void ensure_scratch(Session& S, uint32_t size) {
+static uint32_t mask_words_for(size_t samples) { return uint32_t(((samples + 63) / 64) * 2 + 2); }
+
+// Full-path scratch for rasters of up to `samples` samples (any width x height).
+static void ensure_scratch_samples(Session& S, size_t samples) {
     Scratch& x = S.scratch;
-    if (x.size >= size && x.a.p) return;
-    size_t samples = size_t(size) * size;
-    uint32_t words = mask_words(size);
+    if (x.samples >= samples && x.a.p) return;
+    uint32_t words = mask_words_for(samples);
     x.a = Buf<uint32_t>(S.pool, words);
     x.c = Buf<uint32_t>(S.pool, words);
     x.g = Buf<uint32_t>(S.pool, samples);
@@ -527,7 +529,37 @@ static void ensure_scratch(Session& S, uint32_t size) {
     x.maxes = Buf<uint32_t>(S.pool, 2);
     x.state = Buf<uint32_t>(S.pool, 8);
     x.pop = Buf<unsigned long long>(S.pool, 4);
-    x.size = size;
+    x.samples = samples;
+}
+static void ensure_scratch(Session& S, uint32_t size) { ensure_scratch_samples(S, size_t(size) * size); }
+
+// Coverage distance of two device masks already in scratch a/c (evaluate.cpp:196-209):
+// fills rec (changed, total, ca, cb) and the max squared distance.
+static void mask_distance(Session& S, uint32_t width, uint32_t height, ViewRecord& rec, double& max_d2) {
+    Scratch& x = S.scratch;
+    cudaStream_t st = S.stream;
+    uint32_t words = mask_words_for(size_t(width) * height);
+    launch_popcounts(x.a.p, x.c.p, words, x.pop.p, st);
+    unsigned long long pop[4];
+    B200_CUDA(cudaMemcpyAsync(pop, x.pop.p, sizeof(pop), cudaMemcpyDeviceToHost, st));
+    B200_CUDA(cudaStreamSynchronize(st));
+    rec.changed = uint32_t(pop[0]);
+    rec.total = uint32_t(pop[1]);
+    rec.ca = pop[2] > 0;
+    rec.cb = pop[3] > 0;
+    max_d2 = 0;
+    if (rec.changed && rec.ca && rec.cb) {
+        B200_CUDA(cudaMemsetAsync(x.maxes.p, 0, 8, st));
+        launch_distance(x.a.p, x.c.p, width, height, x.g.p, x.d2.p, x.sv.p, x.sn.p, x.sd.p, x.maxes.p, st);
+        launch_distance(x.c.p, x.a.p, width, height, x.g.p, x.d2.p, x.sv.p, x.sn.p, x.sd.p, x.maxes.p + 1, st);
+        uint32_t m[2];
+        B200_CUDA(cudaMemcpyAsync(m, x.maxes.p, 8, cudaMemcpyDeviceToHost, st));
+        B200_CUDA(cudaStreamSynchronize(st));
+        float fa, fc;
+        std::memcpy(&fa, &m[0], 4);
+        std::memcpy(&fc, &m[1], 4);
+        max_d2 = std::max(double(fa), double(fc));
+    }
 }
 
 // One view at one sampling through the full-raster path.
@@ -541,31 +573,11 @@ static void full_view(Session& S, const DevMesh& ref, const DevMesh& cand, const
     B200_CUDA(cudaMemsetAsync(x.c.p, 0, size_t(words) * 4, st));
     raster(S, ref, cam_host, ss, size, force_two, true, x.a.p, nullptr, x.state.p);
     raster(S, cand, cam_host, ss, size, force_two, true, x.c.p, nullptr, x.state.p + 4);
-    launch_popcounts(x.a.p, x.c.p, words, x.pop.p, st);
-    unsigned long long pop[4];
     uint32_t state[8];
-    B200_CUDA(cudaMemcpyAsync(pop, x.pop.p, sizeof(pop), cudaMemcpyDeviceToHost, st));
     B200_CUDA(cudaMemcpyAsync(state, x.state.p, sizeof(state), cudaMemcpyDeviceToHost, st));
-    B200_CUDA(cudaStreamSynchronize(st));
     rec = ViewRecord{};
-    rec.changed = uint32_t(pop[0]);
-    rec.total = uint32_t(pop[1]);
-    rec.ca = pop[2] > 0;
-    rec.cb = pop[3] > 0;
+    mask_distance(S, size, size, rec, max_d2);
     rec.flags = (state[1] ? kRecClippedRef : 0) | (state[5] ? kRecClippedCand : 0);
-    max_d2 = 0;
-    if (rec.changed && rec.ca && rec.cb) {
-        B200_CUDA(cudaMemsetAsync(x.maxes.p, 0, 8, st));
-        launch_distance(x.a.p, x.c.p, size, x.g.p, x.d2.p, x.sv.p, x.sn.p, x.sd.p, x.maxes.p, st);
-        launch_distance(x.c.p, x.a.p, size, x.g.p, x.d2.p, x.sv.p, x.sn.p, x.sd.p, x.maxes.p + 1, st);
-        uint32_t m[2];
-        B200_CUDA(cudaMemcpyAsync(m, x.maxes.p, 8, cudaMemcpyDeviceToHost, st));
-        B200_CUDA(cudaStreamSynchronize(st));
-        float fa, fc;
-        std::memcpy(&fa, &m[0], 4);
-        std::memcpy(&fc, &m[1], 4);
-        max_d2 = std::max(double(fa), double(fc));
-    }
 }
 
 // evaluate_impl (evaluate.cpp:312-352) over the full-raster path, starting at
@@ -982,6 +994,31 @@ blitz_status blitz_audit_raster(blitz_audit_session* s, const blitz_mesh* mesh, 
         B200_CUDA(cudaStreamSynchronize(S.stream));
         *size_out = size;
         *clipped = st[1] != 0;
+    });
+}
+
+blitz_status blitz_audit_coverage_distance(blitz_audit_session* s, const uint64_t* a, const uint64_t* b,
+                                           uint32_t width, uint32_t height, uint8_t ss, int masks_on_device,
+                                           double* out, char* error, size_t cap) {
+    return guarded(error, cap, [&] {
+        if (!s || !a || !b || !out) throw Failure(BLITZ_INVALID_ARGUMENT, "null argument");
+        if (!width || !height || !ss) throw Failure(BLITZ_INVALID_ARGUMENT, "raster shapes differ");
+        const size_t samples = size_t(width) * height;
+        if (samples > kMaxSamples) throw Failure(BLITZ_BUDGET_LIMITED, "raster exceeds per-view memory budget");
+        Session& S = s->s;
+        DeviceScope scope(S.device);
+        ensure_scratch_samples(S, samples);
+        Scratch& x = S.scratch;
+        const size_t n = (samples + 63) / 64;
+        const cudaMemcpyKind kind = masks_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+        B200_CUDA(cudaMemsetAsync(x.a.p, 0, size_t(mask_words_for(samples)) * 4, S.stream));
+        B200_CUDA(cudaMemsetAsync(x.c.p, 0, size_t(mask_words_for(samples)) * 4, S.stream));
+        B200_CUDA(cudaMemcpyAsync(x.a.p, a, n * 8, kind, S.stream));
+        B200_CUDA(cudaMemcpyAsync(x.c.p, b, n * 8, kind, S.stream));
+        ViewRecord rec{};
+        double max_d2 = 0;
+        mask_distance(S, width, height, rec, max_d2);
+        *out = coverage_value(rec, ss, max_d2);
     });
 }
 

@@ -158,6 +158,16 @@ blitz_status blitz_audit_raster(blitz_audit_session*, const blitz_mesh* mesh, do
                                 uint32_t view, uint8_t force_two_sided, uint64_t* words, size_t word_capacity,
                                 uint32_t* size, uint8_t* clipped, char* error, size_t error_capacity);
 
+/* Symmetric coverage distance in pixels between two packed masks of
+ * width x height samples (the layout of blitz_audit_raster): 0 when the masks
+ * are equal, infinity when exactly one is empty, else sqrt(max squared
+ * distance)/supersample. The twin of blitz::detail::coverage_distance
+ * (coverage.hpp:13, evaluate.cpp:196-216). `masks_on_device` selects device
+ * or host pointers for a and b. */
+blitz_status blitz_audit_coverage_distance(blitz_audit_session*, const uint64_t* a, const uint64_t* b,
+                                           uint32_t width, uint32_t height, uint8_t supersample,
+                                           int masks_on_device, double* out, char* error, size_t error_capacity);
+
 /* Legal directed collapses of the current state, in the reference's
  * enumeration order (action_gpu.cu:626-643 enumerate + DeviceSelect::Flagged).
  * Writes min(count, capacity) collapses with midpoint placement; *count

@@ -45,6 +45,41 @@ def test_raster_masks_match_oracle_icosphere(gpu_lib, oracle):
                     assert np.array_equal(w, wo) and cl == clo, (v, ss, two)
 
 
+def test_coverage_distance_matches_golden(gpu_lib):
+    """The 40 random 13x11 mask pairs of the reference precision test."""
+    g = np.load(GOLDEN / "precision_distance.npz")
+    with br.AuditSession(syn.noisy_icosphere(1, 1)) as s:
+        for t in range(g["a"].shape[0]):
+            for k, ss in enumerate(g["ss"]):
+                assert s.coverage_distance(g["a"][t], g["b"][t], 13, 11, int(ss)) == g["expected"][t, k], (t, ss)
+        empty, one = np.zeros(1, np.uint64), np.ones(1, np.uint64)
+        assert s.coverage_distance(empty, empty, 1, 1, 1) == 0
+        assert np.isinf(s.coverage_distance(empty, one, 1, 1, 1))
+
+
+def _blob_mask(rng, width, height, blobs):
+    yy, xx = np.mgrid[0:height, 0:width]
+    m = np.zeros((height, width), bool)
+    for _ in range(blobs):
+        cx, cy, r = rng.uniform(0, width), rng.uniform(0, height), rng.uniform(2, width / 6)
+        m |= (xx - cx) ** 2 + (yy - cy) ** 2 < r * r
+    bits = np.packbits(m.reshape(-1), bitorder="little")
+    bits = np.concatenate([bits, np.zeros((-bits.size) % 8, np.uint8)])
+    return bits.view(np.uint64)
+
+
+def test_coverage_distance_matches_oracle_random(gpu_lib, oracle):
+    rng = np.random.default_rng(11)
+    with br.AuditSession(syn.noisy_icosphere(1, 1)) as s:
+        for width, height in ((257, 190), (64, 64), (1000, 37), (129, 600)):
+            for trial in range(3):
+                a = _blob_mask(rng, width, height, 3)
+                b = _blob_mask(rng, width, height, 2 + trial)
+                for ss in (1, 3):
+                    want = oracle.coverage_distance(a, b, width, height, ss)
+                    assert s.coverage_distance(a, b, width, height, ss) == want, (width, height, trial, ss)
+
+
 def test_evaluate_matches_golden(gpu_lib):
     g = np.load(GOLDEN / "evaluate_cases.npz")
     sessions = {}
