@@ -168,6 +168,26 @@ blitz_status blitz_audit_coverage_distance(blitz_audit_session*, const uint64_t*
                                            uint32_t width, uint32_t height, uint8_t supersample,
                                            int masks_on_device, double* out, char* error, size_t error_capacity);
 
+/* The same coverage distance computed without allocating anything. This entry
+ * point has no counterpart in the reference. It exists for callers that may
+ * not call cudaMalloc: plugins whose host process gives all device memory to
+ * another allocator (a framework's caching allocator, an engine that hands
+ * out fixed budgets), or loops that must avoid the synchronisation that
+ * cudaMalloc/cudaFree can imply. Its scratch is one static device array of
+ * about 7 MiB, held by every GPU that loads the library until the process
+ * exits; masks are limited to 512 x 512 = 262144 samples (larger masks return
+ * BLITZ_INVALID_ARGUMENT). Inputs are device masks (layout of
+ * blitz_audit_raster, no padding needed) and the result is written to the
+ * device double `out_device`, all enqueued on `stream` (a cudaStream_t, NULL =
+ * default stream) on the current device; the call does not synchronise. The
+ * first call on a device looks up the array's device address (once per
+ * device); make that first call before any stream capture. All calls share
+ * the one array, so calls that overlap on the GPU race: serialise them. */
+blitz_status blitz_audit_coverage_distance_static(const uint64_t* a_device, const uint64_t* b_device,
+                                                  uint32_t width, uint32_t height, uint8_t supersample,
+                                                  double* out_device, void* stream, char* error,
+                                                  size_t error_capacity);
+
 /* Legal directed collapses of the current state, in the reference's
  * enumeration order (action_gpu.cu:626-643 enumerate + DeviceSelect::Flagged).
  * Writes min(count, capacity) collapses with midpoint placement; *count
