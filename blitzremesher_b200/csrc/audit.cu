@@ -19,15 +19,18 @@ constexpr int kAuditWarps = 8;
 #ifndef B200_AUDIT_MIN_BLOCKS
 #define B200_AUDIT_MIN_BLOCKS 3 // resident blocks per SM the register budget targets
 #endif
-constexpr int kRegionWords = 4;  // region width <= 128 samples after 32-alignment
-constexpr int kRegionRows = 128; // region height
-constexpr int kQueue = 256;      // changed samples per (candidate, view)
-constexpr int kMaxOk = 48;       // rasterized (uncluded, unclipped) old + new faces
+constexpr int kRegionWords = 4;     // region width <= 128 samples after 32-alignment
+constexpr int kRegionRows = 64;     // region height
+constexpr int kDeltaSamples = 2048; // region samples (unaligned bbox) with a count delta
+constexpr int kQueue = 160;         // changed samples per (candidate, view)
+constexpr int kMaxOk = 48;          // rasterized (unculled, unclipped) old + new faces
 
 struct WarpScratch {
     double vx[32], vy[32], vz[32]; // projected local vertices; 31 = placement
     FaceSetup faces[kMaxOk];       // old faces carry pad = -1, new faces pad = +1
+    uint32_t work[kMaxOk];         // exclusive prefix of bbox samples per face
     uint32_t region[kRegionRows * kRegionWords];
+    uint32_t delta[kDeltaSamples / 4]; // per-sample count delta + 128, one byte each
     uint32_t queue[kQueue];
 };
 
@@ -123,6 +126,8 @@ template <class M> __device__ uint32_t nearest_d2(const M& mask, uint32_t x, uin
     }
     return best;
 }
+
+__device__ __forceinline__ bool pv_ref_bit(const uint32_t* bits, size_t i) { return (bits[i >> 5] >> (i & 31)) & 1u; }
 
 __device__ __forceinline__ void record_write(ViewRecord* out, const ViewRecord& r) {
     if (lane_id() == 0) *out = r;
@@ -234,53 +239,92 @@ __device__ void audit_unit(const CandidateRecord* __restrict__ rec, const PlanDe
         const int wx0 = x0 & ~31;
         const int words = ((x1 - wx0) >> 5) + 1, rows = y1 - y0 + 1;
         cmask.y0 = uint32_t(y0), cmask.y1 = uint32_t(y1), cmask.c0 = uint32_t(wx0 >> 5), cmask.words = uint32_t(words);
-        if (words > kRegionWords || rows > kRegionRows) {
+        const int bw = x1 - x0 + 1;
+        if (words > kRegionWords || rows > kRegionRows || bw * rows > kDeltaSamples) {
             fallback = true;
         } else {
             samples = uint64_t(rows) * words * 32;
-            // Row span of the faces this lane owns in the compacted list.
-            const bool has0 = lane < nok, has1 = lane + 32 < nok;
-            const int r00 = has0 ? ws.faces[lane].y0 : 1, r01 = has0 ? ws.faces[lane].y1 : 0;
-            const int r10 = has1 ? ws.faces[lane + 32].y0 : 1, r11 = has1 ? ws.faces[lane + 32].y1 : 0;
-            for (int y = y0; y <= y1; ++y) {
-                const uint32_t row0 = __ballot_sync(0xffffffffu, y >= r00 && y <= r01);
-                const uint32_t row1 = __ballot_sync(0xffffffffu, y >= r10 && y <= r11);
-                const size_t row_base = size_t(y) * size;
-                for (int w = 0; w < words; ++w) {
-                    const int x = wx0 + 32 * w + int(lane);
-                    const bool inside = x < int(size);
-                    int delta = 0;
-                    if (inside) {
-                        for (uint32_t m = row0; m; m &= m - 1) {
-                            const FaceSetup& s = ws.faces[__ffs(m) - 1];
-                            if (x >= s.x0 && x <= s.x1 && face_covers(s, x, y)) delta += s.pad;
-                        }
-                        for (uint32_t m = row1; m; m &= m - 1) {
-                            const FaceSetup& s = ws.faces[32 + __ffs(m) - 1];
-                            if (x >= s.x0 && x <= s.x1 && face_covers(s, x, y)) delta += s.pad;
-                        }
-                    }
-                    const size_t i = row_base + size_t(x);
-                    const int pc = inside ? int(pv.state_count[i]) : 0;
-                    const int cc = pc + delta;
-                    const bool rbit = inside && ((pv.ref_bits[i >> 5] >> (i & 31)) & 1u);
-                    const uint32_t Cw = __ballot_sync(0xffffffffu, cc > 0);
-                    const uint32_t Pw = __ballot_sync(0xffffffffu, pc > 0);
-                    const uint32_t Rw = __ballot_sync(0xffffffffu, rbit);
-                    if (__ballot_sync(0xffffffffu, cc < 0)) fallback = true;
-                    if (Cw != Pw) {
-                        dchg += __popc(Cw ^ Rw) - __popc(Pw ^ Rw);
-                        dtot += __popc(Cw | Rw) - __popc(Pw | Rw);
-                        dcov += __popc(Cw) - __popc(Pw);
-                    }
-                    if (lane == 0) ws.region[(y - y0) * words + w] = Cw;
-                    const uint32_t xm = Cw ^ Rw;
-                    if (xm) {
-                        const uint32_t pos = qn + __popc(xm & below);
-                        if (((xm >> lane) & 1u) && pos < kQueue)
-                            ws.queue[pos] = uint32_t(x) | (uint32_t(y) << 15) | (uint32_t(cc > 0) << 30);
-                        qn += __popc(xm);
-                    }
+            // Phase 1: every (face, sample in its bbox) test is an independent
+            // work item spread over the lanes; covered samples add the face's
+            // sign to a per-sample byte (biased by 128, so at most 32 old and
+            // 32 new faces never carry across bytes).
+            const uint32_t delta_words = uint32_t(bw * rows + 3) >> 2;
+            for (uint32_t k = lane; k < delta_words; k += 32) ws.delta[k] = 0x80808080u;
+            uint32_t c0 = 0, c1 = 0;
+            if (lane < nok) {
+                const FaceSetup& s = ws.faces[lane];
+                c0 = uint32_t(s.x1 - s.x0 + 1) * uint32_t(s.y1 - s.y0 + 1);
+            }
+            if (lane + 32 < nok) {
+                const FaceSetup& s = ws.faces[lane + 32];
+                c1 = uint32_t(s.x1 - s.x0 + 1) * uint32_t(s.y1 - s.y0 + 1);
+            }
+            uint32_t i0 = c0, i1 = c1;
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t a = __shfl_up_sync(0xffffffffu, i0, o), b = __shfl_up_sync(0xffffffffu, i1, o);
+                if (lane >= uint32_t(o)) i0 += a, i1 += b;
+            }
+            const uint32_t tot0 = __shfl_sync(0xffffffffu, i0, 31);
+            if (lane < nok) ws.work[lane] = i0 - c0;
+            if (lane + 32 < nok) ws.work[lane + 32] = tot0 + i1 - c1;
+            const uint32_t tests = tot0 + __shfl_sync(0xffffffffu, i1, 31);
+            __syncwarp();
+            for (uint32_t t = lane; t < tests; t += 32) {
+                uint32_t f = 0; // last face whose prefix is <= t
+                for (uint32_t step = 32; step; step >>= 1)
+                    if (f + step < nok && ws.work[f + step] <= t) f += step;
+                const FaceSetup& s = ws.faces[f];
+                const uint32_t fw = uint32_t(s.x1 - s.x0 + 1), r = t - ws.work[f];
+                const int fy = s.y0 + int(r / fw), fx = s.x0 + int(r % fw);
+                if (face_covers(s, fx, fy)) {
+                    const uint32_t d = uint32_t(fy - y0) * uint32_t(bw) + uint32_t(fx - x0);
+                    const uint32_t unit = 1u << (8 * (d & 3));
+                    if (s.pad > 0) atomicAdd(&ws.delta[d >> 2], unit);
+                    else atomicSub(&ws.delta[d >> 2], unit);
+                }
+            }
+            __syncwarp();
+            // Phase 2: coverage words row by row; loads for step t+1 are issued
+            // before step t is consumed.
+            const int steps = rows * words;
+            const bool same_ref = plan.state_is_ref != 0; // state words equal reference words
+            int y = y0, w = 0;
+            int x = wx0 + int(lane);
+            int pc_next = x < int(size) ? int(pv.state_count[size_t(y) * size + size_t(x)]) : 0;
+            bool r_next = !same_ref && x < int(size) && pv_ref_bit(pv.ref_bits, size_t(y) * size + size_t(x));
+            for (int t = 0; t < steps; ++t) {
+                const int pc = pc_next;
+                const bool rbit_own = r_next;
+                const int cx = x, cy = y, cw = w;
+                if (++w == words) w = 0, ++y;
+                x = wx0 + 32 * w + int(lane);
+                if (t + 1 < steps) {
+                    const size_t ni = size_t(y) * size + size_t(x);
+                    pc_next = x < int(size) ? int(pv.state_count[ni]) : 0;
+                    r_next = !same_ref && x < int(size) && pv_ref_bit(pv.ref_bits, ni);
+                }
+                int delta = 0;
+                if (cx >= x0 && cx <= x1) {
+                    const uint32_t d = uint32_t(cy - y0) * uint32_t(bw) + uint32_t(cx - x0);
+                    delta = int((ws.delta[d >> 2] >> (8 * (d & 3))) & 0xffu) - 128;
+                }
+                const int cc = pc + delta;
+                const uint32_t Cw = __ballot_sync(0xffffffffu, cc > 0);
+                const uint32_t Pw = __ballot_sync(0xffffffffu, pc > 0);
+                const uint32_t Rw = same_ref ? Pw : __ballot_sync(0xffffffffu, rbit_own);
+                if (__ballot_sync(0xffffffffu, cc < 0)) fallback = true;
+                if (Cw != Pw) {
+                    dchg += __popc(Cw ^ Rw) - __popc(Pw ^ Rw);
+                    dtot += __popc(Cw | Rw) - __popc(Pw | Rw);
+                    dcov += __popc(Cw) - __popc(Pw);
+                }
+                if (lane == 0) ws.region[(cy - y0) * words + cw] = Cw;
+                const uint32_t xm = Cw ^ Rw;
+                if (xm) {
+                    const uint32_t pos = qn + __popc(xm & below);
+                    if (((xm >> lane) & 1u) && pos < kQueue)
+                        ws.queue[pos] = uint32_t(cx) | (uint32_t(cy) << 15) | (uint32_t(cc > 0) << 30);
+                    qn += __popc(xm);
                 }
             }
             if (qn > uint32_t(kQueue)) fallback = true;
