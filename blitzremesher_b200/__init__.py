@@ -128,8 +128,19 @@ EXPORTS = {
     "blitz_audit_coverage_distance": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint8,
                                        C.c_int, C.POINTER(C.c_double), C.c_char_p, C.c_size_t], C.c_int),
     "blitz_audit_profile_enable": ([C.c_void_p, C.c_int], C.c_int),
+    "blitz_audit_execute": ([C.c_void_p, C.c_uint32, C.c_uint32, C.POINTER(EvalSettings), C.c_void_p, C.c_size_t,
+                             C.c_void_p, C.c_char_p, C.c_size_t], C.c_int),
+    "blitz_audit_state": ([C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p, C.c_size_t, C.POINTER(C.c_uint32),
+                           C.c_char_p, C.c_size_t], C.c_int),
+    "blitz_audit_reset": ([C.c_void_p, C.c_char_p, C.c_size_t], C.c_int),
     "blitz_audit_profile_read": ([C.c_void_p, C.c_void_p], C.c_int),
 }
+
+
+class Execution(C.Structure):
+    _fields_ = [("struct_size", C.c_uint32), ("commits", C.c_uint32), ("trials", C.c_uint32),
+                ("final_faces", C.c_uint32), ("audited", C.c_uint64), ("stop_reason", C.c_uint8),
+                ("reserved", C.c_uint8 * 7)]
 
 
 class AuditProfile(C.Structure):
@@ -308,6 +319,35 @@ class AuditSession:
         err = C.create_string_buffer(512)
         _check(self.lib.blitz_audit_candidates_device(self.handle, collapses_ptr, n, g, verdicts_ptr,
                                                       measurements_ptr or None, stream or None, err, 512), err)
+
+    def execute(self, target_faces: int, trial_budget: int, gates: Sequence[EvalSettings]) -> dict:
+        """Greedy LOD step on the current state (batches of one, ShortestEdge)."""
+        cap = 1 << 22
+        commits = np.zeros(2 * min(cap, 8 * 1024 * 1024), dtype=np.uint32)
+        out = Execution()
+        out.struct_size = C.sizeof(Execution)
+        g = (EvalSettings * 4)(*gates)
+        err = C.create_string_buffer(512)
+        _check(self.lib.blitz_audit_execute(self.handle, target_faces, trial_budget, g, commits.ctypes.data,
+                                            commits.size // 2, C.byref(out), err, 512), err)
+        n = out.commits
+        return {"commits": commits[: 2 * n].reshape(-1, 2).copy(), "trials": out.trials,
+                "final_faces": out.final_faces, "audited": out.audited, "stop": out.stop_reason}
+
+    def state(self):
+        """Current state: (indices, positions)."""
+        faces = C.c_uint32()
+        err = C.create_string_buffer(512)
+        _check(self.lib.blitz_audit_state(self.handle, None, 0, None, 0, C.byref(faces), err, 512), err)
+        idx = np.zeros(3 * faces.value, np.uint32)
+        pos = np.zeros((self._source.pos.shape[0], 3), np.float32)
+        _check(self.lib.blitz_audit_state(self.handle, idx.ctypes.data, idx.size, pos.ctypes.data, pos.size,
+                                          C.byref(faces), err, 512), err)
+        return idx, pos
+
+    def reset(self) -> None:
+        err = C.create_string_buffer(512)
+        _check(self.lib.blitz_audit_reset(self.handle, err, 512), err)
 
     def profile(self, enable: Optional[bool] = None) -> dict:
         """Enables/disables kernel profiling (resetting counters) or reads it."""

@@ -24,11 +24,14 @@ constexpr int kRegionRows = 64;     // region height
 constexpr int kDeltaSamples = 2048; // region samples (unaligned bbox) with a count delta
 constexpr int kQueue = 160;         // changed samples per (candidate, view)
 constexpr int kMaxOk = 48;          // rasterized (unculled, unclipped) old + new faces
+constexpr int kMaxTileSide = 32;    // tile-maxima path for rasters up to 1024 x 1024
+constexpr int kAffected = 8;        // tiles outside the region whose distances may change
 
 struct WarpScratch {
     double vx[32], vy[32], vz[32]; // projected local vertices; 31 = placement
     FaceSetup faces[kMaxOk];       // old faces carry pad = -1, new faces pad = +1
     uint32_t work[kMaxOk];         // exclusive prefix of bbox samples per face
+    uint32_t affected[kAffected];
     uint32_t region[kRegionRows * kRegionWords];
     uint32_t delta[kDeltaSamples / 4]; // per-sample count delta + 128, one byte each
     uint32_t queue[kQueue];
@@ -143,8 +146,10 @@ __device__ void audit_unit(const CandidateRecord* __restrict__ rec, const PlanDe
     r.flags = pv.clipped_ref ? kRecClippedRef : 0;
     r.ca = pv.cov_ref > 0;
     r.max_d2 = 0, r.changed = 0, r.total = 0, r.cb = 0;
-    if (!plan.state_is_ref) {
-        // A state that differs from the reference needs the full distance field.
+    const bool same_ref = plan.state_is_ref != 0; // state words equal reference words
+    if (!same_ref && (!pv.tile_t1 || plan.size > 32 * kMaxTileSide)) {
+        // Without tile maxima a state that differs from the reference needs
+        // the full distance field.
         r.flags |= kRecFallback;
         record_write(out, r);
         return;
@@ -235,12 +240,18 @@ __device__ void audit_unit(const CandidateRecord* __restrict__ rec, const PlanDe
     cmask.region = ws.region;
     cmask.size = size;
     uint64_t samples = 0;
+    // The processed region: the changed faces' bbox widened to whole coverage
+    // words; when the state differs from the reference, widened to whole
+    // 32x32 tiles so every tile is either fully processed or fully outside.
+    const int wx0 = x0 & ~31;
+    const int ry0 = same_ref ? y0 : (y0 & ~31);
+    const int ry1 = same_ref ? y1 : min(int(size) - 1, y1 | 31);
+    const int words = x1 >= 0 ? ((x1 - wx0) >> 5) + 1 : 0;
     if (x1 >= 0) {
-        const int wx0 = x0 & ~31;
-        const int words = ((x1 - wx0) >> 5) + 1, rows = y1 - y0 + 1;
-        cmask.y0 = uint32_t(y0), cmask.y1 = uint32_t(y1), cmask.c0 = uint32_t(wx0 >> 5), cmask.words = uint32_t(words);
-        const int bw = x1 - x0 + 1;
-        if (words > kRegionWords || rows > kRegionRows || bw * rows > kDeltaSamples) {
+        const int rows = ry1 - ry0 + 1;
+        cmask.y0 = uint32_t(ry0), cmask.y1 = uint32_t(ry1), cmask.c0 = uint32_t(wx0 >> 5), cmask.words = uint32_t(words);
+        const int bw = x1 - x0 + 1, bh = y1 - y0 + 1;
+        if (words > kRegionWords || rows > kRegionRows || bw * bh > kDeltaSamples) {
             fallback = true;
         } else {
             samples = uint64_t(rows) * words * 32;
@@ -248,7 +259,7 @@ __device__ void audit_unit(const CandidateRecord* __restrict__ rec, const PlanDe
             // work item spread over the lanes; covered samples add the face's
             // sign to a per-sample byte (biased by 128, so at most 32 old and
             // 32 new faces never carry across bytes).
-            const uint32_t delta_words = uint32_t(bw * rows + 3) >> 2;
+            const uint32_t delta_words = uint32_t(bw * bh + 3) >> 2;
             for (uint32_t k = lane; k < delta_words; k += 32) ws.delta[k] = 0x80808080u;
             uint32_t c0 = 0, c1 = 0;
             if (lane < nok) {
@@ -287,8 +298,7 @@ __device__ void audit_unit(const CandidateRecord* __restrict__ rec, const PlanDe
             // Phase 2: coverage words row by row; loads for step t+1 are issued
             // before step t is consumed.
             const int steps = rows * words;
-            const bool same_ref = plan.state_is_ref != 0; // state words equal reference words
-            int y = y0, w = 0;
+            int y = ry0, w = 0;
             int x = wx0 + int(lane);
             int pc_next = x < int(size) ? int(pv.state_count[size_t(y) * size + size_t(x)]) : 0;
             bool r_next = !same_ref && x < int(size) && pv_ref_bit(pv.ref_bits, size_t(y) * size + size_t(x));
@@ -304,7 +314,7 @@ __device__ void audit_unit(const CandidateRecord* __restrict__ rec, const PlanDe
                     r_next = !same_ref && x < int(size) && pv_ref_bit(pv.ref_bits, ni);
                 }
                 int delta = 0;
-                if (cx >= x0 && cx <= x1) {
+                if (cx >= x0 && cx <= x1 && cy >= y0 && cy <= y1) {
                     const uint32_t d = uint32_t(cy - y0) * uint32_t(bw) + uint32_t(cx - x0);
                     delta = int((ws.delta[d >> 2] >> (8 * (d & 3))) & 0xffu) - 128;
                 }
@@ -318,7 +328,7 @@ __device__ void audit_unit(const CandidateRecord* __restrict__ rec, const PlanDe
                     dtot += __popc(Cw | Rw) - __popc(Pw | Rw);
                     dcov += __popc(Cw) - __popc(Pw);
                 }
-                if (lane == 0) ws.region[(cy - y0) * words + cw] = Cw;
+                if (lane == 0) ws.region[(cy - ry0) * words + cw] = Cw;
                 const uint32_t xm = Cw ^ Rw;
                 if (xm) {
                     const uint32_t pos = qn + __popc(xm & below);
@@ -331,6 +341,70 @@ __device__ void audit_unit(const CandidateRecord* __restrict__ rec, const PlanDe
         }
     }
     __syncwarp();
+    // Outside the region the candidate equals the state. State-only samples
+    // keep their reference distance (tile maxima t1); reference-only samples
+    // keep their state distance unless the region could hold their nearest
+    // covered sample (a tile within sqrt(t2) of the changed bbox): those tiles
+    // are searched again below.
+    int32_t far1 = -1, far2 = -1;
+    uint32_t naff = 0;
+    if (!same_ref && !fallback) {
+        const uint32_t tiles_x = (size + 31) / 32, ntiles = tiles_x * tiles_x;
+        const uint32_t tc0 = uint32_t(wx0 >> 5), tc1 = tc0 + uint32_t(words) - 1;
+        const uint32_t tr0 = uint32_t(ry0 >> 5), tr1 = uint32_t(ry1 >> 5);
+        for (uint32_t base = 0; base < ntiles; base += 32) {
+            const uint32_t k = base + lane;
+            bool aff = false;
+            if (k < ntiles) {
+                const uint32_t tx = k % tiles_x, ty = k / tiles_x;
+                const bool inside = words > 0 && tx >= tc0 && tx <= tc1 && ty >= tr0 && ty <= tr1;
+                if (!inside) {
+                    far1 = max(far1, pv.tile_t1[k]);
+                    const int32_t t2 = pv.tile_t2[k];
+                    if (t2 >= 0) {
+                        if (x1 < 0) {
+                            far2 = max(far2, t2);
+                        } else {
+                            const int64_t gx0 = int64_t(tx) * 32, gy0 = int64_t(ty) * 32;
+                            const int64_t dx = max(int64_t(0), max(gx0 - x1, int64_t(x0) - (gx0 + 31)));
+                            const int64_t dy = max(int64_t(0), max(gy0 - y1, int64_t(y0) - (gy0 + 31)));
+                            if (dx * dx + dy * dy > int64_t(t2)) far2 = max(far2, t2);
+                            else aff = true;
+                        }
+                    }
+                }
+            }
+            const uint32_t m = __ballot_sync(0xffffffffu, aff);
+            const uint32_t pos = naff + __popc(m & below);
+            if (aff && pos < uint32_t(kAffected)) ws.affected[pos] = k;
+            naff += __popc(m);
+        }
+        for (int o = 16; o; o >>= 1) {
+            far1 = max(far1, __shfl_xor_sync(0xffffffffu, far1, o));
+            far2 = max(far2, __shfl_xor_sync(0xffffffffu, far2, o));
+        }
+        if (naff > uint32_t(kAffected)) fallback = true;
+        __syncwarp();
+        // Reference-only samples of affected tiles: one lane per tile row.
+        for (uint32_t a = 0; a < naff && !fallback; ++a) {
+            const uint32_t k = ws.affected[a], tx = k % tiles_x, ty = k / tiles_x;
+            const uint32_t y = ty * 32 + lane;
+            uint32_t bits = 0;
+            if (y < size) bits = chunk_global(pv.ref_bits, size, y, tx) & ~cmask.chunk(y, tx);
+            const uint32_t cnt = __popc(bits);
+            uint32_t incl = cnt;
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= uint32_t(o)) incl += t;
+            }
+            uint32_t pos = qn + incl - cnt;
+            for (uint32_t b = bits; b; b &= b - 1, ++pos)
+                if (pos < uint32_t(kQueue)) ws.queue[pos] = (tx * 32 + uint32_t(__ffs(b) - 1)) | (y << 15);
+            qn += __shfl_sync(0xffffffffu, incl, 31);
+            if (qn > uint32_t(kQueue)) fallback = true;
+        }
+        __syncwarp();
+    }
     r.changed = uint32_t(int64_t(pv.changed) + dchg);
     r.total = uint32_t(int64_t(pv.total) + dtot);
     r.cb = int64_t(pv.cov_state) + dcov > 0;
@@ -340,15 +414,18 @@ __device__ void audit_unit(const CandidateRecord* __restrict__ rec, const PlanDe
         for (uint32_t k = lane; k < qn; k += 32) {
             const uint32_t e = ws.queue[k];
             const uint32_t x = e & 0x7fffu, y = (e >> 15) & 0x7fffu;
-            // Candidate-only sample: nearest reference sample; reference-only
-            // sample: nearest candidate sample.
-            const uint32_t d = (e >> 30) & 1u ? nearest_d2(rmask, x, y) : nearest_d2(cmask, x, y);
+            // Candidate-only sample: distance to the reference (resident field
+            // or search); reference-only sample: search the candidate.
+            uint32_t d;
+            if ((e >> 30) & 1u) d = pv.ref_field ? pv.ref_field[size_t(y) * size + x] : nearest_d2(rmask, x, y);
+            else d = nearest_d2(cmask, x, y);
             best = d > best ? d : best;
         }
         for (int o = 16; o; o >>= 1) {
             const uint32_t y = __shfl_xor_sync(0xffffffffu, best, o);
             best = y > best ? y : best;
         }
+        best = max(best, uint32_t(max(max(far1, far2), 0)));
     }
     r.max_d2 = best;
     if (fallback) r.flags |= kRecFallback;

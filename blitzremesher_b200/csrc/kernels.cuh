@@ -65,6 +65,9 @@ struct PlanView {
     const uint32_t* ref_bits;   // reference mask, CPU semantics (u64 layout as u32 words)
     const uint32_t* state_bits; // current state: count > 0
     const uint8_t* state_count; // current state: covering faces per sample
+    const uint32_t* ref_field;  // exact squared distance to the reference mask, or null
+    const int32_t* tile_t1;     // per 32x32 tile: max ref_field over state-only samples (-1 none)
+    const int32_t* tile_t2;     // per 32x32 tile: max state field over reference-only samples
     uint32_t changed, total;    // state vs reference
     uint32_t cov_ref, cov_state;
     uint32_t clip_state;        // clipped faces of the state
@@ -106,6 +109,19 @@ void launch_popcounts(const uint32_t* a, const uint32_t* b, uint32_t words, unsi
 void launch_distance(const uint32_t* from, const uint32_t* to, uint32_t width, uint32_t height, uint32_t* g,
                      uint32_t* d2, int32_t* stack_v, long long* stack_num, long long* stack_den, uint32_t* out_max,
                      cudaStream_t s);
+void launch_counts_to_bits(const uint8_t* counts, uint32_t size, uint32_t* bits, cudaStream_t s);
+void launch_tile_maxima(const uint32_t* ref_bits, const uint32_t* state_bits, const uint32_t* ref_field,
+                        const uint32_t* state_field, uint32_t size, int32_t* t1, int32_t* t2, cudaStream_t s);
+void launch_field(const uint32_t* bits, uint32_t width, uint32_t height, uint32_t* g, uint32_t* d2, int32_t* stack_v,
+                  long long* stack_num, long long* stack_den, cudaStream_t s);
+// ShortestEdge scores of the legal edits (action_gpu.cu:822-825), keys for a
+// stable descending sort.
+void launch_rank_shortest(const DevMesh& m, const Edit* edits, const uint32_t* count, uint32_t capacity,
+                          double diameter, float* scores, uint32_t* order, cudaStream_t s);
+void launch_gather_window(const Edit* edits, const uint32_t* order, uint32_t first, uint32_t n, void* collapses,
+                          cudaStream_t s);
+cudaError_t sort_scores_desc(const float* keys_in, float* keys_out, const uint32_t* vals_in, uint32_t* vals_out,
+                             uint32_t n, void* temp, size_t& temp_bytes, cudaStream_t s);
 void launch_audit(const CandidateRecord* records, uint32_t n, const PlanDev& plan, ViewRecord* out,
                   unsigned long long* stats, uint32_t* queue, cudaStream_t s);
 struct GateDev {

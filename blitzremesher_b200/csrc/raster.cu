@@ -204,7 +204,64 @@ __global__ void k_directed_max(const uint32_t* from, const uint32_t* to, const u
     }
     if ((threadIdx.x & 31) == 0 && best) atomicMax(out, best);
 }
+// Coverage words from the per-sample face counts (count > 0), u64 layout.
+__global__ void k_counts_to_bits(const uint8_t* counts, size_t samples, uint32_t* bits, uint32_t words) {
+    uint32_t w = blockIdx.x * blockDim.x + threadIdx.x;
+    if (w >= words) return;
+    uint32_t out = 0;
+    size_t base = size_t(w) * 32;
+    for (int k = 0; k < 32; ++k) {
+        size_t i = base + k;
+        if (i < samples && counts[i]) out |= 1u << k;
+    }
+    bits[w] = out;
+}
+
+// Per 32x32 tile: t1 = max reference field over samples covered by the state
+// and not by the reference; t2 = max state field over samples covered by the
+// reference and not by the state; -1 when the tile has no such sample.
+__global__ void k_tile_maxima(const uint32_t* ref_bits, const uint32_t* state_bits, const uint32_t* ref_field,
+                              const uint32_t* state_field, uint32_t size, int32_t* t1, int32_t* t2) {
+    const uint32_t tiles_x = (size + 31) / 32;
+    const uint32_t tile = blockIdx.x, lane = threadIdx.x;
+    const uint32_t tx = tile % tiles_x, ty = tile / tiles_x;
+    const uint32_t x = tx * 32 + lane;
+    int32_t m1 = -1, m2 = -1;
+    if (x < size)
+        for (uint32_t r = 0; r < 32; ++r) {
+            uint32_t y = ty * 32 + r;
+            if (y >= size) break;
+            size_t i = size_t(y) * size + x;
+            bool p = bit_at(state_bits, i), q = bit_at(ref_bits, i);
+            if (p && !q) m1 = max(m1, int32_t(min(ref_field[i], 0x7fffffffu)));
+            if (q && !p) m2 = max(m2, int32_t(min(state_field[i], 0x7fffffffu)));
+        }
+    for (int o = 16; o; o >>= 1) {
+        m1 = max(m1, __shfl_xor_sync(0xffffffffu, m1, o));
+        m2 = max(m2, __shfl_xor_sync(0xffffffffu, m2, o));
+    }
+    if (lane == 0) t1[tile] = m1, t2[tile] = m2;
+}
 } // namespace
+
+void launch_counts_to_bits(const uint8_t* counts, uint32_t size, uint32_t* bits, cudaStream_t s) {
+    size_t samples = size_t(size) * size;
+    uint32_t words = uint32_t((samples + 63) / 64) * 2;
+    k_counts_to_bits<<<blocks_for(words), kThreads, 0, s>>>(counts, samples, bits, words);
+}
+
+void launch_tile_maxima(const uint32_t* ref_bits, const uint32_t* state_bits, const uint32_t* ref_field,
+                        const uint32_t* state_field, uint32_t size, int32_t* t1, int32_t* t2, cudaStream_t s) {
+    uint32_t tiles = ((size + 31) / 32) * ((size + 31) / 32);
+    k_tile_maxima<<<tiles, 32, 0, s>>>(ref_bits, state_bits, ref_field, state_field, size, t1, t2);
+}
+
+// Exact squared distance field of `bits` (d2 = kNone where the mask is empty).
+void launch_field(const uint32_t* bits, uint32_t width, uint32_t height, uint32_t* g, uint32_t* d2, int32_t* stack_v,
+                  long long* stack_num, long long* stack_den, cudaStream_t s) {
+    k_row_nearest<<<blocks_for(height, 64), 64, 0, s>>>(bits, width, height, g);
+    k_column_envelope<<<blocks_for(width, 64), 64, 0, s>>>(g, width, height, d2, stack_v, stack_num, stack_den);
+}
 
 void launch_raster(const DevMesh& m, const Camera* cam_host, const float* center, uint32_t ss, uint32_t size,
                    bool force_two, bool cpu_semantics, uint32_t* bits, uint8_t* counts, uint32_t* state,

@@ -297,16 +297,24 @@ struct PlanKey {
     }
 };
 
+// A plan keeps, per view, the reference mask (CPU semantics) and the current
+// state's per-sample face counts, coverage and popcounts against the
+// reference. Plans of rasters up to 1024 x 1024 also keep both exact distance
+// fields and 32x32 tile maxima, so candidates of a state that differs from the
+// reference stay on the incremental path.
 struct Plan {
     PlanKey key{};
     uint32_t size = 0, views = 0, words = 0;
-    bool resource_limited = false;
+    bool resource_limited = false, tiled = false, ref_box_clip = false;
     Buf<Camera> cameras;
-    Buf<uint32_t> ref_bits, state_bits;
+    std::vector<Camera> hcams;
+    Buf<uint32_t> ref_bits, state_bits, ref_field, state_field;
+    Buf<int32_t> t1, t2;
     Buf<uint8_t> state_count;
     Buf<PlanView> dviews;
     std::vector<PlanView> hviews;
     bool state_is_ref = true;
+    uint64_t state_revision = ~0ull;
     Buf<ViewRecord> records;
     PlanDev dev{};
 };
@@ -327,6 +335,9 @@ struct Session {
     HostMesh source_h, previous_h;
     bool previous_is_source = true;
     DeviceMesh source, previous, state;
+    uint32_t state_faces = 0;       // live faces of the state
+    uint64_t state_revision = 0;    // bumped by every commit
+    bool state_is_source = true;    // no commit since creation or reset
     Bounds bounds{};
     Topology topo;
     std::map<PlanKey, std::unique_ptr<Plan>> plans;
@@ -339,10 +350,15 @@ struct Session {
     Buf<const ViewRecord*> record_table;
     Buf<uint32_t> plan_views, plan_ss;
     Buf<GateDev> gate_table;
-    // exact path
+    // exact path and commits
     DeviceMesh trial;
     Buf<uint32_t> trial_keep, trial_offsets;
     Buf<TrialInfo> trial_info;
+    // executor ranking
+    Buf<float> scores, sorted_scores;
+    Buf<uint32_t> order, sorted_order;
+    Buf<unsigned char> sort_temp;
+    size_t sort_bytes = 0;
     blitz_neural_info info{};
     uint64_t internal_errors = 0;
     // profiling
@@ -368,16 +384,17 @@ struct DeviceScope {
     ~DeviceScope() { cudaSetDevice(previous); }
 };
 
-static void build_topology(Session& S) {
+// Geometric classes of the episode's first mesh, welded once; topology
+// buffers at the session's capacity (the state only loses faces).
+static void init_topology(Session& S) {
     Topology& t = S.topo;
     const DevMesh& m = S.state.view;
     const uint32_t n = m.nv, nf = m.nf;
     Pool& P = S.pool;
-    cudaStream_t st = S.stream;
     t.table_cap = pow2_at_least(2ull * n);
     t.geometry = Buf<uint32_t>(P, n);
     t.table = Buf<uint32_t>(P, t.table_cap);
-    launch_weld(m, t.table.p, t.table_cap, false, t.geometry.p, st);
+    launch_weld(m, t.table.p, t.table_cap, false, t.geometry.p, S.stream);
     t.face_offsets = Buf<uint32_t>(P, n + 1);
     t.faces = Buf<uint32_t>(P, 3ull * nf);
     t.cursor = Buf<uint32_t>(P, 2ull * (n + 1));
@@ -392,27 +409,34 @@ static void build_topology(Session& S) {
     t.slots = Buf<uint32_t>(P, n);
     size_t scan_words = std::max(scan_scratch_words(n + 1), scan_scratch_words(uint32_t(6ull * nf + 1)));
     t.scan = Buf<uint32_t>(P, scan_words + 64);
+    t.edge_base = Buf<uint32_t>(P, n + 1);
+    t.valid = Buf<uint8_t>(P, 6ull * nf + 1);
+    t.edit_slots = Buf<Edit>(P, 6ull * nf + 1);
+    t.offsets = Buf<uint32_t>(P, 6ull * nf + 1);
+    t.edits = Buf<Edit>(P, 6ull * nf + 1);
+    t.flat = Buf<uint32_t>(P, 1);
+    t.pos_cap = pow2_at_least(4ull * n);
+    t.positions = Buf<uint32_t>(P, t.pos_cap);
+    t.view = DevTopology{t.geometry.p, t.geometry.p, t.face_offsets.p, t.faces.p, t.nbr_offsets.p, t.neighbors.p,
+                         t.nbr_count.p, t.boundary.p, t.invalid.p, t.slot_offsets.p, t.slots.p};
+}
+
+// Class CSR, fans, legal actions, flat faces and live positions of the state
+// (action_gpu.cu:1607-1622 rebuild(), on the classes welded at creation).
+static void rebuild_topology(Session& S) {
+    Topology& t = S.topo;
+    const DevMesh& m = S.state.view;
+    const uint32_t n = m.nv;
+    cudaStream_t st = S.stream;
     launch_topology(m, t.geometry.p, t.face_offsets.p, t.faces.p, t.cursor.p, nullptr, t.entries.p, t.nbr_offsets.p,
                     t.neighbors.p, t.nbr_count.p, t.boundary.p, t.invalid.p, t.visited.p, t.slot_offsets.p,
                     t.slots.p, t.scan.p, nullptr, st);
     B200_CUDA(cudaMemcpyAsync(&t.total_nbrs, t.nbr_offsets.p + n, 4, cudaMemcpyDeviceToHost, st));
     B200_CUDA(cudaStreamSynchronize(st));
-    t.view = DevTopology{t.geometry.p, t.geometry.p, t.face_offsets.p, t.faces.p, t.nbr_offsets.p, t.neighbors.p,
-                         t.nbr_count.p, t.boundary.p, t.invalid.p, t.slot_offsets.p, t.slots.p};
-    // Legal actions in enumeration order.
-    t.edge_base = Buf<uint32_t>(P, n + 1);
-    t.valid = Buf<uint8_t>(P, t.total_nbrs + 1);
-    t.edit_slots = Buf<Edit>(P, t.total_nbrs + 1);
-    t.offsets = Buf<uint32_t>(P, t.total_nbrs + 1);
-    t.edits = Buf<Edit>(P, t.total_nbrs + 1);
     launch_enumerate(m, t.view, t.edge_base.p, t.valid.p, t.edit_slots.p, t.offsets.p, t.edits.p, t.scan.p,
                      t.total_nbrs, false, st);
     B200_CUDA(cudaMemcpyAsync(&t.actions, t.offsets.p + t.total_nbrs, 4, cudaMemcpyDeviceToHost, st));
-    // Validation support: flat faces and live positions.
-    t.flat = Buf<uint32_t>(P, 1);
     launch_flat_faces(m, t.flat.p, st);
-    t.pos_cap = pow2_at_least(4ull * n);
-    t.positions = Buf<uint32_t>(P, t.pos_cap);
     launch_position_table(m, t.view, t.positions.p, t.pos_cap, st);
     B200_CUDA(cudaStreamSynchronize(st));
     B200_CUDA(cudaGetLastError());
@@ -423,15 +447,86 @@ static uint32_t mask_words(uint32_t size) {
     return uint32_t(((samples + 63) / 64) * 2 + 2); // u64 layout plus one padding word pair
 }
 
-// Rasterizes a device mesh for one view; returns {any clip, first box clip, clipped faces, overflow}.
+// Rasterizes a device mesh for one view; state_dev receives {first box clip,
+// any clip, clipped faces, count overflow}.
 static void raster(Session& S, const DevMesh& m, const Camera* cam_host, uint32_t ss, uint32_t size, bool force_two,
                    bool cpu_semantics, uint32_t* bits, uint8_t* counts, uint32_t* state_dev) {
     launch_raster(m, cam_host, S.bounds.center, ss, size, force_two, cpu_semantics, bits, counts, state_dev, S.stream);
 }
 
+static void ensure_scratch(Session& S, uint32_t size);
+
+static size_t count_stride(size_t samples) { return (samples + 3) & ~size_t(3); }
+
+// Brings the plan's state data (counts, coverage, fields, tile maxima,
+// popcounts) up to the session's current state.
+static void refresh_state(Session& S, Plan& p) {
+    const PlanKey& key = p.key;
+    const size_t samples = size_t(p.size) * p.size, cstride = count_stride(samples);
+    const bool ref_is_source = key.reference == 0 || S.previous_is_source;
+    p.state_is_ref = S.state_is_source && ref_is_source && !p.ref_box_clip;
+    cudaStream_t st = S.stream;
+    B200_CUDA(cudaMemsetAsync(p.state_count.p, 0, cstride * p.views, st));
+    Buf<uint32_t> state(S.pool, 4 * size_t(p.views));
+    DevMesh live = S.state.view;
+    live.nf = S.state_faces;
+    for (uint32_t v = 0; v < p.views; ++v)
+        raster(S, live, &p.hcams[v], key.ss, p.size, key.force_two, false, nullptr, p.state_count.p + cstride * v,
+               state.p + 4 * v);
+    const bool own_bits = p.tiled || !p.state_is_ref;
+    if (own_bits) {
+        if (!p.state_bits.p) p.state_bits = Buf<uint32_t>(S.pool, size_t(p.words) * p.views);
+        B200_CUDA(cudaMemsetAsync(p.state_bits.p, 0, size_t(p.words) * p.views * 4, st));
+        for (uint32_t v = 0; v < p.views; ++v)
+            launch_counts_to_bits(p.state_count.p + cstride * v, p.size, p.state_bits.p + size_t(p.words) * v, st);
+    }
+    const uint32_t* sbits = own_bits ? p.state_bits.p : p.ref_bits.p;
+    if (p.tiled && !p.state_is_ref) {
+        ensure_scratch(S, p.size);
+        const uint32_t tiles = ((p.size + 31) / 32) * ((p.size + 31) / 32);
+        for (uint32_t v = 0; v < p.views; ++v) {
+            launch_field(sbits + size_t(p.words) * v, p.size, p.size, S.scratch.g.p, p.state_field.p + samples * v,
+                         S.scratch.sv.p, S.scratch.sn.p, S.scratch.sd.p, st);
+            launch_tile_maxima(p.ref_bits.p + size_t(p.words) * v, sbits + size_t(p.words) * v,
+                               p.ref_field.p + samples * v, p.state_field.p + samples * v, p.size, p.t1.p + tiles * v,
+                               p.t2.p + tiles * v, st);
+        }
+    }
+    Buf<unsigned long long> pop(S.pool, 4 * size_t(p.views));
+    for (uint32_t v = 0; v < p.views; ++v)
+        launch_popcounts(p.ref_bits.p + size_t(v) * p.words, sbits + size_t(v) * p.words, p.words, pop.p + 4 * v, st);
+    std::vector<unsigned long long> hpop(4 * size_t(p.views));
+    std::vector<uint32_t> hstate(4 * size_t(p.views));
+    B200_CUDA(cudaMemcpyAsync(hpop.data(), pop.p, hpop.size() * 8, cudaMemcpyDeviceToHost, st));
+    B200_CUDA(cudaMemcpyAsync(hstate.data(), state.p, hstate.size() * 4, cudaMemcpyDeviceToHost, st));
+    B200_CUDA(cudaStreamSynchronize(st));
+    const uint32_t tiles = ((p.size + 31) / 32) * ((p.size + 31) / 32);
+    for (uint32_t v = 0; v < p.views; ++v) {
+        if (hstate[4 * v + 3]) throw Failure(BLITZ_OUT_OF_MEMORY, "more than 255 faces cover one sample");
+        PlanView& pv = p.hviews[v];
+        pv.state_bits = sbits + size_t(v) * p.words;
+        pv.state_count = p.state_count.p + cstride * v;
+        pv.tile_t1 = p.tiled ? p.t1.p + tiles * v : nullptr;
+        pv.tile_t2 = p.tiled ? p.t2.p + tiles * v : nullptr;
+        pv.changed = uint32_t(hpop[4 * v]);
+        pv.total = uint32_t(hpop[4 * v + 1]);
+        pv.cov_ref = uint32_t(hpop[4 * v + 2]);
+        pv.cov_state = uint32_t(hpop[4 * v + 3]);
+        pv.clip_state = hstate[4 * v + 2];
+    }
+    B200_CUDA(cudaMemcpyAsync(p.dviews.p, p.hviews.data(), p.views * sizeof(PlanView), cudaMemcpyHostToDevice, st));
+    p.dev.state_is_ref = p.state_is_ref;
+    p.state_revision = S.state_revision;
+    B200_CUDA(cudaStreamSynchronize(st));
+}
+
 static Plan& plan_for(Session& S, const PlanKey& key) {
     auto it = S.plans.find(key);
-    if (it != S.plans.end()) return *it->second;
+    if (it != S.plans.end()) {
+        Plan& p = *it->second;
+        if (!p.resource_limited && p.state_revision != S.state_revision) refresh_state(S, p);
+        return p;
+    }
     auto plan = std::make_unique<Plan>();
     Plan& p = *plan;
     p.key = key;
@@ -442,73 +537,50 @@ static Plan& plan_for(Session& S, const PlanKey& key) {
         return *(S.plans[key] = std::move(plan));
     }
     p.words = mask_words(p.size);
-    auto cams = make_cameras(S.bounds, key.screen, key.ortho, key.persp, key.seed);
-    p.cameras = Buf<Camera>(S.pool, cams.size());
-    B200_CUDA(cudaMemcpyAsync(p.cameras.p, cams.data(), cams.size() * sizeof(Camera), cudaMemcpyHostToDevice, S.stream));
+    p.tiled = p.size <= 1024;
+    p.hcams = make_cameras(S.bounds, key.screen, key.ortho, key.persp, key.seed);
+    p.cameras = Buf<Camera>(S.pool, p.hcams.size());
+    cudaStream_t st = S.stream;
+    B200_CUDA(cudaMemcpyAsync(p.cameras.p, p.hcams.data(), p.hcams.size() * sizeof(Camera), cudaMemcpyHostToDevice, st));
     const DeviceMesh& ref = key.reference == 0 || S.previous_is_source ? S.source : S.previous;
-    const HostMesh& ref_h = key.reference == 0 || S.previous_is_source ? S.source_h : S.previous_h;
-    bool state_same_mesh = same_data(ref_h, S.source_h) && true; // state is the source in this build
     const size_t samples = size_t(p.size) * p.size;
     p.ref_bits = Buf<uint32_t>(S.pool, size_t(p.words) * p.views);
-    p.state_count = Buf<uint8_t>(S.pool, ((samples + 3) & ~size_t(3)) * p.views);
-    B200_CUDA(cudaMemsetAsync(p.ref_bits.p, 0, size_t(p.words) * p.views * 4, S.stream));
-    B200_CUDA(cudaMemsetAsync(p.state_count.p, 0, ((samples + 3) & ~size_t(3)) * p.views, S.stream));
-    Buf<uint32_t> state(S.pool, 8 * size_t(p.views));
-    std::vector<uint32_t> hstate(8 * size_t(p.views));
-    // Reference masks (CPU semantics) and state counts.
+    p.state_count = Buf<uint8_t>(S.pool, count_stride(samples) * p.views);
+    B200_CUDA(cudaMemsetAsync(p.ref_bits.p, 0, size_t(p.words) * p.views * 4, st));
+    Buf<uint32_t> state(S.pool, 4 * size_t(p.views));
+    for (uint32_t v = 0; v < p.views; ++v)
+        raster(S, ref.view, &p.hcams[v], key.ss, p.size, key.force_two, true, p.ref_bits.p + size_t(v) * p.words,
+               nullptr, state.p + 4 * v);
+    std::vector<uint32_t> hstate(4 * size_t(p.views));
+    B200_CUDA(cudaMemcpyAsync(hstate.data(), state.p, hstate.size() * 4, cudaMemcpyDeviceToHost, st));
+    B200_CUDA(cudaStreamSynchronize(st));
+    p.hviews.assign(p.views, PlanView{});
     for (uint32_t v = 0; v < p.views; ++v) {
-        uint32_t* rb = p.ref_bits.p + size_t(v) * p.words;
-        uint8_t* sc = p.state_count.p + ((samples + 3) & ~size_t(3)) * v;
-        raster(S, ref.view, &cams[v], key.ss, p.size, key.force_two, true, rb, nullptr, state.p + 8 * v);
-        raster(S, S.state.view, &cams[v], key.ss, p.size, key.force_two, false, nullptr, sc, state.p + 8 * v + 4);
+        p.ref_box_clip |= hstate[4 * v] != kNone;
+        p.hviews[v].ref_bits = p.ref_bits.p + size_t(v) * p.words;
+        p.hviews[v].clipped_ref = hstate[4 * v + 1];
     }
-    B200_CUDA(cudaMemcpyAsync(hstate.data(), state.p, hstate.size() * 4, cudaMemcpyDeviceToHost, S.stream));
-    B200_CUDA(cudaStreamSynchronize(S.stream));
-    bool box_clip = false;
-    for (uint32_t v = 0; v < p.views; ++v) {
-        if (hstate[8 * v + 4 + 3]) throw Failure(BLITZ_OUT_OF_MEMORY, "more than 255 faces cover one sample");
-        box_clip |= hstate[8 * v] != kNone;
-    }
-    p.state_is_ref = state_same_mesh && !box_clip;
-    if (p.state_is_ref) {
-        p.state_bits = Buf<uint32_t>(); // shares ref bits
-    } else {
-        p.state_bits = Buf<uint32_t>(S.pool, size_t(p.words) * p.views);
-        B200_CUDA(cudaMemsetAsync(p.state_bits.p, 0, size_t(p.words) * p.views * 4, S.stream));
-        for (uint32_t v = 0; v < p.views; ++v)
-            raster(S, S.state.view, &cams[v], key.ss, p.size, key.force_two, false,
-                   p.state_bits.p + size_t(v) * p.words, nullptr, state.p + 8 * v + 4);
-    }
-    Buf<unsigned long long> pop(S.pool, 4 * size_t(p.views));
-    for (uint32_t v = 0; v < p.views; ++v) {
-        const uint32_t* sb = (p.state_is_ref ? p.ref_bits.p : p.state_bits.p) + size_t(v) * p.words;
-        launch_popcounts(p.ref_bits.p + size_t(v) * p.words, sb, p.words, pop.p + 4 * v, S.stream);
-    }
-    std::vector<unsigned long long> hpop(4 * size_t(p.views));
-    B200_CUDA(cudaMemcpyAsync(hpop.data(), pop.p, hpop.size() * 8, cudaMemcpyDeviceToHost, S.stream));
-    B200_CUDA(cudaMemcpyAsync(hstate.data(), state.p, hstate.size() * 4, cudaMemcpyDeviceToHost, S.stream));
-    B200_CUDA(cudaStreamSynchronize(S.stream));
-    p.hviews.resize(p.views);
-    for (uint32_t v = 0; v < p.views; ++v) {
-        PlanView& pv = p.hviews[v];
-        pv.ref_bits = p.ref_bits.p + size_t(v) * p.words;
-        pv.state_bits = (p.state_is_ref ? p.ref_bits.p : p.state_bits.p) + size_t(v) * p.words;
-        pv.state_count = p.state_count.p + ((samples + 3) & ~size_t(3)) * v;
-        pv.changed = uint32_t(hpop[4 * v]);
-        pv.total = uint32_t(hpop[4 * v + 1]);
-        pv.cov_ref = uint32_t(hpop[4 * v + 2]);
-        pv.cov_state = uint32_t(hpop[4 * v + 3]);
-        pv.clipped_ref = hstate[8 * v + 1];
-        pv.clip_state = hstate[8 * v + 4 + 2];
+    if (p.tiled) {
+        ensure_scratch(S, p.size);
+        const uint32_t tiles = ((p.size + 31) / 32) * ((p.size + 31) / 32);
+        p.ref_field = Buf<uint32_t>(S.pool, samples * p.views);
+        p.state_field = Buf<uint32_t>(S.pool, samples * p.views);
+        p.t1 = Buf<int32_t>(S.pool, size_t(tiles) * p.views);
+        p.t2 = Buf<int32_t>(S.pool, size_t(tiles) * p.views);
+        B200_CUDA(cudaMemsetAsync(p.t1.p, 0xff, size_t(tiles) * p.views * 4, st));
+        B200_CUDA(cudaMemsetAsync(p.t2.p, 0xff, size_t(tiles) * p.views * 4, st));
+        for (uint32_t v = 0; v < p.views; ++v) {
+            launch_field(p.ref_bits.p + size_t(p.words) * v, p.size, p.size, S.scratch.g.p, p.ref_field.p + samples * v,
+                         S.scratch.sv.p, S.scratch.sn.p, S.scratch.sd.p, st);
+            p.hviews[v].ref_field = p.ref_field.p + samples * v;
+        }
     }
     p.dviews = Buf<PlanView>(S.pool, p.views);
-    B200_CUDA(cudaMemcpyAsync(p.dviews.p, p.hviews.data(), p.views * sizeof(PlanView), cudaMemcpyHostToDevice, S.stream));
     p.dev.cameras = p.cameras.p;
     p.dev.views = p.dviews.p;
     for (int k = 0; k < 3; ++k) p.dev.center[k] = S.bounds.center[k];
     p.dev.nviews = p.views, p.dev.ss = key.ss, p.dev.size = p.size, p.dev.force_two = key.force_two;
-    p.dev.state_is_ref = p.state_is_ref;
-    B200_CUDA(cudaStreamSynchronize(S.stream));
+    refresh_state(S, p);
     return *(S.plans[key] = std::move(plan));
 }
 
@@ -619,18 +691,23 @@ struct GateRef {
 };
 
 // Candidate whose verdict needs the full-raster path from gate `first`.
+// Full-trial buffers at the source's capacity (the state only loses faces).
+static void ensure_trial_buffers(Session& S) {
+    if (S.trial.pos.p) return;
+    const DevMesh& src = S.source.view;
+    S.trial.pos = Buf<float>(S.pool, 3ull * src.nv);
+    S.trial.idx = Buf<uint32_t>(S.pool, 3ull * src.nf);
+    if (src.mat) S.trial.mat = Buf<uint16_t>(S.pool, src.nf);
+    S.trial_keep = Buf<uint32_t>(S.pool, src.nf + 1);
+    S.trial_offsets = Buf<uint32_t>(S.pool, src.nf + 1);
+    S.trial_info = Buf<TrialInfo>(S.pool, 1);
+}
+
 static void exact_candidate(Session& S, const blitz_collapse& col, const GateRef* gates, int first,
                             blitz_candidate_verdict& v, Measurement* meas) {
     const DevMesh& m = S.state.view;
     Topology& t = S.topo;
-    if (!S.trial.pos.p) {
-        S.trial.pos = Buf<float>(S.pool, 3ull * m.nv);
-        S.trial.idx = Buf<uint32_t>(S.pool, 3ull * m.nf);
-        if (m.mat) S.trial.mat = Buf<uint16_t>(S.pool, m.nf);
-        S.trial_keep = Buf<uint32_t>(S.pool, m.nf + 1);
-        S.trial_offsets = Buf<uint32_t>(S.pool, m.nf + 1);
-        S.trial_info = Buf<TrialInfo>(S.pool, 1);
-    }
+    ensure_trial_buffers(S);
     Buf<blitz_collapse> one(S.pool, 1);
     B200_CUDA(cudaMemcpyAsync(one.p, &col, sizeof(col), cudaMemcpyHostToDevice, S.stream));
     launch_trial(m, t.view, one.p, S.trial_info.p, S.trial_keep.p, S.trial_offsets.p, S.trial.idx.p, S.trial.mat.p,
@@ -772,6 +849,143 @@ static void audit_candidates(Session& S, const blitz_collapse* cands_dev, const 
     S.info.decoded += nn;
 }
 
+// Applies an accepted collapse to the state: trial build on the GPU
+// (remap, keep, compaction, placement; action_gpu.cu:748-790, 962-1067), the
+// trial becomes the state (commit, 1729-1750), then the topology is rebuilt on
+// the creation-time classes.
+static void commit_collapse(Session& S, const blitz_collapse& col) {
+    ensure_trial_buffers(S);
+    DevMesh& m = S.state.view;
+    cudaStream_t st = S.stream;
+    Buf<blitz_collapse> one(S.pool, 1);
+    B200_CUDA(cudaMemcpyAsync(one.p, &col, sizeof(col), cudaMemcpyHostToDevice, st));
+    launch_trial(m, S.topo.view, one.p, S.trial_info.p, S.trial_keep.p, S.trial_offsets.p, S.trial.idx.p,
+                 S.trial.mat.p, S.trial.pos.p, S.topo.scan.p, st);
+    uint32_t faces = 0;
+    B200_CUDA(cudaMemcpyAsync(&faces, S.trial_offsets.p + m.nf, 4, cudaMemcpyDeviceToHost, st));
+    B200_CUDA(cudaStreamSynchronize(st));
+    if (!faces) throw Failure(BLITZ_INVALID_ARGUMENT, "collapse would remove the entire mesh");
+    B200_CUDA(cudaMemcpyAsync(S.state.idx.p, S.trial.idx.p, size_t(faces) * 12, cudaMemcpyDeviceToDevice, st));
+    B200_CUDA(cudaMemcpyAsync(S.state.pos.p, S.trial.pos.p, size_t(m.nv) * 12, cudaMemcpyDeviceToDevice, st));
+    if (m.mat) B200_CUDA(cudaMemcpyAsync(S.state.mat.p, S.trial.mat.p, size_t(faces) * 2, cudaMemcpyDeviceToDevice, st));
+    m.nf = faces;
+    S.state_faces = faces;
+    ++S.state_revision;
+    S.state_is_source = false;
+    rebuild_topology(S);
+}
+
+static void reset_state(Session& S) {
+    cudaStream_t st = S.stream;
+    const DevMesh& src = S.source.view;
+    B200_CUDA(cudaMemcpyAsync(S.state.idx.p, src.idx, size_t(src.nf) * 12, cudaMemcpyDeviceToDevice, st));
+    B200_CUDA(cudaMemcpyAsync(S.state.pos.p, src.pos, size_t(src.nv) * 12, cudaMemcpyDeviceToDevice, st));
+    if (src.mat) B200_CUDA(cudaMemcpyAsync(S.state.mat.p, src.mat, size_t(src.nf) * 2, cudaMemcpyDeviceToDevice, st));
+    S.state.view.nf = src.nf;
+    S.state_faces = src.nf;
+    ++S.state_revision;
+    S.state_is_source = true;
+    rebuild_topology(S);
+}
+
+// Greedy executor with batches of one (GpuActionState::execute,
+// action_gpu.cu:1947-2086; execute_actions, action.cpp:453-525): rank the legal
+// midpoint collapses by ShortestEdge, walk them in rank order skipping those
+// that would remove more faces than remain above the target, audit each
+// through the four gates and commit the first accepted, then re-rank. Every
+// trial of the walk is audited against the same state, so the walk is audited
+// speculatively in ranked windows (one batched launch each) and replayed in
+// order on the host; the result equals the serial loop trial for trial.
+static void execute(Session& S, uint32_t target, uint32_t budget, const blitz_eval_settings gates[4],
+                    uint32_t* commits_out, size_t capacity, blitz_audit_execution& out) {
+    target = std::max<uint32_t>(1, target);
+    cudaStream_t st = S.stream;
+    Topology& t = S.topo;
+    const double diameter = std::max(1e-20, S.bounds.radius * 2);
+    const size_t cap = 6ull * S.source.view.nf + 1;
+    S.scores.ensure(S.pool, cap);
+    S.sorted_scores.ensure(S.pool, cap);
+    S.order.ensure(S.pool, cap);
+    S.sorted_order.ensure(S.pool, cap);
+    if (!S.sort_temp.p) {
+        size_t bytes = 0;
+        B200_CUDA(sort_scores_desc(nullptr, nullptr, nullptr, nullptr, uint32_t(cap), nullptr, bytes, st));
+        S.sort_temp = Buf<unsigned char>(S.pool, bytes);
+        S.sort_bytes = bytes;
+    }
+    uint32_t window = 64;
+    uint32_t commits = 0, trials = 0;
+    uint64_t audited = 0;
+    uint8_t reason = 3;
+    std::vector<blitz_candidate_verdict> hv;
+    std::vector<blitz_collapse> hc;
+    for (;;) {
+        const uint32_t faces = S.state_faces;
+        if (faces <= target) {
+            reason = 0;
+            break;
+        }
+        if (trials >= budget) {
+            reason = 1;
+            break;
+        }
+        const uint32_t actions = t.actions;
+        if (!actions) {
+            reason = 2;
+            break;
+        }
+        launch_rank_shortest(S.state.view, t.edits.p, t.offsets.p + t.total_nbrs, actions, diameter, S.scores.p,
+                             S.order.p, st);
+        size_t bytes = S.sort_bytes;
+        B200_CUDA(sort_scores_desc(S.scores.p, S.sorted_scores.p, S.order.p, S.sorted_order.p, actions, S.sort_temp.p,
+                                   bytes, st));
+        const uint32_t remaining = faces - target;
+        bool accepted = false;
+        blitz_collapse chosen{};
+        for (uint32_t position = 0; position < actions && trials < budget && !accepted;) {
+            const uint32_t n = std::min(window, actions - position);
+            S.collapse_dev.ensure(S.pool, n);
+            S.verdict_dev.ensure(S.pool, size_t(n) * sizeof(blitz_candidate_verdict));
+            launch_gather_window(t.edits.p, S.sorted_order.p, position, n, S.collapse_dev.p, st);
+            auto* vd = reinterpret_cast<blitz_candidate_verdict*>(S.verdict_dev.p);
+            audit_candidates(S, S.collapse_dev.p, nullptr, n, gates, vd, nullptr, st);
+            audited += n;
+            hv.resize(n);
+            hc.resize(n);
+            B200_CUDA(cudaMemcpyAsync(hv.data(), vd, n * sizeof(blitz_candidate_verdict), cudaMemcpyDeviceToHost, st));
+            B200_CUDA(cudaMemcpyAsync(hc.data(), S.collapse_dev.p, n * sizeof(blitz_collapse), cudaMemcpyDeviceToHost, st));
+            B200_CUDA(cudaStreamSynchronize(st));
+            for (uint32_t k = 0; k < n && trials < budget; ++k) {
+                if (hv[k].removed > remaining) continue;
+                ++trials;
+                if (hv[k].accepted) {
+                    accepted = true;
+                    chosen = hc[k];
+                    break;
+                }
+            }
+            position += n;
+            if (!accepted) window = std::min<uint32_t>(window * 2, 8192);
+        }
+        if (!accepted) {
+            reason = trials >= budget ? 1 : 3;
+            break;
+        }
+        if (commits < capacity && commits_out) {
+            commits_out[2 * commits] = chosen.from;
+            commits_out[2 * commits + 1] = chosen.to;
+        }
+        ++commits;
+        commit_collapse(S, chosen);
+        window = std::max<uint32_t>(32, window / 2);
+    }
+    out.commits = commits;
+    out.trials = trials;
+    out.final_faces = S.state_faces;
+    out.audited = audited;
+    out.stop_reason = reason;
+}
+
 } // namespace b200
 
 // ---------------------------------------------------------------------------
@@ -897,7 +1111,9 @@ blitz_status blitz_audit_session_create(const blitz_mesh* source, const blitz_ne
         S.bounds = b;
         S.source.upload(S.pool, S.source_h, S.stream);
         S.state.upload(S.pool, S.source_h, S.stream);
-        build_topology(S);
+        S.state_faces = S.state.view.nf;
+        init_topology(S);
+        rebuild_topology(S);
         *out = session.release();
     });
 }
@@ -1084,6 +1300,53 @@ blitz_status blitz_audit_candidates(blitz_audit_session* s, const blitz_collapse
         B200_CUDA(cudaStreamSynchronize(S.stream));
         for (size_t i = 0; i < n; ++i) out[i].accepted ? ++S.info.legal_collapses : ++S.info.rejected_collapses;
         S.info.gpu_audit_ns += now_ns() - t0;
+    });
+}
+
+blitz_status blitz_audit_execute(blitz_audit_session* s, uint32_t target_faces, uint32_t trial_budget,
+                                 const blitz_eval_settings gates[4], uint32_t* commits_from_to, size_t capacity,
+                                 blitz_audit_execution* out, char* error, size_t cap) {
+    return guarded(error, cap, [&] {
+        if (!s || !gates || !out || out->struct_size != sizeof(*out))
+            throw Failure(BLITZ_INVALID_ARGUMENT, "null argument or bad execution descriptor");
+        Session& S = s->s;
+        DeviceScope scope(S.device);
+        if (S.options.preserve_uv && !S.source_h.uv.empty())
+            throw Failure(BLITZ_UNAVAILABLE, "uv transport on the candidate path is not implemented");
+        for (int g = 0; g < 4; ++g) gate_of(&gates[g], S.bounds);
+        uint64_t t0 = now_ns();
+        blitz_audit_execution r{};
+        r.struct_size = sizeof(r);
+        execute(S, target_faces, trial_budget, gates, commits_from_to, capacity, r);
+        *out = r;
+        S.info.gpu_audit_ns += now_ns() - t0;
+        S.info.legal_collapses += r.commits;
+        S.info.rejected_collapses += r.trials - r.commits;
+    });
+}
+
+blitz_status blitz_audit_state(blitz_audit_session* s, uint32_t* indices, size_t index_capacity, float* positions,
+                               size_t position_capacity, uint32_t* face_count, char* error, size_t cap) {
+    return guarded(error, cap, [&] {
+        if (!s || !face_count) throw Failure(BLITZ_INVALID_ARGUMENT, "null argument");
+        Session& S = s->s;
+        DeviceScope scope(S.device);
+        const DevMesh& m = S.state.view;
+        *face_count = S.state_faces;
+        if (indices && index_capacity >= size_t(S.state_faces) * 3)
+            B200_CUDA(cudaMemcpyAsync(indices, m.idx, size_t(S.state_faces) * 12, cudaMemcpyDeviceToHost, S.stream));
+        if (positions && position_capacity >= size_t(m.nv) * 3)
+            B200_CUDA(cudaMemcpyAsync(positions, m.pos, size_t(m.nv) * 12, cudaMemcpyDeviceToHost, S.stream));
+        B200_CUDA(cudaStreamSynchronize(S.stream));
+    });
+}
+
+blitz_status blitz_audit_reset(blitz_audit_session* s, char* error, size_t cap) {
+    return guarded(error, cap, [&] {
+        if (!s) throw Failure(BLITZ_INVALID_ARGUMENT, "null session");
+        Session& S = s->s;
+        DeviceScope scope(S.device);
+        reset_state(S);
     });
 }
 

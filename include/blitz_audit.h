@@ -215,6 +215,33 @@ blitz_status blitz_audit_candidates_device(blitz_audit_session*, const blitz_col
                                            blitz_measurement* measurements_device, void* stream,
                                            char* error, size_t error_capacity);
 
+/* Result of blitz_audit_execute (mirrors neural::ActionStats, action.hpp). */
+typedef struct blitz_audit_execution {
+    uint32_t struct_size;
+    uint32_t commits;     /* accepted collapses */
+    uint32_t trials;      /* audited trials, as counted by the reference executor */
+    uint32_t final_faces;
+    uint64_t audited;     /* candidates audited, speculative windows included */
+    uint8_t stop_reason;  /* 0 target reached, 1 trial budget, 2 no legal actions, 3 no accepted action */
+    uint8_t reserved[7];
+} blitz_audit_execution;
+
+/* Greedy LOD step on the session's current state, batches of one, ShortestEdge
+ * ranking, midpoint placement: the reference's GpuActionState::execute
+ * (action_gpu.cu:1947-2086) / execute_actions (action.cpp:453-525) with the
+ * four-gate gate of generate.cpp:365-388 against the source and the bound
+ * previous LOD. Writes the accepted (from, to) pairs in order (up to
+ * `commit_capacity`). The state keeps the result; blitz_audit_state reads it. */
+blitz_status blitz_audit_execute(blitz_audit_session*, uint32_t target_faces, uint32_t trial_budget,
+                                 const blitz_eval_settings gates[4], uint32_t* commits_from_to,
+                                 size_t commit_capacity, blitz_audit_execution* out, char* error,
+                                 size_t error_capacity);
+/* Current state: compacted indices (3 per face) and every vertex slot's position. */
+blitz_status blitz_audit_state(blitz_audit_session*, uint32_t* indices, size_t index_capacity, float* positions,
+                               size_t position_capacity, uint32_t* face_count, char* error, size_t error_capacity);
+/* Restores the state to the source (GpuActionState::reset, action_gpu.cu:1884-1906). */
+blitz_status blitz_audit_reset(blitz_audit_session*, char* error, size_t error_capacity);
+
 /* Device-side profile of the session's own kernels (no reference
  * counterpart; the reference exposes NVTX ranges, timeline.hpp:6-19). When
  * enabled, every candidate call times its kernels with CUDA events on the

@@ -414,12 +414,14 @@ std::vector<uint32_t> weld(const bo_mesh& m, bool with_uv) {
     return root;
 }
 
-// action.cpp:49-145 on the given class ids.
-Topology build_topology(const bo_mesh& m, bool preserve_uv) {
+// action.cpp:49-145 on the given class ids. The executor keeps the classes of
+// the episode's initial mesh across commits (action_gpu.cu:1520-1527 welds once
+// at construction); pass them in `classes`.
+Topology build_topology(const bo_mesh& m, bool preserve_uv, const Topology* classes = nullptr) {
     Topology t;
     t.n = m.vertex_count;
-    t.geometry = weld(m, false);
-    t.canonical = weld(m, preserve_uv);
+    t.geometry = classes ? classes->geometry : weld(m, false);
+    t.canonical = classes ? classes->canonical : weld(m, preserve_uv);
     const uint32_t n = t.n;
     t.offsets.assign(n + 1, 0);
     t.face_offsets.assign(n + 1, 0);
@@ -830,6 +832,58 @@ bo_mesh trial_view(const bo_mesh& m, const Trial& tr) {
     return v;
 }
 
+// Four gates on a built trial (generate.cpp:365-388).
+bool audit_gates(const bo_mesh& cand, const bo_mesh& source, const bo_mesh& previous, const bo_bounds& b,
+                 const bo_eval_settings gates[4], bo_verdict* out) {
+    for (int g = 0; g < 4; ++g) {
+        bo_eval_settings s = gates[g];
+        uint64_t side = uint64_t(std::ceil(s.screen_size + 8));
+        unsigned ss = s.supersample;
+        while (ss < s.max_supersample) { // graph.cpp:5-18
+            unsigned next = std::min<unsigned>(ss * 2, s.max_supersample);
+            if (side * side * next * next > kMaxSamples) break;
+            ss = next;
+        }
+        s.max_supersample = uint8_t(ss);
+        const bo_mesh& ref = (g % 2) ? previous : source;
+        bo_measurement m = evaluate(ref, cand, b, s);
+        if (out) out->gates[g] = m;
+        if (!measurement_passed(m)) {
+            if (out) out->failed_gate = uint8_t(g + 1);
+            return false;
+        }
+    }
+    if (out) out->accepted = 1;
+    return true;
+}
+
+// Working state of the greedy executor: owned streams of the current LOD.
+struct ExecState {
+    std::vector<float> pos, uv;
+    std::vector<uint32_t> idx;
+    std::vector<uint16_t> mat;
+    std::vector<uint8_t> sided;
+    bo_mesh view() const {
+        bo_mesh m{};
+        m.positions = pos.data();
+        m.vertex_count = uint32_t(pos.size() / 3);
+        m.indices = idx.data();
+        m.face_count = uint32_t(idx.size() / 3);
+        m.materials = mat.empty() ? nullptr : mat.data();
+        m.double_sided = sided.empty() ? nullptr : sided.data();
+        m.double_sided_count = uint32_t(sided.size());
+        m.uv = uv.empty() ? nullptr : uv.data();
+        return m;
+    }
+};
+
+// ShortestEdge ranking of rank_actions (action_gpu.cu:822-825): minus the edge
+// length over the origin diameter, with float rounding of the scaled delta.
+float shortest_edge_score(const bo_mesh& m, const bo_edit& e, double diameter) {
+    V3 d = scale3(sub(load3(m.positions, e.to), load3(m.positions, e.from)), 1 / diameter);
+    return -float(length(d));
+}
+
 template <class F> int guarded(F f) {
     try {
         f();
@@ -1008,6 +1062,89 @@ int64_t bo_trial_midpoint(const bo_mesh* m, const bo_edit* e, int preserve_uv, u
         faces = int64_t(tr.indices.size() / 3);
     });
     return status ? -1 : faces;
+}
+
+// Greedy executor with batches of one (execute_actions, action.cpp:453-525;
+// GpuActionState::execute, action_gpu.cu:1947-2086): rank the legal midpoint
+// collapses (ShortestEdge), walk them in rank order skipping those that would
+// remove more faces than remain above target, audit each through the four
+// gates against source and previous, commit the first accepted, re-rank; stop
+// at the target, the trial budget, no legal action or no accepted action.
+// stop: 0 target reached, 1 trial budget, 2 no legal actions, 3 no accepted action.
+int bo_execute(const bo_mesh* source, const bo_mesh* previous, uint32_t target, uint32_t budget,
+               const bo_eval_settings gates[4], int preserve_uv, uint32_t* commits_from_to, uint32_t capacity,
+               uint32_t* commits, uint32_t* trials, uint32_t* out_indices, uint32_t* out_faces, float* out_positions,
+               uint8_t* stop) {
+    return guarded([&] {
+        ExecState st;
+        st.pos.assign(source->positions, source->positions + size_t(source->vertex_count) * 3);
+        st.idx.assign(source->indices, source->indices + size_t(source->face_count) * 3);
+        if (source->materials) st.mat.assign(source->materials, source->materials + source->face_count);
+        if (source->double_sided) st.sided.assign(source->double_sided, source->double_sided + source->double_sided_count);
+        if (source->uv) st.uv.assign(source->uv, source->uv + size_t(source->vertex_count) * 2);
+        bo_bounds b{};
+        bo_bounds_of(source, &b);
+        const double diameter = std::max(1e-20, b.radius * 2);
+        const bo_mesh& prev = previous ? *previous : *source;
+        const Topology classes = build_topology(*source, preserve_uv != 0);
+        const bo_mesh original = *source;
+        target = std::max<uint32_t>(1, target);
+        uint32_t n_commits = 0, n_trials = 0;
+        uint8_t reason = 3;
+        for (;;) {
+            bo_mesh m = st.view();
+            if (m.face_count <= target) {
+                reason = 0;
+                break;
+            }
+            if (n_trials >= budget) {
+                reason = 1;
+                break;
+            }
+            Topology t = build_topology(m, preserve_uv != 0, &classes);
+            std::vector<bo_edit> edits = enumerate(m, t, true, preserve_uv != 0);
+            if (edits.empty()) {
+                reason = 2;
+                break;
+            }
+            std::vector<float> scores(edits.size());
+            for (size_t i = 0; i < edits.size(); ++i) scores[i] = shortest_edge_score(m, edits[i], diameter);
+            std::vector<uint32_t> order(edits.size());
+            std::iota(order.begin(), order.end(), 0);
+            std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t c) { return scores[a] > scores[c]; });
+            const uint32_t remaining = m.face_count - target;
+            bool accepted = false;
+            for (size_t pos = 0; pos < order.size() && n_trials < budget && !accepted; ++pos) {
+                const bo_edit& e = edits[order[pos]];
+                if (e.removed > remaining) continue;
+                Trial tr = make_trial(m, t, original, classes, e, preserve_uv != 0);
+                ++n_trials;
+                if (!tr.valid) continue;
+                bo_mesh cand = trial_view(m, tr);
+                if (!audit_gates(cand, *source, prev, b, gates, nullptr)) continue;
+                if (n_commits < capacity) {
+                    commits_from_to[2 * n_commits] = e.from;
+                    commits_from_to[2 * n_commits + 1] = e.to;
+                }
+                ++n_commits;
+                st.idx = tr.indices;
+                st.pos = tr.positions;
+                if (!st.mat.empty()) st.mat = tr.materials;
+                if (!st.uv.empty()) st.uv = tr.uv;
+                accepted = true;
+            }
+            if (!accepted) {
+                reason = n_trials >= budget ? 1 : 3;
+                break;
+            }
+        }
+        *commits = n_commits;
+        *trials = n_trials;
+        *out_faces = uint32_t(st.idx.size() / 3);
+        std::copy(st.idx.begin(), st.idx.end(), out_indices);
+        std::copy(st.pos.begin(), st.pos.end(), out_positions);
+        *stop = reason;
+    });
 }
 
 // Four-gate acceptance of one candidate (generate.cpp:365-388, chain.cpp:470-483):

@@ -123,6 +123,14 @@ int bo_audit_candidate(const bo_mesh* parent, const bo_edit* e, const bo_mesh* s
                        const bo_mesh* previous, const bo_bounds* b, const bo_eval_settings gates[4],
                        int preserve_uv, bo_verdict* out);
 
+/* Greedy executor, batches of one, ShortestEdge ranking, midpoint placement
+ * (action.cpp:453-525). previous may be NULL (= source). Returns 0 on success;
+ * *stop: 0 target reached, 1 trial budget, 2 no legal actions, 3 no accepted. */
+int bo_execute(const bo_mesh* source, const bo_mesh* previous, uint32_t target, uint32_t budget,
+               const bo_eval_settings gates[4], int preserve_uv, uint32_t* commits_from_to, uint32_t capacity,
+               uint32_t* commits, uint32_t* trials, uint32_t* out_indices, uint32_t* out_faces,
+               float* out_positions, uint8_t* stop);
+
 #ifdef __cplusplus
 }
 #endif

@@ -143,6 +143,29 @@ class Oracle:
         assert self.lib.bo_bounds_of(C.byref(h.c), C.byref(b)) == 0
         return b
 
+    def execute(self, source, target: int, budget: int, gates, previous=None, preserve_uv=True) -> dict:
+        """Greedy executor (batches of one, ShortestEdge, midpoint placement)."""
+        L = self.lib
+        P = C.POINTER
+        L.bo_execute.argtypes = [P(BoMesh), P(BoMesh), C.c_uint32, C.c_uint32, P(BoEvalSettings), C.c_int,
+                                 C.c_void_p, C.c_uint32, P(C.c_uint32), P(C.c_uint32), C.c_void_p, P(C.c_uint32),
+                                 C.c_void_p, P(C.c_uint8)]
+        hs = _MeshHold(source)
+        hp = None if previous is None else _MeshHold(previous)
+        cap = source.face_count
+        ft = np.zeros(2 * cap, np.uint32)
+        idx = np.zeros(source.face_count * 3, np.uint32)
+        pos = np.zeros((source.vertex_count, 3), np.float32)
+        commits, trials, faces, stop = C.c_uint32(), C.c_uint32(), C.c_uint32(), C.c_uint8()
+        g = (BoEvalSettings * 4)(*gates)
+        st = L.bo_execute(C.byref(hs.c), None if hp is None else C.byref(hp.c), target, budget, g, int(preserve_uv),
+                          ft.ctypes.data, cap, C.byref(commits), C.byref(trials), idx.ctypes.data, C.byref(faces),
+                          pos.ctypes.data, C.byref(stop))
+        assert st == 0
+        n = commits.value
+        return {"commits": ft[: 2 * n].reshape(-1, 2), "trials": trials.value, "stop": stop.value,
+                "indices": idx[: 3 * faces.value].copy(), "positions": pos}
+
     def cameras(self, b: BoBounds, screen: float, views: tuple) -> list:
         n = views[0] + views[1]
         out = (BoCamera * n)()

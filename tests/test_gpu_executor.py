@@ -1,0 +1,67 @@
+"""GPU greedy executor against the oracle executor, and candidate audits of a
+state that differs from its references (the tile-maxima path)."""
+import numpy as np
+import pytest
+
+import blitzremesher_b200 as br
+from blitzremesher_b200 import synthetic as syn
+from oracle.oracle import BoEdit, settings as oracle_settings
+
+from conftest import measurement_fields
+
+pytestmark = pytest.mark.gpu
+
+CASES = {
+    "sphere2_96": (lambda: syn.noisy_icosphere(2, 3), (6, 2, 5), 16.0, 4, 200),
+    "sphere3_256": (lambda: syn.noisy_icosphere(3, 4), (8, 0, 0xB1172026), 24.0, 8, 160),
+}
+
+
+def _gates(screen, views, ss):
+    return [(screen, 2.0, views, ss, ss, 1.0), (screen, 1.0, views, ss, ss, 1.0),
+            (screen, 2.0, views, ss, ss, 0.5), (screen, 1.0, views, ss, ss, 0.5)]
+
+
+@pytest.mark.parametrize("case", sorted(CASES))
+def test_executor_matches_oracle(gpu_lib, oracle, case):
+    make, views, screen, ss, budget = CASES[case]
+    mesh = make()
+    args = _gates(screen, views, ss)
+    target = mesh.face_count // 2
+    want = oracle.execute(mesh, target, budget, [oracle_settings(*a) for a in args])
+    with br.AuditSession(mesh) as s:
+        got = s.execute(target, budget, [br.eval_settings(*a) for a in args])
+        idx, pos = s.state()
+        # The same walk again from the source gives the same result.
+        s.reset()
+        again = s.execute(target, budget, [br.eval_settings(*a) for a in args])
+    assert len(want["commits"]) > 5
+    assert np.array_equal(got["commits"], want["commits"])
+    assert got["trials"] == want["trials"] and got["stop"] == want["stop"]
+    assert np.array_equal(idx, want["indices"])
+    assert np.array_equal(pos, want["positions"])
+    assert np.array_equal(again["commits"], got["commits"]) and again["trials"] == got["trials"]
+
+
+def test_candidates_of_committed_state_match_oracle(gpu_lib, oracle):
+    """After commits the state differs from both references: every gate
+    Measurement of a candidate sample still equals the oracle's."""
+    mesh = syn.noisy_icosphere(3, 9)
+    views = (8, 4, 77)
+    args = _gates(24.0, views, 8)
+    with br.AuditSession(mesh) as s:
+        s.execute(mesh.face_count - 60, 400, [br.eval_settings(*a) for a in args])
+        idx, pos = s.state()
+        cands = br.midpoint_collapses(s.actions())
+        picks = cands[:: max(1, cands.size // 40)]
+        verdicts, meas = s.candidates(picks, [br.eval_settings(*a) for a in args], measurements=True)
+    state = syn.Mesh(pos, idx)
+    b = oracle.bounds(mesh)
+    for i, c in enumerate(picks):
+        e = BoEdit()
+        e.from_, e.to = int(c["from"]), int(c["to"])
+        want = oracle.audit_candidate(state, e, mesh, mesh, b, [oracle_settings(*a) for a in args])
+        assert verdicts[i]["accepted"] == want.accepted and verdicts[i]["failed_gate"] == want.failed_gate, i
+        stop = 4 if want.failed_gate == 0 else (want.failed_gate if want.failed_gate <= 4 else 0)
+        for g in range(stop):
+            assert measurement_fields(meas[i, g]) == measurement_fields(want.gates[g]), (i, g)
