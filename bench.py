@@ -312,6 +312,19 @@ def run_gpu(args) -> None:
             "gpu_launches": int(prof["launches"] // max(1, args.steps) * args.steps),
             "kernel_ms": {"prepare": prof["prepare_ms"] / args.steps, "audit": prof["audit_ms"] / args.steps,
                           "verdicts": prof["verdict_ms"] / args.steps}}
+    # LOD-chain step: the greedy executor from the source to 50% of its faces.
+    if not args.no_chain:
+        session.reset()
+        torch.cuda.synchronize(device)
+        t0 = time.perf_counter()
+        chain = session.execute(mesh.face_count // 2, 1 << 30, gates)
+        torch.cuda.synchronize(device)
+        chain_s = time.perf_counter() - t0
+        line["chain"] = {"metric": "LOD-chain s/mesh", "seconds": chain_s, "unit": "s/mesh",
+                         "step": "one LOD step to 50% faces", "commits": int(len(chain["commits"])),
+                         "trials": int(chain["trials"]), "audited": int(chain["audited"]),
+                         "final_faces": int(chain["final_faces"]), "stop": int(chain["stop"]),
+                         "timing": "wall clock around the host-orchestrated executor"}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         r = cpu_reference_sample(args.cpu_sample, 1, 1)
         line["cpu_baseline"] = {"value": r["candidates"] / r["busy_s"], "unit": "collapses/s", "cores": 1,
@@ -336,6 +349,7 @@ def main() -> None:
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-sample", type=int, default=32)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-chain", action="store_true")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

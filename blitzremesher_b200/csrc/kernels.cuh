@@ -114,6 +114,17 @@ void launch_tile_maxima(const uint32_t* ref_bits, const uint32_t* state_bits, co
                         const uint32_t* state_field, uint32_t size, int32_t* t1, int32_t* t2, cudaStream_t s);
 void launch_field(const uint32_t* bits, uint32_t width, uint32_t height, uint32_t* g, uint32_t* d2, int32_t* stack_v,
                   long long* stack_num, long long* stack_den, cudaStream_t s);
+// State data of `nviews` consecutive views of a size x size plan in one pass:
+// per-sample face counts (stride cstride), raster state {-, -, clipped faces,
+// count overflow} per view, coverage words (stride wstride; skipped when
+// state_bits is null), popcounts {changed, total, ref, state} against
+// ref_bits and, when state_field is given, the exact state field and the
+// 32x32 tile maxima. g/sv/sn/sd hold nviews x size^2 entries.
+void launch_refresh_views(const DevMesh& m, const Camera* cams_dev, uint32_t nviews, const float* center, uint32_t ss,
+                          uint32_t size, bool force_two, uint8_t* counts, size_t cstride, uint32_t* state,
+                          uint32_t* state_bits, const uint32_t* ref_bits, uint32_t wstride,
+                          unsigned long long* pop, const uint32_t* ref_field, uint32_t* state_field, uint32_t* g,
+                          int32_t* sv, long long* sn, long long* sd, int32_t* t1, int32_t* t2, cudaStream_t s);
 // ShortestEdge scores of the legal edits (action_gpu.cu:822-825), keys for a
 // stable descending sort.
 void launch_rank_shortest(const DevMesh& m, const Edit* edits, const uint32_t* count, uint32_t capacity,

@@ -102,9 +102,12 @@ __global__ void k_popcounts(const uint32_t* a, const uint32_t* b, uint32_t words
 __device__ __forceinline__ bool bit_at(const uint32_t* bits, size_t i) { return (bits[i >> 5] >> (i & 31)) & 1u; }
 
 // Horizontal distance to the nearest covered sample of each row (INF if none).
+__device__ void k_row_nearest_body(const uint32_t* to, uint32_t width, uint32_t y, uint32_t* g);
 __global__ void k_row_nearest(const uint32_t* to, uint32_t width, uint32_t height, uint32_t* g) {
     uint32_t y = blockIdx.x * blockDim.x + threadIdx.x;
-    if (y >= height) return;
+    if (y < height) k_row_nearest_body(to, width, y, g);
+}
+__device__ void k_row_nearest_body(const uint32_t* to, uint32_t width, uint32_t y, uint32_t* g) {
     size_t row = size_t(y) * width;
     uint32_t last = kNone;
     for (uint32_t x = 0; x < width; ++x) {
@@ -121,10 +124,15 @@ __global__ void k_row_nearest(const uint32_t* to, uint32_t width, uint32_t heigh
 // Lower envelope of the parabolas (y-q)^2 + g(x,q)^2 over rows q with a site
 // (Felzenszwalb–Huttenlocher), in exact integer arithmetic: intersections are
 // kept as fractions and compared by cross-multiplication.
+__device__ void k_column_envelope_body(const uint32_t* g, uint32_t width, uint32_t height, uint32_t x, uint32_t* d2,
+                                       int32_t* sv, long long* snum, long long* sden);
 __global__ void k_column_envelope(const uint32_t* g, uint32_t width, uint32_t height, uint32_t* d2, int32_t* sv,
                                   long long* snum, long long* sden) {
     uint32_t x = blockIdx.x * blockDim.x + threadIdx.x;
-    if (x >= width) return;
+    if (x < width) k_column_envelope_body(g, width, height, x, d2, sv, snum, sden);
+}
+__device__ void k_column_envelope_body(const uint32_t* g, uint32_t width, uint32_t height, uint32_t x, uint32_t* d2,
+                                       int32_t* sv, long long* snum, long long* sden) {
     const uint32_t size = width; // row stride of g and d2
     int32_t* v = sv + size_t(x) * height;
     long long* zn = snum + size_t(x) * height;
@@ -220,10 +228,16 @@ __global__ void k_counts_to_bits(const uint8_t* counts, size_t samples, uint32_t
 // Per 32x32 tile: t1 = max reference field over samples covered by the state
 // and not by the reference; t2 = max state field over samples covered by the
 // reference and not by the state; -1 when the tile has no such sample.
+__device__ void tile_maxima_body(const uint32_t* ref_bits, const uint32_t* state_bits, const uint32_t* ref_field,
+                                 const uint32_t* state_field, uint32_t size, uint32_t tile, int32_t* t1, int32_t* t2);
 __global__ void k_tile_maxima(const uint32_t* ref_bits, const uint32_t* state_bits, const uint32_t* ref_field,
                               const uint32_t* state_field, uint32_t size, int32_t* t1, int32_t* t2) {
+    tile_maxima_body(ref_bits, state_bits, ref_field, state_field, size, blockIdx.x, t1, t2);
+}
+__device__ void tile_maxima_body(const uint32_t* ref_bits, const uint32_t* state_bits, const uint32_t* ref_field,
+                                 const uint32_t* state_field, uint32_t size, uint32_t tile, int32_t* t1, int32_t* t2) {
     const uint32_t tiles_x = (size + 31) / 32;
-    const uint32_t tile = blockIdx.x, lane = threadIdx.x;
+    const uint32_t lane = threadIdx.x;
     const uint32_t tx = tile % tiles_x, ty = tile / tiles_x;
     const uint32_t x = tx * 32 + lane;
     int32_t m1 = -1, m2 = -1;
@@ -242,7 +256,145 @@ __global__ void k_tile_maxima(const uint32_t* ref_bits, const uint32_t* state_bi
     }
     if (lane == 0) t1[tile] = m1, t2[tile] = m2;
 }
+// ---- all views of a plan in one launch (blockIdx.y = view) ----
+struct ViewsArgs {
+    DevMesh m;
+    const Camera* cams;
+    float center[3];
+    uint32_t ss, size, force_two, pad;
+};
+
+__device__ FaceSetup face_setup_view(const ViewsArgs& a, const Camera& cam, uint32_t f) {
+    Proj p[3];
+    for (int j = 0; j < 3; ++j) {
+        uint32_t v = a.m.idx[3 * f + j];
+        p[j] = project(a.m.pos[3 * v], a.m.pos[3 * v + 1], a.m.pos[3 * v + 2], a.center, cam, a.ss, a.size);
+    }
+    bool two = a.force_two;
+    if (!two && a.m.sided) {
+        uint16_t mat = a.m.mat ? a.m.mat[f] : 0;
+        two = mat < a.m.nsided && a.m.sided[mat];
+    }
+    return setup_face(p[0], p[1], p[2], cam.perspective != 0, two, a.size);
+}
+
+// Face counts of every view: state[4v+2] clipped faces, state[4v+3] overflow.
+__global__ void k_count_views(ViewsArgs a, uint8_t* counts, size_t stride, uint32_t* state) {
+    const uint32_t f = blockIdx.x * blockDim.x + threadIdx.x, v = blockIdx.y;
+    if (f >= a.m.nf) return;
+    const Camera cam = a.cams[v];
+    FaceSetup s = face_setup_view(a, cam, f);
+    uint32_t* st = state + 4 * v;
+    if (s.status == kFaceClipBox || s.status == kFaceClipZ) {
+        atomicAdd(st + 2, 1u);
+        return;
+    }
+    if (s.status != kFaceOk) return;
+    uint8_t* c = counts + stride * v;
+    for (int y = s.y0; y <= s.y1; ++y)
+        for (int x = s.x0; x <= s.x1; ++x)
+            if (face_covers(s, x, y)) count_sample(c, size_t(y) * a.size + x, st);
+}
+__global__ void k_counts_to_bits_views(const uint8_t* counts, size_t cstride, size_t samples, uint32_t* bits,
+                                       uint32_t wstride, uint32_t words) {
+    const uint32_t w = blockIdx.x * blockDim.x + threadIdx.x, v = blockIdx.y;
+    if (w >= words) return;
+    const uint8_t* c = counts + cstride * v;
+    uint32_t out = 0;
+    const size_t base = size_t(w) * 32;
+    for (int k = 0; k < 32; ++k) {
+        size_t i = base + k;
+        if (i < samples && c[i]) out |= 1u << k;
+    }
+    bits[size_t(wstride) * v + w] = out;
+}
+__global__ void k_row_nearest_views(const uint32_t* bits, uint32_t wstride, uint32_t size, uint32_t* g) {
+    const uint32_t y = blockIdx.x * blockDim.x + threadIdx.x, v = blockIdx.y;
+    if (y >= size) return;
+    const size_t samples = size_t(size) * size;
+    k_row_nearest_body(bits + size_t(wstride) * v, size, y, g + samples * v);
+}
+__global__ void k_column_envelope_views(const uint32_t* g, uint32_t size, uint32_t* d2, int32_t* sv, long long* sn,
+                                        long long* sd) {
+    const uint32_t x = blockIdx.x * blockDim.x + threadIdx.x, v = blockIdx.y;
+    if (x >= size) return;
+    const size_t samples = size_t(size) * size;
+    k_column_envelope_body(g + samples * v, size, size, x, d2 + samples * v, sv + samples * v, sn + samples * v,
+                           sd + samples * v);
+}
+__global__ void k_tile_maxima_views(const uint32_t* ref_bits, const uint32_t* state_bits, uint32_t wstride,
+                                    const uint32_t* ref_field, const uint32_t* state_field, uint32_t size, int32_t* t1,
+                                    int32_t* t2) {
+    const uint32_t v = blockIdx.y, tiles_x = (size + 31) / 32, tiles = tiles_x * tiles_x;
+    const size_t samples = size_t(size) * size;
+    tile_maxima_body(ref_bits + size_t(wstride) * v, state_bits + size_t(wstride) * v, ref_field + samples * v,
+                     state_field + samples * v, size, blockIdx.x, t1 + size_t(tiles) * v, t2 + size_t(tiles) * v);
+}
+__global__ void k_popcounts_views(const uint32_t* a, const uint32_t* b, uint32_t wstride, uint32_t words,
+                                  unsigned long long* out) {
+    const uint32_t v = blockIdx.y;
+    unsigned long long changed = 0, total = 0, ca = 0, cb = 0;
+    const uint32_t* av = a + size_t(wstride) * v;
+    const uint32_t* bv = b + size_t(wstride) * v;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < words; i += gridDim.x * blockDim.x) {
+        uint32_t x = av[i], y = bv[i];
+        changed += __popc(x ^ y);
+        total += __popc(x | y);
+        ca += __popc(x);
+        cb += __popc(y);
+    }
+    for (int o = 16; o; o >>= 1) {
+        changed += __shfl_down_sync(0xffffffffu, changed, o);
+        total += __shfl_down_sync(0xffffffffu, total, o);
+        ca += __shfl_down_sync(0xffffffffu, ca, o);
+        cb += __shfl_down_sync(0xffffffffu, cb, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        unsigned long long* o = out + 4 * v;
+        if (changed) atomicAdd(o, changed);
+        if (total) atomicAdd(o + 1, total);
+        if (ca) atomicAdd(o + 2, ca);
+        if (cb) atomicAdd(o + 3, cb);
+    }
+}
 } // namespace
+
+// The state data of all views of a plan, refreshed in a handful of launches:
+// counts (and clipped/overflow counters), coverage words, popcounts against the
+// reference and, when fields are kept, the state field and tile maxima.
+void launch_refresh_views(const DevMesh& m, const Camera* cams_dev, uint32_t nviews, const float* center, uint32_t ss,
+                          uint32_t size, bool force_two, uint8_t* counts, size_t cstride, uint32_t* state,
+                          uint32_t* state_bits, const uint32_t* ref_bits, uint32_t wstride,
+                          unsigned long long* pop, const uint32_t* ref_field, uint32_t* state_field, uint32_t* g,
+                          int32_t* sv, long long* sn, long long* sd, int32_t* t1, int32_t* t2, cudaStream_t s) {
+    ViewsArgs a;
+    a.m = m;
+    a.cams = cams_dev;
+    a.center[0] = center[0], a.center[1] = center[1], a.center[2] = center[2];
+    a.ss = ss, a.size = size, a.force_two = force_two, a.pad = 0;
+    const size_t samples = size_t(size) * size;
+    cudaMemsetAsync(counts, 0, cstride * nviews, s);
+    cudaMemsetAsync(state, 0, 16 * size_t(nviews), s);
+    if (m.nf) k_count_views<<<dim3(blocks_for(m.nf, 128), nviews), 128, 0, s>>>(a, counts, cstride, state);
+    const uint32_t words = uint32_t((samples + 63) / 64) * 2;
+    if (state_bits) {
+        k_counts_to_bits_views<<<dim3(blocks_for(words), nviews), kThreads, 0, s>>>(counts, cstride, samples,
+                                                                                     state_bits, wstride, words);
+        if (state_field) {
+            k_row_nearest_views<<<dim3(blocks_for(size, 64), nviews), 64, 0, s>>>(state_bits, wstride, size, g);
+            k_column_envelope_views<<<dim3(blocks_for(size, 64), nviews), 64, 0, s>>>(g, size, state_field, sv, sn,
+                                                                                       sd);
+            const uint32_t tiles = ((size + 31) / 32) * ((size + 31) / 32);
+            k_tile_maxima_views<<<dim3(tiles, nviews), 32, 0, s>>>(ref_bits, state_bits, wstride, ref_field,
+                                                                   state_field, size, t1, t2);
+        }
+    }
+    cudaMemsetAsync(pop, 0, 32 * size_t(nviews), s);
+    uint32_t grid = blocks_for(words);
+    if (grid > 64) grid = 64;
+    k_popcounts_views<<<dim3(grid, nviews), kThreads, 0, s>>>(ref_bits, state_bits ? state_bits : ref_bits, wstride,
+                                                               words, pop);
+}
 
 void launch_counts_to_bits(const uint8_t* counts, uint32_t size, uint32_t* bits, cudaStream_t s) {
     size_t samples = size_t(size) * size;

@@ -316,6 +316,10 @@ struct Plan {
     bool state_is_ref = true;
     uint64_t state_revision = ~0ull;
     Buf<ViewRecord> records;
+    Buf<uint32_t> raster_state;      // 4 words per view
+    Buf<unsigned long long> pop;     // 4 counts per view
+    std::vector<uint32_t> hstate;
+    std::vector<unsigned long long> hpop;
     PlanDev dev{};
 };
 
@@ -325,6 +329,11 @@ struct Scratch {
     Buf<long long> sn, sd;
     Buf<unsigned long long> pop;
     size_t samples = 0;
+    // per-view field scratch of the batched state refresh
+    Buf<uint32_t> vg;
+    Buf<int32_t> vsv;
+    Buf<long long> vsn, vsd;
+    size_t view_entries = 0;
 };
 
 struct Session {
@@ -354,6 +363,7 @@ struct Session {
     DeviceMesh trial;
     Buf<uint32_t> trial_keep, trial_offsets;
     Buf<TrialInfo> trial_info;
+    Buf<blitz_collapse> trial_collapse;
     // executor ranking
     Buf<float> scores, sorted_scores;
     Buf<uint32_t> order, sorted_order;
@@ -466,41 +476,54 @@ static void refresh_state(Session& S, Plan& p) {
     const bool ref_is_source = key.reference == 0 || S.previous_is_source;
     p.state_is_ref = S.state_is_source && ref_is_source && !p.ref_box_clip;
     cudaStream_t st = S.stream;
-    B200_CUDA(cudaMemsetAsync(p.state_count.p, 0, cstride * p.views, st));
-    Buf<uint32_t> state(S.pool, 4 * size_t(p.views));
     DevMesh live = S.state.view;
     live.nf = S.state_faces;
-    for (uint32_t v = 0; v < p.views; ++v)
-        raster(S, live, &p.hcams[v], key.ss, p.size, key.force_two, false, nullptr, p.state_count.p + cstride * v,
-               state.p + 4 * v);
     const bool own_bits = p.tiled || !p.state_is_ref;
-    if (own_bits) {
-        if (!p.state_bits.p) p.state_bits = Buf<uint32_t>(S.pool, size_t(p.words) * p.views);
+    if (own_bits && !p.state_bits.p) {
+        // The padding words past the last sample stay zero for good.
+        p.state_bits = Buf<uint32_t>(S.pool, size_t(p.words) * p.views);
         B200_CUDA(cudaMemsetAsync(p.state_bits.p, 0, size_t(p.words) * p.views * 4, st));
-        for (uint32_t v = 0; v < p.views; ++v)
-            launch_counts_to_bits(p.state_count.p + cstride * v, p.size, p.state_bits.p + size_t(p.words) * v, st);
+    }
+    if (!p.raster_state.p) {
+        p.raster_state = Buf<uint32_t>(S.pool, 4 * size_t(p.views));
+        p.pop = Buf<unsigned long long>(S.pool, 4 * size_t(p.views));
+        p.hstate.assign(4 * size_t(p.views), 0);
+        p.hpop.assign(4 * size_t(p.views), 0);
     }
     const uint32_t* sbits = own_bits ? p.state_bits.p : p.ref_bits.p;
-    if (p.tiled && !p.state_is_ref) {
-        ensure_scratch(S, p.size);
-        const uint32_t tiles = ((p.size + 31) / 32) * ((p.size + 31) / 32);
-        for (uint32_t v = 0; v < p.views; ++v) {
-            launch_field(sbits + size_t(p.words) * v, p.size, p.size, S.scratch.g.p, p.state_field.p + samples * v,
-                         S.scratch.sv.p, S.scratch.sn.p, S.scratch.sd.p, st);
-            launch_tile_maxima(p.ref_bits.p + size_t(p.words) * v, sbits + size_t(p.words) * v,
-                               p.ref_field.p + samples * v, p.state_field.p + samples * v, p.size, p.t1.p + tiles * v,
-                               p.t2.p + tiles * v, st);
+    const bool fields = p.tiled && !p.state_is_ref;
+    const uint32_t tiles = ((p.size + 31) / 32) * ((p.size + 31) / 32);
+    // Views per launch: the field scratch of one chunk stays within 256 MiB.
+    uint32_t chunk = p.views;
+    if (fields) {
+        const size_t per_view = samples * 24;
+        chunk = uint32_t(std::max<size_t>(1, std::min<size_t>(p.views, (size_t(256) << 20) / per_view)));
+        Scratch& x = S.scratch;
+        const size_t entries = samples * chunk;
+        if (x.view_entries < entries) {
+            x.vg = Buf<uint32_t>(S.pool, entries);
+            x.vsv = Buf<int32_t>(S.pool, entries);
+            x.vsn = Buf<long long>(S.pool, entries);
+            x.vsd = Buf<long long>(S.pool, entries);
+            x.view_entries = entries;
         }
     }
-    Buf<unsigned long long> pop(S.pool, 4 * size_t(p.views));
-    for (uint32_t v = 0; v < p.views; ++v)
-        launch_popcounts(p.ref_bits.p + size_t(v) * p.words, sbits + size_t(v) * p.words, p.words, pop.p + 4 * v, st);
-    std::vector<unsigned long long> hpop(4 * size_t(p.views));
-    std::vector<uint32_t> hstate(4 * size_t(p.views));
-    B200_CUDA(cudaMemcpyAsync(hpop.data(), pop.p, hpop.size() * 8, cudaMemcpyDeviceToHost, st));
-    B200_CUDA(cudaMemcpyAsync(hstate.data(), state.p, hstate.size() * 4, cudaMemcpyDeviceToHost, st));
+    for (uint32_t v0 = 0; v0 < p.views; v0 += chunk) {
+        const uint32_t n = std::min(chunk, p.views - v0);
+        const size_t w0 = size_t(p.words) * v0, s0 = samples * v0, t0 = size_t(tiles) * v0;
+        launch_refresh_views(live, p.cameras.p + v0, n, S.bounds.center, key.ss, p.size, key.force_two,
+                             p.state_count.p + cstride * v0, cstride, p.raster_state.p + 4 * v0,
+                             own_bits ? p.state_bits.p + w0 : nullptr, p.ref_bits.p + w0, p.words, p.pop.p + 4 * v0,
+                             fields ? p.ref_field.p + s0 : nullptr, fields ? p.state_field.p + s0 : nullptr,
+                             S.scratch.vg.p, S.scratch.vsv.p, S.scratch.vsn.p, S.scratch.vsd.p,
+                             fields ? p.t1.p + t0 : nullptr, fields ? p.t2.p + t0 : nullptr, st);
+    }
+    std::vector<unsigned long long>& hpop = p.hpop;
+    std::vector<uint32_t>& hstate = p.hstate;
+    B200_CUDA(cudaMemcpyAsync(hpop.data(), p.pop.p, hpop.size() * 8, cudaMemcpyDeviceToHost, st));
+    B200_CUDA(cudaMemcpyAsync(hstate.data(), p.raster_state.p, hstate.size() * 4, cudaMemcpyDeviceToHost, st));
     B200_CUDA(cudaStreamSynchronize(st));
-    const uint32_t tiles = ((p.size + 31) / 32) * ((p.size + 31) / 32);
+    B200_CUDA(cudaGetLastError());
     for (uint32_t v = 0; v < p.views; ++v) {
         if (hstate[4 * v + 3]) throw Failure(BLITZ_OUT_OF_MEMORY, "more than 255 faces cover one sample");
         PlanView& pv = p.hviews[v];
@@ -701,6 +724,7 @@ static void ensure_trial_buffers(Session& S) {
     S.trial_keep = Buf<uint32_t>(S.pool, src.nf + 1);
     S.trial_offsets = Buf<uint32_t>(S.pool, src.nf + 1);
     S.trial_info = Buf<TrialInfo>(S.pool, 1);
+    S.trial_collapse = Buf<blitz_collapse>(S.pool, 1);
 }
 
 static void exact_candidate(Session& S, const blitz_collapse& col, const GateRef* gates, int first,
@@ -708,9 +732,8 @@ static void exact_candidate(Session& S, const blitz_collapse& col, const GateRef
     const DevMesh& m = S.state.view;
     Topology& t = S.topo;
     ensure_trial_buffers(S);
-    Buf<blitz_collapse> one(S.pool, 1);
-    B200_CUDA(cudaMemcpyAsync(one.p, &col, sizeof(col), cudaMemcpyHostToDevice, S.stream));
-    launch_trial(m, t.view, one.p, S.trial_info.p, S.trial_keep.p, S.trial_offsets.p, S.trial.idx.p, S.trial.mat.p,
+    B200_CUDA(cudaMemcpyAsync(S.trial_collapse.p, &col, sizeof(col), cudaMemcpyHostToDevice, S.stream));
+    launch_trial(m, t.view, S.trial_collapse.p, S.trial_info.p, S.trial_keep.p, S.trial_offsets.p, S.trial.idx.p, S.trial.mat.p,
                  S.trial.pos.p, t.scan.p, S.stream);
     uint32_t faces = 0;
     B200_CUDA(cudaMemcpyAsync(&faces, S.trial_offsets.p + m.nf, 4, cudaMemcpyDeviceToHost, S.stream));
@@ -857,9 +880,8 @@ static void commit_collapse(Session& S, const blitz_collapse& col) {
     ensure_trial_buffers(S);
     DevMesh& m = S.state.view;
     cudaStream_t st = S.stream;
-    Buf<blitz_collapse> one(S.pool, 1);
-    B200_CUDA(cudaMemcpyAsync(one.p, &col, sizeof(col), cudaMemcpyHostToDevice, st));
-    launch_trial(m, S.topo.view, one.p, S.trial_info.p, S.trial_keep.p, S.trial_offsets.p, S.trial.idx.p,
+    B200_CUDA(cudaMemcpyAsync(S.trial_collapse.p, &col, sizeof(col), cudaMemcpyHostToDevice, st));
+    launch_trial(m, S.topo.view, S.trial_collapse.p, S.trial_info.p, S.trial_keep.p, S.trial_offsets.p, S.trial.idx.p,
                  S.trial.mat.p, S.trial.pos.p, S.topo.scan.p, st);
     uint32_t faces = 0;
     B200_CUDA(cudaMemcpyAsync(&faces, S.trial_offsets.p + m.nf, 4, cudaMemcpyDeviceToHost, st));
