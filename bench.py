@@ -312,19 +312,23 @@ def run_gpu(args) -> None:
             "gpu_launches": int(prof["launches"] // max(1, args.steps) * args.steps),
             "kernel_ms": {"prepare": prof["prepare_ms"] / args.steps, "audit": prof["audit_ms"] / args.steps,
                           "verdicts": prof["verdict_ms"] / args.steps}}
-    # LOD-chain step: the greedy executor from the source to 50% of its faces.
+    # LOD-chain step: the greedy executor from the source to 50% of its faces,
+    # with batches of one (the reference's sequential walk) and of 64.
     if not args.no_chain:
-        session.reset()
-        torch.cuda.synchronize(device)
-        t0 = time.perf_counter()
-        chain = session.execute(mesh.face_count // 2, 1 << 30, gates)
-        torch.cuda.synchronize(device)
-        chain_s = time.perf_counter() - t0
-        line["chain"] = {"metric": "LOD-chain s/mesh", "seconds": chain_s, "unit": "s/mesh",
-                         "step": "one LOD step to 50% faces", "commits": int(len(chain["commits"])),
-                         "trials": int(chain["trials"]), "audited": int(chain["audited"]),
-                         "final_faces": int(chain["final_faces"]), "stop": int(chain["stop"]),
+        line["chain"] = {"metric": "LOD-chain s/mesh", "unit": "s/mesh", "step": "one LOD step to 50% faces",
                          "timing": "wall clock around the host-orchestrated executor"}
+        for batch in (1, 64):
+            session.reset()
+            torch.cuda.synchronize(device)
+            t0 = time.perf_counter()
+            chain = session.execute(mesh.face_count // 2, 1 << 30, gates, batch=batch)
+            torch.cuda.synchronize(device)
+            chain_s = time.perf_counter() - t0
+            line["chain"][f"batch{batch}"] = {
+                "seconds": chain_s, "commits": int(len(chain["commits"])), "trials": int(chain["trials"]),
+                "audited": int(chain["audited"]), "final_faces": int(chain["final_faces"]),
+                "stop": int(chain["stop"])}
+        line["chain"]["seconds"] = line["chain"]["batch1"]["seconds"]
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         r = cpu_reference_sample(args.cpu_sample, 1, 1)
         line["cpu_baseline"] = {"value": r["candidates"] / r["busy_s"], "unit": "collapses/s", "cores": 1,

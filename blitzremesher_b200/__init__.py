@@ -130,6 +130,9 @@ EXPORTS = {
     "blitz_audit_profile_enable": ([C.c_void_p, C.c_int], C.c_int),
     "blitz_audit_execute": ([C.c_void_p, C.c_uint32, C.c_uint32, C.POINTER(EvalSettings), C.c_void_p, C.c_size_t,
                              C.c_void_p, C.c_char_p, C.c_size_t], C.c_int),
+    "blitz_audit_execute_ex": ([C.c_void_p, C.c_uint32, C.c_uint32, C.POINTER(EvalSettings), C.c_void_p,
+                                C.c_void_p, C.c_size_t, C.c_void_p, C.c_char_p, C.c_size_t], C.c_int),
+    "blitz_execute_options_init": ([C.c_void_p], None),
     "blitz_audit_state": ([C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p, C.c_size_t, C.POINTER(C.c_uint32),
                            C.c_char_p, C.c_size_t], C.c_int),
     "blitz_audit_reset": ([C.c_void_p, C.c_char_p, C.c_size_t], C.c_int),
@@ -141,6 +144,10 @@ class Execution(C.Structure):
     _fields_ = [("struct_size", C.c_uint32), ("commits", C.c_uint32), ("trials", C.c_uint32),
                 ("final_faces", C.c_uint32), ("audited", C.c_uint64), ("stop_reason", C.c_uint8),
                 ("reserved", C.c_uint8 * 7)]
+
+
+class ExecuteOptions(C.Structure):
+    _fields_ = [("struct_size", C.c_uint32), ("batch", C.c_uint32), ("reserved", C.c_uint32 * 6)]
 
 
 class AuditProfile(C.Structure):
@@ -320,16 +327,24 @@ class AuditSession:
         _check(self.lib.blitz_audit_candidates_device(self.handle, collapses_ptr, n, g, verdicts_ptr,
                                                       measurements_ptr or None, stream or None, err, 512), err)
 
-    def execute(self, target_faces: int, trial_budget: int, gates: Sequence[EvalSettings]) -> dict:
-        """Greedy LOD step on the current state (batches of one, ShortestEdge)."""
-        cap = 1 << 22
-        commits = np.zeros(2 * min(cap, 8 * 1024 * 1024), dtype=np.uint32)
+    def execute(self, target_faces: int, trial_budget: int, gates: Sequence[EvalSettings], batch: int = 1) -> dict:
+        """Greedy LOD step on the current state (ShortestEdge ranking), with
+        batches of up to `batch` independent collapses per audited trial."""
+        commits = np.zeros(2 * max(16, self._source.idx.size // 3), dtype=np.uint32)
         out = Execution()
         out.struct_size = C.sizeof(Execution)
         g = (EvalSettings * 4)(*gates)
         err = C.create_string_buffer(512)
-        _check(self.lib.blitz_audit_execute(self.handle, target_faces, trial_budget, g, commits.ctypes.data,
-                                            commits.size // 2, C.byref(out), err, 512), err)
+        if batch == 1:
+            _check(self.lib.blitz_audit_execute(self.handle, target_faces, trial_budget, g, commits.ctypes.data,
+                                                commits.size // 2, C.byref(out), err, 512), err)
+        else:
+            opts = ExecuteOptions()
+            self.lib.blitz_execute_options_init(C.byref(opts))
+            opts.batch = batch
+            _check(self.lib.blitz_audit_execute_ex(self.handle, target_faces, trial_budget, g, C.byref(opts),
+                                                   commits.ctypes.data, commits.size // 2, C.byref(out), err, 512),
+                   err)
         n = out.commits
         return {"commits": commits[: 2 * n].reshape(-1, 2).copy(), "trials": out.trials,
                 "final_faces": out.final_faces, "audited": out.audited, "stop": out.stop_reason}

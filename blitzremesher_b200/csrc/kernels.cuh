@@ -125,6 +125,24 @@ void launch_refresh_views(const DevMesh& m, const Camera* cams_dev, uint32_t nvi
                           uint32_t* state_bits, const uint32_t* ref_bits, uint32_t wstride,
                           unsigned long long* pop, const uint32_t* ref_field, uint32_t* state_field, uint32_t* g,
                           int32_t* sv, long long* sn, long long* sd, int32_t* t1, int32_t* t2, cudaStream_t s);
+// Per view, the max of t1 and of t2 over its tiles: out[2v], out[2v+1].
+void launch_view_maxima(const int32_t* t1, const int32_t* t2, uint32_t tiles, uint32_t nviews, int32_t* out,
+                        cudaStream_t s);
+// Disjoint-footprint batch selection (select_batch, action_gpu.cu:865-899).
+// ctl = {ranked position, faces that may still be removed}; out = {selected,
+// first selected position, next position}. used_global: (nv+31)/32 words,
+// used when the claimed-id bitmap does not fit in shared memory.
+size_t select_batch_smem(uint32_t nv);
+cudaError_t launch_select_batch(const DevTopology& t, const Edit* edits, const uint32_t* order, uint32_t ranked,
+                                const uint32_t* ctl, uint32_t maximum, uint32_t nv, uint32_t* used_global,
+                                uint32_t* selected, uint32_t* out, cudaStream_t s);
+// Combined trial of `count` selected edits with midpoint placements, then
+// validate_placement over it; info[0] = 1 when the placement is invalid.
+// remap/owner: nv words; table: table_cap (power of two >= 2 nv) words.
+void launch_batch_trial(const DevMesh& m, const DevTopology& t, const Edit* edits, const uint32_t* selected,
+                        uint32_t count, uint32_t* remap, uint32_t* owner, float* placements, uint32_t* keep,
+                        uint32_t* offsets, uint32_t* out_idx, uint16_t* out_mat, float* out_pos, uint32_t* table,
+                        uint32_t table_cap, uint32_t* info, uint32_t* scan_scratch, cudaStream_t s);
 // ShortestEdge scores of the legal edits (action_gpu.cu:822-825), keys for a
 // stable descending sort.
 void launch_rank_shortest(const DevMesh& m, const Edit* edits, const uint32_t* count, uint32_t capacity,

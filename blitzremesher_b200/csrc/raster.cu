@@ -396,6 +396,36 @@ void launch_refresh_views(const DevMesh& m, const Camera* cams_dev, uint32_t nvi
                                                                words, pop);
 }
 
+namespace {
+// Per view: max over its 32x32 tiles of t1 and t2 (-1 when no tile has a sample).
+__global__ void k_view_maxima(const int32_t* t1, const int32_t* t2, uint32_t tiles, int32_t* out) {
+    const uint32_t v = blockIdx.x;
+    int32_t m1 = -1, m2 = -1;
+    for (uint32_t i = threadIdx.x; i < tiles; i += blockDim.x) {
+        m1 = max(m1, t1[size_t(v) * tiles + i]);
+        m2 = max(m2, t2[size_t(v) * tiles + i]);
+    }
+    for (int o = 16; o; o >>= 1) {
+        m1 = max(m1, __shfl_xor_sync(0xffffffffu, m1, o));
+        m2 = max(m2, __shfl_xor_sync(0xffffffffu, m2, o));
+    }
+    __shared__ int32_t r1[32], r2[32];
+    const uint32_t w = threadIdx.x >> 5;
+    if ((threadIdx.x & 31) == 0) r1[w] = m1, r2[w] = m2;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (uint32_t k = 1; k < blockDim.x / 32; ++k) m1 = max(m1, r1[k]), m2 = max(m2, r2[k]);
+        out[2 * v] = m1;
+        out[2 * v + 1] = m2;
+    }
+}
+} // namespace
+
+void launch_view_maxima(const int32_t* t1, const int32_t* t2, uint32_t tiles, uint32_t nviews, int32_t* out,
+                        cudaStream_t s) {
+    if (nviews) k_view_maxima<<<nviews, 256, 0, s>>>(t1, t2, tiles, out);
+}
+
 void launch_counts_to_bits(const uint8_t* counts, uint32_t size, uint32_t* bits, cudaStream_t s) {
     size_t samples = size_t(size) * size;
     uint32_t words = uint32_t((samples + 63) / 64) * 2;

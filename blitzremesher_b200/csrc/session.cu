@@ -320,6 +320,16 @@ struct Plan {
     Buf<unsigned long long> pop;     // 4 counts per view
     std::vector<uint32_t> hstate;
     std::vector<unsigned long long> hpop;
+    // The last combined trial evaluated on this plan, laid out like the state
+    // data (so a commit of that trial swaps it in).
+    Buf<uint8_t> trial_count;
+    Buf<uint32_t> trial_bits, trial_field, trial_state;
+    Buf<int32_t> trial_t1, trial_t2, trial_max;
+    Buf<unsigned long long> trial_pop;
+    std::vector<uint32_t> trial_hstate;
+    std::vector<unsigned long long> trial_hpop;
+    std::vector<int32_t> trial_hmax;
+    uint64_t trial_tag = 0;
     PlanDev dev{};
 };
 
@@ -364,6 +374,12 @@ struct Session {
     Buf<uint32_t> trial_keep, trial_offsets;
     Buf<TrialInfo> trial_info;
     Buf<blitz_collapse> trial_collapse;
+    // batched executor
+    Buf<uint32_t> batch_selected, batch_ctl, batch_out, batch_used, batch_remap, batch_owner, batch_table,
+        batch_info;
+    Buf<float> batch_placements;
+    uint32_t batch_table_cap = 0;
+    uint64_t trial_tag = 0;
     // executor ranking
     Buf<float> scores, sorted_scores;
     Buf<uint32_t> order, sorted_order;
@@ -910,6 +926,316 @@ static void reset_state(Session& S) {
     rebuild_topology(S);
 }
 
+// ---------------------------------------------------------------------------
+// Batched executor.
+
+// Gate settings and plans of the four gates (generate.cpp:365-388): gates 1
+// and 3 against the source, 2 and 4 against the bound previous LOD.
+static void resolve_gates(Session& S, const blitz_eval_settings gates_in[4], GateRef gates[4], PlanKey keys[4]) {
+    for (int g = 0; g < 4; ++g) {
+        gates[g].es = &gates_in[g];
+        gates[g].g = gate_of(&gates_in[g], S.bounds);
+        gates[g].g.max_supersample = uint8_t(
+            bounded_refinement(gates[g].g.screen_size, gates[g].g.supersample, gates[g].g.max_supersample));
+        gates[g].reference = g % 2;
+        keys[g] = PlanKey{(g % 2) && !S.previous_is_source ? 1 : 0, gates_in[g].views_orthographic,
+                          gates_in[g].views_perspective, gates_in[g].views_seed, gates_in[g].screen_size,
+                          gates_in[g].supersample, gates_in[g].force_two_sided};
+    }
+}
+
+// Per-view data of a whole candidate mesh against the plan's reference, all
+// views in a handful of launches (counts, coverage, exact field, tile maxima,
+// popcounts, per-view maxima), left in the plan's trial buffers.
+static void trial_views(Session& S, Plan& p, const DevMesh& cand, uint64_t tag) {
+    cudaStream_t st = S.stream;
+    const size_t samples = size_t(p.size) * p.size, cstride = count_stride(samples);
+    const uint32_t tiles = ((p.size + 31) / 32) * ((p.size + 31) / 32);
+    if (!p.trial_count.p) {
+        p.trial_count = Buf<uint8_t>(S.pool, cstride * p.views);
+        p.trial_bits = Buf<uint32_t>(S.pool, size_t(p.words) * p.views);
+        B200_CUDA(cudaMemsetAsync(p.trial_bits.p, 0, size_t(p.words) * p.views * 4, st));
+        p.trial_field = Buf<uint32_t>(S.pool, samples * p.views);
+        p.trial_state = Buf<uint32_t>(S.pool, 4 * size_t(p.views));
+        p.trial_t1 = Buf<int32_t>(S.pool, size_t(tiles) * p.views);
+        p.trial_t2 = Buf<int32_t>(S.pool, size_t(tiles) * p.views);
+        p.trial_max = Buf<int32_t>(S.pool, 2 * size_t(p.views));
+        p.trial_pop = Buf<unsigned long long>(S.pool, 4 * size_t(p.views));
+        p.trial_hstate.assign(4 * size_t(p.views), 0);
+        p.trial_hpop.assign(4 * size_t(p.views), 0);
+        p.trial_hmax.assign(2 * size_t(p.views), 0);
+    }
+    const uint32_t chunk =
+        uint32_t(std::max<size_t>(1, std::min<size_t>(p.views, (size_t(256) << 20) / (samples * 24))));
+    Scratch& x = S.scratch;
+    if (x.view_entries < samples * chunk) {
+        x.vg = Buf<uint32_t>(S.pool, samples * chunk);
+        x.vsv = Buf<int32_t>(S.pool, samples * chunk);
+        x.vsn = Buf<long long>(S.pool, samples * chunk);
+        x.vsd = Buf<long long>(S.pool, samples * chunk);
+        x.view_entries = samples * chunk;
+    }
+    for (uint32_t v0 = 0; v0 < p.views; v0 += chunk) {
+        const uint32_t n = std::min(chunk, p.views - v0);
+        const size_t w0 = size_t(p.words) * v0, s0 = samples * v0, t0 = size_t(tiles) * v0;
+        launch_refresh_views(cand, p.cameras.p + v0, n, S.bounds.center, p.key.ss, p.size, p.key.force_two,
+                             p.trial_count.p + cstride * v0, cstride, p.trial_state.p + 4 * v0, p.trial_bits.p + w0,
+                             p.ref_bits.p + w0, p.words, p.trial_pop.p + 4 * v0, p.ref_field.p + s0,
+                             p.trial_field.p + s0, x.vg.p, x.vsv.p, x.vsn.p, x.vsd.p, p.trial_t1.p + t0,
+                             p.trial_t2.p + t0, st);
+    }
+    launch_view_maxima(p.trial_t1.p, p.trial_t2.p, tiles, p.views, p.trial_max.p, st);
+    B200_CUDA(cudaMemcpyAsync(p.trial_hpop.data(), p.trial_pop.p, p.trial_hpop.size() * 8, cudaMemcpyDeviceToHost, st));
+    B200_CUDA(cudaMemcpyAsync(p.trial_hstate.data(), p.trial_state.p, p.trial_hstate.size() * 4,
+                              cudaMemcpyDeviceToHost, st));
+    B200_CUDA(cudaMemcpyAsync(p.trial_hmax.data(), p.trial_max.p, p.trial_hmax.size() * 4, cudaMemcpyDeviceToHost, st));
+    B200_CUDA(cudaStreamSynchronize(st));
+    B200_CUDA(cudaGetLastError());
+    for (uint32_t v = 0; v < p.views; ++v)
+        if (p.trial_hstate[4 * v + 3]) throw Failure(BLITZ_OUT_OF_MEMORY, "more than 255 faces cover one sample");
+    p.trial_tag = tag;
+    S.profile.launches += 8;
+}
+
+// evaluate_impl (evaluate.cpp:312-352) over the per-view data of trial_views.
+// Returns false when a view would refine to a finer sampling (the caller then
+// takes the full-raster path for the gate).
+static bool gate_from_trial(const Plan& p, const GateSettings& g, Measurement& result) {
+    result = default_measurement();
+    result.supersample = g.supersample;
+    for (uint32_t v = 0; v < p.views; ++v) {
+        ViewRecord rec{};
+        rec.changed = uint32_t(p.trial_hpop[4 * v]);
+        rec.total = uint32_t(p.trial_hpop[4 * v + 1]);
+        rec.ca = p.trial_hpop[4 * v + 2] > 0;
+        rec.cb = p.trial_hpop[4 * v + 3] > 0;
+        rec.flags = uint8_t((p.hviews[v].clipped_ref ? kRecClippedRef : 0) |
+                            (p.trial_hstate[4 * v + 2] ? kRecClippedCand : 0));
+        double max_d2 = 0;
+        if (rec.changed && rec.ca && rec.cb)
+            max_d2 = double(std::max(std::max(p.trial_hmax[2 * v], p.trial_hmax[2 * v + 1]), 0));
+        Measurement cur = default_measurement();
+        cur.worst_view = v;
+        finish_view(cur, rec, g, p.key.ss, max_d2);
+        if (!refinement_done(cur, g, p.key.ss)) return false;
+        if (!aggregate_view(result, cur, v)) return true;
+    }
+    return true;
+}
+
+// The four gates of the combined trial in the session's trial buffers.
+// Returns the failed gate (1..4) or 0 when accepted.
+static int gates_of_trial(Session& S, const DevMesh& cand, const GateRef gates[4], const PlanKey keys[4],
+                          uint64_t tag) {
+    for (int gi = 0; gi < 4; ++gi) {
+        Plan& p = plan_for(S, keys[gi]);
+        Measurement r;
+        bool done = false;
+        if (!p.resource_limited && p.tiled) {
+            if (p.trial_tag != tag) trial_views(S, p, cand, tag);
+            done = gate_from_trial(p, gates[gi].g, r);
+        }
+        if (!done) {
+            const DevMesh& ref = gates[gi].reference == 0 || S.previous_is_source ? S.source.view : S.previous.view;
+            r = evaluate_full(S, ref, cand, gates[gi].es, gates[gi].g);
+        }
+        if (!measurement_accepted(r)) return gi + 1;
+    }
+    return 0;
+}
+
+// Makes the trial in the session's trial buffers the state; plans that
+// evaluated this trial take its data as their state data.
+static void commit_trial(Session& S, uint32_t faces, uint64_t tag) {
+    DevMesh& m = S.state.view;
+    cudaStream_t st = S.stream;
+    B200_CUDA(cudaMemcpyAsync(S.state.idx.p, S.trial.idx.p, size_t(faces) * 12, cudaMemcpyDeviceToDevice, st));
+    B200_CUDA(cudaMemcpyAsync(S.state.pos.p, S.trial.pos.p, size_t(m.nv) * 12, cudaMemcpyDeviceToDevice, st));
+    if (m.mat) B200_CUDA(cudaMemcpyAsync(S.state.mat.p, S.trial.mat.p, size_t(faces) * 2, cudaMemcpyDeviceToDevice, st));
+    m.nf = faces;
+    S.state_faces = faces;
+    ++S.state_revision;
+    S.state_is_source = false;
+    for (auto& kv : S.plans) {
+        Plan& p = *kv.second;
+        if (p.resource_limited || !p.tiled || p.trial_tag != tag || !p.state_bits.p) continue;
+        std::swap(p.state_count, p.trial_count);
+        std::swap(p.state_bits, p.trial_bits);
+        std::swap(p.state_field, p.trial_field);
+        std::swap(p.t1, p.trial_t1);
+        std::swap(p.t2, p.trial_t2);
+        std::swap(p.raster_state, p.trial_state);
+        std::swap(p.pop, p.trial_pop);
+        std::swap(p.hstate, p.trial_hstate);
+        std::swap(p.hpop, p.trial_hpop);
+        p.trial_tag = 0;
+        const size_t samples = size_t(p.size) * p.size, cstride = count_stride(samples);
+        const uint32_t tiles = ((p.size + 31) / 32) * ((p.size + 31) / 32);
+        p.state_is_ref = false;
+        for (uint32_t v = 0; v < p.views; ++v) {
+            PlanView& pv = p.hviews[v];
+            pv.state_bits = p.state_bits.p + size_t(v) * p.words;
+            pv.state_count = p.state_count.p + cstride * v;
+            pv.tile_t1 = p.t1.p + size_t(tiles) * v;
+            pv.tile_t2 = p.t2.p + size_t(tiles) * v;
+            pv.changed = uint32_t(p.hpop[4 * v]);
+            pv.total = uint32_t(p.hpop[4 * v + 1]);
+            pv.cov_ref = uint32_t(p.hpop[4 * v + 2]);
+            pv.cov_state = uint32_t(p.hpop[4 * v + 3]);
+            pv.clip_state = p.hstate[4 * v + 2];
+        }
+        B200_CUDA(cudaMemcpyAsync(p.dviews.p, p.hviews.data(), p.views * sizeof(PlanView), cudaMemcpyHostToDevice, st));
+        p.dev.state_is_ref = 0;
+        p.state_revision = S.state_revision;
+    }
+    rebuild_topology(S);
+}
+
+// Builds the combined trial of the first `count` selected edits; returns its
+// face count and whether validate_placement rejected it.
+static uint32_t build_batch_trial(Session& S, uint32_t count, bool& invalid) {
+    const DevMesh& m = S.state.view;
+    Topology& t = S.topo;
+    cudaStream_t st = S.stream;
+    launch_batch_trial(m, t.view, t.edits.p, S.batch_selected.p, count, S.batch_remap.p, S.batch_owner.p,
+                       S.batch_placements.p, S.trial_keep.p, S.trial_offsets.p, S.trial.idx.p, S.trial.mat.p,
+                       S.trial.pos.p, S.batch_table.p, S.batch_table_cap, S.batch_info.p, t.scan.p, st);
+    uint32_t host[2] = {0, 0};
+    B200_CUDA(cudaMemcpyAsync(&host[0], S.trial_offsets.p + m.nf, 4, cudaMemcpyDeviceToHost, st));
+    B200_CUDA(cudaMemcpyAsync(&host[1], S.batch_info.p, 4, cudaMemcpyDeviceToHost, st));
+    B200_CUDA(cudaStreamSynchronize(st));
+    B200_CUDA(cudaGetLastError());
+    S.profile.launches += 5;
+    invalid = host[1] != 0;
+    return host[0];
+}
+
+// Executor with batches of up to `batch` collapses (GpuActionState::execute,
+// action_gpu.cu:1947-2086 with select_batch and verdict, 865-915;
+// execute_actions, action.cpp:453-525): rank, select a disjoint batch from the
+// ranked position, audit the combined trial through the four gates, halve it
+// on rejection; a rejected singleton moves the position one past the batch's
+// first edit; an accepted batch is committed and the edits re-ranked.
+static void execute_batched(Session& S, uint32_t target, uint32_t budget, const blitz_eval_settings gates_in[4],
+                            uint32_t batch, uint32_t* commits_out, size_t capacity, blitz_audit_execution& out) {
+    target = std::max<uint32_t>(1, target);
+    cudaStream_t st = S.stream;
+    Topology& t = S.topo;
+    const DevMesh& src = S.source.view;
+    const double diameter = std::max(1e-20, S.bounds.radius * 2);
+    const size_t cap = 6ull * src.nf + 1;
+    S.scores.ensure(S.pool, cap);
+    S.sorted_scores.ensure(S.pool, cap);
+    S.order.ensure(S.pool, cap);
+    S.sorted_order.ensure(S.pool, cap);
+    if (!S.sort_temp.p) {
+        size_t bytes = 0;
+        B200_CUDA(sort_scores_desc(nullptr, nullptr, nullptr, nullptr, uint32_t(cap), nullptr, bytes, st));
+        S.sort_temp = Buf<unsigned char>(S.pool, bytes);
+        S.sort_bytes = bytes;
+    }
+    ensure_trial_buffers(S);
+    if (!S.batch_selected.p) {
+        S.batch_selected = Buf<uint32_t>(S.pool, 64);
+        S.batch_ctl = Buf<uint32_t>(S.pool, 2);
+        S.batch_out = Buf<uint32_t>(S.pool, 3);
+        S.batch_used = Buf<uint32_t>(S.pool, (src.nv + 31) / 32 + 1);
+        S.batch_remap = Buf<uint32_t>(S.pool, src.nv);
+        S.batch_owner = Buf<uint32_t>(S.pool, src.nv);
+        S.batch_table_cap = uint32_t(pow2_at_least(2ull * src.nv));
+        S.batch_table = Buf<uint32_t>(S.pool, S.batch_table_cap);
+        S.batch_info = Buf<uint32_t>(S.pool, 1);
+        S.batch_placements = Buf<float>(S.pool, 3 * 64);
+    }
+    GateRef gates[4];
+    PlanKey keys[4];
+    resolve_gates(S, gates_in, gates, keys);
+    uint32_t commits = 0, trials = 0;
+    uint64_t audited = 0;
+    uint8_t reason = 3;
+    std::vector<blitz_collapse> chosen(64);
+    for (;;) {
+        const uint32_t faces = S.state_faces;
+        if (faces <= target) {
+            reason = 0;
+            break;
+        }
+        if (trials >= budget) {
+            reason = 1;
+            break;
+        }
+        const uint32_t actions = t.actions;
+        if (!actions) {
+            reason = 2;
+            break;
+        }
+        launch_rank_shortest(S.state.view, t.edits.p, t.offsets.p + t.total_nbrs, actions, diameter, S.scores.p,
+                             S.order.p, st);
+        size_t bytes = S.sort_bytes;
+        B200_CUDA(sort_scores_desc(S.scores.p, S.sorted_scores.p, S.order.p, S.sorted_order.p, actions, S.sort_temp.p,
+                                   bytes, st));
+        bool accepted = false;
+        uint32_t position = 0;
+        while (position < actions && trials < budget && !accepted) {
+            const uint32_t ctl[2] = {position, faces - target};
+            B200_CUDA(cudaMemcpyAsync(S.batch_ctl.p, ctl, 8, cudaMemcpyHostToDevice, st));
+            B200_CUDA(launch_select_batch(t.view, t.edits.p, S.sorted_order.p, actions, S.batch_ctl.p, batch,
+                                          S.state.view.nv, S.batch_used.p, S.batch_selected.p, S.batch_out.p, st));
+            uint32_t sel[3];
+            B200_CUDA(cudaMemcpyAsync(sel, S.batch_out.p, 12, cudaMemcpyDeviceToHost, st));
+            B200_CUDA(cudaStreamSynchronize(st));
+            S.profile.launches += 1;
+            uint32_t count = sel[0];
+            const uint32_t first = sel[1];
+            if (!count) break;
+            while (count && trials < budget) {
+                bool invalid = false;
+                const uint32_t trial_faces = build_batch_trial(S, count, invalid);
+                const uint64_t tag = ++S.trial_tag;
+                ++trials;
+                audited += count;
+                DevMesh cand = S.state.view;
+                cand.pos = S.trial.pos.p;
+                cand.idx = S.trial.idx.p;
+                cand.mat = S.state.view.mat ? S.trial.mat.p : nullptr;
+                cand.nf = trial_faces;
+                if (!invalid && trial_faces && gates_of_trial(S, cand, gates, keys, tag) == 0) {
+                    S.collapse_dev.ensure(S.pool, 64);
+                    launch_gather_window(t.edits.p, S.batch_selected.p, 0, count, S.collapse_dev.p, st);
+                    B200_CUDA(cudaMemcpyAsync(chosen.data(), S.collapse_dev.p, count * sizeof(blitz_collapse),
+                                              cudaMemcpyDeviceToHost, st));
+                    B200_CUDA(cudaStreamSynchronize(st));
+                    for (uint32_t k = 0; k < count; ++k) {
+                        if (commits < capacity && commits_out) {
+                            commits_out[2 * commits] = chosen[k].from;
+                            commits_out[2 * commits + 1] = chosen[k].to;
+                        }
+                        ++commits;
+                    }
+                    commit_trial(S, trial_faces, tag);
+                    accepted = true;
+                    break;
+                }
+                if (count > 1) {
+                    count /= 2;
+                } else {
+                    count = 0;
+                    position = first + 1;
+                }
+            }
+        }
+        if (!accepted) {
+            reason = trials >= budget ? 1 : 3;
+            break;
+        }
+    }
+    out.commits = commits;
+    out.trials = trials;
+    out.final_faces = S.state_faces;
+    out.audited = audited;
+    out.stop_reason = reason;
+}
+
 // Greedy executor with batches of one (GpuActionState::execute,
 // action_gpu.cu:1947-2086; execute_actions, action.cpp:453-525): rank the legal
 // midpoint collapses by ShortestEdge, walk them in rank order skipping those
@@ -1344,6 +1670,44 @@ blitz_status blitz_audit_execute(blitz_audit_session* s, uint32_t target_faces, 
         S.info.gpu_audit_ns += now_ns() - t0;
         S.info.legal_collapses += r.commits;
         S.info.rejected_collapses += r.trials - r.commits;
+    });
+}
+
+void blitz_execute_options_init(blitz_execute_options* o) {
+    if (!o) return;
+    std::memset(o, 0, sizeof(*o));
+    o->struct_size = sizeof(*o);
+    o->batch = 1;
+}
+
+blitz_status blitz_audit_execute_ex(blitz_audit_session* s, uint32_t target_faces, uint32_t trial_budget,
+                                    const blitz_eval_settings gates[4], const blitz_execute_options* options,
+                                    uint32_t* commits_from_to, size_t capacity, blitz_audit_execution* out,
+                                    char* error, size_t cap) {
+    return guarded(error, cap, [&] {
+        if (!s || !gates || !out || !options || out->struct_size != sizeof(*out) ||
+            options->struct_size != sizeof(*options))
+            throw Failure(BLITZ_INVALID_ARGUMENT, "null argument or bad execution descriptor");
+        if (options->batch < 1 || options->batch > 64)
+            throw Failure(BLITZ_INVALID_ARGUMENT, "action batch outside 1..64");
+        for (uint32_t r : options->reserved)
+            if (r) throw Failure(BLITZ_INVALID_ARGUMENT, "reserved execution options must be zero");
+        Session& S = s->s;
+        DeviceScope scope(S.device);
+        if (S.options.preserve_uv && !S.source_h.uv.empty())
+            throw Failure(BLITZ_UNAVAILABLE, "uv transport on the candidate path is not implemented");
+        for (int g = 0; g < 4; ++g) gate_of(&gates[g], S.bounds);
+        uint64_t t0 = now_ns();
+        blitz_audit_execution r{};
+        r.struct_size = sizeof(r);
+        if (options->batch == 1)
+            execute(S, target_faces, trial_budget, gates, commits_from_to, capacity, r);
+        else
+            execute_batched(S, target_faces, trial_budget, gates, options->batch, commits_from_to, capacity, r);
+        *out = r;
+        S.info.gpu_audit_ns += now_ns() - t0;
+        S.info.legal_collapses += r.commits;
+        S.info.rejected_collapses += r.trials - std::min(r.trials, r.commits);
     });
 }
 

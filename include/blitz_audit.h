@@ -236,6 +236,26 @@ blitz_status blitz_audit_execute(blitz_audit_session*, uint32_t target_faces, ui
                                  const blitz_eval_settings gates[4], uint32_t* commits_from_to,
                                  size_t commit_capacity, blitz_audit_execution* out, char* error,
                                  size_t error_capacity);
+/* Executor options (the reference's neural option `action_batch`,
+ * blitz.h:130-133, and GpuActionState::execute's `batch`, action_gpu.cu:1947-1954). */
+typedef struct blitz_execute_options {
+    uint32_t struct_size;
+    uint32_t batch;        /* 1..64 independent collapses audited as one combined trial */
+    uint32_t reserved[6];  /* zero */
+} blitz_execute_options;
+void blitz_execute_options_init(blitz_execute_options*);
+
+/* blitz_audit_execute with options. batch = 1 is blitz_audit_execute; batch > 1
+ * selects disjoint-footprint batches in rank order (select_batch,
+ * action_gpu.cu:865-899), audits each batch's combined trial through the four
+ * gates, halves a rejected batch and after a rejected singleton resumes one
+ * past the batch's first edit (verdict, action_gpu.cu:904-915; execute_actions,
+ * action.cpp:486-515). `trials` counts audited batch trials, `commits` the
+ * collapses they committed. */
+blitz_status blitz_audit_execute_ex(blitz_audit_session*, uint32_t target_faces, uint32_t trial_budget,
+                                    const blitz_eval_settings gates[4], const blitz_execute_options* options,
+                                    uint32_t* commits_from_to, size_t commit_capacity,
+                                    blitz_audit_execution* out, char* error, size_t error_capacity);
 /* Current state: compacted indices (3 per face) and every vertex slot's position. */
 blitz_status blitz_audit_state(blitz_audit_session*, uint32_t* indices, size_t index_capacity, float* positions,
                                size_t position_capacity, uint32_t* face_count, char* error, size_t error_capacity);

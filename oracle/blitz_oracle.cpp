@@ -701,12 +701,19 @@ uint32_t hash_position(V3 p) {
 // class `to` with uv transported from the closest original incident face
 // (action_gpu.cu:962-1067), then validate_placement (action_gpu.cu:1103-1156).
 // `original` is the episode's initial mesh (attribute charts); `ot` its topology.
+// A batch applies several collapses with disjoint footprints at once
+// (ActionState::trial(span), action.cpp:308-345): one remap over all wedges,
+// each edit's placement on the slots of its own `to` class.
 Trial make_trial(const bo_mesh& m, const Topology& t, const bo_mesh& original, const Topology& ot,
-                 const bo_edit& e, bool preserve_uv) {
+                 const std::vector<bo_edit>& batch, bool preserve_uv) {
     Trial out;
     const uint32_t n = m.vertex_count;
-    std::vector<uint32_t> remap(n, kNone);
-    for (unsigned j = 0; j < e.wedges; ++j) remap[e.source[j]] = e.target[j];
+    std::vector<uint32_t> remap(n, kNone), owner(n, kNone);
+    for (uint32_t k = 0; k < batch.size(); ++k) {
+        const bo_edit& e = batch[k];
+        for (unsigned j = 0; j < e.wedges; ++j) remap[e.source[j]] = e.target[j];
+        owner[e.to] = k;
+    }
     std::vector<uint8_t> keep(m.face_count);
     for (uint32_t f = 0; f < m.face_count; ++f) {
         uint32_t ids[3];
@@ -728,11 +735,14 @@ Trial make_trial(const bo_mesh& m, const Topology& t, const bo_mesh& original, c
         if (m.materials) out.materials.push_back(m.materials[f]);
     }
     // place_vertices
-    V3 p = midpoint(m, e);
+    std::vector<V3> placements(batch.size());
+    for (uint32_t k = 0; k < batch.size(); ++k) placements[k] = midpoint(m, batch[k]);
     out.positions.assign(m.positions, m.positions + size_t(n) * 3);
     if (m.uv) out.uv.assign(m.uv, m.uv + size_t(n) * 2);
     for (uint32_t v = 0; v < n; ++v) {
-        if (t.geometry[v] == e.to) {
+        if (owner[t.geometry[v]] != kNone) {
+            const bo_edit& e = batch[owner[t.geometry[v]]];
+            const V3 p = placements[owner[t.geometry[v]]];
             out.positions[3 * v] = p.x, out.positions[3 * v + 1] = p.y, out.positions[3 * v + 2] = p.z;
             if (m.uv) {
                 uint32_t roots[2] = {t.canonical[v], kNone};
@@ -818,6 +828,40 @@ Trial make_trial(const bo_mesh& m, const Topology& t, const bo_mesh& original, c
                 }
             if (!placed) bucket.push_back(v);
         }
+    }
+    return out;
+}
+Trial make_trial(const bo_mesh& m, const Topology& t, const bo_mesh& original, const Topology& ot,
+                 const bo_edit& e, bool preserve_uv) {
+    return make_trial(m, t, original, ot, std::vector<bo_edit>{e}, preserve_uv);
+}
+
+// Greedy disjoint-footprint batch from ranked position `start` (select_batch,
+// action_gpu.cu:865-899; ActionState::independent, action.cpp:261-304): skip
+// edits removing more faces than remain, claim {from, to} and their class
+// neighbours, stop at `maximum` edits or when nothing remains. Returns ranked
+// positions.
+std::vector<size_t> select_batch(const Topology& t, const std::vector<bo_edit>& edits,
+                                 const std::vector<uint32_t>& order, size_t start, uint32_t maximum,
+                                 uint32_t remaining) {
+    std::vector<uint8_t> used(t.n);
+    std::vector<size_t> out;
+    for (size_t k = start; k < order.size() && remaining; ++k) {
+        const bo_edit& e = edits[order[k]];
+        if (e.removed > remaining) continue;
+        bool overlaps = false;
+        for (uint32_t u : {e.from, e.to}) {
+            overlaps |= used[u] != 0;
+            for (uint32_t j = t.offsets[u]; j < t.offsets[u + 1]; ++j) overlaps |= used[t.neighbors[j]] != 0;
+        }
+        if (overlaps) continue;
+        for (uint32_t u : {e.from, e.to}) {
+            used[u] = 1;
+            for (uint32_t j = t.offsets[u]; j < t.offsets[u + 1]; ++j) used[t.neighbors[j]] = 1;
+        }
+        out.push_back(k);
+        remaining -= e.removed;
+        if (out.size() == maximum) break;
     }
     return out;
 }
@@ -1075,6 +1119,20 @@ int bo_execute(const bo_mesh* source, const bo_mesh* previous, uint32_t target, 
                const bo_eval_settings gates[4], int preserve_uv, uint32_t* commits_from_to, uint32_t capacity,
                uint32_t* commits, uint32_t* trials, uint32_t* out_indices, uint32_t* out_faces, float* out_positions,
                uint8_t* stop) {
+    return bo_execute_batched(source, previous, target, budget, gates, preserve_uv, 1, commits_from_to, capacity,
+                              commits, trials, out_indices, out_faces, out_positions, stop);
+}
+
+// The same walk with batches of up to `batch` independent collapses: select a
+// disjoint batch from the current ranked position, audit its combined trial,
+// halve it on rejection, and after a rejected singleton continue one past the
+// batch's first edit (execute_actions, action.cpp:486-515; select_batch and
+// verdict, action_gpu.cu:865-915).
+int bo_execute_batched(const bo_mesh* source, const bo_mesh* previous, uint32_t target, uint32_t budget,
+                       const bo_eval_settings gates[4], int preserve_uv, uint32_t batch,
+                       uint32_t* commits_from_to, uint32_t capacity, uint32_t* commits, uint32_t* trials,
+                       uint32_t* out_indices, uint32_t* out_faces, float* out_positions, uint8_t* stop) {
+    if (!batch || batch > 64) return 1;
     return guarded([&] {
         ExecState st;
         st.pos.assign(source->positions, source->positions + size_t(source->vertex_count) * 3);
@@ -1114,24 +1172,34 @@ int bo_execute(const bo_mesh* source, const bo_mesh* previous, uint32_t target, 
             std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t c) { return scores[a] > scores[c]; });
             const uint32_t remaining = m.face_count - target;
             bool accepted = false;
-            for (size_t pos = 0; pos < order.size() && n_trials < budget && !accepted; ++pos) {
-                const bo_edit& e = edits[order[pos]];
-                if (e.removed > remaining) continue;
-                Trial tr = make_trial(m, t, original, classes, e, preserve_uv != 0);
-                ++n_trials;
-                if (!tr.valid) continue;
-                bo_mesh cand = trial_view(m, tr);
-                if (!audit_gates(cand, *source, prev, b, gates, nullptr)) continue;
-                if (n_commits < capacity) {
-                    commits_from_to[2 * n_commits] = e.from;
-                    commits_from_to[2 * n_commits + 1] = e.to;
+            for (size_t pos = 0; pos < order.size() && n_trials < budget && !accepted;) {
+                std::vector<size_t> picked = select_batch(t, edits, order, pos, batch, remaining);
+                if (picked.empty()) break;
+                const size_t first = picked.front();
+                while (n_trials < budget) {
+                    std::vector<bo_edit> chosen;
+                    for (size_t k : picked) chosen.push_back(edits[order[k]]);
+                    Trial tr = make_trial(m, t, original, classes, chosen, preserve_uv != 0);
+                    ++n_trials;
+                    if (tr.valid && audit_gates(trial_view(m, tr), *source, prev, b, gates, nullptr)) {
+                        for (const bo_edit& e : chosen) {
+                            if (n_commits < capacity) {
+                                commits_from_to[2 * n_commits] = e.from;
+                                commits_from_to[2 * n_commits + 1] = e.to;
+                            }
+                            ++n_commits;
+                        }
+                        st.idx = tr.indices;
+                        st.pos = tr.positions;
+                        if (!st.mat.empty()) st.mat = tr.materials;
+                        if (!st.uv.empty()) st.uv = tr.uv;
+                        accepted = true;
+                        break;
+                    }
+                    if (picked.size() == 1) break;
+                    picked.resize(picked.size() / 2);
                 }
-                ++n_commits;
-                st.idx = tr.indices;
-                st.pos = tr.positions;
-                if (!st.mat.empty()) st.mat = tr.materials;
-                if (!st.uv.empty()) st.uv = tr.uv;
-                accepted = true;
+                pos = first + 1;
             }
             if (!accepted) {
                 reason = n_trials >= budget ? 1 : 3;

@@ -130,6 +130,12 @@ int bo_execute(const bo_mesh* source, const bo_mesh* previous, uint32_t target, 
                const bo_eval_settings gates[4], int preserve_uv, uint32_t* commits_from_to, uint32_t capacity,
                uint32_t* commits, uint32_t* trials, uint32_t* out_indices, uint32_t* out_faces,
                float* out_positions, uint8_t* stop);
+/* The same executor with batches of 1..64 independent collapses, each batch
+ * audited as one combined trial and halved on rejection (action.cpp:486-515). */
+int bo_execute_batched(const bo_mesh* source, const bo_mesh* previous, uint32_t target, uint32_t budget,
+                       const bo_eval_settings gates[4], int preserve_uv, uint32_t batch,
+                       uint32_t* commits_from_to, uint32_t capacity, uint32_t* commits, uint32_t* trials,
+                       uint32_t* out_indices, uint32_t* out_faces, float* out_positions, uint8_t* stop);
 
 #ifdef __cplusplus
 }

@@ -143,13 +143,14 @@ class Oracle:
         assert self.lib.bo_bounds_of(C.byref(h.c), C.byref(b)) == 0
         return b
 
-    def execute(self, source, target: int, budget: int, gates, previous=None, preserve_uv=True) -> dict:
-        """Greedy executor (batches of one, ShortestEdge, midpoint placement)."""
+    def execute(self, source, target: int, budget: int, gates, previous=None, preserve_uv=True, batch=1) -> dict:
+        """Greedy executor (ShortestEdge, midpoint placement), batches of up to
+        `batch` independent collapses audited as one trial."""
         L = self.lib
         P = C.POINTER
-        L.bo_execute.argtypes = [P(BoMesh), P(BoMesh), C.c_uint32, C.c_uint32, P(BoEvalSettings), C.c_int,
-                                 C.c_void_p, C.c_uint32, P(C.c_uint32), P(C.c_uint32), C.c_void_p, P(C.c_uint32),
-                                 C.c_void_p, P(C.c_uint8)]
+        L.bo_execute_batched.argtypes = [P(BoMesh), P(BoMesh), C.c_uint32, C.c_uint32, P(BoEvalSettings), C.c_int,
+                                         C.c_uint32, C.c_void_p, C.c_uint32, P(C.c_uint32), P(C.c_uint32),
+                                         C.c_void_p, P(C.c_uint32), C.c_void_p, P(C.c_uint8)]
         hs = _MeshHold(source)
         hp = None if previous is None else _MeshHold(previous)
         cap = source.face_count
@@ -158,9 +159,9 @@ class Oracle:
         pos = np.zeros((source.vertex_count, 3), np.float32)
         commits, trials, faces, stop = C.c_uint32(), C.c_uint32(), C.c_uint32(), C.c_uint8()
         g = (BoEvalSettings * 4)(*gates)
-        st = L.bo_execute(C.byref(hs.c), None if hp is None else C.byref(hp.c), target, budget, g, int(preserve_uv),
-                          ft.ctypes.data, cap, C.byref(commits), C.byref(trials), idx.ctypes.data, C.byref(faces),
-                          pos.ctypes.data, C.byref(stop))
+        st = L.bo_execute_batched(C.byref(hs.c), None if hp is None else C.byref(hp.c), target, budget, g,
+                                  int(preserve_uv), batch, ft.ctypes.data, cap, C.byref(commits), C.byref(trials),
+                                  idx.ctypes.data, C.byref(faces), pos.ctypes.data, C.byref(stop))
         assert st == 0
         n = commits.value
         return {"commits": ft[: 2 * n].reshape(-1, 2), "trials": trials.value, "stop": stop.value,

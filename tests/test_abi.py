@@ -60,12 +60,15 @@ int main(void) {
 
 
 def test_descriptor_layouts_match_python(tmp_path):
-    extra = "S(blitz_eval_settings) S(blitz_measurement) S(blitz_collapse) S(blitz_candidate_verdict)"
+    extra = ("S(blitz_eval_settings) S(blitz_measurement) S(blitz_collapse) S(blitz_candidate_verdict) "
+             "S(blitz_execute_options) S(blitz_audit_execution)")
     lay = _c_layout(LAYOUT_SRC % ("blitz_audit.h", extra), ROOT / "include", tmp_path)
     assert int(lay["blitz_mesh"]) == C.sizeof(br.BlitzMesh)
     assert int(lay["blitz_neural_options_v2"]) == C.sizeof(br.NeuralOptionsV2)
     assert int(lay["blitz_neural_info"]) == C.sizeof(br.NeuralInfo)
     assert int(lay["blitz_eval_settings"]) == C.sizeof(br.EvalSettings)
+    assert int(lay["blitz_execute_options"]) == C.sizeof(br.ExecuteOptions)
+    assert int(lay["blitz_audit_execution"]) == C.sizeof(br.Execution)
     assert int(lay["blitz_measurement"]) == C.sizeof(br.Measurement) == br.MEASUREMENT_DTYPE.itemsize
     assert int(lay["blitz_collapse"]) == C.sizeof(br.Collapse) == br.COLLAPSE_DTYPE.itemsize
     assert int(lay["blitz_candidate_verdict"]) == C.sizeof(br.Verdict) == br.VERDICT_DTYPE.itemsize

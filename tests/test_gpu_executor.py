@@ -43,6 +43,25 @@ def test_executor_matches_oracle(gpu_lib, oracle, case):
     assert np.array_equal(again["commits"], got["commits"]) and again["trials"] == got["trials"]
 
 
+@pytest.mark.parametrize("case,batch", [("sphere2_96", 8), ("sphere2_96", 64), ("sphere3_256", 16)])
+def test_batched_executor_matches_oracle(gpu_lib, oracle, case, batch):
+    """Batches of independent collapses audited as one combined trial, halved
+    on rejection: the same commits, trials and final state as the oracle."""
+    make, views, screen, ss, budget = CASES[case]
+    mesh = make()
+    args = _gates(screen, views, ss)
+    target = mesh.face_count // 2
+    want = oracle.execute(mesh, target, budget, [oracle_settings(*a) for a in args], batch=batch)
+    with br.AuditSession(mesh) as s:
+        got = s.execute(target, budget, [br.eval_settings(*a) for a in args], batch=batch)
+        idx, pos = s.state()
+    assert len(want["commits"]) > 5
+    assert np.array_equal(got["commits"], want["commits"])
+    assert got["trials"] == want["trials"] and got["stop"] == want["stop"]
+    assert np.array_equal(idx, want["indices"])
+    assert np.array_equal(pos, want["positions"])
+
+
 def test_candidates_of_committed_state_match_oracle(gpu_lib, oracle):
     """After commits the state differs from both references: every gate
     Measurement of a candidate sample still equals the oracle's."""
