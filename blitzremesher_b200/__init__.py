@@ -133,6 +133,21 @@ EXPORTS = {
     "blitz_audit_execute_ex": ([C.c_void_p, C.c_uint32, C.c_uint32, C.POINTER(EvalSettings), C.c_void_p,
                                 C.c_void_p, C.c_size_t, C.c_void_p, C.c_char_p, C.c_size_t], C.c_int),
     "blitz_execute_options_init": ([C.c_void_p], None),
+    "blitz_surrogate_create": ([C.c_int, C.c_uint32, C.c_void_p, C.c_char_p, C.c_size_t], C.c_int),
+    "blitz_surrogate_destroy": ([C.c_void_p], None),
+    "blitz_surrogate_load": ([C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p, C.c_void_p, C.c_char_p, C.c_size_t],
+                             C.c_int),
+    "blitz_surrogate_save": ([C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p, C.c_void_p, C.c_char_p, C.c_size_t],
+                             C.c_int),
+    "blitz_surrogate_score": ([C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p, C.c_void_p, C.c_char_p, C.c_size_t],
+                              C.c_int),
+    "blitz_surrogate_gradients": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p, C.c_size_t,
+                                   C.POINTER(C.c_float), C.c_char_p, C.c_size_t], C.c_int),
+    "blitz_surrogate_train_step": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t, C.c_float,
+                                    C.POINTER(C.c_float), C.c_void_p, C.c_char_p, C.c_size_t], C.c_int),
+    "blitz_audit_surrogate_features": ([C.c_void_p, C.c_double, C.c_double, C.c_void_p, C.c_void_p, C.c_size_t,
+                                        C.POINTER(C.c_size_t), C.c_char_p, C.c_size_t], C.c_int),
+    "blitz_audit_attach_surrogate": ([C.c_void_p, C.c_void_p, C.c_char_p, C.c_size_t], C.c_int),
     "blitz_audit_state": ([C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p, C.c_size_t, C.POINTER(C.c_uint32),
                            C.c_char_p, C.c_size_t], C.c_int),
     "blitz_audit_reset": ([C.c_void_p, C.c_char_p, C.c_size_t], C.c_int),
@@ -143,11 +158,12 @@ EXPORTS = {
 class Execution(C.Structure):
     _fields_ = [("struct_size", C.c_uint32), ("commits", C.c_uint32), ("trials", C.c_uint32),
                 ("final_faces", C.c_uint32), ("audited", C.c_uint64), ("stop_reason", C.c_uint8),
-                ("reserved", C.c_uint8 * 7)]
+                ("fallbacks", C.c_uint8), ("reserved", C.c_uint8 * 6)]
 
 
 class ExecuteOptions(C.Structure):
-    _fields_ = [("struct_size", C.c_uint32), ("batch", C.c_uint32), ("reserved", C.c_uint32 * 6)]
+    _fields_ = [("struct_size", C.c_uint32), ("batch", C.c_uint32), ("keep_permille", C.c_uint32),
+                ("reserved", C.c_uint32 * 5)]
 
 
 class AuditProfile(C.Structure):
@@ -327,27 +343,53 @@ class AuditSession:
         _check(self.lib.blitz_audit_candidates_device(self.handle, collapses_ptr, n, g, verdicts_ptr,
                                                       measurements_ptr or None, stream or None, err, 512), err)
 
-    def execute(self, target_faces: int, trial_budget: int, gates: Sequence[EvalSettings], batch: int = 1) -> dict:
+    def execute(self, target_faces: int, trial_budget: int, gates: Sequence[EvalSettings], batch: int = 1,
+                keep_permille: int = 0) -> dict:
         """Greedy LOD step on the current state (ShortestEdge ranking), with
-        batches of up to `batch` independent collapses per audited trial."""
+        batches of up to `batch` independent collapses per audited trial; with
+        `keep_permille` the attached surrogate prunes the ranked edits first."""
         commits = np.zeros(2 * max(16, self._source.idx.size // 3), dtype=np.uint32)
         out = Execution()
         out.struct_size = C.sizeof(Execution)
         g = (EvalSettings * 4)(*gates)
         err = C.create_string_buffer(512)
-        if batch == 1:
+        if batch == 1 and not keep_permille:
             _check(self.lib.blitz_audit_execute(self.handle, target_faces, trial_budget, g, commits.ctypes.data,
                                                 commits.size // 2, C.byref(out), err, 512), err)
         else:
             opts = ExecuteOptions()
             self.lib.blitz_execute_options_init(C.byref(opts))
             opts.batch = batch
+            opts.keep_permille = keep_permille
             _check(self.lib.blitz_audit_execute_ex(self.handle, target_faces, trial_budget, g, C.byref(opts),
                                                    commits.ctypes.data, commits.size // 2, C.byref(out), err, 512),
                    err)
         n = out.commits
         return {"commits": commits[: 2 * n].reshape(-1, 2).copy(), "trials": out.trials,
-                "final_faces": out.final_faces, "audited": out.audited, "stop": out.stop_reason}
+                "final_faces": out.final_faces, "audited": out.audited, "stop": out.stop_reason,
+                "fallbacks": out.fallbacks}
+
+    def surrogate_features(self, screen: float, screen2: float):
+        """Features (torch CUDA tensor n x 48) of the current state's legal
+        edits, with those edits as midpoint collapses (numpy)."""
+        import torch
+        count = C.c_size_t()
+        err = C.create_string_buffer(512)
+        _check(self.lib.blitz_audit_surrogate_features(self.handle, screen, screen2, None, None, 0, C.byref(count),
+                                                       err, 512), err)
+        n = count.value
+        feats = torch.zeros((max(n, 1), SURROGATE_FEATURES), dtype=torch.float32, device="cuda")
+        cols = np.zeros(max(n, 1), dtype=COLLAPSE_DTYPE)
+        _check(self.lib.blitz_audit_surrogate_features(self.handle, screen, screen2, feats.data_ptr(),
+                                                       cols.ctypes.data, n, C.byref(count), err, 512), err)
+        torch.cuda.synchronize()
+        return feats[:n], cols[:n]
+
+    def attach_surrogate(self, model: Optional["Surrogate"]) -> None:
+        err = C.create_string_buffer(512)
+        _check(self.lib.blitz_audit_attach_surrogate(self.handle, model.handle if model is not None else None,
+                                                     err, 512), err)
+        self._surrogate = model
 
     def state(self):
         """Current state: (indices, positions)."""
@@ -378,6 +420,76 @@ class AuditSession:
         i.struct_size = C.sizeof(NeuralInfo)
         assert self.lib.blitz_audit_session_info(self.handle, C.byref(i)) == BLITZ_OK
         return {k: getattr(i, k) for k, _ in i._fields_ if k != "struct_size"}
+
+
+SURROGATE_FEATURES = 48
+SURROGATE_PARAMS = 26896
+
+
+class Surrogate:
+    """The learned audit surrogate (48 -> 128 -> 128 -> 2 BF16 MLP) on one GPU.
+    Device arrays are torch CUDA tensors (float32, contiguous)."""
+
+    def __init__(self, seed: int = 1, device: int = 0):
+        self.lib = load()
+        self.handle = C.c_void_p()
+        err = C.create_string_buffer(512)
+        _check(self.lib.blitz_surrogate_create(device, seed, C.byref(self.handle), err, 512), err)
+
+    def close(self) -> None:
+        if self.handle:
+            self.lib.blitz_surrogate_destroy(self.handle)
+            self.handle = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def parameters(self):
+        p = np.zeros(SURROGATE_PARAMS, np.float32)
+        mean = np.zeros(SURROGATE_FEATURES, np.float32)
+        inv = np.zeros(SURROGATE_FEATURES, np.float32)
+        err = C.create_string_buffer(512)
+        _check(self.lib.blitz_surrogate_save(self.handle, p.ctypes.data, p.size, mean.ctypes.data, inv.ctypes.data,
+                                             err, 512), err)
+        return p, mean, inv
+
+    def load(self, params, mean=None, inv_std=None) -> None:
+        p = np.ascontiguousarray(params, np.float32)
+        m = None if mean is None else np.ascontiguousarray(mean, np.float32)
+        v = None if inv_std is None else np.ascontiguousarray(inv_std, np.float32)
+        err = C.create_string_buffer(512)
+        _check(self.lib.blitz_surrogate_load(self.handle, p.ctypes.data, p.size, None if m is None else m.ctypes.data,
+                                             None if v is None else v.ctypes.data, err, 512), err)
+
+    def score(self, features):
+        import torch
+        n = features.shape[0]
+        out = torch.empty((max(n, 1), 2), dtype=torch.float32, device=features.device)
+        err = C.create_string_buffer(512)
+        _check(self.lib.blitz_surrogate_score(self.handle, features.data_ptr(), n, out.data_ptr(),
+                                              torch.cuda.current_stream().cuda_stream, err, 512), err)
+        return out[:n]
+
+    def gradients(self, features, labels):
+        g = np.zeros(SURROGATE_PARAMS, np.float32)
+        loss = C.c_float()
+        err = C.create_string_buffer(512)
+        _check(self.lib.blitz_surrogate_gradients(self.handle, features.data_ptr(), labels.data_ptr(),
+                                                  features.shape[0], g.ctypes.data, g.size, C.byref(loss), err, 512),
+               err)
+        return g, loss.value
+
+    def train_step(self, features, labels, lr: float) -> float:
+        import torch
+        loss = C.c_float()
+        err = C.create_string_buffer(512)
+        _check(self.lib.blitz_surrogate_train_step(self.handle, features.data_ptr(), labels.data_ptr(),
+                                                   features.shape[0], lr, C.byref(loss),
+                                                   torch.cuda.current_stream().cuda_stream, err, 512), err)
+        return loss.value
 
 
 def evaluate(reference, candidate, settings: EvalSettings, session: Optional[AuditSession] = None) -> Measurement:

@@ -6,6 +6,7 @@
 // through the session pool, which enforces blitz_neural_options_v2::memory_mib.
 #include "../../include/blitz_audit.h"
 #include "kernels.cuh"
+#include "surrogate.cuh"
 
 #include <algorithm>
 #include <chrono>
@@ -346,6 +347,44 @@ struct Scratch {
     size_t view_entries = 0;
 };
 
+// Surrogate parameters on one device: FP32 masters (W1 128x64, b1 128, W2
+// 128x128, b2 128, W3 16x128, b3 16), Adam moments, BF16 copies at the same
+// offsets, gradient accumulators and the feature normalisation.
+constexpr uint32_t kOffW1 = 0, kOffB1 = 8192, kOffW2 = 8320, kOffB2 = 24704, kOffW3 = 24832, kOffB3 = 26880,
+                   kParams = 26896;
+struct SurrogateModel {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    Pool pool;
+    Buf<float> master, grads, m, v, norm, loss;
+    Buf<__nv_bfloat16> wb;
+    Buf<uint8_t> mask;
+    Buf<uint32_t> error;
+    uint32_t step = 0;
+    SurrogateDev dev() const {
+        SurrogateDev d{};
+        d.w1b = wb.p + kOffW1, d.w2b = wb.p + kOffW2, d.w3b = wb.p + kOffW3;
+        d.b1 = master.p + kOffB1, d.b2 = master.p + kOffB2, d.b3 = master.p + kOffB3;
+        d.mean = norm.p, d.inv_std = norm.p + kSurrogateIn;
+        d.gw1 = grads.p + kOffW1, d.gw2 = grads.p + kOffW2, d.gw3 = grads.p + kOffW3;
+        d.gb1 = grads.p + kOffB1, d.gb2 = grads.p + kOffB2, d.gb3 = grads.p + kOffB3;
+        return d;
+    }
+    ~SurrogateModel() {
+        master.release(), grads.release(), m.release(), v.release(), norm.release(), loss.release();
+        wb.release(), mask.release(), error.release();
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+// Parameters that exist (the padding of W1's inputs and of W3/b3's outputs
+// stays zero).
+static bool surrogate_param_live(uint32_t i) {
+    if (i < kOffB1) return (i % 64) < uint32_t(kSurrogateIn);
+    if (i >= kOffW3 && i < kOffB3) return (i - kOffW3) / 128 < 2;
+    if (i >= kOffB3) return i - kOffB3 < 2;
+    return true;
+}
+
 struct Session {
     int device = 0;
     cudaStream_t stream = nullptr;
@@ -374,6 +413,12 @@ struct Session {
     Buf<uint32_t> trial_keep, trial_offsets;
     Buf<TrialInfo> trial_info;
     Buf<blitz_collapse> trial_collapse;
+    // surrogate pruning (non-owning model; buffers at the edit capacity)
+    struct SurrogateModel* surrogate = nullptr;
+    Buf<float> sur_features, sur_out, sur_keys_in, sur_keys_out;
+    Buf<uint32_t> sur_idx_in, sur_idx_out, sur_flags, sur_rank_flags, sur_offsets, sur_order;
+    Buf<unsigned char> sur_sort_temp;
+    size_t sur_sort_bytes = 0;
     // batched executor
     Buf<uint32_t> batch_selected, batch_ctl, batch_out, batch_used, batch_remap, batch_owner, batch_table,
         batch_info;
@@ -1116,8 +1161,40 @@ static uint32_t build_batch_trial(Session& S, uint32_t count, bool& invalid) {
 // ranked position, audit the combined trial through the four gates, halve it
 // on rejection; a rejected singleton moves the position one past the batch's
 // first edit; an accepted batch is committed and the edits re-ranked.
+// Surrogate pruning of the ranked edits: features and MLP scores of every
+// legal edit, the `keep` edits with the highest acceptance logits, and the
+// ShortestEdge order restricted to them (S.sur_order).
+static void prune_ranked(Session& S, uint32_t actions, uint32_t keep, float px, float px2) {
+    SurrogateModel& model = *S.surrogate;
+    Topology& t = S.topo;
+    cudaStream_t st = S.stream;
+    const size_t cap = 6ull * S.source.view.nf + 1;
+    S.sur_features.ensure(S.pool, cap * kSurrogateIn);
+    S.sur_out.ensure(S.pool, 2 * cap);
+    S.sur_keys_in.ensure(S.pool, cap);
+    S.sur_keys_out.ensure(S.pool, cap);
+    S.sur_idx_in.ensure(S.pool, cap);
+    S.sur_idx_out.ensure(S.pool, cap);
+    S.sur_flags.ensure(S.pool, cap);
+    S.sur_rank_flags.ensure(S.pool, cap + 1);
+    S.sur_offsets.ensure(S.pool, cap + 1);
+    S.sur_order.ensure(S.pool, cap);
+    launch_features(S.state.view, t.view, t.edits.p, t.offsets.p + t.total_nbrs, actions, px, px2,
+                    S.sur_features.p, st);
+    B200_CUDA(launch_mlp(model.dev(), S.sur_features.p, actions, S.sur_out.p, nullptr, 0.f, nullptr, model.error.p,
+                         148, st));
+    launch_prune_prepare(S.sur_out.p, actions, S.sur_keys_in.p, S.sur_idx_in.p, st);
+    size_t bytes = S.sort_bytes;
+    B200_CUDA(sort_scores_desc(S.sur_keys_in.p, S.sur_keys_out.p, S.sur_idx_in.p, S.sur_idx_out.p, actions,
+                               S.sort_temp.p, bytes, st));
+    launch_prune_order(S.sur_idx_out.p, actions, keep, S.sur_flags.p, S.sorted_order.p, S.sur_rank_flags.p,
+                       S.sur_offsets.p, t.scan.p, S.sur_order.p, st);
+    S.profile.launches += 7;
+}
+
 static void execute_batched(Session& S, uint32_t target, uint32_t budget, const blitz_eval_settings gates_in[4],
-                            uint32_t batch, uint32_t* commits_out, size_t capacity, blitz_audit_execution& out) {
+                            uint32_t batch, uint32_t keep_permille, uint32_t* commits_out, size_t capacity,
+                            blitz_audit_execution& out) {
     target = std::max<uint32_t>(1, target);
     cudaStream_t st = S.stream;
     Topology& t = S.topo;
@@ -1150,6 +1227,9 @@ static void execute_batched(Session& S, uint32_t target, uint32_t budget, const 
     GateRef gates[4];
     PlanKey keys[4];
     resolve_gates(S, gates_in, gates, keys);
+    const float px = float(gates_in[0].screen_size / std::max(1e-20, 2 * S.bounds.radius));
+    const float px2 = float(gates_in[2].screen_size / std::max(1e-20, 2 * S.bounds.radius));
+    uint32_t fallbacks = 0;
     uint32_t commits = 0, trials = 0;
     uint64_t audited = 0;
     uint8_t reason = 3;
@@ -1175,11 +1255,26 @@ static void execute_batched(Session& S, uint32_t target, uint32_t budget, const 
         B200_CUDA(sort_scores_desc(S.scores.p, S.sorted_scores.p, S.order.p, S.sorted_order.p, actions, S.sort_temp.p,
                                    bytes, st));
         bool accepted = false;
+        // With a surrogate the walk first covers the pruned order; the full
+        // order is the fallback when nothing there is accepted.
+        const uint32_t* walk_order = S.sorted_order.p;
+        uint32_t walk_count = actions;
+        bool pruned = false;
+        if (keep_permille && S.surrogate) {
+            const uint32_t keep = std::max<uint32_t>(1, uint32_t((uint64_t(actions) * keep_permille + 999) / 1000));
+            if (keep < actions) {
+                prune_ranked(S, actions, keep, px, px2);
+                walk_order = S.sur_order.p;
+                walk_count = keep;
+                pruned = true;
+            }
+        }
         uint32_t position = 0;
-        while (position < actions && trials < budget && !accepted) {
+        for (;;) {
+        while (position < walk_count && trials < budget && !accepted) {
             const uint32_t ctl[2] = {position, faces - target};
             B200_CUDA(cudaMemcpyAsync(S.batch_ctl.p, ctl, 8, cudaMemcpyHostToDevice, st));
-            B200_CUDA(launch_select_batch(t.view, t.edits.p, S.sorted_order.p, actions, S.batch_ctl.p, batch,
+            B200_CUDA(launch_select_batch(t.view, t.edits.p, walk_order, walk_count, S.batch_ctl.p, batch,
                                           S.state.view.nv, S.batch_used.p, S.batch_selected.p, S.batch_out.p, st));
             uint32_t sel[3];
             B200_CUDA(cudaMemcpyAsync(sel, S.batch_out.p, 12, cudaMemcpyDeviceToHost, st));
@@ -1224,16 +1319,31 @@ static void execute_batched(Session& S, uint32_t target, uint32_t budget, const 
                 }
             }
         }
+        if (accepted || !pruned || trials >= budget) break;
+        // exhaustive fallback over the full ranked order
+        pruned = false;
+        walk_order = S.sorted_order.p;
+        walk_count = actions;
+        position = 0;
+        ++fallbacks;
+        }
         if (!accepted) {
             reason = trials >= budget ? 1 : 3;
             break;
         }
+    }
+    if (S.surrogate) {
+        uint32_t err = 0;
+        B200_CUDA(cudaMemcpyAsync(&err, S.surrogate->error.p, 4, cudaMemcpyDeviceToHost, st));
+        B200_CUDA(cudaStreamSynchronize(st));
+        if (err) throw Failure(BLITZ_INTERNAL_ERROR, "surrogate tensor-core wait timed out");
     }
     out.commits = commits;
     out.trials = trials;
     out.final_faces = S.state_faces;
     out.audited = audited;
     out.stop_reason = reason;
+    out.reserved[0] = uint8_t(std::min<uint32_t>(fallbacks, 255));
 }
 
 // Greedy executor with batches of one (GpuActionState::execute,
@@ -1690,6 +1800,12 @@ blitz_status blitz_audit_execute_ex(blitz_audit_session* s, uint32_t target_face
             throw Failure(BLITZ_INVALID_ARGUMENT, "null argument or bad execution descriptor");
         if (options->batch < 1 || options->batch > 64)
             throw Failure(BLITZ_INVALID_ARGUMENT, "action batch outside 1..64");
+        if (options->keep_permille > 1000)
+            throw Failure(BLITZ_INVALID_ARGUMENT, "surrogate keep share above 1000 permille");
+        if (options->keep_permille && options->batch == 1)
+            throw Failure(BLITZ_INVALID_ARGUMENT, "surrogate pruning needs the batched executor (batch > 1)");
+        if (options->keep_permille && !s->s.surrogate)
+            throw Failure(BLITZ_INVALID_ARGUMENT, "no surrogate attached to the session");
         for (uint32_t r : options->reserved)
             if (r) throw Failure(BLITZ_INVALID_ARGUMENT, "reserved execution options must be zero");
         Session& S = s->s;
@@ -1703,7 +1819,8 @@ blitz_status blitz_audit_execute_ex(blitz_audit_session* s, uint32_t target_face
         if (options->batch == 1)
             execute(S, target_faces, trial_budget, gates, commits_from_to, capacity, r);
         else
-            execute_batched(S, target_faces, trial_budget, gates, options->batch, commits_from_to, capacity, r);
+            execute_batched(S, target_faces, trial_budget, gates, options->batch, options->keep_permille,
+                            commits_from_to, capacity, r);
         *out = r;
         S.info.gpu_audit_ns += now_ns() - t0;
         S.info.legal_collapses += r.commits;
@@ -1766,3 +1883,213 @@ blitz_status blitz_audit_session_info(const blitz_audit_session* s, blitz_neural
 }
 
 } // extern "C"
+
+// ---------------------------------------------------------------------------
+// Learned audit surrogate (no reference counterpart).
+struct blitz_surrogate {
+    SurrogateModel m;
+};
+
+namespace {
+uint64_t mix64(uint64_t& s) {
+    uint64_t z = (s += 0x9e3779b97f4a7c15ull);
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+    return z ^ (z >> 31);
+}
+// Uploads the FP32 masters, refreshes the BF16 copies and resets Adam.
+void upload_params(SurrogateModel& M, const float* params, const float* mean, const float* inv_std) {
+    cudaStream_t st = M.stream;
+    std::vector<float> p(params, params + kParams);
+    for (uint32_t i = 0; i < kParams; ++i)
+        if (!surrogate_param_live(i)) p[i] = 0;
+    std::vector<__nv_bfloat16> pb(kParams);
+    for (uint32_t i = 0; i < kParams; ++i) pb[i] = __float2bfloat16_rn(p[i]);
+    B200_CUDA(cudaMemcpyAsync(M.master.p, p.data(), kParams * 4, cudaMemcpyHostToDevice, st));
+    B200_CUDA(cudaMemcpyAsync(M.wb.p, pb.data(), kParams * 2, cudaMemcpyHostToDevice, st));
+    B200_CUDA(cudaMemsetAsync(M.m.p, 0, kParams * 4, st));
+    B200_CUDA(cudaMemsetAsync(M.v.p, 0, kParams * 4, st));
+    B200_CUDA(cudaMemsetAsync(M.grads.p, 0, kParams * 4, st));
+    if (mean) B200_CUDA(cudaMemcpyAsync(M.norm.p, mean, kSurrogateIn * 4, cudaMemcpyHostToDevice, st));
+    if (inv_std) B200_CUDA(cudaMemcpyAsync(M.norm.p + kSurrogateIn, inv_std, kSurrogateIn * 4, cudaMemcpyHostToDevice, st));
+    B200_CUDA(cudaStreamSynchronize(st));
+    M.step = 0;
+}
+// One fused forward + backward pass over n rows into the gradient accumulators.
+float accumulate_gradients(SurrogateModel& M, const float* features, const float* labels, size_t n, cudaStream_t st) {
+    if (!features || !labels || !n || n > (size_t(1) << 31)) throw Failure(BLITZ_INVALID_ARGUMENT, "bad training batch");
+    B200_CUDA(cudaMemsetAsync(M.loss.p, 0, 4, st));
+    B200_CUDA(cudaMemsetAsync(M.error.p, 0, 4, st));
+    B200_CUDA(launch_mlp(M.dev(), features, uint32_t(n), nullptr, labels, float(1.0 / double(n)), M.loss.p,
+                         M.error.p, 148, st));
+    float loss = 0;
+    uint32_t err = 0;
+    B200_CUDA(cudaMemcpyAsync(&loss, M.loss.p, 4, cudaMemcpyDeviceToHost, st));
+    B200_CUDA(cudaMemcpyAsync(&err, M.error.p, 4, cudaMemcpyDeviceToHost, st));
+    B200_CUDA(cudaStreamSynchronize(st));
+    if (err) throw Failure(BLITZ_INTERNAL_ERROR, "surrogate tensor-core wait timed out");
+    return loss / float(n);
+}
+} // namespace
+
+blitz_status blitz_surrogate_create(int device, uint32_t seed, blitz_surrogate** out, char* error, size_t cap) {
+    return guarded(error, cap, [&] {
+        if (!out) throw Failure(BLITZ_INVALID_ARGUMENT, "null output");
+        *out = nullptr;
+        int count = 0;
+        if (cudaGetDeviceCount(&count) != cudaSuccess || device < 0 || device >= count) {
+            cudaGetLastError();
+            throw Failure(BLITZ_UNAVAILABLE, "no CUDA device for the surrogate");
+        }
+        auto h = std::make_unique<blitz_surrogate>();
+        SurrogateModel& M = h->m;
+        M.device = device;
+        M.pool.limit = size_t(64) << 20;
+        DeviceScope scope(device);
+        B200_CUDA(cudaStreamCreateWithFlags(&M.stream, cudaStreamNonBlocking));
+        M.master = Buf<float>(M.pool, kParams);
+        M.grads = Buf<float>(M.pool, kParams);
+        M.m = Buf<float>(M.pool, kParams);
+        M.v = Buf<float>(M.pool, kParams);
+        M.wb = Buf<__nv_bfloat16>(M.pool, kParams);
+        M.norm = Buf<float>(M.pool, 2 * kSurrogateIn);
+        M.loss = Buf<float>(M.pool, 1);
+        M.error = Buf<uint32_t>(M.pool, 1);
+        M.mask = Buf<uint8_t>(M.pool, kParams);
+        std::vector<uint8_t> mask(kParams);
+        for (uint32_t i = 0; i < kParams; ++i) mask[i] = surrogate_param_live(i);
+        B200_CUDA(cudaMemcpyAsync(M.mask.p, mask.data(), kParams, cudaMemcpyHostToDevice, M.stream));
+        B200_CUDA(cudaMemsetAsync(M.error.p, 0, 4, M.stream));
+        // He-uniform weights (fan-in 48, 128, 128), zero biases.
+        std::vector<float> p(kParams, 0.f);
+        uint64_t state = seed;
+        auto uni = [&](float bound) {
+            return float((double(mix64(state) >> 11) * 0x1.0p-53 * 2 - 1) * bound);
+        };
+        for (uint32_t i = 0; i < 8192; ++i) p[kOffW1 + i] = uni(std::sqrt(6.f / kSurrogateIn));
+        for (uint32_t i = 0; i < 16384; ++i) p[kOffW2 + i] = uni(std::sqrt(6.f / 128));
+        for (uint32_t i = 0; i < 2048; ++i) p[kOffW3 + i] = uni(std::sqrt(6.f / 128));
+        std::vector<float> mean(kSurrogateIn, 0.f), inv(kSurrogateIn, 1.f);
+        upload_params(M, p.data(), mean.data(), inv.data());
+        *out = h.release();
+    });
+}
+
+void blitz_surrogate_destroy(blitz_surrogate* h) {
+    if (!h) return;
+    int previous = 0;
+    cudaGetDevice(&previous);
+    cudaSetDevice(h->m.device);
+    delete h;
+    cudaSetDevice(previous);
+}
+
+blitz_status blitz_surrogate_load(blitz_surrogate* h, const float* params, size_t count, const float* mean,
+                                  const float* inv_std, char* error, size_t cap) {
+    return guarded(error, cap, [&] {
+        if (!h || !params || count != kParams) throw Failure(BLITZ_INVALID_ARGUMENT, "bad surrogate parameters");
+        DeviceScope scope(h->m.device);
+        upload_params(h->m, params, mean, inv_std);
+    });
+}
+
+blitz_status blitz_surrogate_save(const blitz_surrogate* h, float* params, size_t capacity, float* mean,
+                                  float* inv_std, char* error, size_t cap) {
+    return guarded(error, cap, [&] {
+        if (!h || (params && capacity < kParams)) throw Failure(BLITZ_INVALID_ARGUMENT, "bad surrogate output");
+        const SurrogateModel& M = h->m;
+        DeviceScope scope(M.device);
+        if (params) B200_CUDA(cudaMemcpyAsync(params, M.master.p, kParams * 4, cudaMemcpyDeviceToHost, M.stream));
+        if (mean) B200_CUDA(cudaMemcpyAsync(mean, M.norm.p, kSurrogateIn * 4, cudaMemcpyDeviceToHost, M.stream));
+        if (inv_std)
+            B200_CUDA(cudaMemcpyAsync(inv_std, M.norm.p + kSurrogateIn, kSurrogateIn * 4, cudaMemcpyDeviceToHost,
+                                      M.stream));
+        B200_CUDA(cudaStreamSynchronize(M.stream));
+    });
+}
+
+blitz_status blitz_surrogate_score(blitz_surrogate* h, const float* features, size_t n, float* out, void* stream,
+                                   char* error, size_t cap) {
+    return guarded(error, cap, [&] {
+        if (!h || (n && (!features || !out)) || n > (size_t(1) << 31))
+            throw Failure(BLITZ_INVALID_ARGUMENT, "bad surrogate scoring arguments");
+        SurrogateModel& M = h->m;
+        DeviceScope scope(M.device);
+        cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : M.stream;
+        B200_CUDA(cudaMemsetAsync(M.error.p, 0, 4, st));
+        B200_CUDA(launch_mlp(M.dev(), features, uint32_t(n), out, nullptr, 0.f, nullptr, M.error.p, 148, st));
+        uint32_t err = 0;
+        B200_CUDA(cudaMemcpyAsync(&err, M.error.p, 4, cudaMemcpyDeviceToHost, st));
+        B200_CUDA(cudaStreamSynchronize(st));
+        if (err) throw Failure(BLITZ_INTERNAL_ERROR, "surrogate tensor-core wait timed out");
+    });
+}
+
+blitz_status blitz_surrogate_gradients(blitz_surrogate* h, const float* features, const float* labels, size_t n,
+                                       float* gradients, size_t capacity, float* loss, char* error, size_t cap) {
+    return guarded(error, cap, [&] {
+        if (!h || !gradients || capacity < kParams) throw Failure(BLITZ_INVALID_ARGUMENT, "bad gradient output");
+        SurrogateModel& M = h->m;
+        DeviceScope scope(M.device);
+        B200_CUDA(cudaMemsetAsync(M.grads.p, 0, kParams * 4, M.stream));
+        const float l = accumulate_gradients(M, features, labels, n, M.stream);
+        B200_CUDA(cudaMemcpyAsync(gradients, M.grads.p, kParams * 4, cudaMemcpyDeviceToHost, M.stream));
+        B200_CUDA(cudaMemsetAsync(M.grads.p, 0, kParams * 4, M.stream));
+        B200_CUDA(cudaStreamSynchronize(M.stream));
+        if (loss) *loss = l;
+    });
+}
+
+blitz_status blitz_surrogate_train_step(blitz_surrogate* h, const float* features, const float* labels, size_t n,
+                                        float lr, float* loss, void* stream, char* error, size_t cap) {
+    return guarded(error, cap, [&] {
+        if (!h || !(lr > 0)) throw Failure(BLITZ_INVALID_ARGUMENT, "bad training step");
+        SurrogateModel& M = h->m;
+        DeviceScope scope(M.device);
+        cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : M.stream;
+        const float l = accumulate_gradients(M, features, labels, n, st);
+        ++M.step;
+        launch_adam(M.master.p, M.grads.p, M.m.p, M.v.p, M.wb.p, kParams, lr, 0.9f, 0.999f, 1e-8f, M.step, M.mask.p,
+                    st);
+        B200_CUDA(cudaGetLastError());
+        if (loss) *loss = l;
+    });
+}
+
+blitz_status blitz_audit_surrogate_features(blitz_audit_session* s, double screen, double screen2, float* features,
+                                            blitz_collapse* collapses, size_t capacity, size_t* count, char* error,
+                                            size_t cap) {
+    return guarded(error, cap, [&] {
+        if (!s || !count || !(screen > 0) || !(screen2 > 0))
+            throw Failure(BLITZ_INVALID_ARGUMENT, "bad feature arguments");
+        Session& S = s->s;
+        DeviceScope scope(S.device);
+        Topology& t = S.topo;
+        *count = t.actions;
+        if (!features || capacity < t.actions) return;
+        const float px = float(screen / std::max(1e-20, 2 * S.bounds.radius));
+        const float px2 = float(screen2 / std::max(1e-20, 2 * S.bounds.radius));
+        launch_features(S.state.view, t.view, t.edits.p, t.offsets.p + t.total_nbrs, t.actions, px, px2, features,
+                        S.stream);
+        if (collapses && t.actions) {
+            S.order.ensure(S.pool, t.actions);
+            std::vector<uint32_t> iota(t.actions);
+            for (uint32_t i = 0; i < t.actions; ++i) iota[i] = i;
+            B200_CUDA(cudaMemcpyAsync(S.order.p, iota.data(), t.actions * 4, cudaMemcpyHostToDevice, S.stream));
+            S.collapse_dev.ensure(S.pool, t.actions);
+            launch_gather_window(t.edits.p, S.order.p, 0, t.actions, S.collapse_dev.p, S.stream);
+            B200_CUDA(cudaMemcpyAsync(collapses, S.collapse_dev.p, t.actions * sizeof(blitz_collapse),
+                                      cudaMemcpyDeviceToHost, S.stream));
+        }
+        B200_CUDA(cudaStreamSynchronize(S.stream));
+        B200_CUDA(cudaGetLastError());
+    });
+}
+
+blitz_status blitz_audit_attach_surrogate(blitz_audit_session* s, blitz_surrogate* h, char* error, size_t cap) {
+    return guarded(error, cap, [&] {
+        if (!s) throw Failure(BLITZ_INVALID_ARGUMENT, "null session");
+        if (h && h->m.device != s->s.device) throw Failure(BLITZ_INVALID_ARGUMENT, "surrogate on another device");
+        s->s.surrogate = h ? &h->m : nullptr;
+    });
+}

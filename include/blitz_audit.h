@@ -223,7 +223,8 @@ typedef struct blitz_audit_execution {
     uint32_t final_faces;
     uint64_t audited;     /* candidates audited, speculative windows included */
     uint8_t stop_reason;  /* 0 target reached, 1 trial budget, 2 no legal actions, 3 no accepted action */
-    uint8_t reserved[7];
+    uint8_t fallbacks;    /* surrogate walks that fell back to the full order (saturates at 255) */
+    uint8_t reserved[6];
 } blitz_audit_execution;
 
 /* Greedy LOD step on the session's current state, batches of one, ShortestEdge
@@ -240,8 +241,10 @@ blitz_status blitz_audit_execute(blitz_audit_session*, uint32_t target_faces, ui
  * blitz.h:130-133, and GpuActionState::execute's `batch`, action_gpu.cu:1947-1954). */
 typedef struct blitz_execute_options {
     uint32_t struct_size;
-    uint32_t batch;        /* 1..64 independent collapses audited as one combined trial */
-    uint32_t reserved[6];  /* zero */
+    uint32_t batch;         /* 1..64 independent collapses audited as one combined trial */
+    uint32_t keep_permille; /* 0: no surrogate; else the share of ranked edits the attached surrogate
+                               keeps (250 = top 25%), with the full order as fallback; batch > 1 only */
+    uint32_t reserved[5];   /* zero */
 } blitz_execute_options;
 void blitz_execute_options_init(blitz_execute_options*);
 
@@ -256,6 +259,57 @@ blitz_status blitz_audit_execute_ex(blitz_audit_session*, uint32_t target_faces,
                                     const blitz_eval_settings gates[4], const blitz_execute_options* options,
                                     uint32_t* commits_from_to, size_t commit_capacity,
                                     blitz_audit_execution* out, char* error, size_t error_capacity);
+/* ---- Learned audit surrogate ---------------------------------------------
+ * A 48 -> 128 -> 128 -> 2 MLP (ReLU) with BF16 weights and FP32 accumulation,
+ * run by the library's own tcgen05 kernels, that predicts per candidate
+ * collapse the logit of acceptance by the exact four-gate audit and the ratio
+ * error / limit of the worst gate. It has no reference counterpart: the
+ * reference's learned policies (inference.cu, fused.cu) rank endpoint edits
+ * with FP32 networks; this model only prunes the ranked edits of the batched
+ * executor and never accepts a collapse itself. */
+#define BLITZ_SURROGATE_FEATURES 48
+/* FP32 parameters in this order: W1 128x64 (inputs padded 48 -> 64), b1 128,
+ * W2 128x128, b2 128, W3 16x128 (outputs padded 2 -> 16), b3 16; row-major
+ * [out][in]. Padding entries are zero. */
+#define BLITZ_SURROGATE_PARAMS 26896
+typedef struct blitz_surrogate blitz_surrogate;
+/* New model on `device` with He-uniform weights drawn from `seed`, zero
+ * biases, identity feature normalisation. */
+blitz_status blitz_surrogate_create(int device, uint32_t seed, blitz_surrogate** out, char* error,
+                                    size_t error_capacity);
+void blitz_surrogate_destroy(blitz_surrogate*);
+/* Parameters (BLITZ_SURROGATE_PARAMS floats) and the feature normalisation
+ * x' = (x - mean) * inv_std (48 floats each; null keeps the current one).
+ * Loading resets the Adam state. */
+blitz_status blitz_surrogate_load(blitz_surrogate*, const float* params, size_t count, const float* mean,
+                                  const float* inv_std, char* error, size_t error_capacity);
+blitz_status blitz_surrogate_save(const blitz_surrogate*, float* params, size_t capacity, float* mean,
+                                  float* inv_std, char* error, size_t error_capacity);
+/* Forward pass over n rows of device features (n x 48 FP32) into device
+ * outputs (n x 2: acceptance logit, predicted error / limit), enqueued on
+ * `stream` (NULL = the model's stream); synchronises before returning. */
+blitz_status blitz_surrogate_score(blitz_surrogate*, const float* features_device, size_t n, float* out_device,
+                                   void* stream, char* error, size_t error_capacity);
+/* Gradients of mean over the n rows of BCE(logit, accepted) + Huber(pred -
+ * error ratio) (labels_device: n x 2 = {accepted 0/1, error / limit}) in the
+ * parameter order above, without updating the model; *loss = the mean loss. */
+blitz_status blitz_surrogate_gradients(blitz_surrogate*, const float* features_device, const float* labels_device,
+                                       size_t n, float* gradients_host, size_t capacity, float* loss, char* error,
+                                       size_t error_capacity);
+/* One Adam step (beta 0.9 / 0.999, eps 1e-8) on the mean loss of the n rows. */
+blitz_status blitz_surrogate_train_step(blitz_surrogate*, const float* features_device, const float* labels_device,
+                                        size_t n, float learning_rate, float* loss, void* stream, char* error,
+                                        size_t error_capacity);
+/* Features (n x 48, device) of the session state's legal edits in the order
+ * of blitz_audit_actions, with those edits as midpoint collapses on the host
+ * (capacity rows each); `screen` and `screen2` are the search and audit
+ * screen sizes in pixels. */
+blitz_status blitz_audit_surrogate_features(blitz_audit_session*, double screen, double screen2,
+                                            float* features_device, blitz_collapse* collapses, size_t capacity,
+                                            size_t* count, char* error, size_t error_capacity);
+/* Attaches a model (same device; NULL detaches) for blitz_execute_options.keep_permille. */
+blitz_status blitz_audit_attach_surrogate(blitz_audit_session*, blitz_surrogate*, char* error, size_t error_capacity);
+
 /* Current state: compacted indices (3 per face) and every vertex slot's position. */
 blitz_status blitz_audit_state(blitz_audit_session*, uint32_t* indices, size_t index_capacity, float* positions,
                                size_t position_capacity, uint32_t* face_count, char* error, size_t error_capacity);
