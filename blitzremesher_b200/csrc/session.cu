@@ -788,6 +788,30 @@ static void ensure_trial_buffers(Session& S) {
     S.trial_collapse = Buf<blitz_collapse>(S.pool, 1);
 }
 
+static void trial_views(Session& S, Plan& p, const DevMesh& cand, uint64_t tag);
+static bool gate_from_trial(const Plan& p, const GateSettings& g, Measurement& result);
+
+// Plan of gate `gi` (gates 1 and 3 against the source, 2 and 4 against the
+// bound previous LOD).
+static PlanKey plan_key_of(const Session& S, int gi, const blitz_eval_settings& es) {
+    return PlanKey{(gi % 2) && !S.previous_is_source ? 1 : 0, es.views_orthographic, es.views_perspective,
+                   es.views_seed, es.screen_size, es.supersample, es.force_two_sided};
+}
+
+// One gate of a built trial: all views at once from the plan's reference
+// fields when the plan keeps them and no view clips or refines, else the
+// per-view full-raster path.
+static Measurement gate_of_trial(Session& S, const DevMesh& cand, const GateRef& gate, int gi, uint64_t tag) {
+    Plan& p = plan_for(S, plan_key_of(S, gi, *gate.es));
+    Measurement r;
+    if (!p.resource_limited && p.tiled) {
+        if (p.trial_tag != tag) trial_views(S, p, cand, tag);
+        if (gate_from_trial(p, gate.g, r)) return r;
+    }
+    const DevMesh& ref = gate.reference == 0 || S.previous_is_source ? S.source.view : S.previous.view;
+    return evaluate_full(S, ref, cand, gate.es, gate.g);
+}
+
 static void exact_candidate(Session& S, const blitz_collapse& col, const GateRef* gates, int first,
                             blitz_candidate_verdict& v, Measurement* meas) {
     const DevMesh& m = S.state.view;
@@ -807,9 +831,9 @@ static void exact_candidate(Session& S, const blitz_collapse& col, const GateRef
     v.exact_path = 1;
     v.failed_gate = 0;
     v.accepted = 0;
+    const uint64_t tag = ++S.trial_tag;
     for (int gi = first; gi < 4; ++gi) {
-        const DevMesh& ref = gates[gi].reference == 0 || S.previous_is_source ? S.source.view : S.previous.view;
-        Measurement r = evaluate_full(S, ref, cand, gates[gi].es, gates[gi].g);
+        Measurement r = gate_of_trial(S, cand, gates[gi], gi, tag);
         if (meas) meas[gi] = r;
         if (!measurement_accepted(r)) {
             v.failed_gate = uint8_t(gi + 1);
@@ -1056,6 +1080,9 @@ static bool gate_from_trial(const Plan& p, const GateSettings& g, Measurement& r
         rec.cb = p.trial_hpop[4 * v + 3] > 0;
         rec.flags = uint8_t((p.hviews[v].clipped_ref ? kRecClippedRef : 0) |
                             (p.trial_hstate[4 * v + 2] ? kRecClippedCand : 0));
+        // A clipped view's reference raster stops at the first clipped face;
+        // its changed area comes from the full-raster path.
+        if (rec.flags) return false;
         double max_d2 = 0;
         if (rec.changed && rec.ca && rec.cb)
             max_d2 = double(std::max(std::max(p.trial_hmax[2 * v], p.trial_hmax[2 * v + 1]), 0));
@@ -1072,20 +1099,9 @@ static bool gate_from_trial(const Plan& p, const GateSettings& g, Measurement& r
 // Returns the failed gate (1..4) or 0 when accepted.
 static int gates_of_trial(Session& S, const DevMesh& cand, const GateRef gates[4], const PlanKey keys[4],
                           uint64_t tag) {
-    for (int gi = 0; gi < 4; ++gi) {
-        Plan& p = plan_for(S, keys[gi]);
-        Measurement r;
-        bool done = false;
-        if (!p.resource_limited && p.tiled) {
-            if (p.trial_tag != tag) trial_views(S, p, cand, tag);
-            done = gate_from_trial(p, gates[gi].g, r);
-        }
-        if (!done) {
-            const DevMesh& ref = gates[gi].reference == 0 || S.previous_is_source ? S.source.view : S.previous.view;
-            r = evaluate_full(S, ref, cand, gates[gi].es, gates[gi].g);
-        }
-        if (!measurement_accepted(r)) return gi + 1;
-    }
+    (void)keys;
+    for (int gi = 0; gi < 4; ++gi)
+        if (!measurement_accepted(gate_of_trial(S, cand, gates[gi], gi, tag))) return gi + 1;
     return 0;
 }
 
