@@ -19,22 +19,36 @@ constexpr int kAuditWarps = 8;
 #ifndef B200_AUDIT_MIN_BLOCKS
 #define B200_AUDIT_MIN_BLOCKS 3 // resident blocks per SM the register budget targets
 #endif
-constexpr int kRegionWords = 4;     // region width <= 128 samples after 32-alignment
-constexpr int kRegionRows = 64;     // region height
-constexpr int kDeltaSamples = 2048; // region samples (unaligned bbox) with a count delta
-constexpr int kQueue = 160;         // changed samples per (candidate, view)
 constexpr int kMaxOk = 48;          // rasterized (unculled, unclipped) old + new faces
 constexpr int kMaxTileSide = 32;    // tile-maxima path for rasters up to 1024 x 1024
-constexpr int kAffected = 8;        // tiles outside the region whose distances may change
 
-struct WarpScratch {
+// Per-warp limits of one (candidate, view) unit. The common tier keeps its
+// scratch small so that many warps stay resident; units that overflow it are
+// spilled to the large tier (few warps per SM, 256 x 256-sample regions).
+struct LimitsSmall {
+    static constexpr int kRegionWords = 4;     // region width <= 128 samples after 32-alignment
+    static constexpr int kRegionRows = 64;     // region height
+    static constexpr int kDeltaSamples = 2048; // region samples (unaligned bbox) with a count delta
+    static constexpr int kQueue = 160;         // changed samples per (candidate, view)
+    static constexpr int kAffected = 8;        // tiles outside the region whose distances may change
+};
+struct LimitsLarge {
+    static constexpr int kRegionWords = 8;
+    static constexpr int kRegionRows = 256;
+    static constexpr int kDeltaSamples = 32768;
+    static constexpr int kQueue = 4096;
+    static constexpr int kAffected = 32;
+};
+constexpr int kLargeWarps = 3; // warps per block of the large tier
+
+template <class L> struct WarpScratch {
     double vx[32], vy[32], vz[32]; // projected local vertices; 31 = placement
     FaceSetup faces[kMaxOk];       // old faces carry pad = -1, new faces pad = +1
     uint32_t work[kMaxOk];         // exclusive prefix of bbox samples per face
-    uint32_t affected[kAffected];
-    uint32_t region[kRegionRows * kRegionWords];
-    uint32_t delta[kDeltaSamples / 4]; // per-sample count delta + 128, one byte each
-    uint32_t queue[kQueue];
+    uint32_t affected[L::kAffected];
+    uint32_t region[L::kRegionRows * L::kRegionWords];
+    uint32_t delta[L::kDeltaSamples / 4]; // per-sample count delta + 128, one byte each
+    uint32_t queue[L::kQueue];
 };
 
 __device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31; }
@@ -136,8 +150,14 @@ __device__ __forceinline__ void record_write(ViewRecord* out, const ViewRecord& 
     if (lane_id() == 0) *out = r;
 }
 
+// `spill` (small tier only): units that overflow the tier's limits append
+// their unit index `u` there for the large tier instead of falling back.
+template <class L>
 __device__ void audit_unit(const CandidateRecord* __restrict__ rec, const PlanDev& plan, uint32_t v,
-                           WarpScratch& ws, ViewRecord* out, unsigned long long* stats) {
+                           WarpScratch<L>& ws, ViewRecord* out, unsigned long long* stats, uint32_t u,
+                           uint32_t* spill) {
+    constexpr int kRegionWords = L::kRegionWords, kRegionRows = L::kRegionRows;
+    constexpr int kDeltaSamples = L::kDeltaSamples, kQueue = L::kQueue, kAffected = L::kAffected;
     const uint32_t lane = lane_id();
     const PlanView pv = plan.views[v];
     const uint32_t size = plan.size;
@@ -431,6 +451,7 @@ __device__ void audit_unit(const CandidateRecord* __restrict__ rec, const PlanDe
     if (fallback) r.flags |= kRecFallback;
     if (best >= kExactLimit) r.flags |= kRecLarge;
     if (lane == 0) {
+        if (fallback && spill) spill[1 + atomicAdd(spill, 1u)] = u;
         *out = r;
         if (stats) {
             atomicAdd(stats, 1ull);
@@ -444,9 +465,10 @@ __device__ void audit_unit(const CandidateRecord* __restrict__ rec, const PlanDe
 // Persistent warps pull (candidate, view) units, candidate-major, from `queue`.
 __global__ void __launch_bounds__(kAuditWarps * 32, B200_AUDIT_MIN_BLOCKS) k_audit(const CandidateRecord* __restrict__ recs, uint32_t n,
                                                              PlanDev plan, ViewRecord* out,
-                                                             unsigned long long* stats, uint32_t* queue) {
+                                                             unsigned long long* stats, uint32_t* queue,
+                                                             uint32_t* spill) {
     extern __shared__ __align__(16) unsigned char smem[];
-    WarpScratch& ws = reinterpret_cast<WarpScratch*>(smem)[threadIdx.x >> 5];
+    WarpScratch<LimitsSmall>& ws = reinterpret_cast<WarpScratch<LimitsSmall>*>(smem)[threadIdx.x >> 5];
     const uint32_t lane = lane_id();
     const uint64_t total = uint64_t(n) * plan.nviews;
     for (;;) {
@@ -463,7 +485,27 @@ __global__ void __launch_bounds__(kAuditWarps * 32, B200_AUDIT_MIN_BLOCKS) k_aud
             record_write(slot, r);
             continue;
         }
-        audit_unit(rec, plan, v, ws, slot, stats);
+        audit_unit(rec, plan, v, ws, slot, stats, u, spill);
+    }
+}
+
+// The large tier: persistent warps over the spilled unit list {count, units}.
+__global__ void __launch_bounds__(kLargeWarps * 32, 1) k_audit_large(const CandidateRecord* __restrict__ recs,
+                                                                     PlanDev plan, ViewRecord* out,
+                                                                     unsigned long long* stats,
+                                                                     const uint32_t* spill, uint32_t* cursor) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    WarpScratch<LimitsLarge>& ws = reinterpret_cast<WarpScratch<LimitsLarge>*>(smem)[threadIdx.x >> 5];
+    const uint32_t lane = lane_id();
+    const uint32_t count = spill[0];
+    for (;;) {
+        uint32_t k = 0;
+        if (lane == 0) k = atomicAdd(cursor, 1u);
+        k = __shfl_sync(0xffffffffu, k, 0);
+        if (k >= count) break;
+        const uint32_t u = spill[1 + k];
+        const uint32_t c = u / plan.nviews, v = u - c * plan.nviews;
+        audit_unit(recs + c, plan, v, ws, out + u, stats, u, nullptr);
     }
 }
 
@@ -529,16 +571,21 @@ __global__ void k_verdicts(const ViewRecord* const* plan_records, const uint32_t
 }
 } // namespace
 
-size_t audit_smem_bytes() { return kAuditWarps * sizeof(WarpScratch); }
+size_t audit_smem_bytes() { return kAuditWarps * sizeof(WarpScratch<LimitsSmall>); }
+size_t audit_large_smem_bytes() { return kLargeWarps * sizeof(WarpScratch<LimitsLarge>); }
 
 void launch_audit(const CandidateRecord* records, uint32_t n, const PlanDev& plan, ViewRecord* out,
-                  unsigned long long* stats, uint32_t* queue, cudaStream_t s) {
+                  unsigned long long* stats, uint32_t* queue, uint32_t* spill, cudaStream_t s) {
     if (!n) return;
-    static int configured_smem = 0;
-    const size_t smem = audit_smem_bytes();
+    static int configured_smem = 0, configured_large = 0;
+    const size_t smem = audit_smem_bytes(), large = audit_large_smem_bytes();
     if (configured_smem != int(smem)) {
         cudaFuncSetAttribute(k_audit, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
         configured_smem = int(smem);
+    }
+    if (spill && configured_large != int(large)) {
+        cudaFuncSetAttribute(k_audit_large, cudaFuncAttributeMaxDynamicSharedMemorySize, int(large));
+        configured_large = int(large);
     }
     int sms = 148, dev = 0;
     if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -549,8 +596,10 @@ void launch_audit(const CandidateRecord* records, uint32_t n, const PlanDev& pla
     uint64_t grid = uint64_t(sms) * per_sm;
     uint64_t needed = (units + kAuditWarps - 1) / kAuditWarps;
     if (grid > needed) grid = needed;
-    cudaMemsetAsync(queue, 0, 4, s);
-    k_audit<<<uint32_t(grid), kAuditWarps * 32, smem, s>>>(records, n, plan, out, stats, queue);
+    cudaMemsetAsync(queue, 0, spill ? 8 : 4, s);
+    if (spill) cudaMemsetAsync(spill, 0, 4, s);
+    k_audit<<<uint32_t(grid), kAuditWarps * 32, smem, s>>>(records, n, plan, out, stats, queue, spill);
+    if (spill) k_audit_large<<<uint32_t(sms), kLargeWarps * 32, large, s>>>(records, plan, out, stats, spill, queue + 1);
 }
 
 void launch_verdicts(const ViewRecord* const* plan_records, const uint32_t* plan_views, const uint32_t* plan_ss,

@@ -151,8 +151,11 @@ void launch_gather_window(const Edit* edits, const uint32_t* order, uint32_t fir
                           cudaStream_t s);
 cudaError_t sort_scores_desc(const float* keys_in, float* keys_out, const uint32_t* vals_in, uint32_t* vals_out,
                              uint32_t n, void* temp, size_t& temp_bytes, cudaStream_t s);
+// queue: 2 words (work cursors); spill: 1 + n * nviews words for the units
+// that overflow the warp tier's limits and go to the large tier (null: no
+// large tier, such units fall back to the full-raster path).
 void launch_audit(const CandidateRecord* records, uint32_t n, const PlanDev& plan, ViewRecord* out,
-                  unsigned long long* stats, uint32_t* queue, cudaStream_t s);
+                  unsigned long long* stats, uint32_t* queue, uint32_t* spill, cudaStream_t s);
 struct GateDev {
     GateSettings settings;
     uint32_t plan;

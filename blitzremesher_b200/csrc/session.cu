@@ -404,7 +404,7 @@ struct Session {
     Buf<uint8_t> verdict_dev;
     Buf<Measurement> meas_dev;
     Buf<blitz_collapse> collapse_dev;
-    Buf<uint32_t> exact_count, work_queue;
+    Buf<uint32_t> exact_count, work_queue, spill;
     Buf<const ViewRecord*> record_table;
     Buf<uint32_t> plan_views, plan_ss;
     Buf<GateDev> gate_table;
@@ -885,8 +885,9 @@ static void audit_candidates(Session& S, const blitz_collapse* cands_dev, const 
         Plan& p = *plans[i];
         if (p.resource_limited) throw Failure(BLITZ_BUDGET_LIMITED, "raster exceeds per-view sample budget");
         p.records.ensure(S.pool, size_t(nn) * p.views);
-        S.work_queue.ensure(S.pool, 1);
-        launch_audit(S.records.p, nn, p.dev, p.records.p, prof ? S.stats.p : nullptr, S.work_queue.p, st);
+        S.work_queue.ensure(S.pool, 2);
+        S.spill.ensure(S.pool, size_t(nn) * p.views + 1);
+        launch_audit(S.records.p, nn, p.dev, p.records.p, prof ? S.stats.p : nullptr, S.work_queue.p, S.spill.p, st);
         if (nn) S.profile.launches += 1, S.profile.audit_launches += 1;
         table[i] = p.records.p;
         pviews[i] = p.views;

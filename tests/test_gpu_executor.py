@@ -84,3 +84,32 @@ def test_candidates_of_committed_state_match_oracle(gpu_lib, oracle):
         stop = 4 if want.failed_gate == 0 else (want.failed_gate if want.failed_gate <= 4 else 0)
         for g in range(stop):
             assert measurement_fields(meas[i, g]) == measurement_fields(want.gates[g]), (i, g)
+
+
+@pytest.mark.parametrize("commit", [False, True])
+def test_large_regions_match_oracle(gpu_lib, oracle, commit):
+    """Coarse triangles at 64 px x ss 8: most (candidate, view) regions
+    overflow the warp tier and go to the large tier; verdicts and every gate
+    Measurement still equal the oracle's, and few candidates need the
+    full-raster path."""
+    mesh = syn.noisy_icosphere(2, 5)
+    views = (6, 0, 91)
+    args = _gates(64.0, views, 8)
+    with br.AuditSession(mesh) as s:
+        if commit:
+            s.execute(mesh.face_count - 40, 100, [br.eval_settings(*a) for a in args], batch=8)
+        idx, pos = s.state()
+        cands = br.midpoint_collapses(s.actions())
+        picks = cands[:: max(1, cands.size // 36)]
+        verdicts, meas = s.candidates(picks, [br.eval_settings(*a) for a in args], measurements=True)
+    assert np.mean(verdicts["exact_path"]) < (0.5 if commit else 0.25)
+    state = syn.Mesh(pos, idx)
+    b = oracle.bounds(mesh)
+    for i, c in enumerate(picks):
+        e = BoEdit()
+        e.from_, e.to = int(c["from"]), int(c["to"])
+        want = oracle.audit_candidate(state, e, mesh, mesh, b, [oracle_settings(*a) for a in args])
+        assert verdicts[i]["accepted"] == want.accepted and verdicts[i]["failed_gate"] == want.failed_gate, i
+        stop = 4 if want.failed_gate == 0 else (want.failed_gate if want.failed_gate <= 4 else 0)
+        for g in range(stop):
+            assert measurement_fields(meas[i, g]) == measurement_fields(want.gates[g]), (i, g)
