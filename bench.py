@@ -48,8 +48,8 @@ def peaks() -> dict:
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
         d = json.loads(p.read_text())
-        return {"hbm_gbs": float(d["hbm_gbs"]), "source": "measured"}
-    return {"hbm_gbs": 6650.0, "source": "fallback"}
+        return {"hbm_gbs": float(d["hbm_gbs"]), "bf16_tflops": float(d["bf16_tflops"]), "source": "measured"}
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "source": "fallback"}
 
 
 class ClockSampler:
@@ -312,19 +312,52 @@ def run_gpu(args) -> None:
             "gpu_launches": int(prof["launches"] // max(1, args.steps) * args.steps),
             "kernel_ms": {"prepare": prof["prepare_ms"] / args.steps, "audit": prof["audit_ms"] / args.steps,
                           "verdicts": prof["verdict_ms"] / args.steps}}
+    # Learned surrogate: trained on exact-audit labels of the icosphere family
+    # (seeds 2..9, states at 100/70/50/35/25% faces), judged on 16 held-out
+    # seeds (1001..1016): pruning to the top 25% and whole LOD steps.
+    model = None
+    if not args.no_surrogate:
+        from blitzremesher_b200 import surrogate_train as st
+        t0 = time.perf_counter()
+        train = st.generate(range(2, 10), [1.0, 0.7, 0.5, 0.35, 0.25], gates)
+        label_s = time.perf_counter() - t0
+        model = br.Surrogate(seed=1, device=local)
+        t0 = time.perf_counter()
+        history = st.fit(model, train)
+        fit_s = time.perf_counter() - t0
+        held_seeds = list(range(1001, 1017))
+        held = st.generate(held_seeds, [1.0, 0.5], gates)
+        cmp = st.chain_compare(model, held_seeds, 0.5, gates)
+        mlp = st.mlp_timing(model, held.features, held.labels)
+        line["surrogate"] = {
+            "model": "MLP 48-128-128-2, BF16 weights, FP32 accumulate (tcgen05)", "train_rows": int(
+                train.features.shape[0]), "label_s": label_s, "fit_s": fit_s, "loss": history,
+            "held_out_meshes": len(held_seeds), "held_rows": int(held.features.shape[0]),
+            "keep": 0.25, "pruning": st.pruning_stats(model, held), "lod_step_50pct": cmp["total"],
+            "triangle_gap": cmp["triangle_gap"], "speedup_vs_plain_batched": cmp["speedup_vs_plain_batched"],
+            "mlp": mlp,
+            "roofline": {"bound": "tensor", "kernel": "k_mlp<false>", "achieved": mlp["forward_tflops"],
+                         "peak": pk["bf16_tflops"], "unit": "TFLOP/s",
+                         "frac": mlp["forward_tflops"] / pk["bf16_tflops"],
+                         "peak_source": pk["source"] + " bf16_tflops (burst)"}}
     # LOD-chain step: the greedy executor from the source to 50% of its faces,
-    # with batches of one (the reference's sequential walk) and of 64.
+    # with batches of one (the reference's sequential walk), of 64, and of 64
+    # pruned by the surrogate.
     if not args.no_chain:
         line["chain"] = {"metric": "LOD-chain s/mesh", "unit": "s/mesh", "step": "one LOD step to 50% faces",
                          "timing": "wall clock around the host-orchestrated executor"}
-        for batch in (1, 64):
+        if model is not None:
+            session.attach_surrogate(model)
+        for batch, keep in ((1, 0), (64, 0), (64, 250)):
+            if keep and model is None:
+                continue
             session.reset()
             torch.cuda.synchronize(device)
             t0 = time.perf_counter()
-            chain = session.execute(mesh.face_count // 2, 1 << 30, gates, batch=batch)
+            chain = session.execute(mesh.face_count // 2, 1 << 30, gates, batch=batch, keep_permille=keep)
             torch.cuda.synchronize(device)
             chain_s = time.perf_counter() - t0
-            line["chain"][f"batch{batch}"] = {
+            line["chain"][f"batch{batch}" + ("_surrogate" if keep else "")] = {
                 "seconds": chain_s, "commits": int(len(chain["commits"])), "trials": int(chain["trials"]),
                 "audited": int(chain["audited"]), "final_faces": int(chain["final_faces"]),
                 "stop": int(chain["stop"])}
@@ -354,6 +387,7 @@ def main() -> None:
     ap.add_argument("--cpu-sample", type=int, default=32)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-chain", action="store_true")
+    ap.add_argument("--no-surrogate", action="store_true")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

@@ -99,7 +99,7 @@ def normalisation(features):
     return mean.float().cpu().numpy(), (1.0 / std).float().cpu().numpy()
 
 
-def fit(model: br.Surrogate, data: LabelSet, epochs: int = 4, batch_size: int = 8192, lr: float = 2e-3,
+def fit(model: br.Surrogate, data: LabelSet, epochs: int = 4, batch_size: int = 8192, lr: float = 1e-3,
         seed: int = 0) -> List[float]:
     """Adam on shuffled minibatches, halving the rate each epoch; returns the
     mean loss of each epoch."""
@@ -185,3 +185,79 @@ def chain_compare(model: br.Surrogate, seeds: Sequence[int], fraction: float, ga
     gap = (total["surrogate"]["final_faces"] - total["plain"]["final_faces"]) / max(1, total["plain"]["final_faces"])
     return {"meshes": rows, "total": total, "triangle_gap": gap,
             "speedup_vs_plain_batched": total["plain"]["seconds"] / max(1e-9, total["surrogate"]["seconds"])}
+
+
+def mlp_timing(model: br.Surrogate, features, labels, repeats: int = 5) -> dict:
+    """Device time of the tensor-core forward over all rows and of one fused
+    train step over the first 8192 rows (CUDA events on the current stream)."""
+    import torch
+    n = features.shape[0]
+    m = min(8192, n)
+    f8, l8 = features[:m].contiguous(), labels[:m].contiguous()
+    model.score(features)
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(repeats):
+        model.score(features)
+    b.record()
+    torch.cuda.synchronize()
+    fwd_ms = a.elapsed_time(b) / repeats
+    params, mean, inv = model.parameters()
+    a.record()
+    for _ in range(repeats):
+        model.gradients(f8, l8)
+    b.record()
+    torch.cuda.synchronize()
+    train_ms = a.elapsed_time(b) / repeats
+    model.load(params, mean, inv)
+    flops_row = 2 * (48 * 128 + 128 * 128 + 128 * 2)
+    return {"forward_rows": int(n), "forward_ms": fwd_ms, "forward_rows_per_s": n / (fwd_ms * 1e-3),
+            "forward_tflops": flops_row * n / (fwd_ms * 1e-3) / 1e12, "train_rows": int(m),
+            "train_ms_incl_host": train_ms, "train_tflops": 3 * flops_row * m / (train_ms * 1e-3) / 1e12,
+            "flops_per_row_forward": flops_row}
+
+
+def main(argv=None) -> None:
+    """Trains a surrogate on exact-audit labels of the 20,480-face icosphere
+    family and reports pruning and LOD-step statistics on held-out meshes."""
+    import argparse
+    import json
+    ap = argparse.ArgumentParser(description=main.__doc__)
+    ap.add_argument("--train-seeds", type=int, default=8)
+    ap.add_argument("--held-seeds", type=int, default=4)
+    ap.add_argument("--screen", type=float, default=24.0)
+    ap.add_argument("--views", type=int, default=32)
+    ap.add_argument("--epochs", type=int, default=4)
+    ap.add_argument("--fraction", type=float, default=0.5)
+    ap.add_argument("--keep-permille", type=int, default=250)
+    ap.add_argument("--fractions", default="1,0.7,0.5,0.35,0.25", help="label states (face fractions)")
+    ap.add_argument("--out", default=None, help="write the trained parameters (.npz)")
+    a = ap.parse_args(argv)
+    gates = c1_gates(screen=a.screen, views=a.views)
+    fractions = [float(x) for x in a.fractions.split(",")]
+    t0 = time.perf_counter()
+    train = generate(range(2, 2 + a.train_seeds), fractions, gates)
+    gen_s = time.perf_counter() - t0
+    model = br.Surrogate(seed=1)
+    t0 = time.perf_counter()
+    history = fit(model, train, epochs=a.epochs)
+    fit_s = time.perf_counter() - t0
+    held_seeds = list(range(1001, 1001 + a.held_seeds))
+    held = generate(held_seeds, fractions, gates)
+    untrained = br.Surrogate(seed=1)
+    untrained.load(untrained.parameters()[0], *normalisation(train.features))
+    report = {"screen": a.screen, "train_rows": int(train.features.shape[0]), "label_s": gen_s, "fit_s": fit_s,
+              "loss": history, "held_rows": int(held.features.shape[0]),
+              "pruning": pruning_stats(model, held, a.keep_permille / 1000),
+              "pruning_untrained": pruning_stats(untrained, held, a.keep_permille / 1000),
+              "chain": chain_compare(model, held_seeds, a.fraction, gates, keep_permille=a.keep_permille)["total"],
+              "mlp": mlp_timing(model, held.features, held.labels)}
+    if a.out:
+        p, mean, inv = model.parameters()
+        np.savez(a.out, params=p, mean=mean, inv_std=inv)
+    print(json.dumps(report), flush=True)
+
+
+if __name__ == "__main__":
+    main()
