@@ -44,6 +44,13 @@ GATE_ARGS = [(SCREEN, SOURCE_LIMIT, VIEWS, SS, SS, 1.0), (SCREEN, TRANSITION_LIM
              (SCREEN, SOURCE_LIMIT, VIEWS, SS, SS, 1.0), (SCREEN, TRANSITION_LIMIT, VIEWS, SS, SS, 1.0)]
 
 
+# DRAM bytes (read + write) of one k_audit launch of this workload and its
+# issue-slot utilisation, from one ncu --set full capture on a B200: the
+# working set is L2-resident, the kernel is issue-bound.
+K_AUDIT_TRAFFIC = 45_381_120
+K_AUDIT_ISSUE_PCT = 65.6
+
+
 def peaks() -> dict:
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -300,7 +307,8 @@ def run_gpu(args) -> None:
                        "l2": "resident working set 2.5 MB < L2 (no flush); per step all candidates re-audited",
                        "parallelism": f"dp{world} (one mesh per rank)"},
             "roofline": {"bound": "hbm", "achieved": achieved_gbs, "peak": pk["hbm_gbs"], "unit": "GB/s",
-                         "frac": achieved_gbs / pk["hbm_gbs"], "traffic": None,
+                         "frac": achieved_gbs / pk["hbm_gbs"], "traffic": K_AUDIT_TRAFFIC,
+                         "issue_active_pct_ncu": K_AUDIT_ISSUE_PCT,
                          "kernel": "k_audit", "kernel_ms": audit_ms, "algorithmic_bytes": alg_bytes,
                          "peak_source": pk["source"] + " hbm_gbs (burst)",
                          "units_per_launch": prof["units"] / launches,
