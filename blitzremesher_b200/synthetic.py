@@ -139,3 +139,190 @@ def grid(n: int, scale: float = 1.0, bend: float = 0.0, two_sided: bool = True) 
 def config1_mesh(seed: int = 1) -> Mesh:
     """Plain-audit workload mesh: icosphere level 5 (20,480 faces), +-2% radial noise."""
     return noisy_icosphere(5, seed, 0.02)
+
+
+# ---------------------------------------------------------------------------
+# Batched-audit mesh set: noise-displaced spheres, tori (R/r = 3) and open
+# heightfield grids, each with FP32 UVs split into 4-16 charts. A chart seam
+# duplicates its vertices (same position, different UV), so the position weld
+# joins them into one geometric class with two wedges.
+
+def _hash3(ix, iy, iz, seed: int) -> np.ndarray:
+    """Vectorised 64-bit lattice hash -> doubles in [0, 1)."""
+    with np.errstate(over="ignore"):
+        h = (ix.astype(np.uint64) * np.uint64(0x9E3779B97F4A7C15)) ^ \
+            (iy.astype(np.uint64) * np.uint64(0xC2B2AE3D27D4EB4F)) ^ \
+            (iz.astype(np.uint64) * np.uint64(0x165667B19E3779F9)) ^ np.uint64(seed * 0x27D4EB2F165667C5 & MASK64)
+        h ^= h >> np.uint64(30)
+        h *= np.uint64(0xBF58476D1CE4E5B9)
+        h ^= h >> np.uint64(27)
+        h *= np.uint64(0x94D049BB133111EB)
+        h ^= h >> np.uint64(31)
+    return (h >> np.uint64(11)).astype(np.float64) * (1.0 / (1 << 53))
+
+
+def value_noise(p: np.ndarray, seed: int, octaves: int = 4, frequency: float = 2.0) -> np.ndarray:
+    """Sum of `octaves` octaves of trilinear value noise (smoothstep weights),
+    amplitude halving and frequency doubling per octave, in about [-1, 1]."""
+    p = np.asarray(p, np.float64)
+    if p.shape[1] == 2:
+        p = np.concatenate([p, np.zeros((p.shape[0], 1))], 1)
+    total = np.zeros(p.shape[0])
+    amp, norm = 1.0, 0.0
+    for o in range(octaves):
+        q = p * frequency * (2 ** o)
+        i = np.floor(q).astype(np.int64)
+        f = q - i
+        w = f * f * (3 - 2 * f)
+        acc = np.zeros(p.shape[0])
+        for dx in (0, 1):
+            for dy in (0, 1):
+                for dz in (0, 1):
+                    h = _hash3(i[:, 0] + dx, i[:, 1] + dy, i[:, 2] + dz, seed + 7919 * o)
+                    wx = w[:, 0] if dx else 1 - w[:, 0]
+                    wy = w[:, 1] if dy else 1 - w[:, 1]
+                    wz = w[:, 2] if dz else 1 - w[:, 2]
+                    acc += (2 * h - 1) * wx * wy * wz
+        total += amp * acc
+        norm += amp
+        amp *= 0.5
+    return total / norm
+
+
+def _cuts(n: int, parts: int) -> list:
+    parts = max(1, min(parts, n))
+    return [round(k * n / parts) for k in range(parts + 1)]
+
+
+def _chart_grid(nu: int, nv: int, cuts_u: list, cuts_v: list, position, wrap_u: bool, wrap_v: bool):
+    """Grid of nu x nv cells split into charts at the cut lines. `position(i, j)`
+    maps integer lattice coordinates (already wrapped) to (k, 3) float32
+    positions. Each chart owns its vertices; its UVs tile an atlas."""
+    pos, uv, faces = [], [], []
+    base = 0
+    cu, cv = len(cuts_u) - 1, len(cuts_v) - 1
+    for a in range(cu):
+        for b in range(cv):
+            u0, u1, v0, v1 = cuts_u[a], cuts_u[a + 1], cuts_v[b], cuts_v[b + 1]
+            ii, jj = np.meshgrid(np.arange(u0, u1 + 1), np.arange(v0, v1 + 1), indexing="ij")
+            ii, jj = ii.reshape(-1), jj.reshape(-1)
+            wi = ii % nu if wrap_u else ii
+            wj = jj % nv if wrap_v else jj
+            pos.append(position(wi, wj))
+            tile_u = (a + (ii - u0) / max(1, u1 - u0) * 0.9) / cu
+            tile_v = (b + (jj - v0) / max(1, v1 - v0) * 0.9) / cv
+            uv.append(np.stack([tile_u, tile_v], 1).astype(np.float32))
+            w = v1 - v0 + 1
+            ci, cj = np.meshgrid(np.arange(u1 - u0), np.arange(v1 - v0), indexing="ij")
+            ci, cj = ci.reshape(-1), cj.reshape(-1)
+            p00 = base + ci * w + cj
+            p10, p01 = p00 + w, p00 + 1
+            p11 = p10 + 1
+            faces.append(np.stack([np.stack([p00, p10, p11], 1), np.stack([p00, p11, p01], 1)], 1).reshape(-1, 3))
+            base += ii.size
+    return np.concatenate(pos).astype(np.float32), np.concatenate(faces), np.concatenate(uv)
+
+
+def _orient_by(pos: np.ndarray, faces: np.ndarray, outward: np.ndarray) -> np.ndarray:
+    """Flips faces whose normal points against `outward` (per face)."""
+    a, b, c = pos[faces[:, 0]].astype(np.float64), pos[faces[:, 1]].astype(np.float64), pos[faces[:, 2]].astype(
+        np.float64)
+    n = np.cross(b - a, c - a)
+    flip = (n * outward).sum(1) < 0
+    faces = faces.copy()
+    faces[flip, 1], faces[flip, 2] = faces[flip, 2].copy(), faces[flip, 1].copy()
+    return faces
+
+
+def seamed_sphere(target_faces: int, seed: int, amplitude: float = 0.05) -> Mesh:
+    """Cube-sphere (each cube face a chart, or two) with value-noise radial
+    displacement; about target_faces faces (12 n^2)."""
+    n = max(2, int(round((target_faces / 12) ** 0.5)))
+    split = int(splitmix64(seed ^ 0x5EA, 1)[0] % np.uint64(2)) + 1  # 6 or 12 charts
+    pos, faces, uv = [], [], []
+    base = 0
+    axes = [(0, 1, 2, 1.0), (0, 1, 2, -1.0), (1, 2, 0, 1.0), (1, 2, 0, -1.0), (2, 0, 1, 1.0), (2, 0, 1, -1.0)]
+    for k, (ax, a1, a2, sign) in enumerate(axes):
+        def position(i, j, ax=ax, a1=a1, a2=a2, sign=sign):
+            c = np.zeros((i.size, 3))
+            c[:, ax] = sign
+            c[:, a1] = -1.0 + 2.0 * i / n
+            c[:, a2] = -1.0 + 2.0 * j / n
+            d = c / np.linalg.norm(c, axis=1, keepdims=True)
+            r = 1.0 + amplitude * value_noise(d, seed)
+            return (d * r[:, None]).astype(np.float32)
+        p, f, t = _chart_grid(n, n, _cuts(n, split), [0, n], position, False, False)
+        t = (t + np.array([k % 3, k // 3], np.float32)) / np.array([3, 2], np.float32)
+        pos.append(p)
+        faces.append(f + base)
+        uv.append(t.astype(np.float32))
+        base += p.shape[0]
+    pos = np.concatenate(pos)
+    faces = np.concatenate(faces)
+    cent = pos[faces].astype(np.float64).mean(1)
+    faces = _orient_by(pos, faces, cent)
+    return Mesh(pos, faces.astype(np.uint32).reshape(-1), uv=np.concatenate(uv), name=f"sphere-{seed}",
+                meta={"kind": "sphere", "charts": 6 * split, "seed": seed})
+
+
+def seamed_torus(target_faces: int, seed: int, charts: int, amplitude: float = 0.02) -> Mesh:
+    """Torus with R/r = 3 (R = 0.75, r = 0.25), nu = 3 nv cells, charts cut
+    along both directions, light value-noise displacement."""
+    nv = max(3, int(round((target_faces / 6) ** 0.5)))
+    nu = 3 * nv
+    cu = max(2, min(charts // 2, nu))
+    cv = max(1, charts // cu)
+    R, r = 0.75, 0.25
+
+    def position(i, j):
+        tu, tv = 2 * np.pi * i / nu, 2 * np.pi * j / nv
+        base = np.stack([np.cos(tu), np.sin(tu), np.zeros_like(tu)], 1)
+        p = base * (R + r * np.cos(tv))[:, None]
+        p[:, 2] = r * np.sin(tv)
+        return (p * (1.0 + amplitude * value_noise(p, seed))[:, None]).astype(np.float32)
+
+    pos, faces, uv = _chart_grid(nu, nv, _cuts(nu, cu), _cuts(nv, cv), position, True, True)
+    c = pos[faces].astype(np.float64).mean(1)
+    ring = c.copy()
+    ring[:, 2] = 0
+    ring = ring / np.linalg.norm(ring, axis=1, keepdims=True) * R
+    faces = _orient_by(pos, faces, c - ring)
+    return Mesh(pos, faces.astype(np.uint32).reshape(-1), uv=uv, name=f"torus-{seed}",
+                meta={"kind": "torus", "charts": cu * cv, "seed": seed})
+
+
+def seamed_heightfield(target_faces: int, seed: int, charts: int, height: float = 0.15) -> Mesh:
+    """Open n x n grid over [-1, 1]^2 with 4-octave value-noise heights."""
+    n = max(2, int(round((target_faces / 2) ** 0.5)))
+    cu = max(2, int(round(charts ** 0.5)))
+    cv = max(2, charts // cu)
+
+    def position(i, j):
+        x, y = -1.0 + 2.0 * i / n, -1.0 + 2.0 * j / n
+        z = height * value_noise(np.stack([x, y], 1), seed, octaves=4)
+        return np.stack([x, y, z], 1).astype(np.float32)
+
+    pos, faces, uv = _chart_grid(n, n, _cuts(n, cu), _cuts(n, cv), position, False, False)
+    up = np.zeros((faces.shape[0], 3))
+    up[:, 2] = 1
+    faces = _orient_by(pos, faces, up)
+    return Mesh(pos, faces.astype(np.uint32).reshape(-1), uv=uv, name=f"heightfield-{seed}",
+                meta={"kind": "heightfield", "charts": cu * cv, "seed": seed})
+
+
+def batched_set(count: int = 64, seed: int = 2, lo: int = 2000, hi: int = 200000) -> list:
+    """The batched-audit mesh set: `count` meshes cycling sphere / torus /
+    heightfield, face counts log-uniform in [lo, hi], 4-16 UV charts each."""
+    u = uniform(seed, 2 * count, 0.0, 1.0)
+    meshes = []
+    for k in range(count):
+        faces = int(round(np.exp(np.log(lo) + (np.log(hi) - np.log(lo)) * u[k])))
+        charts = 4 + int(u[count + k] * 13)
+        s = seed * 1000 + k
+        if k % 3 == 0:
+            meshes.append(seamed_sphere(faces, s))
+        elif k % 3 == 1:
+            meshes.append(seamed_torus(faces, s, charts))
+        else:
+            meshes.append(seamed_heightfield(faces, s, charts))
+    return meshes
