@@ -148,6 +148,11 @@ EXPORTS = {
     "blitz_audit_surrogate_features": ([C.c_void_p, C.c_double, C.c_double, C.c_void_p, C.c_void_p, C.c_size_t,
                                         C.POINTER(C.c_size_t), C.c_char_p, C.c_size_t], C.c_int),
     "blitz_audit_attach_surrogate": ([C.c_void_p, C.c_void_p, C.c_char_p, C.c_size_t], C.c_int),
+    "blitz_audit_batch_create": ([C.c_void_p, C.c_size_t, C.c_void_p, C.c_char_p, C.c_size_t], C.c_int),
+    "blitz_audit_batch_destroy": ([C.c_void_p], None),
+    "blitz_audit_batch_candidates": ([C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(EvalSettings), C.c_void_p,
+                                      C.c_uint32, C.c_void_p, C.c_char_p, C.c_size_t], C.c_int),
+    "blitz_audit_batch_read_info": ([C.c_void_p, C.c_void_p], C.c_int),
     "blitz_audit_state": ([C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p, C.c_size_t, C.POINTER(C.c_uint32),
                            C.c_char_p, C.c_size_t], C.c_int),
     "blitz_audit_reset": ([C.c_void_p, C.c_char_p, C.c_size_t], C.c_int),
@@ -164,6 +169,15 @@ class Execution(C.Structure):
 class ExecuteOptions(C.Structure):
     _fields_ = [("struct_size", C.c_uint32), ("batch", C.c_uint32), ("keep_permille", C.c_uint32),
                 ("reserved", C.c_uint32 * 5)]
+
+
+class BatchInfo(C.Structure):
+    _fields_ = [("struct_size", C.c_uint32), ("sessions", C.c_uint32), ("tier", C.c_uint32), ("tuned", C.c_uint32),
+                ("graph_captured", C.c_uint32), ("tune_ms", C.c_float * 2), ("graph_launches", C.c_uint64),
+                ("exact_candidates", C.c_uint64)]
+
+
+BATCH_GRAPH, BATCH_AUTOTUNE = 1, 2
 
 
 class AuditProfile(C.Structure):
@@ -420,6 +434,58 @@ class AuditSession:
         i.struct_size = C.sizeof(NeuralInfo)
         assert self.lib.blitz_audit_session_info(self.handle, C.byref(i)) == BLITZ_OK
         return {k: getattr(i, k) for k, _ in i._fields_ if k != "struct_size"}
+
+
+class AuditBatch:
+    """Several sessions audited together: one persistent audit launch per plan
+    slot over all their (candidate, view) units, optionally replayed from a
+    captured CUDA graph and with the warp tier picked by timing both."""
+
+    def __init__(self, sessions: Sequence[AuditSession]):
+        self.lib = load()
+        self.sessions = list(sessions)
+        arr = (C.c_void_p * len(self.sessions))(*[s.handle for s in self.sessions])
+        self.handle = C.c_void_p()
+        err = C.create_string_buffer(512)
+        _check(self.lib.blitz_audit_batch_create(arr, len(self.sessions), C.byref(self.handle), err, 512), err)
+
+    def close(self) -> None:
+        if self.handle:
+            self.lib.blitz_audit_batch_destroy(self.handle)
+            self.handle = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def candidates_device(self, collapses_ptr: int, counts: Sequence[int], gates: Sequence[EvalSettings],
+                          verdicts_ptr: int, flags: int = 0, stream: int = 0) -> None:
+        cnt = (C.c_size_t * len(counts))(*counts)
+        g = (EvalSettings * 4)(*gates)
+        err = C.create_string_buffer(512)
+        _check(self.lib.blitz_audit_batch_candidates(self.handle, collapses_ptr, cnt, g, verdicts_ptr, flags,
+                                                     stream or None, err, 512), err)
+
+    def candidates(self, collapses: Sequence[np.ndarray], gates: Sequence[EvalSettings], flags: int = 0):
+        """Host convenience: per-session collapse arrays in, per-session verdicts out."""
+        import torch
+        counts = [int(c.size) for c in collapses]
+        cat = np.concatenate([np.ascontiguousarray(c, dtype=COLLAPSE_DTYPE) for c in collapses])
+        dev = torch.from_numpy(cat.view(np.uint8).copy()).cuda()
+        out = torch.zeros(max(1, cat.size) * VERDICT_DTYPE.itemsize, dtype=torch.uint8, device="cuda")
+        self.candidates_device(dev.data_ptr(), counts, gates, out.data_ptr(), flags)
+        v = out.cpu().numpy().view(VERDICT_DTYPE)[: cat.size]
+        return np.split(v, np.cumsum(counts)[:-1])
+
+    def info(self) -> dict:
+        i = BatchInfo()
+        i.struct_size = C.sizeof(BatchInfo)
+        assert self.lib.blitz_audit_batch_read_info(self.handle, C.byref(i)) == BLITZ_OK
+        d = {k: getattr(i, k) for k, _ in i._fields_ if k != "struct_size"}
+        d["tune_ms"] = list(i.tune_ms)
+        return d
 
 
 SURROGATE_FEATURES = 48

@@ -32,6 +32,15 @@ struct LimitsSmall {
     static constexpr int kQueue = 160;         // changed samples per (candidate, view)
     static constexpr int kAffected = 8;        // tiles outside the region whose distances may change
 };
+// A wider warp tier for workloads whose units often overflow the small one
+// (one block of 8 warps per SM instead of three).
+struct LimitsMedium {
+    static constexpr int kRegionWords = 8;
+    static constexpr int kRegionRows = 128;
+    static constexpr int kDeltaSamples = 8192;
+    static constexpr int kQueue = 640;
+    static constexpr int kAffected = 16;
+};
 struct LimitsLarge {
     static constexpr int kRegionWords = 8;
     static constexpr int kRegionRows = 256;
@@ -40,6 +49,16 @@ struct LimitsLarge {
     static constexpr int kAffected = 32;
 };
 constexpr int kLargeWarps = 3; // warps per block of the large tier
+// The huge tier keeps its per-warp scratch in global memory (L2-resident
+// working set per unit): regions up to 1024 x 1024 samples.
+struct LimitsHuge {
+    static constexpr int kRegionWords = 32;
+    static constexpr int kRegionRows = 1024;
+    static constexpr int kDeltaSamples = 1 << 20;
+    static constexpr int kQueue = 16384;
+    static constexpr int kAffected = 64;
+};
+constexpr int kHugeWarps = 8;
 
 template <class L> struct WarpScratch {
     double vx[32], vy[32], vz[32]; // projected local vertices; 31 = placement
@@ -462,38 +481,62 @@ __device__ void audit_unit(const CandidateRecord* __restrict__ rec, const PlanDe
     __syncwarp();
 }
 
+// Unit u of a job -> its plan, candidate record, output slot and local index.
+// A job is one plan over one candidate array, or a table of entries (one per
+// session of a batch) whose units are concatenated in entry order.
+__device__ __forceinline__ void resolve_unit(const AuditJob& job, uint32_t u, const PlanDev*& plan,
+                                             const CandidateRecord*& recs, ViewRecord*& out, uint32_t& local) {
+    if (!job.entries) {
+        plan = &job.plan, recs = job.recs, out = job.out, local = u;
+        return;
+    }
+    uint32_t lo = 0, hi = job.nentries - 1;
+    while (lo < hi) { // last entry whose first unit is <= u
+        const uint32_t mid = (lo + hi + 1) >> 1;
+        if (job.entries[mid].first_unit <= u) lo = mid;
+        else hi = mid - 1;
+    }
+    const AuditEntry& e = job.entries[lo];
+    plan = &e.plan, recs = e.recs, out = e.out, local = u - uint32_t(e.first_unit);
+}
+
 // Persistent warps pull (candidate, view) units, candidate-major, from `queue`.
-__global__ void __launch_bounds__(kAuditWarps * 32, B200_AUDIT_MIN_BLOCKS) k_audit(const CandidateRecord* __restrict__ recs, uint32_t n,
-                                                             PlanDev plan, ViewRecord* out,
-                                                             unsigned long long* stats, uint32_t* queue,
-                                                             uint32_t* spill) {
+// kMulti = false: a single plan (kernel parameters only, no table lookup).
+// L: the warp tier's limits; kMinBlocks: resident blocks the registers target.
+template <bool kMulti, class L, int kMinBlocks>
+__global__ void __launch_bounds__(kAuditWarps * 32, kMinBlocks)
+    k_audit(const __grid_constant__ AuditJob job, unsigned long long* stats, uint32_t* queue, uint32_t* spill) {
     extern __shared__ __align__(16) unsigned char smem[];
-    WarpScratch<LimitsSmall>& ws = reinterpret_cast<WarpScratch<LimitsSmall>*>(smem)[threadIdx.x >> 5];
+    WarpScratch<L>& ws = reinterpret_cast<WarpScratch<L>*>(smem)[threadIdx.x >> 5];
     const uint32_t lane = lane_id();
-    const uint64_t total = uint64_t(n) * plan.nviews;
     for (;;) {
         uint32_t u = 0;
         if (lane == 0) u = atomicAdd(queue, 1u);
         u = __shfl_sync(0xffffffffu, u, 0);
-        if (u >= total) break;
-        const uint32_t c = u / plan.nviews, v = u - c * plan.nviews;
+        if (u >= job.total) break;
+        const PlanDev* plan = &job.plan;
+        const CandidateRecord* recs = job.recs;
+        ViewRecord* out = job.out;
+        uint32_t lu = u;
+        if (kMulti) resolve_unit(job, u, plan, recs, out, lu);
+        const uint32_t c = lu / plan->nviews, v = lu - c * plan->nviews;
         const CandidateRecord* rec = recs + c;
-        ViewRecord* slot = out + u;
+        ViewRecord* slot = out + lu;
         if (!rec->valid || !rec->fast) {
             ViewRecord r{};
             r.flags = rec->valid ? kRecFallback : 0;
             record_write(slot, r);
             continue;
         }
-        audit_unit(rec, plan, v, ws, slot, stats, u, spill);
+        audit_unit(rec, *plan, v, ws, slot, stats, u, spill);
     }
 }
 
-// The large tier: persistent warps over the spilled unit list {count, units}.
-__global__ void __launch_bounds__(kLargeWarps * 32, 1) k_audit_large(const CandidateRecord* __restrict__ recs,
-                                                                     PlanDev plan, ViewRecord* out,
-                                                                     unsigned long long* stats,
-                                                                     const uint32_t* spill, uint32_t* cursor) {
+// The large tier: persistent warps over the spilled unit list {count,
+// units}; what overflows it too is appended to `spill_next` (may be null).
+__global__ void __launch_bounds__(kLargeWarps * 32, 1)
+    k_audit_large(const __grid_constant__ AuditJob job, unsigned long long* stats, const uint32_t* spill,
+                  uint32_t* cursor, uint32_t* spill_next) {
     extern __shared__ __align__(16) unsigned char smem[];
     WarpScratch<LimitsLarge>& ws = reinterpret_cast<WarpScratch<LimitsLarge>*>(smem)[threadIdx.x >> 5];
     const uint32_t lane = lane_id();
@@ -504,8 +547,39 @@ __global__ void __launch_bounds__(kLargeWarps * 32, 1) k_audit_large(const Candi
         k = __shfl_sync(0xffffffffu, k, 0);
         if (k >= count) break;
         const uint32_t u = spill[1 + k];
-        const uint32_t c = u / plan.nviews, v = u - c * plan.nviews;
-        audit_unit(recs + c, plan, v, ws, out + u, stats, u, nullptr);
+        const PlanDev* plan;
+        const CandidateRecord* recs;
+        ViewRecord* out;
+        uint32_t lu;
+        resolve_unit(job, u, plan, recs, out, lu);
+        const uint32_t c = lu / plan->nviews, v = lu - c * plan->nviews;
+        audit_unit(recs + c, *plan, v, ws, out + lu, stats, u, spill_next);
+    }
+}
+
+// The huge tier: the same over the large tier's spill list, each warp with
+// its own slot of global scratch (`scratch`, one WarpScratch<LimitsHuge> per
+// resident warp).
+__global__ void __launch_bounds__(kHugeWarps * 32, 1)
+    k_audit_huge(const __grid_constant__ AuditJob job, unsigned long long* stats, const uint32_t* spill,
+                 uint32_t* cursor, unsigned char* scratch) {
+    const uint32_t lane = lane_id();
+    const uint32_t slot = blockIdx.x * kHugeWarps + (threadIdx.x >> 5);
+    WarpScratch<LimitsHuge>& ws = reinterpret_cast<WarpScratch<LimitsHuge>*>(scratch)[slot];
+    const uint32_t count = spill[0];
+    for (;;) {
+        uint32_t k = 0;
+        if (lane == 0) k = atomicAdd(cursor, 1u);
+        k = __shfl_sync(0xffffffffu, k, 0);
+        if (k >= count) break;
+        const uint32_t u = spill[1 + k];
+        const PlanDev* plan;
+        const CandidateRecord* recs;
+        ViewRecord* out;
+        uint32_t lu;
+        resolve_unit(job, u, plan, recs, out, lu);
+        const uint32_t c = lu / plan->nviews, v = lu - c * plan->nviews;
+        audit_unit(recs + c, *plan, v, ws, out + lu, stats, u, nullptr);
     }
 }
 
@@ -573,33 +647,54 @@ __global__ void k_verdicts(const ViewRecord* const* plan_records, const uint32_t
 
 size_t audit_smem_bytes() { return kAuditWarps * sizeof(WarpScratch<LimitsSmall>); }
 size_t audit_large_smem_bytes() { return kLargeWarps * sizeof(WarpScratch<LimitsLarge>); }
+size_t audit_huge_scratch_bytes(uint32_t sms) { return size_t(sms) * kHugeWarps * sizeof(WarpScratch<LimitsHuge>); }
 
-void launch_audit(const CandidateRecord* records, uint32_t n, const PlanDev& plan, ViewRecord* out,
-                  unsigned long long* stats, uint32_t* queue, uint32_t* spill, cudaStream_t s) {
-    if (!n) return;
-    static int configured_smem = 0, configured_large = 0;
-    const size_t smem = audit_smem_bytes(), large = audit_large_smem_bytes();
-    if (configured_smem != int(smem)) {
-        cudaFuncSetAttribute(k_audit, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-        configured_smem = int(smem);
+namespace {
+template <class K> void set_smem(K kernel, size_t bytes) {
+    cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes));
+}
+// Warp tier kernels: [variant][multi]
+using AuditKernel = void (*)(AuditJob, unsigned long long*, uint32_t*, uint32_t*);
+AuditKernel warp_tier(int variant, bool multi) {
+    if (variant == kAuditTierMedium) return multi ? k_audit<true, LimitsMedium, 1> : k_audit<false, LimitsMedium, 1>;
+    return multi ? k_audit<true, LimitsSmall, B200_AUDIT_MIN_BLOCKS> : k_audit<false, LimitsSmall, B200_AUDIT_MIN_BLOCKS>;
+}
+size_t warp_tier_smem(int variant) {
+    return kAuditWarps * (variant == kAuditTierMedium ? sizeof(WarpScratch<LimitsMedium>) : sizeof(WarpScratch<LimitsSmall>));
+}
+} // namespace
+
+void launch_audit(const AuditJob& job, unsigned long long* stats, uint32_t* queue, uint32_t* spill,
+                  uint32_t* spill_huge, unsigned char* huge_scratch, uint32_t huge_blocks, cudaStream_t s,
+                  int variant) {
+    if (!job.total) return;
+    static bool configured = false;
+    const size_t large = audit_large_smem_bytes();
+    if (!configured) {
+        for (int v = 0; v < 2; ++v)
+            for (int m = 0; m < 2; ++m) set_smem(warp_tier(v, m != 0), warp_tier_smem(v));
+        set_smem(k_audit_large, large);
+        configured = true;
     }
-    if (spill && configured_large != int(large)) {
-        cudaFuncSetAttribute(k_audit_large, cudaFuncAttributeMaxDynamicSharedMemorySize, int(large));
-        configured_large = int(large);
-    }
+    const AuditKernel kernel = warp_tier(variant, job.entries != nullptr);
+    const size_t smem = warp_tier_smem(variant);
     int sms = 148, dev = 0;
     if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_audit, kAuditWarps * 32, smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kAuditWarps * 32, smem);
     if (per_sm < 1) per_sm = 1;
-    uint64_t units = uint64_t(n) * plan.nviews;
     uint64_t grid = uint64_t(sms) * per_sm;
-    uint64_t needed = (units + kAuditWarps - 1) / kAuditWarps;
+    uint64_t needed = (job.total + kAuditWarps - 1) / kAuditWarps;
     if (grid > needed) grid = needed;
-    cudaMemsetAsync(queue, 0, spill ? 8 : 4, s);
+    const bool huge = spill && spill_huge && huge_scratch && huge_blocks;
+    cudaMemsetAsync(queue, 0, spill ? (huge ? 12 : 8) : 4, s);
     if (spill) cudaMemsetAsync(spill, 0, 4, s);
-    k_audit<<<uint32_t(grid), kAuditWarps * 32, smem, s>>>(records, n, plan, out, stats, queue, spill);
-    if (spill) k_audit_large<<<uint32_t(sms), kLargeWarps * 32, large, s>>>(records, plan, out, stats, spill, queue + 1);
+    if (huge) cudaMemsetAsync(spill_huge, 0, 4, s);
+    kernel<<<uint32_t(grid), kAuditWarps * 32, smem, s>>>(job, stats, queue, spill);
+    if (spill)
+        k_audit_large<<<uint32_t(sms), kLargeWarps * 32, large, s>>>(job, stats, spill, queue + 1,
+                                                                     huge ? spill_huge : nullptr);
+    if (huge) k_audit_huge<<<huge_blocks, kHugeWarps * 32, 0, s>>>(job, stats, spill_huge, queue + 2, huge_scratch);
 }
 
 void launch_verdicts(const ViewRecord* const* plan_records, const uint32_t* plan_views, const uint32_t* plan_ss,

@@ -151,11 +151,34 @@ void launch_gather_window(const Edit* edits, const uint32_t* order, uint32_t fir
                           cudaStream_t s);
 cudaError_t sort_scores_desc(const float* keys_in, float* keys_out, const uint32_t* vals_in, uint32_t* vals_out,
                              uint32_t n, void* temp, size_t& temp_bytes, cudaStream_t s);
-// queue: 2 words (work cursors); spill: 1 + n * nviews words for the units
+// queue: 3 words (work cursors); spill: 1 + n * nviews words for the units
 // that overflow the warp tier's limits and go to the large tier (null: no
-// large tier, such units fall back to the full-raster path).
-void launch_audit(const CandidateRecord* records, uint32_t n, const PlanDev& plan, ViewRecord* out,
-                  unsigned long long* stats, uint32_t* queue, uint32_t* spill, cudaStream_t s);
+// large tier, such units fall back to the full-raster path); spill_huge: the
+// same for units that overflow the large tier, audited by the huge tier with
+// huge_scratch (audit_huge_scratch_bytes(huge_blocks)) in global memory.
+// One plan's units (candidates x views), or (entries != null) the
+// concatenated units of several sessions' plans audited in one launch.
+struct AuditEntry {
+    PlanDev plan;
+    const CandidateRecord* recs;
+    ViewRecord* out;
+    uint64_t first_unit;
+};
+struct AuditJob {
+    PlanDev plan;
+    const CandidateRecord* recs;
+    ViewRecord* out;
+    const AuditEntry* entries; // device table, sorted by first_unit, or null
+    uint32_t nentries;
+    uint64_t total;            // units
+};
+// variant: the warp tier's limits (kAuditTierSmall: regions up to 128 x 64
+// samples, 3 blocks per SM; kAuditTierMedium: 256 x 128, 1 block per SM).
+constexpr int kAuditTierSmall = 0, kAuditTierMedium = 1;
+void launch_audit(const AuditJob& job, unsigned long long* stats, uint32_t* queue, uint32_t* spill,
+                  uint32_t* spill_huge, unsigned char* huge_scratch, uint32_t huge_blocks, cudaStream_t s,
+                  int variant = kAuditTierSmall);
+size_t audit_huge_scratch_bytes(uint32_t blocks);
 struct GateDev {
     GateSettings settings;
     uint32_t plan;

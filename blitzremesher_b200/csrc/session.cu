@@ -13,6 +13,7 @@
 #include <cstdio>
 #include <map>
 #include <memory>
+#include <mutex>
 #include <stdexcept>
 #include <string>
 #include <tuple>
@@ -404,7 +405,7 @@ struct Session {
     Buf<uint8_t> verdict_dev;
     Buf<Measurement> meas_dev;
     Buf<blitz_collapse> collapse_dev;
-    Buf<uint32_t> exact_count, work_queue, spill;
+    Buf<uint32_t> exact_count, work_queue, spill, spill_huge;
     Buf<const ViewRecord*> record_table;
     Buf<uint32_t> plan_views, plan_ss;
     Buf<GateDev> gate_table;
@@ -736,19 +737,25 @@ static void full_view(Session& S, const DevMesh& ref, const DevMesh& cand, const
     rec.flags = (state[1] ? kRecClippedRef : 0) | (state[5] ? kRecClippedCand : 0);
 }
 
-// evaluate_impl (evaluate.cpp:312-352) over the full-raster path, starting at
-// view `first_view` with a default result (the exact path resumes whole gates).
+// evaluate_impl (evaluate.cpp:312-352) over the full-raster path. `recs`
+// (host, one per view, or null) are the incremental path's records of this
+// candidate at the gate's first sampling: a record without flags equals the
+// full raster's and is used as is, so only flagged views (fallback, clipped,
+// distance beyond 2^24) and refinements are rasterized in full.
 static Measurement evaluate_full(Session& S, const DevMesh& ref, const DevMesh& cand, const blitz_eval_settings* es,
-                                 const GateSettings& g) {
+                                 const GateSettings& g, const ViewRecord* recs = nullptr) {
     Measurement result = default_measurement();
     result.supersample = g.supersample;
     auto cams = make_cameras(S.bounds, g.screen_size, es->views_orthographic, es->views_perspective, es->views_seed);
-    Buf<Camera> dcams(S.pool, cams.size());
-    B200_CUDA(cudaMemcpyAsync(dcams.p, cams.data(), cams.size() * sizeof(Camera), cudaMemcpyHostToDevice, S.stream));
     for (uint32_t v = 0; v < cams.size(); ++v) {
         Measurement cur = default_measurement();
         cur.worst_view = v;
         for (uint32_t ss = g.supersample;; ss = std::min<uint32_t>(g.max_supersample, ss * 2)) {
+            if (recs && ss == g.supersample && recs[v].flags == 0) {
+                finish_view(cur, recs[v], g, ss, double(recs[v].max_d2));
+                if (refinement_done(cur, g, ss)) break;
+                continue;
+            }
             uint32_t size = raster_size(g.screen_size, ss);
             if (uint64_t(size) * size > kMaxSamples) {
                 result.complete = 0;
@@ -791,6 +798,55 @@ static void ensure_trial_buffers(Session& S) {
 static void trial_views(Session& S, Plan& p, const DevMesh& cand, uint64_t tag);
 static bool gate_from_trial(const Plan& p, const GateSettings& g, Measurement& result);
 
+// Global-memory scratch of the huge audit tier, one per device and shared by
+// all sessions on it (allocated on first need, kept until exit). Launches that
+// use it are ordered on the device by an event: a session's stream waits for
+// the previous user before its huge-tier launch and records the event after.
+struct HugeScratch {
+    std::mutex lock;
+    unsigned char* p = nullptr;
+    uint32_t blocks = 0;
+    cudaEvent_t done = nullptr;
+};
+static HugeScratch& huge_scratch(int device) {
+    static HugeScratch per_device[64];
+    if (device < 0 || device >= 64) throw Failure(BLITZ_INVALID_ARGUMENT, "device index out of range");
+    return per_device[device];
+}
+
+// Plans of rasters above 256 x 256 can hold regions beyond the large tier.
+static void run_audit(Session& S, Plan& p, uint32_t n, unsigned long long* stats, cudaStream_t st) {
+    S.work_queue.ensure(S.pool, 3);
+    S.spill.ensure(S.pool, size_t(n) * p.views + 1);
+    AuditJob job{};
+    job.plan = p.dev, job.recs = S.records.p, job.out = p.records.p, job.total = uint64_t(n) * p.views;
+    if (p.size <= 256) {
+        launch_audit(job, stats, S.work_queue.p, S.spill.p, nullptr, nullptr, 0, st);
+        return;
+    }
+    S.spill_huge.ensure(S.pool, size_t(n) * p.views + 1);
+    HugeScratch& h = huge_scratch(S.device);
+    std::lock_guard<std::mutex> guard(h.lock);
+    if (!h.p) {
+        int sms = 148;
+        B200_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, S.device));
+        const uint32_t blocks = uint32_t(std::max(1, sms / 2));
+        void* q = nullptr;
+        cudaError_t e = cudaMalloc(&q, audit_huge_scratch_bytes(blocks));
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            throw Failure(BLITZ_OUT_OF_MEMORY, "huge-tier audit scratch");
+        }
+        B200_CUDA(cudaEventCreateWithFlags(&h.done, cudaEventDisableTiming));
+        h.p = static_cast<unsigned char*>(q);
+        h.blocks = blocks;
+    } else {
+        B200_CUDA(cudaStreamWaitEvent(st, h.done, 0));
+    }
+    launch_audit(job, stats, S.work_queue.p, S.spill.p, S.spill_huge.p, h.p, h.blocks, st);
+    B200_CUDA(cudaEventRecord(h.done, st));
+}
+
 // Plan of gate `gi` (gates 1 and 3 against the source, 2 and 4 against the
 // bound previous LOD).
 static PlanKey plan_key_of(const Session& S, int gi, const blitz_eval_settings& es) {
@@ -801,19 +857,28 @@ static PlanKey plan_key_of(const Session& S, int gi, const blitz_eval_settings& 
 // One gate of a built trial: all views at once from the plan's reference
 // fields when the plan keeps them and no view clips or refines, else the
 // per-view full-raster path.
-static Measurement gate_of_trial(Session& S, const DevMesh& cand, const GateRef& gate, int gi, uint64_t tag) {
+static Measurement gate_of_trial(Session& S, const DevMesh& cand, const GateRef& gate, int gi, uint64_t tag,
+                                 const ViewRecord* recs_dev = nullptr) {
     Plan& p = plan_for(S, plan_key_of(S, gi, *gate.es));
     Measurement r;
     if (!p.resource_limited && p.tiled) {
         if (p.trial_tag != tag) trial_views(S, p, cand, tag);
         if (gate_from_trial(p, gate.g, r)) return r;
     }
+    std::vector<ViewRecord> recs;
+    if (recs_dev && !p.resource_limited) {
+        recs.resize(p.views);
+        B200_CUDA(cudaMemcpyAsync(recs.data(), recs_dev, p.views * sizeof(ViewRecord), cudaMemcpyDeviceToHost,
+                                  S.stream));
+        B200_CUDA(cudaStreamSynchronize(S.stream));
+    }
     const DevMesh& ref = gate.reference == 0 || S.previous_is_source ? S.source.view : S.previous.view;
-    return evaluate_full(S, ref, cand, gate.es, gate.g);
+    return evaluate_full(S, ref, cand, gate.es, gate.g, recs.empty() ? nullptr : recs.data());
 }
 
 static void exact_candidate(Session& S, const blitz_collapse& col, const GateRef* gates, int first,
-                            blitz_candidate_verdict& v, Measurement* meas) {
+                            blitz_candidate_verdict& v, Measurement* meas,
+                            const ViewRecord* const* gate_records = nullptr) {
     const DevMesh& m = S.state.view;
     Topology& t = S.topo;
     ensure_trial_buffers(S);
@@ -833,7 +898,7 @@ static void exact_candidate(Session& S, const blitz_collapse& col, const GateRef
     v.accepted = 0;
     const uint64_t tag = ++S.trial_tag;
     for (int gi = first; gi < 4; ++gi) {
-        Measurement r = gate_of_trial(S, cand, gates[gi], gi, tag);
+        Measurement r = gate_of_trial(S, cand, gates[gi], gi, tag, gate_records ? gate_records[gi] : nullptr);
         if (meas) meas[gi] = r;
         if (!measurement_accepted(r)) {
             v.failed_gate = uint8_t(gi + 1);
@@ -843,32 +908,99 @@ static void exact_candidate(Session& S, const blitz_collapse& col, const GateRef
     v.accepted = 1;
 }
 
+// Gates, distinct plans and the gate -> plan map of one audit call.
+struct AuditSetup {
+    GateRef gates[4];
+    std::vector<PlanKey> keys;
+    uint32_t plan_of[4];
+    std::vector<Plan*> plans;
+};
+static void setup_audit(Session& S, const blitz_eval_settings gates_in[4], AuditSetup& a) {
+    a.keys.clear();
+    a.plans.clear();
+    for (int g = 0; g < 4; ++g) {
+        a.gates[g].es = &gates_in[g];
+        a.gates[g].g = gate_of(&gates_in[g], S.bounds);
+        a.gates[g].g.max_supersample = uint8_t(
+            bounded_refinement(a.gates[g].g.screen_size, a.gates[g].g.supersample, a.gates[g].g.max_supersample));
+        a.gates[g].reference = g % 2;
+        const PlanKey k = plan_key_of(S, g, gates_in[g]);
+        auto it = std::find_if(a.keys.begin(), a.keys.end(), [&](const PlanKey& o) { return !(o < k) && !(k < o); });
+        a.plan_of[g] = uint32_t(it - a.keys.begin());
+        if (it == a.keys.end()) a.keys.push_back(k);
+    }
+    for (auto& k : a.keys) {
+        Plan& p = plan_for(S, k);
+        if (p.resource_limited) throw Failure(BLITZ_BUDGET_LIMITED, "raster exceeds per-view sample budget");
+        a.plans.push_back(&p);
+    }
+}
+// Per-plan record tables of k_verdicts for n candidates (records sized here).
+static void upload_verdict_tables(Session& S, const AuditSetup& a, uint32_t n, cudaStream_t st) {
+    std::vector<const ViewRecord*> table(a.plans.size());
+    std::vector<uint32_t> pviews(a.plans.size()), pss(a.plans.size());
+    for (size_t i = 0; i < a.plans.size(); ++i) {
+        Plan& p = *a.plans[i];
+        p.records.ensure(S.pool, std::max<size_t>(1, size_t(n) * p.views));
+        table[i] = p.records.p;
+        pviews[i] = p.views;
+        pss[i] = p.key.ss;
+    }
+    S.record_table.ensure(S.pool, 4);
+    S.plan_views.ensure(S.pool, 4);
+    S.plan_ss.ensure(S.pool, 4);
+    S.gate_table.ensure(S.pool, 4);
+    S.exact_count.ensure(S.pool, 1);
+    GateDev gd[4];
+    for (int g = 0; g < 4; ++g) gd[g] = GateDev{a.gates[g].g, a.plan_of[g]};
+    B200_CUDA(cudaMemcpyAsync(S.record_table.p, table.data(), table.size() * sizeof(void*), cudaMemcpyHostToDevice, st));
+    B200_CUDA(cudaMemcpyAsync(S.plan_views.p, pviews.data(), pviews.size() * 4, cudaMemcpyHostToDevice, st));
+    B200_CUDA(cudaMemcpyAsync(S.plan_ss.p, pss.data(), pss.size() * 4, cudaMemcpyHostToDevice, st));
+    B200_CUDA(cudaMemcpyAsync(S.gate_table.p, gd, sizeof(gd), cudaMemcpyHostToDevice, st));
+}
+// Candidates whose verdict needs the full-raster path (k_verdicts flagged
+// them): resolved one by one from their resume gate.
+static void resolve_exact(Session& S, AuditSetup& a, const blitz_collapse* cands_dev, uint32_t nn,
+                          blitz_candidate_verdict* out_dev, Measurement* meas_dev, cudaStream_t st) {
+    std::vector<blitz_candidate_verdict> hv(nn);
+    B200_CUDA(cudaMemcpyAsync(hv.data(), out_dev, nn * sizeof(blitz_candidate_verdict), cudaMemcpyDeviceToHost, st));
+    std::vector<blitz_collapse> hc(nn);
+    B200_CUDA(cudaMemcpyAsync(hc.data(), cands_dev, nn * sizeof(blitz_collapse), cudaMemcpyDeviceToHost, st));
+    B200_CUDA(cudaStreamSynchronize(st));
+    cudaStream_t saved = S.stream;
+    S.stream = st;
+    for (uint32_t c = 0; c < nn; ++c) {
+        if (!hv[c].exact_path) continue;
+        int first = hv[c].reserved; // resume gate
+        Measurement m4[4];
+        if (meas_dev) {
+            B200_CUDA(cudaMemcpyAsync(m4, meas_dev + size_t(c) * 4, sizeof(m4), cudaMemcpyDeviceToHost, st));
+            B200_CUDA(cudaStreamSynchronize(st));
+        }
+        const ViewRecord* recs[4];
+        for (int g = 0; g < 4; ++g) {
+            const Plan& p = *a.plans[a.plan_of[g]];
+            recs[g] = p.records.p + size_t(c) * p.views;
+        }
+        exact_candidate(S, hc[c], a.gates, first, hv[c], meas_dev ? m4 : nullptr, recs);
+        hv[c].reserved = 0;
+        B200_CUDA(cudaMemcpyAsync(out_dev + c, &hv[c], sizeof(hv[c]), cudaMemcpyHostToDevice, st));
+        if (meas_dev) B200_CUDA(cudaMemcpyAsync(meas_dev + size_t(c) * 4, m4, sizeof(m4), cudaMemcpyHostToDevice, st));
+        B200_CUDA(cudaStreamSynchronize(st));
+    }
+    S.stream = saved;
+}
+
 static void audit_candidates(Session& S, const blitz_collapse* cands_dev, const blitz_collapse* cands_host, size_t n,
                              const blitz_eval_settings gates_in[4], blitz_candidate_verdict* out_dev,
                              Measurement* meas_dev, cudaStream_t st) {
     if (n > UINT32_MAX / 2) throw Failure(BLITZ_INVALID_ARGUMENT, "too many candidates");
-    GateRef gates[4];
-    std::vector<PlanKey> keys;
-    uint32_t plan_of[4];
-    for (int g = 0; g < 4; ++g) {
-        gates[g].es = &gates_in[g];
-        gates[g].g = gate_of(&gates_in[g], S.bounds);
-        gates[g].g.max_supersample = uint8_t(
-            bounded_refinement(gates[g].g.screen_size, gates[g].g.supersample, gates[g].g.max_supersample));
-        gates[g].reference = g % 2;
-        PlanKey k{(g % 2) && !S.previous_is_source ? 1 : 0, gates_in[g].views_orthographic,
-                  gates_in[g].views_perspective, gates_in[g].views_seed, gates_in[g].screen_size,
-                  gates_in[g].supersample, gates_in[g].force_two_sided};
-        auto it = std::find_if(keys.begin(), keys.end(), [&](const PlanKey& o) { return !(o < k) && !(k < o); });
-        plan_of[g] = uint32_t(it - keys.begin());
-        if (it == keys.end()) keys.push_back(k);
-    }
     (void)cands_host;
+    AuditSetup a;
+    setup_audit(S, gates_in, a);
     const uint32_t nn = uint32_t(n);
     Topology& t = S.topo;
     S.records.ensure(S.pool, nn);
-    std::vector<Plan*> plans;
-    for (auto& k : keys) plans.push_back(&plan_for(S, k));
     const bool prof = S.profiling && nn;
     if (prof) {
         S.stats.ensure(S.pool, 4);
@@ -879,32 +1011,12 @@ static void audit_candidates(Session& S, const blitz_collapse* cands_dev, const 
                    S.options.preserve_uv != 0, S.records.p, st);
     if (prof) B200_CUDA(cudaEventRecord(S.ev[1], st));
     S.profile.launches += nn ? 1 : 0;
-    std::vector<const ViewRecord*> table(plans.size());
-    std::vector<uint32_t> pviews(plans.size()), pss(plans.size());
-    for (size_t i = 0; i < plans.size(); ++i) {
-        Plan& p = *plans[i];
-        if (p.resource_limited) throw Failure(BLITZ_BUDGET_LIMITED, "raster exceeds per-view sample budget");
-        p.records.ensure(S.pool, size_t(nn) * p.views);
-        S.work_queue.ensure(S.pool, 2);
-        S.spill.ensure(S.pool, size_t(nn) * p.views + 1);
-        launch_audit(S.records.p, nn, p.dev, p.records.p, prof ? S.stats.p : nullptr, S.work_queue.p, S.spill.p, st);
+    upload_verdict_tables(S, a, nn, st);
+    for (Plan* pp : a.plans) {
+        run_audit(S, *pp, nn, prof ? S.stats.p : nullptr, st);
         if (nn) S.profile.launches += 1, S.profile.audit_launches += 1;
-        table[i] = p.records.p;
-        pviews[i] = p.views;
-        pss[i] = p.key.ss;
     }
     if (prof) B200_CUDA(cudaEventRecord(S.ev[4], st));
-    S.record_table.ensure(S.pool, 4);
-    S.plan_views.ensure(S.pool, 4);
-    S.plan_ss.ensure(S.pool, 4);
-    S.gate_table.ensure(S.pool, 4);
-    S.exact_count.ensure(S.pool, 1);
-    GateDev gd[4];
-    for (int g = 0; g < 4; ++g) gd[g] = GateDev{gates[g].g, plan_of[g]};
-    B200_CUDA(cudaMemcpyAsync(S.record_table.p, table.data(), table.size() * sizeof(void*), cudaMemcpyHostToDevice, st));
-    B200_CUDA(cudaMemcpyAsync(S.plan_views.p, pviews.data(), pviews.size() * 4, cudaMemcpyHostToDevice, st));
-    B200_CUDA(cudaMemcpyAsync(S.plan_ss.p, pss.data(), pss.size() * 4, cudaMemcpyHostToDevice, st));
-    B200_CUDA(cudaMemcpyAsync(S.gate_table.p, gd, sizeof(gd), cudaMemcpyHostToDevice, st));
     B200_CUDA(cudaMemsetAsync(S.exact_count.p, 0, 4, st));
     if (prof) B200_CUDA(cudaEventRecord(S.ev[2], st));
     launch_verdicts(S.record_table.p, S.plan_views.p, S.plan_ss.p, S.gate_table.p, S.records.p, nn, out_dev, meas_dev,
@@ -916,45 +1028,21 @@ static void audit_candidates(Session& S, const blitz_collapse* cands_dev, const 
     B200_CUDA(cudaStreamSynchronize(st));
     B200_CUDA(cudaGetLastError());
     if (prof) {
-        float a = 0, b = 0, c = 0;
-        B200_CUDA(cudaEventElapsedTime(&a, S.ev[0], S.ev[1]));
-        B200_CUDA(cudaEventElapsedTime(&b, S.ev[1], S.ev[4]));
-        B200_CUDA(cudaEventElapsedTime(&c, S.ev[2], S.ev[3]));
+        float ta = 0, tb = 0, tc = 0;
+        B200_CUDA(cudaEventElapsedTime(&ta, S.ev[0], S.ev[1]));
+        B200_CUDA(cudaEventElapsedTime(&tb, S.ev[1], S.ev[4]));
+        B200_CUDA(cudaEventElapsedTime(&tc, S.ev[2], S.ev[3]));
         unsigned long long h[4];
         B200_CUDA(cudaMemcpy(h, S.stats.p, sizeof(h), cudaMemcpyDeviceToHost));
-        S.profile.prepare_ms += a;
-        S.profile.audit_ms += b;
-        S.profile.verdict_ms += c;
+        S.profile.prepare_ms += ta;
+        S.profile.audit_ms += tb;
+        S.profile.verdict_ms += tc;
         S.profile.units += h[0];
         S.profile.region_samples += h[1];
         S.profile.changed_samples += h[2];
-        S.profile.record_bytes += uint64_t(nn) * sizeof(CandidateRecord) * plans.size();
+        S.profile.record_bytes += uint64_t(nn) * sizeof(CandidateRecord) * a.plans.size();
     }
-    if (exact) {
-        std::vector<blitz_candidate_verdict> hv(nn);
-        B200_CUDA(cudaMemcpyAsync(hv.data(), out_dev, nn * sizeof(blitz_candidate_verdict), cudaMemcpyDeviceToHost, st));
-        std::vector<blitz_collapse> hc(nn);
-        B200_CUDA(cudaMemcpyAsync(hc.data(), cands_dev, nn * sizeof(blitz_collapse), cudaMemcpyDeviceToHost, st));
-        B200_CUDA(cudaStreamSynchronize(st));
-        cudaStream_t saved = S.stream;
-        S.stream = st;
-        for (uint32_t c = 0; c < nn; ++c) {
-            if (!hv[c].exact_path) continue;
-            int first = hv[c].reserved; // resume gate
-            Measurement m4[4];
-            if (meas_dev) {
-                B200_CUDA(cudaMemcpyAsync(m4, meas_dev + size_t(c) * 4, sizeof(m4), cudaMemcpyDeviceToHost, st));
-                B200_CUDA(cudaStreamSynchronize(st));
-            }
-            exact_candidate(S, hc[c], gates, first, hv[c], meas_dev ? m4 : nullptr);
-            hv[c].reserved = 0;
-            B200_CUDA(cudaMemcpyAsync(out_dev + c, &hv[c], sizeof(hv[c]), cudaMemcpyHostToDevice, st));
-            if (meas_dev)
-                B200_CUDA(cudaMemcpyAsync(meas_dev + size_t(c) * 4, m4, sizeof(m4), cudaMemcpyHostToDevice, st));
-            B200_CUDA(cudaStreamSynchronize(st));
-        }
-        S.stream = saved;
-    }
+    if (exact) resolve_exact(S, a, cands_dev, nn, out_dev, meas_dev, st);
     S.info.decoded += nn;
 }
 
@@ -2109,4 +2197,236 @@ blitz_status blitz_audit_attach_surrogate(blitz_audit_session* s, blitz_surrogat
         if (h && h->m.device != s->s.device) throw Failure(BLITZ_INVALID_ARGUMENT, "surrogate on another device");
         s->s.surrogate = h ? &h->m : nullptr;
     });
+}
+
+// ---------------------------------------------------------------------------
+// Batched audit of several sessions' candidates in one persistent launch.
+struct blitz_audit_batch {
+    std::vector<blitz_audit_session*> sessions;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    Pool pool;
+    Buf<CandidateRecord> records;
+    std::vector<Buf<AuditEntry>> entries; // per plan slot
+    std::vector<uint32_t> nentries;
+    std::vector<uint64_t> units;
+    Buf<uint32_t> queue, spill, spill_huge, exact;
+    Buf<unsigned char> huge;
+    uint32_t huge_blocks = 0;
+    int variant = kAuditTierSmall;
+    bool tuned = false;
+    float tune_ms[2] = {0, 0};
+    // captured launch sequence and the inputs it was captured for
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    std::vector<uint8_t> signature;
+    uint64_t graph_launches = 0, exact_candidates = 0;
+    ~blitz_audit_batch() {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        records.release(), queue.release(), spill.release(), spill_huge.release(), exact.release(), huge.release();
+        entries.clear();
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
+blitz_status blitz_audit_batch_create(blitz_audit_session* const* sessions, size_t count, blitz_audit_batch** out,
+                                      char* error, size_t cap) {
+    return guarded(error, cap, [&] {
+        if (!out || !sessions || !count) throw Failure(BLITZ_INVALID_ARGUMENT, "no sessions");
+        *out = nullptr;
+        auto b = std::make_unique<blitz_audit_batch>();
+        for (size_t i = 0; i < count; ++i) {
+            if (!sessions[i]) throw Failure(BLITZ_INVALID_ARGUMENT, "null session");
+            if (sessions[i]->s.device != sessions[0]->s.device)
+                throw Failure(BLITZ_INVALID_ARGUMENT, "sessions on different devices");
+            b->sessions.push_back(sessions[i]);
+        }
+        b->device = sessions[0]->s.device;
+        b->pool.limit = size_t(1) << 40;
+        DeviceScope scope(b->device);
+        B200_CUDA(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
+        *out = b.release();
+    });
+}
+
+void blitz_audit_batch_destroy(blitz_audit_batch* b) {
+    if (!b) return;
+    int previous = 0;
+    cudaGetDevice(&previous);
+    cudaSetDevice(b->device);
+    delete b;
+    cudaSetDevice(previous);
+}
+
+blitz_status blitz_audit_batch_candidates(blitz_audit_batch* b, const blitz_collapse* cands, const size_t* counts,
+                                          const blitz_eval_settings gates_in[4], blitz_candidate_verdict* out,
+                                          uint32_t flags, void* stream, char* error, size_t cap) {
+    return guarded(error, cap, [&] {
+        if (!b || !counts || !gates_in || flags > 3) throw Failure(BLITZ_INVALID_ARGUMENT, "bad batch arguments");
+        DeviceScope scope(b->device);
+        cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : b->stream;
+        const size_t ns = b->sessions.size();
+        std::vector<uint64_t> off(ns + 1, 0);
+        for (size_t i = 0; i < ns; ++i) {
+            if (counts[i] > UINT32_MAX / 2) throw Failure(BLITZ_INVALID_ARGUMENT, "too many candidates");
+            off[i + 1] = off[i] + counts[i];
+        }
+        if (off[ns] && (!cands || !out)) throw Failure(BLITZ_INVALID_ARGUMENT, "null candidate or verdict array");
+        if (off[ns] > UINT32_MAX) throw Failure(BLITZ_INVALID_ARGUMENT, "too many candidates");
+        for (int g = 0; g < 4; ++g) gate_of(&gates_in[g], b->sessions[0]->s.bounds);
+        // Plans (built or refreshed on each session's own stream) and tables.
+        std::vector<AuditSetup> setup(ns);
+        size_t slots = 0;
+        bool big = false;
+        for (size_t i = 0; i < ns; ++i) {
+            Session& S = b->sessions[i]->s;
+            setup_audit(S, gates_in, setup[i]);
+            upload_verdict_tables(S, setup[i], uint32_t(counts[i]), S.stream);
+            B200_CUDA(cudaStreamSynchronize(S.stream));
+            slots = std::max(slots, setup[i].plans.size());
+            for (Plan* p : setup[i].plans) big |= p->size > 256;
+        }
+        b->records.ensure(b->pool, std::max<uint64_t>(1, off[ns]));
+        b->entries.resize(slots);
+        b->nentries.assign(slots, 0);
+        b->units.assign(slots, 0);
+        uint64_t max_units = 0;
+        for (size_t j = 0; j < slots; ++j) {
+            std::vector<AuditEntry> e;
+            uint64_t first = 0;
+            for (size_t i = 0; i < ns; ++i) {
+                if (j >= setup[i].plans.size() || !counts[i]) continue;
+                Plan& p = *setup[i].plans[j];
+                e.push_back(AuditEntry{p.dev, b->records.p + off[i], p.records.p, first});
+                first += uint64_t(counts[i]) * p.views;
+            }
+            if (first > UINT32_MAX) throw Failure(BLITZ_INVALID_ARGUMENT, "too many (candidate, view) units");
+            b->entries[j].ensure(b->pool, std::max<size_t>(1, e.size()));
+            if (!e.empty())
+                B200_CUDA(cudaMemcpyAsync(b->entries[j].p, e.data(), e.size() * sizeof(AuditEntry),
+                                          cudaMemcpyHostToDevice, st));
+            b->nentries[j] = uint32_t(e.size());
+            b->units[j] = first;
+            max_units = std::max(max_units, first);
+        }
+        b->queue.ensure(b->pool, 3);
+        b->spill.ensure(b->pool, max_units + 1);
+        b->exact.ensure(b->pool, ns);
+        if (big && !b->huge.p) {
+            int sms = 148;
+            B200_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device));
+            b->huge_blocks = uint32_t(std::max(1, sms / 2));
+            b->huge = Buf<unsigned char>(b->pool, audit_huge_scratch_bytes(b->huge_blocks));
+        }
+        if (big) b->spill_huge.ensure(b->pool, max_units + 1);
+        B200_CUDA(cudaStreamSynchronize(st));
+        // The launch sequence: per-session records, one audit job per plan
+        // slot over all sessions, per-session verdicts.
+        auto body = [&](int variant) {
+            for (size_t i = 0; i < ns; ++i) {
+                if (!counts[i]) continue;
+                Session& S = b->sessions[i]->s;
+                Topology& t = S.topo;
+                launch_prepare(S.state.view, t.view, S.state.view, t.view, cands + off[i], uint32_t(counts[i]),
+                               t.positions.p, t.pos_cap, t.flat.p, S.options.preserve_uv != 0, b->records.p + off[i],
+                               st);
+            }
+            for (size_t j = 0; j < slots; ++j) {
+                if (!b->units[j]) continue;
+                AuditJob job{};
+                job.entries = b->entries[j].p, job.nentries = b->nentries[j], job.total = b->units[j];
+                launch_audit(job, nullptr, b->queue.p, b->spill.p, big ? b->spill_huge.p : nullptr,
+                             big ? b->huge.p : nullptr, big ? b->huge_blocks : 0, st, variant);
+            }
+            cudaMemsetAsync(b->exact.p, 0, 4 * ns, st);
+            for (size_t i = 0; i < ns; ++i) {
+                if (!counts[i]) continue;
+                Session& S = b->sessions[i]->s;
+                launch_verdicts(S.record_table.p, S.plan_views.p, S.plan_ss.p, S.gate_table.p, b->records.p + off[i],
+                                uint32_t(counts[i]), out + off[i], nullptr, b->exact.p + i, st);
+            }
+        };
+        // Autotune: time both warp-tier variants on this call, keep the faster.
+        if ((flags & 2u) && off[ns]) {
+            cudaEvent_t e0, e1;
+            B200_CUDA(cudaEventCreate(&e0));
+            B200_CUDA(cudaEventCreate(&e1));
+            for (int v = 0; v < 2; ++v) {
+                body(v); // warm
+                B200_CUDA(cudaEventRecord(e0, st));
+                body(v);
+                B200_CUDA(cudaEventRecord(e1, st));
+                B200_CUDA(cudaEventSynchronize(e1));
+                B200_CUDA(cudaEventElapsedTime(&b->tune_ms[v], e0, e1));
+            }
+            cudaEventDestroy(e0);
+            cudaEventDestroy(e1);
+            b->variant = b->tune_ms[1] < b->tune_ms[0] ? kAuditTierMedium : kAuditTierSmall;
+            b->tuned = true;
+            if (b->exec) cudaGraphExecDestroy(b->exec), b->exec = nullptr;
+            if (b->graph) cudaGraphDestroy(b->graph), b->graph = nullptr;
+        }
+        // Inputs a captured graph is bound to.
+        std::vector<uint8_t> sig;
+        auto put = [&](const void* p, size_t n) {
+            const uint8_t* c = static_cast<const uint8_t*>(p);
+            sig.insert(sig.end(), c, c + n);
+        };
+        put(&cands, sizeof cands), put(&out, sizeof out), put(&st, sizeof st), put(counts, ns * sizeof(size_t));
+        put(gates_in, 4 * sizeof(blitz_eval_settings)), put(&b->variant, sizeof b->variant);
+        for (size_t i = 0; i < ns; ++i) {
+            Session& S = b->sessions[i]->s;
+            put(&S.state_revision, sizeof(uint64_t));
+            put(&S.record_table.p, sizeof(void*));
+            for (Plan* p : setup[i].plans) put(&p->records.p, sizeof(void*)), put(&p->dviews.p, sizeof(void*));
+        }
+        for (auto& e : b->entries) put(&e.p, sizeof(void*));
+        for (const void* q : {(const void*)b->records.p, (const void*)b->queue.p, (const void*)b->spill.p,
+                              (const void*)b->spill_huge.p, (const void*)b->huge.p, (const void*)b->exact.p})
+            put(&q, sizeof(q));
+        if ((flags & 1u) && off[ns]) {
+            if (b->exec && sig == b->signature) {
+                B200_CUDA(cudaGraphLaunch(b->exec, st));
+                ++b->graph_launches;
+            } else {
+                if (b->exec) cudaGraphExecDestroy(b->exec), b->exec = nullptr;
+                if (b->graph) cudaGraphDestroy(b->graph), b->graph = nullptr;
+                body(b->variant); // this call's results; the capture below records the same sequence
+                B200_CUDA(cudaStreamSynchronize(st));
+                B200_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+                body(b->variant);
+                cudaError_t e = cudaStreamEndCapture(st, &b->graph);
+                if (e != cudaSuccess) throw Failure(BLITZ_INTERNAL_ERROR, "batch graph capture failed");
+                B200_CUDA(cudaGraphInstantiate(&b->exec, b->graph, 0));
+                b->signature = sig;
+            }
+        } else {
+            body(b->variant);
+        }
+        std::vector<uint32_t> exact(ns, 0);
+        B200_CUDA(cudaMemcpyAsync(exact.data(), b->exact.p, 4 * ns, cudaMemcpyDeviceToHost, st));
+        B200_CUDA(cudaStreamSynchronize(st));
+        B200_CUDA(cudaGetLastError());
+        for (size_t i = 0; i < ns; ++i) {
+            if (!exact[i]) continue;
+            b->exact_candidates += exact[i];
+            resolve_exact(b->sessions[i]->s, setup[i], cands + off[i], uint32_t(counts[i]), out + off[i], nullptr,
+                          st);
+        }
+        for (size_t i = 0; i < ns; ++i) b->sessions[i]->s.info.decoded += counts[i];
+    });
+}
+
+blitz_status blitz_audit_batch_read_info(const blitz_audit_batch* b, blitz_audit_batch_info* out) {
+    if (!b || !out || out->struct_size != sizeof(*out)) return BLITZ_INVALID_ARGUMENT;
+    out->sessions = uint32_t(b->sessions.size());
+    out->tier = uint32_t(b->variant);
+    out->tuned = b->tuned ? 1u : 0u;
+    out->graph_captured = b->exec ? 1u : 0u;
+    out->tune_ms[0] = b->tune_ms[0];
+    out->tune_ms[1] = b->tune_ms[1];
+    out->graph_launches = b->graph_launches;
+    out->exact_candidates = b->exact_candidates;
+    return BLITZ_OK;
 }

@@ -310,6 +310,40 @@ blitz_status blitz_audit_surrogate_features(blitz_audit_session*, double screen,
 /* Attaches a model (same device; NULL detaches) for blitz_execute_options.keep_permille. */
 blitz_status blitz_audit_attach_surrogate(blitz_audit_session*, blitz_surrogate*, char* error, size_t error_capacity);
 
+/* ---- Batched audit over several sessions ----------------------------------
+ * Candidates of many meshes audited together: one k_prepare per session, one
+ * persistent audit launch per distinct plan slot over all sessions' (candidate,
+ * view) units, one k_verdicts per session. Verdicts equal those of
+ * blitz_audit_candidates on each session. The reference audits one mesh at a
+ * time (AuditCuda::certify_candidates, evaluate.cu:2394-2412, at most 8
+ * candidates); this entry point has no reference counterpart. The sessions
+ * must be on one device and must not be used by other threads meanwhile. */
+typedef struct blitz_audit_batch blitz_audit_batch;
+#define BLITZ_BATCH_GRAPH 1u    /* capture the launch sequence once and replay it while the candidate and
+                                   verdict buffers, counts, gates, stream and session states are unchanged */
+#define BLITZ_BATCH_AUTOTUNE 2u /* time the two warp-tier variants on this call and keep the faster */
+typedef struct blitz_audit_batch_info {
+    uint32_t struct_size;
+    uint32_t sessions;
+    uint32_t tier;            /* 0: 128 x 64-sample warp tier, 3 blocks/SM; 1: 256 x 128, 1 block/SM */
+    uint32_t tuned, graph_captured;
+    float tune_ms[2];         /* device time of one batch with each tier when tuned */
+    uint64_t graph_launches;  /* replays of the captured graph */
+    uint64_t exact_candidates;
+} blitz_audit_batch_info;
+blitz_status blitz_audit_batch_create(blitz_audit_session* const* sessions, size_t count, blitz_audit_batch** out,
+                                      char* error, size_t error_capacity);
+void blitz_audit_batch_destroy(blitz_audit_batch*);
+/* candidates_device: the sessions' candidates concatenated in session order
+ * (counts[i] each, relative to each session's current state); verdicts_device
+ * the same layout. `stream`: a cudaStream_t or NULL (the batch's stream).
+ * Synchronises before returning. */
+blitz_status blitz_audit_batch_candidates(blitz_audit_batch*, const blitz_collapse* candidates_device,
+                                          const size_t* counts, const blitz_eval_settings gates[4],
+                                          blitz_candidate_verdict* verdicts_device, uint32_t flags, void* stream,
+                                          char* error, size_t error_capacity);
+blitz_status blitz_audit_batch_read_info(const blitz_audit_batch*, blitz_audit_batch_info* out);
+
 /* Current state: compacted indices (3 per face) and every vertex slot's position. */
 blitz_status blitz_audit_state(blitz_audit_session*, uint32_t* indices, size_t index_capacity, float* positions,
                                size_t position_capacity, uint32_t* face_count, char* error, size_t error_capacity);
