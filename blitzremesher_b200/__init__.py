@@ -174,10 +174,11 @@ class ExecuteOptions(C.Structure):
 class BatchInfo(C.Structure):
     _fields_ = [("struct_size", C.c_uint32), ("sessions", C.c_uint32), ("tier", C.c_uint32), ("tuned", C.c_uint32),
                 ("graph_captured", C.c_uint32), ("tune_ms", C.c_float * 2), ("graph_launches", C.c_uint64),
-                ("exact_candidates", C.c_uint64)]
+                ("exact_candidates", C.c_uint64), ("audit_ms", C.c_float), ("units", C.c_uint64),
+                ("region_samples", C.c_uint64), ("changed_samples", C.c_uint64)]
 
 
-BATCH_GRAPH, BATCH_AUTOTUNE = 1, 2
+BATCH_GRAPH, BATCH_AUTOTUNE, BATCH_PROFILE = 1, 2, 4
 
 
 class AuditProfile(C.Structure):

@@ -55,7 +55,7 @@ struct LimitsHuge {
     static constexpr int kRegionWords = 32;
     static constexpr int kRegionRows = 1024;
     static constexpr int kDeltaSamples = 1 << 20;
-    static constexpr int kQueue = 16384;
+    static constexpr int kQueue = 65536;
     static constexpr int kAffected = 64;
 };
 constexpr int kHugeWarps = 8;

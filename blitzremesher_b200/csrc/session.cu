@@ -2221,7 +2221,15 @@ struct blitz_audit_batch {
     cudaGraphExec_t exec = nullptr;
     std::vector<uint8_t> signature;
     uint64_t graph_launches = 0, exact_candidates = 0;
+    // profile of the last call with BLITZ_BATCH_PROFILE
+    Buf<unsigned long long> stats;
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    float audit_ms = 0;
+    unsigned long long prof[3] = {0, 0, 0};
     ~blitz_audit_batch() {
+        for (auto e : ev)
+            if (e) cudaEventDestroy(e);
+        stats.release();
         if (exec) cudaGraphExecDestroy(exec);
         if (graph) cudaGraphDestroy(graph);
         records.release(), queue.release(), spill.release(), spill_huge.release(), exact.release(), huge.release();
@@ -2263,7 +2271,9 @@ blitz_status blitz_audit_batch_candidates(blitz_audit_batch* b, const blitz_coll
                                           const blitz_eval_settings gates_in[4], blitz_candidate_verdict* out,
                                           uint32_t flags, void* stream, char* error, size_t cap) {
     return guarded(error, cap, [&] {
-        if (!b || !counts || !gates_in || flags > 3) throw Failure(BLITZ_INVALID_ARGUMENT, "bad batch arguments");
+        if (!b || !counts || !gates_in || flags > 7) throw Failure(BLITZ_INVALID_ARGUMENT, "bad batch arguments");
+        const bool profile = (flags & 4u) != 0;
+        if (profile && (flags & 1u)) throw Failure(BLITZ_INVALID_ARGUMENT, "profiling runs without graph replay");
         DeviceScope scope(b->device);
         cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : b->stream;
         const size_t ns = b->sessions.size();
@@ -2323,6 +2333,11 @@ blitz_status blitz_audit_batch_candidates(blitz_audit_batch* b, const blitz_coll
         B200_CUDA(cudaStreamSynchronize(st));
         // The launch sequence: per-session records, one audit job per plan
         // slot over all sessions, per-session verdicts.
+        if (profile && !b->stats.p) {
+            b->stats = Buf<unsigned long long>(b->pool, 4);
+            B200_CUDA(cudaEventCreate(&b->ev[0]));
+            B200_CUDA(cudaEventCreate(&b->ev[1]));
+        }
         auto body = [&](int variant) {
             for (size_t i = 0; i < ns; ++i) {
                 if (!counts[i]) continue;
@@ -2332,13 +2347,19 @@ blitz_status blitz_audit_batch_candidates(blitz_audit_batch* b, const blitz_coll
                                t.positions.p, t.pos_cap, t.flat.p, S.options.preserve_uv != 0, b->records.p + off[i],
                                st);
             }
+            if (profile) {
+                cudaMemsetAsync(b->stats.p, 0, 32, st);
+                cudaEventRecord(b->ev[0], st);
+            }
             for (size_t j = 0; j < slots; ++j) {
                 if (!b->units[j]) continue;
                 AuditJob job{};
                 job.entries = b->entries[j].p, job.nentries = b->nentries[j], job.total = b->units[j];
-                launch_audit(job, nullptr, b->queue.p, b->spill.p, big ? b->spill_huge.p : nullptr,
-                             big ? b->huge.p : nullptr, big ? b->huge_blocks : 0, st, variant);
+                launch_audit(job, profile ? b->stats.p : nullptr, b->queue.p, b->spill.p,
+                             big ? b->spill_huge.p : nullptr, big ? b->huge.p : nullptr, big ? b->huge_blocks : 0,
+                             st, variant);
             }
+            if (profile) cudaEventRecord(b->ev[1], st);
             cudaMemsetAsync(b->exact.p, 0, 4 * ns, st);
             for (size_t i = 0; i < ns; ++i) {
                 if (!counts[i]) continue;
@@ -2408,6 +2429,10 @@ blitz_status blitz_audit_batch_candidates(blitz_audit_batch* b, const blitz_coll
         B200_CUDA(cudaMemcpyAsync(exact.data(), b->exact.p, 4 * ns, cudaMemcpyDeviceToHost, st));
         B200_CUDA(cudaStreamSynchronize(st));
         B200_CUDA(cudaGetLastError());
+        if (profile && off[ns]) {
+            B200_CUDA(cudaEventElapsedTime(&b->audit_ms, b->ev[0], b->ev[1]));
+            B200_CUDA(cudaMemcpy(b->prof, b->stats.p, sizeof(b->prof), cudaMemcpyDeviceToHost));
+        }
         for (size_t i = 0; i < ns; ++i) {
             if (!exact[i]) continue;
             b->exact_candidates += exact[i];
@@ -2428,5 +2453,9 @@ blitz_status blitz_audit_batch_read_info(const blitz_audit_batch* b, blitz_audit
     out->tune_ms[1] = b->tune_ms[1];
     out->graph_launches = b->graph_launches;
     out->exact_candidates = b->exact_candidates;
+    out->audit_ms = b->audit_ms;
+    out->units = b->prof[0];
+    out->region_samples = b->prof[1];
+    out->changed_samples = b->prof[2];
     return BLITZ_OK;
 }

@@ -322,6 +322,7 @@ typedef struct blitz_audit_batch blitz_audit_batch;
 #define BLITZ_BATCH_GRAPH 1u    /* capture the launch sequence once and replay it while the candidate and
                                    verdict buffers, counts, gates, stream and session states are unchanged */
 #define BLITZ_BATCH_AUTOTUNE 2u /* time the two warp-tier variants on this call and keep the faster */
+#define BLITZ_BATCH_PROFILE 4u  /* record the audit launches' device time and work counters (no graph) */
 typedef struct blitz_audit_batch_info {
     uint32_t struct_size;
     uint32_t sessions;
@@ -330,6 +331,11 @@ typedef struct blitz_audit_batch_info {
     float tune_ms[2];         /* device time of one batch with each tier when tuned */
     uint64_t graph_launches;  /* replays of the captured graph */
     uint64_t exact_candidates;
+    /* last BLITZ_BATCH_PROFILE call: audit launches' device time, (candidate,
+     * view) units audited by any tier, region samples rasterized, changed
+     * samples measured */
+    float audit_ms;
+    uint64_t units, region_samples, changed_samples;
 } blitz_audit_batch_info;
 blitz_status blitz_audit_batch_create(blitz_audit_session* const* sessions, size_t count, blitz_audit_batch** out,
                                       char* error, size_t error_capacity);
