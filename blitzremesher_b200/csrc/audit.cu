@@ -21,6 +21,7 @@ constexpr int kAuditWarps = 8;
 #endif
 constexpr int kMaxOk = 48;          // rasterized (unculled, unclipped) old + new faces
 constexpr int kMaxTileSide = 32;    // tile-maxima path for rasters up to 1024 x 1024
+constexpr uint32_t kDirectTests = 4096; // bbox samples up to which phase 1 tests every sample
 
 // Per-warp limits of one (candidate, view) unit. The common tier keeps its
 // scratch small so that many warps stay resident; units that overflow it are
@@ -139,13 +140,15 @@ template <class M> __device__ uint32_t nearest_in_row(const M& mask, uint32_t ro
     return best <= maxdx ? best : kNone;
 }
 
-// Exact squared Euclidean distance from (x, y) to the nearest covered sample.
-template <class M> __device__ uint32_t nearest_d2(const M& mask, uint32_t x, uint32_t y) {
+// Exact squared Euclidean distance from (x, y) to the nearest covered sample,
+// or any value <= `enough` once a covered sample that close is found (the
+// caller only needs distances above `enough`: the running maximum).
+template <class M> __device__ uint32_t nearest_d2(const M& mask, uint32_t x, uint32_t y, uint32_t enough = 0) {
     const uint32_t size = mask.size;
     uint32_t best = kNone;
     for (uint32_t dy = 0;; ++dy) {
         uint64_t dy2 = uint64_t(dy) * dy;
-        if (best != kNone && dy2 >= best) break;
+        if (best != kNone && (dy2 >= best || best <= enough)) break;
         bool any = false;
         for (int side = 0; side < (dy ? 2 : 1); ++side) {
             int64_t row = side ? int64_t(y) + dy : int64_t(y) - dy;
@@ -294,21 +297,33 @@ __device__ void audit_unit(const CandidateRecord* __restrict__ rec, const PlanDe
             fallback = true;
         } else {
             samples = uint64_t(rows) * words * 32;
-            // Phase 1: every (face, sample in its bbox) test is an independent
-            // work item spread over the lanes; covered samples add the face's
-            // sign to a per-sample byte (biased by 128, so at most 32 old and
-            // 32 new faces never carry across bytes).
+            // Phase 1: per (face, row) the covered samples form one interval:
+            // each edge term of the reference's test is monotone in x (IEEE
+            // rounding is monotone), so three binary searches over the same
+            // FP64 expressions find its ends exactly. Intervals are added to a
+            // per-sample byte difference map (biased by 128: at most 32 old
+            // and 32 new faces), which a per-row prefix scan turns into the
+            // candidate's count delta (new faces +1, old faces -1).
             const uint32_t delta_words = uint32_t(bw * bh + 3) >> 2;
             for (uint32_t k = lane; k < delta_words; k += 32) ws.delta[k] = 0x80808080u;
+            // Small units test every (face, sample in its bbox) directly; large
+            // ones take the interval route below. Both give the same map.
+            uint32_t area = 0;
+            if (lane < nok) area += uint32_t(ws.faces[lane].x1 - ws.faces[lane].x0 + 1) * uint32_t(ws.faces[lane].y1 - ws.faces[lane].y0 + 1);
+            if (lane + 32 < nok)
+                area += uint32_t(ws.faces[lane + 32].x1 - ws.faces[lane + 32].x0 + 1) *
+                        uint32_t(ws.faces[lane + 32].y1 - ws.faces[lane + 32].y0 + 1);
+            for (int o = 16; o; o >>= 1) area += __shfl_xor_sync(0xffffffffu, area, o);
+            // (the small tier's regions are too small for intervals to pay)
+            const bool direct = L::kDeltaSamples <= 2048 || area <= kDirectTests;
             uint32_t c0 = 0, c1 = 0;
-            if (lane < nok) {
-                const FaceSetup& s = ws.faces[lane];
-                c0 = uint32_t(s.x1 - s.x0 + 1) * uint32_t(s.y1 - s.y0 + 1);
-            }
-            if (lane + 32 < nok) {
-                const FaceSetup& s = ws.faces[lane + 32];
-                c1 = uint32_t(s.x1 - s.x0 + 1) * uint32_t(s.y1 - s.y0 + 1);
-            }
+            if (lane < nok)
+                c0 = direct ? uint32_t(ws.faces[lane].x1 - ws.faces[lane].x0 + 1) * uint32_t(ws.faces[lane].y1 - ws.faces[lane].y0 + 1)
+                            : uint32_t(ws.faces[lane].y1 - ws.faces[lane].y0 + 1);
+            if (lane + 32 < nok)
+                c1 = direct ? uint32_t(ws.faces[lane + 32].x1 - ws.faces[lane + 32].x0 + 1) *
+                                  uint32_t(ws.faces[lane + 32].y1 - ws.faces[lane + 32].y0 + 1)
+                            : uint32_t(ws.faces[lane + 32].y1 - ws.faces[lane + 32].y0 + 1);
             uint32_t i0 = c0, i1 = c1;
             for (int o = 1; o < 32; o <<= 1) {
                 const uint32_t a = __shfl_up_sync(0xffffffffu, i0, o), b = __shfl_up_sync(0xffffffffu, i1, o);
@@ -317,64 +332,166 @@ __device__ void audit_unit(const CandidateRecord* __restrict__ rec, const PlanDe
             const uint32_t tot0 = __shfl_sync(0xffffffffu, i0, 31);
             if (lane < nok) ws.work[lane] = i0 - c0;
             if (lane + 32 < nok) ws.work[lane + 32] = tot0 + i1 - c1;
-            const uint32_t tests = tot0 + __shfl_sync(0xffffffffu, i1, 31);
+            const uint32_t items = tot0 + __shfl_sync(0xffffffffu, i1, 31);
             __syncwarp();
-            for (uint32_t t = lane; t < tests; t += 32) {
-                uint32_t f = 0; // last face whose prefix is <= t
-                for (uint32_t step = 32; step; step >>= 1)
-                    if (f + step < nok && ws.work[f + step] <= t) f += step;
+            if (direct) {
+                for (uint32_t t = lane; t < items; t += 32) {
+                    uint32_t f = 0; // last face whose prefix is <= t
+                    for (uint32_t step = 32; step; step >>= 1)
+                        if (f + step < nok && ws.work[f + step] <= t) f += step;
+                    const FaceSetup& s = ws.faces[f];
+                    const uint32_t fw = uint32_t(s.x1 - s.x0 + 1), r = t - ws.work[f];
+                    const int fy = s.y0 + int(r / fw), fx = s.x0 + int(r % fw);
+                    if (face_covers(s, fx, fy)) {
+                        const uint32_t d = uint32_t(fy - y0) * uint32_t(bw) + uint32_t(fx - x0);
+                        const uint32_t unit = 1u << (8 * (d & 3));
+                        if (s.pad > 0) atomicAdd(&ws.delta[d >> 2], unit);
+                        else atomicSub(&ws.delta[d >> 2], unit);
+                    }
+                }
+            }
+            uint32_t f = 0;
+            for (uint32_t t = direct ? items : lane; t < items; t += 32) {
+                while (f + 1 < nok && ws.work[f + 1] <= t) ++f;
                 const FaceSetup& s = ws.faces[f];
-                const uint32_t fw = uint32_t(s.x1 - s.x0 + 1), r = t - ws.work[f];
-                const int fy = s.y0 + int(r / fw), fx = s.x0 + int(r % fw);
-                if (face_covers(s, fx, fy)) {
-                    const uint32_t d = uint32_t(fy - y0) * uint32_t(bw) + uint32_t(fx - x0);
-                    const uint32_t unit = 1u << (8 * (d & 3));
-                    if (s.pad > 0) atomicAdd(&ws.delta[d >> 2], unit);
-                    else atomicSub(&ws.delta[d >> 2], unit);
+                const int fy = s.y0 + int(t - ws.work[f]);
+                int lo = s.x0, hi = s.x1;
+                const double py = double(fy) + .5;
+                // edge (d, e), edge (e, a), edge (a, d) of face_covers
+                const double ax3[3] = {s.dx, s.ex, s.ax}, ay3[3] = {s.dy, s.ey, s.ay};
+                const double bx3[3] = {s.ex, s.ax, s.dx}, by3[3] = {s.ey, s.ay, s.dy};
+                const double r3[3] = {s.r0, s.r1, s.r2};
+                for (int e = 0; e < 3 && lo <= hi; ++e) {
+                    const double ax = ax3[e], ay = ay3[e], r = r3[e];
+                    const double t1 = (bx3[e] - ax) * (py - ay), c = by3[e] - ay;
+                    // covered(x) = !((t1 - c * (x + .5 - ax)) + r < 0)
+                    auto ok = [&](int x) { return !((t1 - c * ((double(x) + .5) - ax)) + r < 0); };
+                    if (c > 0) { // true then false: last covered x
+                        if (!ok(lo)) { hi = lo - 1; break; }
+                        int a = lo, b = hi;
+                        while (a < b) {
+                            const int m = a + (b - a + 1) / 2;
+                            if (ok(m)) a = m;
+                            else b = m - 1;
+                        }
+                        hi = a;
+                    } else if (c < 0) { // false then true: first covered x
+                        if (!ok(hi)) { hi = lo - 1; break; }
+                        int a = lo, b = hi;
+                        while (a < b) {
+                            const int m = a + (b - a) / 2;
+                            if (ok(m)) b = m;
+                            else a = m + 1;
+                        }
+                        lo = a;
+                    } else if (!ok(lo)) {
+                        hi = lo - 1;
+                    }
+                }
+                if (lo <= hi) {
+                    const uint32_t row = uint32_t(fy - y0) * uint32_t(bw);
+                    const uint32_t d0 = row + uint32_t(lo - x0);
+                    const uint32_t u0 = 1u << (8 * (d0 & 3));
+                    if (s.pad > 0) atomicAdd(&ws.delta[d0 >> 2], u0);
+                    else atomicSub(&ws.delta[d0 >> 2], u0);
+                    if (hi < x1) {
+                        const uint32_t d1 = row + uint32_t(hi + 1 - x0);
+                        const uint32_t u1 = 1u << (8 * (d1 & 3));
+                        if (s.pad > 0) atomicSub(&ws.delta[d1 >> 2], u1);
+                        else atomicAdd(&ws.delta[d1 >> 2], u1);
+                    }
                 }
             }
             __syncwarp();
-            // Phase 2: coverage words row by row; loads for step t+1 are issued
-            // before step t is consumed.
-            const int steps = rows * words;
-            int y = ry0, w = 0;
-            int x = wx0 + int(lane);
-            int pc_next = x < int(size) ? int(pv.state_count[size_t(y) * size + size_t(x)]) : 0;
-            bool r_next = !same_ref && x < int(size) && pv_ref_bit(pv.ref_bits, size_t(y) * size + size_t(x));
-            for (int t = 0; t < steps; ++t) {
-                const int pc = pc_next;
-                const bool rbit_own = r_next;
-                const int cx = x, cy = y, cw = w;
-                if (++w == words) w = 0, ++y;
-                x = wx0 + 32 * w + int(lane);
-                if (t + 1 < steps) {
-                    const size_t ni = size_t(y) * size + size_t(x);
-                    pc_next = x < int(size) ? int(pv.state_count[ni]) : 0;
-                    r_next = !same_ref && x < int(size) && pv_ref_bit(pv.ref_bits, ni);
+            // Row prefix sums: difference map -> per-sample delta (bias kept).
+            if (!direct) {
+                unsigned char* db = reinterpret_cast<unsigned char*>(ws.delta);
+                for (int ry = 0; ry < bh; ++ry) {
+                    int carry = 0;
+                    for (int bx = 0; bx < bw; bx += 32) {
+                        const int x = bx + int(lane);
+                        const uint32_t i = uint32_t(ry) * uint32_t(bw) + uint32_t(x);
+                        int v = x < bw ? int(db[i]) - 128 : 0;
+                        for (int o = 1; o < 32; o <<= 1) {
+                            const int n = __shfl_up_sync(0xffffffffu, v, o);
+                            if (lane >= uint32_t(o)) v += n;
+                        }
+                        v += carry;
+                        if (x < bw) db[i] = (unsigned char)(v + 128);
+                        carry = __shfl_sync(0xffffffffu, v, 31);
+                    }
                 }
-                int delta = 0;
-                if (cx >= x0 && cx <= x1 && cy >= y0 && cy <= y1) {
-                    const uint32_t d = uint32_t(cy - y0) * uint32_t(bw) + uint32_t(cx - x0);
-                    delta = int((ws.delta[d >> 2] >> (8 * (d & 3))) & 0xffu) - 128;
+            }
+            __syncwarp();
+            // Phase 2: the candidate's coverage words over the region start as
+            // the state's words (independent word loads, 32 per warp
+            // iteration); only samples with a non-zero count delta read their
+            // state count, and their bit flips where covered-ness changes.
+            const int nwords = rows * words;
+            const uint32_t cbase = uint32_t(wx0 >> 5);
+            for (int k = int(lane); k < nwords; k += 32)
+                ws.region[k] = chunk_global(pv.state_bits, size, uint32_t(ry0 + k / words), cbase + uint32_t(k % words));
+            __syncwarp();
+            const uint32_t nd = uint32_t(bw * bh);
+            const float inv_bw = 1.0f / float(bw);
+            bool negative = false;
+            for (uint32_t k = lane; k < delta_words; k += 32) {
+                const uint32_t dw = ws.delta[k];
+                if (dw == 0x80808080u) continue;
+                for (uint32_t j = 0; j < 4; ++j) {
+                    const int dv = int((dw >> (8 * j)) & 0xffu) - 128;
+                    const uint32_t d = 4 * k + j;
+                    if (!dv || d >= nd) continue;
+                    uint32_t q = uint32_t(float(d) * inv_bw); // row in the bbox, corrected below
+                    while (q * uint32_t(bw) > d) --q;
+                    while ((q + 1) * uint32_t(bw) <= d) ++q;
+                    const int y = y0 + int(q), x = x0 + int(d - q * uint32_t(bw));
+                    const int pc = int(pv.state_count[size_t(y) * size + size_t(x)]);
+                    const int cc = pc + dv;
+                    negative |= cc < 0;
+                    if ((cc > 0) != (pc > 0))
+                        atomicXor(&ws.region[(y - ry0) * words + ((x - wx0) >> 5)], 1u << ((x - wx0) & 31));
                 }
-                const int cc = pc + delta;
-                const uint32_t Cw = __ballot_sync(0xffffffffu, cc > 0);
-                const uint32_t Pw = __ballot_sync(0xffffffffu, pc > 0);
-                const uint32_t Rw = same_ref ? Pw : __ballot_sync(0xffffffffu, rbit_own);
-                if (__ballot_sync(0xffffffffu, cc < 0)) fallback = true;
-                if (Cw != Pw) {
-                    dchg += __popc(Cw ^ Rw) - __popc(Pw ^ Rw);
-                    dtot += __popc(Cw | Rw) - __popc(Pw | Rw);
-                    dcov += __popc(Cw) - __popc(Pw);
+            }
+            if (__any_sync(0xffffffffu, negative)) fallback = true;
+            __syncwarp();
+            // Popcount deltas against the reference and the changed-sample
+            // queue (candidate xor reference), one region word per lane.
+            for (int base = 0; base < nwords; base += 32) {
+                const int k = base + int(lane);
+                uint32_t Cw = 0, Rw = 0;
+                int ry = 0, cw = 0;
+                if (k < nwords) {
+                    ry = ry0 + k / words, cw = k % words;
+                    const uint32_t Pw = chunk_global(pv.state_bits, size, uint32_t(ry), cbase + uint32_t(cw));
+                    Cw = ws.region[k];
+                    Rw = same_ref ? Pw : chunk_global(pv.ref_bits, size, uint32_t(ry), cbase + uint32_t(cw));
+                    if (Cw != Pw) {
+                        dchg += __popc(Cw ^ Rw) - __popc(Pw ^ Rw);
+                        dtot += __popc(Cw | Rw) - __popc(Pw | Rw);
+                        dcov += __popc(Cw) - __popc(Pw);
+                    }
                 }
-                if (lane == 0) ws.region[(cy - ry0) * words + cw] = Cw;
                 const uint32_t xm = Cw ^ Rw;
-                if (xm) {
-                    const uint32_t pos = qn + __popc(xm & below);
-                    if (((xm >> lane) & 1u) && pos < kQueue)
-                        ws.queue[pos] = uint32_t(cx) | (uint32_t(cy) << 15) | (uint32_t(cc > 0) << 30);
-                    qn += __popc(xm);
+                const uint32_t cnt = __popc(xm);
+                uint32_t incl = cnt;
+                for (int o = 1; o < 32; o <<= 1) {
+                    const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+                    if (lane >= uint32_t(o)) incl += t;
                 }
+                uint32_t pos = qn + incl - cnt;
+                for (uint32_t b = xm; b; b &= b - 1, ++pos) {
+                    const uint32_t bit = uint32_t(__ffs(b) - 1);
+                    if (pos < uint32_t(kQueue))
+                        ws.queue[pos] = (uint32_t(wx0) + 32 * uint32_t(cw) + bit) | (uint32_t(ry) << 15) |
+                                        (((Cw >> bit) & 1u) << 30);
+                }
+                qn += __shfl_sync(0xffffffffu, incl, 31);
+            }
+            for (int o = 16; o; o >>= 1) {
+                dchg += __shfl_xor_sync(0xffffffffu, dchg, o);
+                dtot += __shfl_xor_sync(0xffffffffu, dtot, o);
+                dcov += __shfl_xor_sync(0xffffffffu, dcov, o);
             }
             if (qn > uint32_t(kQueue)) fallback = true;
         }
@@ -450,21 +567,27 @@ __device__ void audit_unit(const CandidateRecord* __restrict__ rec, const PlanDe
     uint32_t best = 0;
     if (!fallback && r.changed && r.ca && r.cb) {
         RefMask rmask{pv.ref_bits, size};
-        for (uint32_t k = lane; k < qn; k += 32) {
-            const uint32_t e = ws.queue[k];
-            const uint32_t x = e & 0x7fffu, y = (e >> 15) & 0x7fffu;
-            // Candidate-only sample: distance to the reference (resident field
-            // or search); reference-only sample: search the candidate.
-            uint32_t d;
-            if ((e >> 30) & 1u) d = pv.ref_field ? pv.ref_field[size_t(y) * size + x] : nearest_d2(rmask, x, y);
-            else d = nearest_d2(cmask, x, y);
-            best = d > best ? d : best;
+        // The running maximum (warp-wide after each round of 32 samples)
+        // bounds every search: a sample whose nearest covered sample is
+        // closer cannot raise it.
+        best = uint32_t(max(max(far1, far2), 0));
+        for (uint32_t base = 0; base < qn; base += 32) {
+            const uint32_t k = base + lane;
+            if (k < qn) {
+                const uint32_t e = ws.queue[k];
+                const uint32_t x = e & 0x7fffu, y = (e >> 15) & 0x7fffu;
+                // Candidate-only sample: distance to the reference (resident
+                // field or search); reference-only sample: search the candidate.
+                uint32_t d;
+                if ((e >> 30) & 1u) d = pv.ref_field ? pv.ref_field[size_t(y) * size + x] : nearest_d2(rmask, x, y, best);
+                else d = nearest_d2(cmask, x, y, best);
+                best = d > best ? d : best;
+            }
+            for (int o = 16; o; o >>= 1) {
+                const uint32_t y = __shfl_xor_sync(0xffffffffu, best, o);
+                best = y > best ? y : best;
+            }
         }
-        for (int o = 16; o; o >>= 1) {
-            const uint32_t y = __shfl_xor_sync(0xffffffffu, best, o);
-            best = y > best ? y : best;
-        }
-        best = max(best, uint32_t(max(max(far1, far2), 0)));
     }
     r.max_d2 = best;
     if (fallback) r.flags |= kRecFallback;
