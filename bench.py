@@ -497,7 +497,7 @@ def run_batched(args, rank: int, world: int, local: int) -> dict:
     device = torch.device("cuda", local)
     stream = torch.cuda.current_stream(device)
     t0 = time.perf_counter()
-    meshes = syn.batched_set(BATCH_MESHES, seed=2 + 1000 * rank)
+    meshes = syn.batched_set(args.meshes, seed=2 + 1000 * rank)
     opts = br.neural_options(device=local, preserve_uv=0)
     sessions = [br.AuditSession(m, opts) for m in meshes]
     gates = [br.eval_settings(*a) for a in BATCH_GATE_ARGS]
@@ -563,10 +563,12 @@ def run_batched(args, rank: int, world: int, local: int) -> dict:
             "config": {"workload": BATCH_WORKLOAD, "meshes": len(meshes), "faces_min": min(faces),
                        "faces_max": max(faces), "faces_total": int(sum(faces)),
                        "kinds": "sphere/torus/heightfield cycling, seeded 2+1000*rank", "uv_charts": "4-16, seams",
+                       "candidates_note": "first of the set if --meshes < 64 (then not the workload)",
                        "views": 64, "raster": "4160x4160 (512 px x ss8)", "gates": 4,
                        "candidates_per_step": n, "candidates_per_mesh": BATCH_PER_MESH,
                        "accepted": int(verdicts["accepted"].sum()), "setup_s": setup_s,
-                       "warp_tier": ["small 128x64", "medium 256x128"][info["tier"]],
+                       "warp_tier": ["small 128x64", "medium 256x128"][info["tier"] & 1]
+                                    + (", heavy units to the huge tier" if info["tier"] & 2 else ""),
                        "autotune_ms": info["tune_ms"], "graph": "captured once, replayed every step",
                        "exact_path_candidates": int(verdicts["exact_path"].sum()),
                        "l2": "inputs larger than L2 (about 1.2 GB of state counts and masks per mesh)",
@@ -634,6 +636,7 @@ def main() -> None:
     ap.add_argument("--no-surrogate", action="store_true")
     ap.add_argument("--config", default="batched", choices=["batched", "icosphere"])
     ap.add_argument("--no-icosphere", action="store_true")
+    ap.add_argument("--meshes", type=int, default=BATCH_MESHES, help="meshes of the batched set (64 = the workload)")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

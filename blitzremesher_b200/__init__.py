@@ -173,7 +173,7 @@ class ExecuteOptions(C.Structure):
 
 class BatchInfo(C.Structure):
     _fields_ = [("struct_size", C.c_uint32), ("sessions", C.c_uint32), ("tier", C.c_uint32), ("tuned", C.c_uint32),
-                ("graph_captured", C.c_uint32), ("tune_ms", C.c_float * 2), ("graph_launches", C.c_uint64),
+                ("graph_captured", C.c_uint32), ("tune_ms", C.c_float * 4), ("graph_launches", C.c_uint64),
                 ("exact_candidates", C.c_uint64), ("audit_ms", C.c_float), ("units", C.c_uint64),
                 ("region_samples", C.c_uint64), ("changed_samples", C.c_uint64)]
 

@@ -22,6 +22,7 @@ constexpr int kAuditWarps = 8;
 constexpr int kMaxOk = 48;          // rasterized (unculled, unclipped) old + new faces
 constexpr int kMaxTileSide = 32;    // tile-maxima path for rasters up to 1024 x 1024
 constexpr uint32_t kDirectTests = 4096; // bbox samples up to which phase 1 tests every sample
+constexpr uint32_t kHeavyUnit = 512;    // changed samples above which a warp-tier unit may spill
 
 // Per-warp limits of one (candidate, view) unit. The common tier keeps its
 // scratch small so that many warps stay resident; units that overflow it are
@@ -30,7 +31,7 @@ struct LimitsSmall {
     static constexpr int kRegionWords = 4;     // region width <= 128 samples after 32-alignment
     static constexpr int kRegionRows = 64;     // region height
     static constexpr int kDeltaSamples = 2048; // region samples (unaligned bbox) with a count delta
-    static constexpr int kQueue = 160;         // changed samples per (candidate, view)
+    static constexpr int kQueue = 160;         // reference-only samples of affected tiles (>= 64)
     static constexpr int kAffected = 8;        // tiles outside the region whose distances may change
 };
 // A wider warp tier for workloads whose units often overflow the small one
@@ -177,7 +178,7 @@ __device__ __forceinline__ void record_write(ViewRecord* out, const ViewRecord& 
 template <class L>
 __device__ void audit_unit(const CandidateRecord* __restrict__ rec, const PlanDev& plan, uint32_t v,
                            WarpScratch<L>& ws, ViewRecord* out, unsigned long long* stats, uint32_t u,
-                           uint32_t* spill) {
+                           uint32_t* spill, uint32_t heavy = 0xffffffffu) {
     constexpr int kRegionWords = L::kRegionWords, kRegionRows = L::kRegionRows;
     constexpr int kDeltaSamples = L::kDeltaSamples, kQueue = L::kQueue, kAffected = L::kAffected;
     const uint32_t lane = lane_id();
@@ -275,7 +276,8 @@ __device__ void audit_unit(const CandidateRecord* __restrict__ rec, const PlanDe
     }
     __syncwarp();
     int dchg = 0, dtot = 0, dcov = 0;
-    uint32_t qn = 0;
+    uint32_t qn = 0, region_changed = 0;
+    int region_words = 0;
     bool fallback = false;
     CandMask cmask;
     cmask.state = pv.state_bits;
@@ -455,8 +457,9 @@ __device__ void audit_unit(const CandidateRecord* __restrict__ rec, const PlanDe
             }
             if (__any_sync(0xffffffffu, negative)) fallback = true;
             __syncwarp();
-            // Popcount deltas against the reference and the changed-sample
-            // queue (candidate xor reference), one region word per lane.
+            // Popcount deltas against the reference, one region word per lane;
+            // the distance phase walks the same words for the changed samples.
+            region_words = nwords;
             for (int base = 0; base < nwords; base += 32) {
                 const int k = base + int(lane);
                 uint32_t Cw = 0, Rw = 0;
@@ -472,28 +475,17 @@ __device__ void audit_unit(const CandidateRecord* __restrict__ rec, const PlanDe
                         dcov += __popc(Cw) - __popc(Pw);
                     }
                 }
-                const uint32_t xm = Cw ^ Rw;
-                const uint32_t cnt = __popc(xm);
-                uint32_t incl = cnt;
-                for (int o = 1; o < 32; o <<= 1) {
-                    const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
-                    if (lane >= uint32_t(o)) incl += t;
-                }
-                uint32_t pos = qn + incl - cnt;
-                for (uint32_t b = xm; b; b &= b - 1, ++pos) {
-                    const uint32_t bit = uint32_t(__ffs(b) - 1);
-                    if (pos < uint32_t(kQueue))
-                        ws.queue[pos] = (uint32_t(wx0) + 32 * uint32_t(cw) + bit) | (uint32_t(ry) << 15) |
-                                        (((Cw >> bit) & 1u) << 30);
-                }
-                qn += __shfl_sync(0xffffffffu, incl, 31);
+                region_changed += __popc(Cw ^ Rw);
             }
             for (int o = 16; o; o >>= 1) {
                 dchg += __shfl_xor_sync(0xffffffffu, dchg, o);
                 dtot += __shfl_xor_sync(0xffffffffu, dtot, o);
                 dcov += __shfl_xor_sync(0xffffffffu, dcov, o);
+                region_changed += __shfl_xor_sync(0xffffffffu, region_changed, o);
             }
-            if (qn > uint32_t(kQueue)) fallback = true;
+            // A unit with many changed samples goes to the next tier when
+            // that one runs more warps per SM.
+            if (spill && region_changed > heavy) fallback = true;
         }
     }
     __syncwarp();
@@ -571,22 +563,71 @@ __device__ void audit_unit(const CandidateRecord* __restrict__ rec, const PlanDe
         // bounds every search: a sample whose nearest covered sample is
         // closer cannot raise it.
         best = uint32_t(max(max(far1, far2), 0));
+        // Reference-only samples of the affected tiles outside the region.
         for (uint32_t base = 0; base < qn; base += 32) {
             const uint32_t k = base + lane;
             if (k < qn) {
                 const uint32_t e = ws.queue[k];
                 const uint32_t x = e & 0x7fffu, y = (e >> 15) & 0x7fffu;
-                // Candidate-only sample: distance to the reference (resident
-                // field or search); reference-only sample: search the candidate.
-                uint32_t d;
-                if ((e >> 30) & 1u) d = pv.ref_field ? pv.ref_field[size_t(y) * size + x] : nearest_d2(rmask, x, y, best);
-                else d = nearest_d2(cmask, x, y, best);
+                const uint32_t d = nearest_d2(cmask, x, y, best);
                 best = d > best ? d : best;
             }
             for (int o = 16; o; o >>= 1) {
                 const uint32_t y = __shfl_xor_sync(0xffffffffu, best, o);
                 best = y > best ? y : best;
             }
+        }
+        __syncwarp();
+        // Changed samples of the region, straight from its coverage words, 32
+        // words per round: the round's masks and a prefix of their counts go
+        // to shared memory and every lane takes samples by rank.
+        // Candidate-only samples measure to the reference (resident field or
+        // search), reference-only samples search the candidate.
+        const uint32_t cbase = uint32_t(wx0 >> 5);
+        uint32_t* rmask_s = ws.queue;       // 32 xor masks (the queue is consumed)
+        uint32_t* cmask_s = ws.queue + 32;  // 32 candidate words
+        uint32_t* pre = ws.work;            // 33 prefix counts
+        for (int base = 0; base < region_words; base += 32) {
+            const int k = base + int(lane);
+            uint32_t xm = 0, Cw = 0;
+            if (k < region_words) {
+                Cw = ws.region[k];
+                xm = Cw ^ chunk_global(same_ref ? pv.state_bits : pv.ref_bits, size, uint32_t(ry0 + k / words),
+                                       cbase + uint32_t(k % words));
+            }
+            if (!__any_sync(0xffffffffu, xm != 0)) continue; // no changed sample in these 32 words
+            const uint32_t cnt = __popc(xm);
+            uint32_t incl = cnt;
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= uint32_t(o)) incl += t;
+            }
+            rmask_s[lane] = xm;
+            cmask_s[lane] = Cw;
+            pre[lane + 1] = incl;
+            if (lane == 0) pre[0] = 0;
+            const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
+            __syncwarp();
+            for (uint32_t j = lane; j < total; j += 32) {
+                uint32_t w = 0; // last word whose prefix is <= j
+                for (uint32_t step = 16; step; step >>= 1)
+                    if (pre[w + step] <= j) w += step;
+                const uint32_t m = rmask_s[w];
+                const uint32_t bit = __fns(m, 0, int(j - pre[w]) + 1);
+                const int kw = base + int(w);
+                const uint32_t ry = uint32_t(ry0 + kw / words), cw = uint32_t(kw % words);
+                const uint32_t x = uint32_t(wx0) + 32 * cw + bit;
+                uint32_t d;
+                if ((cmask_s[w] >> bit) & 1u)
+                    d = pv.ref_field ? pv.ref_field[size_t(ry) * size + x] : nearest_d2(rmask, x, ry, best);
+                else d = nearest_d2(cmask, x, ry, best);
+                best = d > best ? d : best;
+            }
+            for (int o = 16; o; o >>= 1) {
+                const uint32_t y = __shfl_xor_sync(0xffffffffu, best, o);
+                best = y > best ? y : best;
+            }
+            __syncwarp();
         }
     }
     r.max_d2 = best;
@@ -598,7 +639,7 @@ __device__ void audit_unit(const CandidateRecord* __restrict__ rec, const PlanDe
         if (stats) {
             atomicAdd(stats, 1ull);
             atomicAdd(stats + 1, (unsigned long long)samples);
-            atomicAdd(stats + 2, (unsigned long long)qn);
+            atomicAdd(stats + 2, (unsigned long long)(qn + region_changed));
         }
     }
     __syncwarp();
@@ -651,7 +692,7 @@ __global__ void __launch_bounds__(kAuditWarps * 32, kMinBlocks)
             record_write(slot, r);
             continue;
         }
-        audit_unit(rec, *plan, v, ws, slot, stats, u, spill);
+        audit_unit(rec, *plan, v, ws, slot, stats, u, spill, job.heavy);
     }
 }
 
@@ -799,8 +840,9 @@ void launch_audit(const AuditJob& job, unsigned long long* stats, uint32_t* queu
         set_smem(k_audit_large, large);
         configured = true;
     }
-    const AuditKernel kernel = warp_tier(variant, job.entries != nullptr);
-    const size_t smem = warp_tier_smem(variant);
+    const int tier = variant & 1;
+    const AuditKernel kernel = warp_tier(tier, job.entries != nullptr);
+    const size_t smem = warp_tier_smem(tier);
     int sms = 148, dev = 0;
     if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     int per_sm = 0;
@@ -810,10 +852,17 @@ void launch_audit(const AuditJob& job, unsigned long long* stats, uint32_t* queu
     uint64_t needed = (job.total + kAuditWarps - 1) / kAuditWarps;
     if (grid > needed) grid = needed;
     const bool huge = spill && spill_huge && huge_scratch && huge_blocks;
+    AuditJob tuned = job;
+    tuned.heavy = (variant & kAuditSpillHeavy) && huge && huge_blocks >= uint32_t(sms) ? kHeavyUnit : 0xffffffffu;
     cudaMemsetAsync(queue, 0, spill ? (huge ? 12 : 8) : 4, s);
     if (spill) cudaMemsetAsync(spill, 0, 4, s);
     if (huge) cudaMemsetAsync(spill_huge, 0, 4, s);
-    kernel<<<uint32_t(grid), kAuditWarps * 32, smem, s>>>(job, stats, queue, spill);
+    kernel<<<uint32_t(grid), kAuditWarps * 32, smem, s>>>(tuned, stats, queue, spill);
+    if (huge && huge_blocks >= uint32_t(sms)) {
+        // enough huge-tier warps: units the warp tier spills go there directly
+        k_audit_huge<<<huge_blocks, kHugeWarps * 32, 0, s>>>(job, stats, spill, queue + 1, huge_scratch);
+        return;
+    }
     if (spill)
         k_audit_large<<<uint32_t(sms), kLargeWarps * 32, large, s>>>(job, stats, spill, queue + 1,
                                                                      huge ? spill_huge : nullptr);

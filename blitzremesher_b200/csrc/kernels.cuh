@@ -171,10 +171,14 @@ struct AuditJob {
     const AuditEntry* entries; // device table, sorted by first_unit, or null
     uint32_t nentries;
     uint64_t total;            // units
+    uint32_t heavy;            // set by launch_audit
 };
 // variant: the warp tier's limits (kAuditTierSmall: regions up to 128 x 64
 // samples, 3 blocks per SM; kAuditTierMedium: 256 x 128, 1 block per SM).
 constexpr int kAuditTierSmall = 0, kAuditTierMedium = 1;
+// variant | kAuditSpillHeavy: warp-tier units with many changed samples go to
+// the huge tier when it runs at least one block per SM.
+constexpr int kAuditSpillHeavy = 2;
 void launch_audit(const AuditJob& job, unsigned long long* stats, uint32_t* queue, uint32_t* spill,
                   uint32_t* spill_huge, unsigned char* huge_scratch, uint32_t huge_blocks, cudaStream_t s,
                   int variant = kAuditTierSmall);

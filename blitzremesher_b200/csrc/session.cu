@@ -2215,7 +2215,7 @@ struct blitz_audit_batch {
     uint32_t huge_blocks = 0;
     int variant = kAuditTierSmall;
     bool tuned = false;
-    float tune_ms[2] = {0, 0};
+    float tune_ms[4] = {0, 0, 0, 0};
     // captured launch sequence and the inputs it was captured for
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
@@ -2326,7 +2326,7 @@ blitz_status blitz_audit_batch_candidates(blitz_audit_batch* b, const blitz_coll
         if (big && !b->huge.p) {
             int sms = 148;
             B200_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device));
-            b->huge_blocks = uint32_t(std::max(1, sms / 2));
+            b->huge_blocks = uint32_t(std::max(1, 2 * sms));
             b->huge = Buf<unsigned char>(b->pool, audit_huge_scratch_bytes(b->huge_blocks));
         }
         if (big) b->spill_huge.ensure(b->pool, max_units + 1);
@@ -2373,17 +2373,21 @@ blitz_status blitz_audit_batch_candidates(blitz_audit_batch* b, const blitz_coll
             cudaEvent_t e0, e1;
             B200_CUDA(cudaEventCreate(&e0));
             B200_CUDA(cudaEventCreate(&e1));
-            for (int v = 0; v < 2; ++v) {
+            float best_ms = 0;
+            for (int v = 0; v < 4; ++v) {
+                if ((v & kAuditSpillHeavy) && !big) continue;
                 body(v); // warm
                 B200_CUDA(cudaEventRecord(e0, st));
                 body(v);
                 B200_CUDA(cudaEventRecord(e1, st));
                 B200_CUDA(cudaEventSynchronize(e1));
-                B200_CUDA(cudaEventElapsedTime(&b->tune_ms[v], e0, e1));
+                float ms = 0;
+                B200_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+                b->tune_ms[v] = ms;
+                if (v == 0 || ms < best_ms) best_ms = ms, b->variant = v;
             }
             cudaEventDestroy(e0);
             cudaEventDestroy(e1);
-            b->variant = b->tune_ms[1] < b->tune_ms[0] ? kAuditTierMedium : kAuditTierSmall;
             b->tuned = true;
             if (b->exec) cudaGraphExecDestroy(b->exec), b->exec = nullptr;
             if (b->graph) cudaGraphDestroy(b->graph), b->graph = nullptr;
@@ -2449,8 +2453,7 @@ blitz_status blitz_audit_batch_read_info(const blitz_audit_batch* b, blitz_audit
     out->tier = uint32_t(b->variant);
     out->tuned = b->tuned ? 1u : 0u;
     out->graph_captured = b->exec ? 1u : 0u;
-    out->tune_ms[0] = b->tune_ms[0];
-    out->tune_ms[1] = b->tune_ms[1];
+    for (int v = 0; v < 4; ++v) out->tune_ms[v] = b->tune_ms[v];
     out->graph_launches = b->graph_launches;
     out->exact_candidates = b->exact_candidates;
     out->audit_ms = b->audit_ms;

@@ -321,14 +321,15 @@ blitz_status blitz_audit_attach_surrogate(blitz_audit_session*, blitz_surrogate*
 typedef struct blitz_audit_batch blitz_audit_batch;
 #define BLITZ_BATCH_GRAPH 1u    /* capture the launch sequence once and replay it while the candidate and
                                    verdict buffers, counts, gates, stream and session states are unchanged */
-#define BLITZ_BATCH_AUTOTUNE 2u /* time the two warp-tier variants on this call and keep the faster */
+#define BLITZ_BATCH_AUTOTUNE 2u /* time the audit variants on this call and keep the fastest */
 #define BLITZ_BATCH_PROFILE 4u  /* record the audit launches' device time and work counters (no graph) */
 typedef struct blitz_audit_batch_info {
     uint32_t struct_size;
     uint32_t sessions;
-    uint32_t tier;            /* 0: 128 x 64-sample warp tier, 3 blocks/SM; 1: 256 x 128, 1 block/SM */
+    uint32_t tier;            /* bit 0: warp tier (0: 128 x 64-sample regions, 3 blocks/SM; 1: 256 x 128,
+                                 1 block/SM); bit 1: units with many changed samples go to the huge tier */
     uint32_t tuned, graph_captured;
-    float tune_ms[2];         /* device time of one batch with each tier when tuned */
+    float tune_ms[4];         /* device time of one batch with each variant when tuned (0: not tried) */
     uint64_t graph_launches;  /* replays of the captured graph */
     uint64_t exact_candidates;
     /* last BLITZ_BATCH_PROFILE call: audit launches' device time, (candidate,
