@@ -61,8 +61,18 @@ struct LimitsHuge {
     static constexpr int kAffected = 64;
 };
 constexpr int kHugeWarps = 8;
+// The giant tier: any region of a raster up to 4160 x 4160 (512 px x ss 8),
+// for the rare units beyond the huge tier; few warps, global scratch.
+struct LimitsGiant {
+    static constexpr int kRegionWords = 136;
+    static constexpr int kRegionRows = 4160;
+    static constexpr int kDeltaSamples = 4352 * 4160;
+    static constexpr int kQueue = 65536;
+    static constexpr int kAffected = 64;
+};
+constexpr int kGiantWarps = 8;
 
-template <class L> struct WarpScratch {
+template <class L> struct alignas(16) WarpScratch {
     double vx[32], vy[32], vz[32]; // projected local vertices; 31 = placement
     FaceSetup faces[kMaxOk];       // old faces carry pad = -1, new faces pad = +1
     uint32_t work[kMaxOk];         // exclusive prefix of bbox samples per face
@@ -295,7 +305,8 @@ __device__ void audit_unit(const CandidateRecord* __restrict__ rec, const PlanDe
         const int rows = ry1 - ry0 + 1;
         cmask.y0 = uint32_t(ry0), cmask.y1 = uint32_t(ry1), cmask.c0 = uint32_t(wx0 >> 5), cmask.words = uint32_t(words);
         const int bw = x1 - x0 + 1, bh = y1 - y0 + 1;
-        if (words > kRegionWords || rows > kRegionRows || bw * bh > kDeltaSamples) {
+        const int bws = (bw + 15) & ~15; // delta map row stride: whole 16-byte vectors
+        if (words > kRegionWords || rows > kRegionRows || bws * bh > kDeltaSamples) {
             fallback = true;
         } else {
             samples = uint64_t(rows) * words * 32;
@@ -306,7 +317,7 @@ __device__ void audit_unit(const CandidateRecord* __restrict__ rec, const PlanDe
             // per-sample byte difference map (biased by 128: at most 32 old
             // and 32 new faces), which a per-row prefix scan turns into the
             // candidate's count delta (new faces +1, old faces -1).
-            const uint32_t delta_words = uint32_t(bw * bh + 3) >> 2;
+            const uint32_t delta_words = uint32_t(bws * bh) >> 2;
             for (uint32_t k = lane; k < delta_words; k += 32) ws.delta[k] = 0x80808080u;
             // Small units test every (face, sample in its bbox) directly; large
             // ones take the interval route below. Both give the same map.
@@ -345,7 +356,7 @@ __device__ void audit_unit(const CandidateRecord* __restrict__ rec, const PlanDe
                     const uint32_t fw = uint32_t(s.x1 - s.x0 + 1), r = t - ws.work[f];
                     const int fy = s.y0 + int(r / fw), fx = s.x0 + int(r % fw);
                     if (face_covers(s, fx, fy)) {
-                        const uint32_t d = uint32_t(fy - y0) * uint32_t(bw) + uint32_t(fx - x0);
+                        const uint32_t d = uint32_t(fy - y0) * uint32_t(bws) + uint32_t(fx - x0);
                         const uint32_t unit = 1u << (8 * (d & 3));
                         if (s.pad > 0) atomicAdd(&ws.delta[d >> 2], unit);
                         else atomicSub(&ws.delta[d >> 2], unit);
@@ -391,7 +402,7 @@ __device__ void audit_unit(const CandidateRecord* __restrict__ rec, const PlanDe
                     }
                 }
                 if (lo <= hi) {
-                    const uint32_t row = uint32_t(fy - y0) * uint32_t(bw);
+                    const uint32_t row = uint32_t(fy - y0) * uint32_t(bws);
                     const uint32_t d0 = row + uint32_t(lo - x0);
                     const uint32_t u0 = 1u << (8 * (d0 & 3));
                     if (s.pad > 0) atomicAdd(&ws.delta[d0 >> 2], u0);
@@ -407,20 +418,22 @@ __device__ void audit_unit(const CandidateRecord* __restrict__ rec, const PlanDe
             __syncwarp();
             // Row prefix sums: difference map -> per-sample delta (bias kept).
             if (!direct) {
-                unsigned char* db = reinterpret_cast<unsigned char*>(ws.delta);
-                for (int ry = 0; ry < bh; ++ry) {
+                // one row per lane, 16 samples per vector load
+                for (int ry = int(lane); ry < bh; ry += 32) {
+                    uint4* rowp = reinterpret_cast<uint4*>(ws.delta) + size_t(ry) * uint32_t(bws >> 4);
                     int carry = 0;
-                    for (int bx = 0; bx < bw; bx += 32) {
-                        const int x = bx + int(lane);
-                        const uint32_t i = uint32_t(ry) * uint32_t(bw) + uint32_t(x);
-                        int v = x < bw ? int(db[i]) - 128 : 0;
-                        for (int o = 1; o < 32; o <<= 1) {
-                            const int n = __shfl_up_sync(0xffffffffu, v, o);
-                            if (lane >= uint32_t(o)) v += n;
+                    for (int c = 0; c < (bws >> 4); ++c) {
+                        uint4 v = rowp[c];
+                        uint32_t* w4 = reinterpret_cast<uint32_t*>(&v);
+                        for (int q = 0; q < 4; ++q) {
+                            uint32_t out = 0;
+                            for (int b = 0; b < 4; ++b) {
+                                carry += int((w4[q] >> (8 * b)) & 0xffu) - 128;
+                                out |= uint32_t(carry + 128) << (8 * b);
+                            }
+                            w4[q] = out;
                         }
-                        v += carry;
-                        if (x < bw) db[i] = (unsigned char)(v + 128);
-                        carry = __shfl_sync(0xffffffffu, v, 31);
+                        rowp[c] = v;
                     }
                 }
             }
@@ -434,8 +447,7 @@ __device__ void audit_unit(const CandidateRecord* __restrict__ rec, const PlanDe
             for (int k = int(lane); k < nwords; k += 32)
                 ws.region[k] = chunk_global(pv.state_bits, size, uint32_t(ry0 + k / words), cbase + uint32_t(k % words));
             __syncwarp();
-            const uint32_t nd = uint32_t(bw * bh);
-            const float inv_bw = 1.0f / float(bw);
+            const float inv_bws = 1.0f / float(bws);
             bool negative = false;
             for (uint32_t k = lane; k < delta_words; k += 32) {
                 const uint32_t dw = ws.delta[k];
@@ -443,11 +455,12 @@ __device__ void audit_unit(const CandidateRecord* __restrict__ rec, const PlanDe
                 for (uint32_t j = 0; j < 4; ++j) {
                     const int dv = int((dw >> (8 * j)) & 0xffu) - 128;
                     const uint32_t d = 4 * k + j;
-                    if (!dv || d >= nd) continue;
-                    uint32_t q = uint32_t(float(d) * inv_bw); // row in the bbox, corrected below
-                    while (q * uint32_t(bw) > d) --q;
-                    while ((q + 1) * uint32_t(bw) <= d) ++q;
-                    const int y = y0 + int(q), x = x0 + int(d - q * uint32_t(bw));
+                    if (!dv) continue;
+                    uint32_t q = uint32_t(float(d) * inv_bws); // row in the bbox, corrected below
+                    while (q * uint32_t(bws) > d) --q;
+                    while ((q + 1) * uint32_t(bws) <= d) ++q;
+                    if (d - q * uint32_t(bws) >= uint32_t(bw)) continue; // row padding
+                    const int y = y0 + int(q), x = x0 + int(d - q * uint32_t(bws));
                     const int pc = int(pv.state_count[size_t(y) * size + size_t(x)]);
                     const int cc = pc + dv;
                     negative |= cc < 0;
@@ -721,15 +734,16 @@ __global__ void __launch_bounds__(kLargeWarps * 32, 1)
     }
 }
 
-// The huge tier: the same over the large tier's spill list, each warp with
-// its own slot of global scratch (`scratch`, one WarpScratch<LimitsHuge> per
-// resident warp).
-__global__ void __launch_bounds__(kHugeWarps * 32, 1)
-    k_audit_huge(const __grid_constant__ AuditJob job, unsigned long long* stats, const uint32_t* spill,
-                 uint32_t* cursor, unsigned char* scratch) {
+// The huge and giant tiers: the same over a spill list, each warp with its
+// own slot of global scratch (`scratch`, one WarpScratch<L> per resident
+// warp); what overflows goes to `spill_next` (may be null).
+template <class L, int kWarps>
+__global__ void __launch_bounds__(kWarps * 32, 1)
+    k_audit_global(const __grid_constant__ AuditJob job, unsigned long long* stats, const uint32_t* spill,
+                   uint32_t* cursor, unsigned char* scratch, uint32_t* spill_next) {
     const uint32_t lane = lane_id();
-    const uint32_t slot = blockIdx.x * kHugeWarps + (threadIdx.x >> 5);
-    WarpScratch<LimitsHuge>& ws = reinterpret_cast<WarpScratch<LimitsHuge>*>(scratch)[slot];
+    const uint32_t slot = blockIdx.x * kWarps + (threadIdx.x >> 5);
+    WarpScratch<L>& ws = reinterpret_cast<WarpScratch<L>*>(scratch)[slot];
     const uint32_t count = spill[0];
     for (;;) {
         uint32_t k = 0;
@@ -743,7 +757,7 @@ __global__ void __launch_bounds__(kHugeWarps * 32, 1)
         uint32_t lu;
         resolve_unit(job, u, plan, recs, out, lu);
         const uint32_t c = lu / plan->nviews, v = lu - c * plan->nviews;
-        audit_unit(recs + c, *plan, v, ws, out + lu, stats, u, nullptr);
+        audit_unit(recs + c, *plan, v, ws, out + lu, stats, u, spill_next);
     }
 }
 
@@ -812,6 +826,9 @@ __global__ void k_verdicts(const ViewRecord* const* plan_records, const uint32_t
 size_t audit_smem_bytes() { return kAuditWarps * sizeof(WarpScratch<LimitsSmall>); }
 size_t audit_large_smem_bytes() { return kLargeWarps * sizeof(WarpScratch<LimitsLarge>); }
 size_t audit_huge_scratch_bytes(uint32_t sms) { return size_t(sms) * kHugeWarps * sizeof(WarpScratch<LimitsHuge>); }
+size_t audit_giant_scratch_bytes(uint32_t blocks) {
+    return size_t(blocks) * kGiantWarps * sizeof(WarpScratch<LimitsGiant>);
+}
 
 namespace {
 template <class K> void set_smem(K kernel, size_t bytes) {
@@ -830,7 +847,7 @@ size_t warp_tier_smem(int variant) {
 
 void launch_audit(const AuditJob& job, unsigned long long* stats, uint32_t* queue, uint32_t* spill,
                   uint32_t* spill_huge, unsigned char* huge_scratch, uint32_t huge_blocks, cudaStream_t s,
-                  int variant) {
+                  int variant, const GiantTier* giant) {
     if (!job.total) return;
     static bool configured = false;
     const size_t large = audit_large_smem_bytes();
@@ -852,21 +869,30 @@ void launch_audit(const AuditJob& job, unsigned long long* stats, uint32_t* queu
     uint64_t needed = (job.total + kAuditWarps - 1) / kAuditWarps;
     if (grid > needed) grid = needed;
     const bool huge = spill && spill_huge && huge_scratch && huge_blocks;
+    const bool big = huge && giant && giant->spill && giant->scratch && giant->blocks;
     AuditJob tuned = job;
     tuned.heavy = (variant & kAuditSpillHeavy) && huge && huge_blocks >= uint32_t(sms) ? kHeavyUnit : 0xffffffffu;
-    cudaMemsetAsync(queue, 0, spill ? (huge ? 12 : 8) : 4, s);
+    cudaMemsetAsync(queue, 0, 16, s);
     if (spill) cudaMemsetAsync(spill, 0, 4, s);
     if (huge) cudaMemsetAsync(spill_huge, 0, 4, s);
+    if (big) cudaMemsetAsync(giant->spill, 0, 4, s);
+    uint32_t* next = big ? giant->spill : nullptr;
     kernel<<<uint32_t(grid), kAuditWarps * 32, smem, s>>>(tuned, stats, queue, spill);
     if (huge && huge_blocks >= uint32_t(sms)) {
         // enough huge-tier warps: units the warp tier spills go there directly
-        k_audit_huge<<<huge_blocks, kHugeWarps * 32, 0, s>>>(job, stats, spill, queue + 1, huge_scratch);
-        return;
+        k_audit_global<LimitsHuge, kHugeWarps>
+            <<<huge_blocks, kHugeWarps * 32, 0, s>>>(job, stats, spill, queue + 1, huge_scratch, next);
+    } else {
+        if (spill)
+            k_audit_large<<<uint32_t(sms), kLargeWarps * 32, large, s>>>(job, stats, spill, queue + 1,
+                                                                         huge ? spill_huge : nullptr);
+        if (huge)
+            k_audit_global<LimitsHuge, kHugeWarps>
+                <<<huge_blocks, kHugeWarps * 32, 0, s>>>(job, stats, spill_huge, queue + 2, huge_scratch, next);
     }
-    if (spill)
-        k_audit_large<<<uint32_t(sms), kLargeWarps * 32, large, s>>>(job, stats, spill, queue + 1,
-                                                                     huge ? spill_huge : nullptr);
-    if (huge) k_audit_huge<<<huge_blocks, kHugeWarps * 32, 0, s>>>(job, stats, spill_huge, queue + 2, huge_scratch);
+    if (big)
+        k_audit_global<LimitsGiant, kGiantWarps>
+            <<<giant->blocks, kGiantWarps * 32, 0, s>>>(job, stats, giant->spill, queue + 3, giant->scratch, nullptr);
 }
 
 void launch_verdicts(const ViewRecord* const* plan_records, const uint32_t* plan_views, const uint32_t* plan_ss,

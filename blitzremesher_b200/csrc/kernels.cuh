@@ -179,10 +179,20 @@ constexpr int kAuditTierSmall = 0, kAuditTierMedium = 1;
 // variant | kAuditSpillHeavy: warp-tier units with many changed samples go to
 // the huge tier when it runs at least one block per SM.
 constexpr int kAuditSpillHeavy = 2;
+// The giant tier (regions up to 4160 x 4160 samples) for what overflows the
+// huge tier: its spill list (1 + units words), scratch
+// (audit_giant_scratch_bytes(blocks)) and blocks.
+struct GiantTier {
+    uint32_t* spill;
+    unsigned char* scratch;
+    uint32_t blocks;
+};
+// queue: 4 words (work cursors).
 void launch_audit(const AuditJob& job, unsigned long long* stats, uint32_t* queue, uint32_t* spill,
                   uint32_t* spill_huge, unsigned char* huge_scratch, uint32_t huge_blocks, cudaStream_t s,
-                  int variant = kAuditTierSmall);
+                  int variant = kAuditTierSmall, const GiantTier* giant = nullptr);
 size_t audit_huge_scratch_bytes(uint32_t blocks);
+size_t audit_giant_scratch_bytes(uint32_t blocks);
 struct GateDev {
     GateSettings settings;
     uint32_t plan;

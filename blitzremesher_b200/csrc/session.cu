@@ -405,7 +405,7 @@ struct Session {
     Buf<uint8_t> verdict_dev;
     Buf<Measurement> meas_dev;
     Buf<blitz_collapse> collapse_dev;
-    Buf<uint32_t> exact_count, work_queue, spill, spill_huge;
+    Buf<uint32_t> exact_count, work_queue, spill, spill_huge, spill_giant;
     Buf<const ViewRecord*> record_table;
     Buf<uint32_t> plan_views, plan_ss;
     Buf<GateDev> gate_table;
@@ -806,8 +806,10 @@ struct HugeScratch {
     std::mutex lock;
     unsigned char* p = nullptr;
     uint32_t blocks = 0;
+    unsigned char* giant = nullptr; // giant tier, for rasters above 1024 x 1024
     cudaEvent_t done = nullptr;
 };
+constexpr uint32_t kGiantBlocks = 8;
 static HugeScratch& huge_scratch(int device) {
     static HugeScratch per_device[64];
     if (device < 0 || device >= 64) throw Failure(BLITZ_INVALID_ARGUMENT, "device index out of range");
@@ -816,7 +818,7 @@ static HugeScratch& huge_scratch(int device) {
 
 // Plans of rasters above 256 x 256 can hold regions beyond the large tier.
 static void run_audit(Session& S, Plan& p, uint32_t n, unsigned long long* stats, cudaStream_t st) {
-    S.work_queue.ensure(S.pool, 3);
+    S.work_queue.ensure(S.pool, 4);
     S.spill.ensure(S.pool, size_t(n) * p.views + 1);
     AuditJob job{};
     job.plan = p.dev, job.recs = S.records.p, job.out = p.records.p, job.total = uint64_t(n) * p.views;
@@ -843,7 +845,22 @@ static void run_audit(Session& S, Plan& p, uint32_t n, unsigned long long* stats
     } else {
         B200_CUDA(cudaStreamWaitEvent(st, h.done, 0));
     }
-    launch_audit(job, stats, S.work_queue.p, S.spill.p, S.spill_huge.p, h.p, h.blocks, st);
+    GiantTier giant{};
+    if (p.size > 1024) {
+        if (!h.giant) {
+            void* q = nullptr;
+            cudaError_t e = cudaMalloc(&q, audit_giant_scratch_bytes(kGiantBlocks));
+            if (e != cudaSuccess) {
+                cudaGetLastError();
+                throw Failure(BLITZ_OUT_OF_MEMORY, "giant-tier audit scratch");
+            }
+            h.giant = static_cast<unsigned char*>(q);
+        }
+        S.spill_giant.ensure(S.pool, size_t(n) * p.views + 1);
+        giant = GiantTier{S.spill_giant.p, h.giant, kGiantBlocks};
+    }
+    launch_audit(job, stats, S.work_queue.p, S.spill.p, S.spill_huge.p, h.p, h.blocks, st, kAuditTierSmall,
+                 giant.scratch ? &giant : nullptr);
     B200_CUDA(cudaEventRecord(h.done, st));
 }
 
@@ -2210,8 +2227,8 @@ struct blitz_audit_batch {
     std::vector<Buf<AuditEntry>> entries; // per plan slot
     std::vector<uint32_t> nentries;
     std::vector<uint64_t> units;
-    Buf<uint32_t> queue, spill, spill_huge, exact;
-    Buf<unsigned char> huge;
+    Buf<uint32_t> queue, spill, spill_huge, spill_giant, exact;
+    Buf<unsigned char> huge, giant;
     uint32_t huge_blocks = 0;
     int variant = kAuditTierSmall;
     bool tuned = false;
@@ -2233,6 +2250,7 @@ struct blitz_audit_batch {
         if (exec) cudaGraphExecDestroy(exec);
         if (graph) cudaGraphDestroy(graph);
         records.release(), queue.release(), spill.release(), spill_huge.release(), exact.release(), huge.release();
+        spill_giant.release(), giant.release();
         entries.clear();
         if (stream) cudaStreamDestroy(stream);
     }
@@ -2288,14 +2306,14 @@ blitz_status blitz_audit_batch_candidates(blitz_audit_batch* b, const blitz_coll
         // Plans (built or refreshed on each session's own stream) and tables.
         std::vector<AuditSetup> setup(ns);
         size_t slots = 0;
-        bool big = false;
+        bool big = false, giant = false;
         for (size_t i = 0; i < ns; ++i) {
             Session& S = b->sessions[i]->s;
             setup_audit(S, gates_in, setup[i]);
             upload_verdict_tables(S, setup[i], uint32_t(counts[i]), S.stream);
             B200_CUDA(cudaStreamSynchronize(S.stream));
             slots = std::max(slots, setup[i].plans.size());
-            for (Plan* p : setup[i].plans) big |= p->size > 256;
+            for (Plan* p : setup[i].plans) big |= p->size > 256, giant |= p->size > 1024;
         }
         b->records.ensure(b->pool, std::max<uint64_t>(1, off[ns]));
         b->entries.resize(slots);
@@ -2320,7 +2338,7 @@ blitz_status blitz_audit_batch_candidates(blitz_audit_batch* b, const blitz_coll
             b->units[j] = first;
             max_units = std::max(max_units, first);
         }
-        b->queue.ensure(b->pool, 3);
+        b->queue.ensure(b->pool, 4);
         b->spill.ensure(b->pool, max_units + 1);
         b->exact.ensure(b->pool, ns);
         if (big && !b->huge.p) {
@@ -2330,6 +2348,9 @@ blitz_status blitz_audit_batch_candidates(blitz_audit_batch* b, const blitz_coll
             b->huge = Buf<unsigned char>(b->pool, audit_huge_scratch_bytes(b->huge_blocks));
         }
         if (big) b->spill_huge.ensure(b->pool, max_units + 1);
+        if (giant && !b->giant.p) b->giant = Buf<unsigned char>(b->pool, audit_giant_scratch_bytes(kGiantBlocks));
+        if (giant) b->spill_giant.ensure(b->pool, max_units + 1);
+        const GiantTier giant_tier{b->spill_giant.p, b->giant.p, kGiantBlocks};
         B200_CUDA(cudaStreamSynchronize(st));
         // The launch sequence: per-session records, one audit job per plan
         // slot over all sessions, per-session verdicts.
@@ -2357,7 +2378,7 @@ blitz_status blitz_audit_batch_candidates(blitz_audit_batch* b, const blitz_coll
                 job.entries = b->entries[j].p, job.nentries = b->nentries[j], job.total = b->units[j];
                 launch_audit(job, profile ? b->stats.p : nullptr, b->queue.p, b->spill.p,
                              big ? b->spill_huge.p : nullptr, big ? b->huge.p : nullptr, big ? b->huge_blocks : 0,
-                             st, variant);
+                             st, variant, giant ? &giant_tier : nullptr);
             }
             if (profile) cudaEventRecord(b->ev[1], st);
             cudaMemsetAsync(b->exact.p, 0, 4 * ns, st);
@@ -2408,7 +2429,8 @@ blitz_status blitz_audit_batch_candidates(blitz_audit_batch* b, const blitz_coll
         }
         for (auto& e : b->entries) put(&e.p, sizeof(void*));
         for (const void* q : {(const void*)b->records.p, (const void*)b->queue.p, (const void*)b->spill.p,
-                              (const void*)b->spill_huge.p, (const void*)b->huge.p, (const void*)b->exact.p})
+                              (const void*)b->spill_huge.p, (const void*)b->huge.p, (const void*)b->exact.p,
+                              (const void*)b->spill_giant.p, (const void*)b->giant.p})
             put(&q, sizeof(q));
         if ((flags & 1u) && off[ns]) {
             if (b->exec && sig == b->signature) {

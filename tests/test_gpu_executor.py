@@ -136,3 +136,26 @@ def test_huge_regions_match_oracle(gpu_lib, oracle):
         stop = 4 if want.failed_gate == 0 else (want.failed_gate if want.failed_gate <= 4 else 0)
         for g in range(stop):
             assert measurement_fields(meas[i, g]) == measurement_fields(want.gates[g]), (i, g)
+
+
+def test_giant_regions_match_oracle(gpu_lib, oracle):
+    """An 80-face sphere at 256 px x ss 8 (2112 x 2112 samples): 1-ring
+    regions beyond 1024 samples go to the giant tier; verdicts and gate
+    Measurements equal the oracle's."""
+    mesh = syn.noisy_icosphere(1, 7)
+    views = (4, 0, 93)
+    args = _gates(256.0, views, 8)
+    with br.AuditSession(mesh) as s:
+        cands = br.midpoint_collapses(s.actions())
+        picks = cands[:: max(1, cands.size // 10)]
+        verdicts, meas = s.candidates(picks, [br.eval_settings(*a) for a in args], measurements=True)
+    assert np.mean(verdicts["exact_path"]) < 0.25
+    b = oracle.bounds(mesh)
+    for i, c in enumerate(picks):
+        e = BoEdit()
+        e.from_, e.to = int(c["from"]), int(c["to"])
+        want = oracle.audit_candidate(mesh, e, mesh, mesh, b, [oracle_settings(*a) for a in args])
+        assert verdicts[i]["accepted"] == want.accepted and verdicts[i]["failed_gate"] == want.failed_gate, i
+        stop = 4 if want.failed_gate == 0 else (want.failed_gate if want.failed_gate <= 4 else 0)
+        for g in range(stop):
+            assert measurement_fields(meas[i, g]) == measurement_fields(want.gates[g]), (i, g)
