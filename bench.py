@@ -594,6 +594,43 @@ def run_batched(args, rank: int, world: int, local: int) -> dict:
     return line
 
 
+ROCK_CHAIN = {"levels": 6, "base": 240.0, "last": 7.5, "curve": ((0.0, 1.0), (1.0, 3.0)), "lod0": 2.0,
+              "views": 32, "ss": 8, "batch": 64, "budget": 300}
+
+
+def run_rock_chain(args, local: int) -> dict:
+    """Multi-level LOD chain of a ridged-noise rock (81,920 faces, 8 UV charts):
+    6 levels scheduled 240 -> 7.5 px (the 1024 -> 32 px ratio of the 1M-face
+    configuration), transition 1 -> 3 px, LOD0 bound 2 px, 32 ortho views at
+    ss 8, batches of 64, 300 trials per level, each level confirmed."""
+    import torch
+
+    import blitzremesher_b200 as br
+    from blitzremesher_b200 import synthetic as syn
+
+    c = ROCK_CHAIN
+    mesh = syn.rock(6, 3)
+    session = br.AuditSession(mesh, br.neural_options(device=local, preserve_uv=0))
+    settings = br.chain_settings(c["levels"], c["base"], c["last"], c["curve"], c["lod0"], (c["views"], 0, 0xB1172024),
+                                 (c["views"], 0, 0xB1172026), c["ss"], c["ss"], c["ss"], 1.0, c["batch"], 0,
+                                 c["budget"], 1)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    levels, _ = session.chain(settings, meshes=False)
+    torch.cuda.synchronize()
+    seconds = time.perf_counter() - t0
+    session.close()
+    return {"metric": "LOD-chain s/mesh", "seconds": seconds, "unit": "s/mesh",
+            "mesh": f"rock: icosphere level 6 ({mesh.face_count} faces), 6-octave ridged noise, 8 UV charts "
+                    "(uv not preserved)",
+            "schedule": c, "levels": [{k: (round(v, 4) if isinstance(v, float) else v) for k, v in l.items()
+                                       if k not in ("source_audit", "transition_audit")}
+                                      | {"source_error": l["source_audit"].error,
+                                         "transition_error": l["transition_audit"].error} for l in levels],
+            "all_confirmed": all(l["confirmed"] for l in levels),
+            "timing": "wall clock around blitz_audit_chain (executor, previous-level binding, confirmation)"}
+
+
 def run_gpu(args) -> None:
     import torch
 
@@ -609,6 +646,8 @@ def run_gpu(args) -> None:
     torch.cuda.set_device(local)
     if args.config == "batched":
         line = run_batched(args, rank, world, local)
+        if not args.no_rock:
+            line["lod_chain_rock"] = run_rock_chain(args, local)
         if not args.no_icosphere:
             ico = run_icosphere(args, rank, world, local)
             for k in ("metric", "n_gpus", "steps", "warmup", "higher_is_better", "scaling", "vs_baseline", "data"):
@@ -636,6 +675,7 @@ def main() -> None:
     ap.add_argument("--no-surrogate", action="store_true")
     ap.add_argument("--config", default="batched", choices=["batched", "icosphere"])
     ap.add_argument("--no-icosphere", action="store_true")
+    ap.add_argument("--no-rock", action="store_true")
     ap.add_argument("--meshes", type=int, default=BATCH_MESHES, help="meshes of the batched set (64 = the workload)")
     args = ap.parse_args()
     if args.impl == "reference":

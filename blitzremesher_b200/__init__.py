@@ -148,6 +148,9 @@ EXPORTS = {
     "blitz_audit_surrogate_features": ([C.c_void_p, C.c_double, C.c_double, C.c_void_p, C.c_void_p, C.c_size_t,
                                         C.POINTER(C.c_size_t), C.c_char_p, C.c_size_t], C.c_int),
     "blitz_audit_attach_surrogate": ([C.c_void_p, C.c_void_p, C.c_char_p, C.c_size_t], C.c_int),
+    "blitz_chain_settings_init": ([C.c_void_p], None),
+    "blitz_audit_chain": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p, C.c_void_p, C.c_char_p,
+                           C.c_size_t], C.c_int),
     "blitz_audit_batch_create": ([C.c_void_p, C.c_size_t, C.c_void_p, C.c_char_p, C.c_size_t], C.c_int),
     "blitz_audit_batch_destroy": ([C.c_void_p], None),
     "blitz_audit_batch_candidates": ([C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(EvalSettings), C.c_void_p,
@@ -169,6 +172,48 @@ class Execution(C.Structure):
 class ExecuteOptions(C.Structure):
     _fields_ = [("struct_size", C.c_uint32), ("batch", C.c_uint32), ("keep_permille", C.c_uint32),
                 ("reserved", C.c_uint32 * 5)]
+
+
+class ChainSettings(C.Structure):
+    _fields_ = [("struct_size", C.c_uint32), ("levels", C.c_uint32), ("base_pixels", C.c_double),
+                ("last_pixels", C.c_double), ("max_lod0_delta_px", C.c_double), ("transition_curve", C.c_float * 16),
+                ("transition_points", C.c_uint32), ("search_orthographic", C.c_uint16),
+                ("search_perspective", C.c_uint16), ("search_seed", C.c_uint32), ("audit_orthographic", C.c_uint16),
+                ("audit_perspective", C.c_uint16), ("audit_seed", C.c_uint32), ("search_supersample", C.c_uint8),
+                ("audit_supersample", C.c_uint8), ("max_supersample", C.c_uint8), ("force_two_sided", C.c_uint8),
+                ("max_changed_area", C.c_double), ("batch", C.c_uint32), ("keep_permille", C.c_uint32),
+                ("trial_budget", C.c_uint32), ("min_faces", C.c_uint32), ("reserved", C.c_uint32 * 4)]
+
+
+class ChainLevel(C.Structure):
+    _fields_ = [("struct_size", C.c_uint32), ("level", C.c_uint32), ("pixels", C.c_double),
+                ("transition", C.c_double), ("source_bound", C.c_double), ("faces", C.c_uint32),
+                ("commits", C.c_uint32), ("trials", C.c_uint32), ("stop_reason", C.c_uint8),
+                ("confirmed", C.c_uint8), ("reserved", C.c_uint8 * 2), ("source_audit", Measurement),
+                ("transition_audit", Measurement), ("seconds", C.c_double)]
+
+
+CHAIN_EMIT = C.CFUNCTYPE(None, C.c_void_p, C.c_uint32, C.POINTER(C.c_uint32), C.c_uint32, C.POINTER(C.c_float),
+                         C.c_uint32)
+
+
+def chain_settings(levels: int, base_pixels: float, last_pixels: float, curve=((0.0, 1.0),),
+                   max_lod0_delta_px: float = 2.0, search_views=(42, 12, 0xB1172024), audit_views=(642, 64, 0xB1172026),
+                   search_supersample: int = 4, audit_supersample: int = 8, max_supersample: int = 32,
+                   max_changed_area: float = 1.0, batch: int = 64, keep_permille: int = 0,
+                   trial_budget: int = 1 << 30, min_faces: int = 1) -> ChainSettings:
+    c = ChainSettings()
+    load().blitz_chain_settings_init(C.byref(c))
+    c.levels, c.base_pixels, c.last_pixels, c.max_lod0_delta_px = levels, base_pixels, last_pixels, max_lod0_delta_px
+    for i, (x, y) in enumerate(curve):
+        c.transition_curve[2 * i], c.transition_curve[2 * i + 1] = x, y
+    c.transition_points = len(curve)
+    c.search_orthographic, c.search_perspective, c.search_seed = search_views
+    c.audit_orthographic, c.audit_perspective, c.audit_seed = audit_views
+    c.search_supersample, c.audit_supersample, c.max_supersample = search_supersample, audit_supersample, max_supersample
+    c.max_changed_area, c.batch, c.keep_permille = max_changed_area, batch, keep_permille
+    c.trial_budget, c.min_faces = trial_budget, min_faces
+    return c
 
 
 class BatchInfo(C.Structure):
@@ -383,6 +428,29 @@ class AuditSession:
         return {"commits": commits[: 2 * n].reshape(-1, 2).copy(), "trials": out.trials,
                 "final_faces": out.final_faces, "audited": out.audited, "stop": out.stop_reason,
                 "fallbacks": out.fallbacks}
+
+    def chain(self, settings: ChainSettings, meshes: bool = True):
+        """LOD chain from the source (blitz_audit_chain): per-level records and,
+        with `meshes`, each level's (indices, positions)."""
+        out = (ChainLevel * (settings.levels - 1))()
+        emitted = []
+
+        def on_level(user, level, idx, faces, pos, nv):
+            emitted.append((np.ctypeslib.as_array(idx, shape=(faces * 3,)).copy(),
+                            np.ctypeslib.as_array(pos, shape=(nv * 3,)).reshape(-1, 3).copy()))
+
+        cb = CHAIN_EMIT(on_level) if meshes else None
+        err = C.create_string_buffer(512)
+        _check(self.lib.blitz_audit_chain(self.handle, C.byref(settings), out, len(out),
+                                          C.cast(cb, C.c_void_p) if cb else None, None, err, 512), err)
+        levels = []
+        for l in out:
+            d = {k: getattr(l, k) for k, _ in l._fields_ if k not in ("struct_size", "reserved", "source_audit",
+                                                                      "transition_audit")}
+            d["source_audit"] = l.source_audit
+            d["transition_audit"] = l.transition_audit
+            levels.append(d)
+        return levels, emitted
 
     def surrogate_features(self, screen: float, screen2: float):
         """Features (torch CUDA tensor n x 48) of the current state's legal

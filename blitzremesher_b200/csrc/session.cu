@@ -2484,3 +2484,158 @@ blitz_status blitz_audit_batch_read_info(const blitz_audit_batch* b, blitz_audit
     out->changed_samples = b->prof[2];
     return BLITZ_OK;
 }
+
+// ---------------------------------------------------------------------------
+// LOD chain: schedule, per-level executor and confirmation.
+namespace {
+// Curve::at (chain.cpp:25-36).
+double curve_at(const blitz_chain_settings& c, double t) {
+    const float* xy = c.transition_curve;
+    const uint32_t n = c.transition_points;
+    if (t <= xy[0]) return xy[1];
+    for (uint32_t i = 1; i < n; ++i)
+        if (t <= xy[2 * i]) {
+            const double u = (t - xy[2 * i - 2]) / (double(xy[2 * i]) - xy[2 * i - 2]);
+            return xy[2 * i - 1] * (1 - u) + xy[2 * i + 1] * u;
+        }
+    return xy[2 * n - 1];
+}
+blitz_eval_settings chain_gate(const blitz_chain_settings& c, double pixels, double limit, bool audit) {
+    blitz_eval_settings e;
+    std::memset(&e, 0, sizeof e);
+    e.struct_size = sizeof e;
+    e.profile = 0;
+    e.supersample = audit ? c.audit_supersample : c.search_supersample;
+    e.max_supersample = c.max_supersample;
+    e.force_two_sided = c.force_two_sided;
+    e.conservative_screen = 0;
+    e.views_orthographic = audit ? c.audit_orthographic : c.search_orthographic;
+    e.views_perspective = audit ? c.audit_perspective : c.search_perspective;
+    e.views_seed = audit ? c.audit_seed : c.search_seed;
+    e.screen_size = pixels;
+    e.limit = limit;
+    e.max_changed_area = audit ? c.max_changed_area : 1.0;
+    return e;
+}
+} // namespace
+
+void blitz_chain_settings_init(blitz_chain_settings* c) {
+    if (!c) return;
+    std::memset(c, 0, sizeof(*c));
+    c->struct_size = sizeof(*c);
+    c->levels = 2;
+    c->base_pixels = c->last_pixels = 24;
+    c->max_lod0_delta_px = 2;
+    c->transition_curve[0] = 0, c->transition_curve[1] = 1;
+    c->transition_points = 1;
+    c->search_orthographic = 42, c->search_perspective = 12, c->search_seed = 0xB1172024u;
+    c->audit_orthographic = 642, c->audit_perspective = 64, c->audit_seed = 0xB1172026u;
+    c->search_supersample = 4, c->audit_supersample = 8, c->max_supersample = 32;
+    c->max_changed_area = 1.0;
+    c->batch = 64;
+    c->trial_budget = 1u << 30;
+    c->min_faces = 1;
+}
+
+blitz_status blitz_audit_chain(blitz_audit_session* s, const blitz_chain_settings* c, blitz_chain_level* out,
+                               size_t capacity, blitz_chain_emit emit, void* user, char* error, size_t cap) {
+    return guarded(error, cap, [&] {
+        if (!s || !c || c->struct_size != sizeof(*c)) throw Failure(BLITZ_INVALID_ARGUMENT, "bad chain settings");
+        if (c->levels < 2 || c->levels > 32) throw Failure(BLITZ_INVALID_ARGUMENT, "level count must be 2..32");
+        if (!(c->base_pixels >= c->last_pixels) || !(c->last_pixels > 0) || c->base_pixels > 16384)
+            throw Failure(BLITZ_INVALID_ARGUMENT, "base pixels must be >= last pixels and <= 16384");
+        if (c->transition_points < 1 || c->transition_points > 8)
+            throw Failure(BLITZ_INVALID_ARGUMENT, "transition curve needs 1..8 points");
+        if (c->batch < 1 || c->batch > 64) throw Failure(BLITZ_INVALID_ARGUMENT, "action batch outside 1..64");
+        if (out && capacity < c->levels - 1) throw Failure(BLITZ_INVALID_ARGUMENT, "level output too small");
+        Session& S = s->s;
+        DeviceScope scope(S.device);
+        if (c->keep_permille && !S.surrogate) throw Failure(BLITZ_INVALID_ARGUMENT, "no surrogate attached");
+        if (S.options.preserve_uv && !S.source_h.uv.empty())
+            throw Failure(BLITZ_UNAVAILABLE, "uv transport on the candidate path is not implemented");
+        reset_state(S);
+        auto bind_previous_source = [&] {
+            S.previous_is_source = true;
+            S.previous = DeviceMesh{};
+            S.previous_h = HostMesh{};
+            for (auto it = S.plans.begin(); it != S.plans.end();)
+                it = it->first.reference == 1 ? S.plans.erase(it) : std::next(it);
+        };
+        bind_previous_source();
+        double prev_pixels = c->base_pixels, cumulative = 0;
+        std::vector<uint32_t> idx;
+        std::vector<float> pos;
+        for (uint32_t level = 1; level < c->levels; ++level) {
+            const uint64_t t0 = now_ns();
+            // schedule (chain.cpp:101-118)
+            const double pixels =
+                c->base_pixels * std::pow(c->last_pixels / c->base_pixels, double(level) / (c->levels - 1));
+            const double delta = curve_at(*c, c->levels == 2 ? 0 : double(level - 1) / (c->levels - 2));
+            cumulative = cumulative * pixels / prev_pixels + delta;
+            const double bound = c->max_lod0_delta_px > 0 ? std::min(cumulative, c->max_lod0_delta_px) : cumulative;
+            prev_pixels = pixels;
+            blitz_eval_settings gates[4] = {chain_gate(*c, pixels, bound, false), chain_gate(*c, pixels, delta, false),
+                                            chain_gate(*c, pixels, bound, true), chain_gate(*c, pixels, delta, true)};
+            for (int g = 0; g < 4; ++g) gate_of(&gates[g], S.bounds);
+            // previous level = the state now (the source for level 1)
+            if (level >= 2) {
+                HostMesh h;
+                const DevMesh& m = S.state.view;
+                h.idx.resize(size_t(S.state_faces) * 3);
+                h.pos.resize(size_t(m.nv) * 3);
+                B200_CUDA(cudaMemcpyAsync(h.idx.data(), m.idx, h.idx.size() * 4, cudaMemcpyDeviceToHost, S.stream));
+                B200_CUDA(cudaMemcpyAsync(h.pos.data(), m.pos, h.pos.size() * 4, cudaMemcpyDeviceToHost, S.stream));
+                if (m.mat) {
+                    h.mat.resize(S.state_faces);
+                    B200_CUDA(cudaMemcpyAsync(h.mat.data(), m.mat, h.mat.size() * 2, cudaMemcpyDeviceToHost, S.stream));
+                }
+                h.sided = S.source_h.sided;
+                B200_CUDA(cudaStreamSynchronize(S.stream));
+                S.previous_h = std::move(h);
+                S.previous.upload(S.pool, S.previous_h, S.stream);
+                S.previous_is_source = false;
+                for (auto it = S.plans.begin(); it != S.plans.end();)
+                    it = it->first.reference == 1 ? S.plans.erase(it) : std::next(it);
+            }
+            blitz_audit_execution r{};
+            r.struct_size = sizeof(r);
+            if (c->batch == 1 && !c->keep_permille)
+                execute(S, c->min_faces, c->trial_budget, gates, nullptr, 0, r);
+            else
+                execute_batched(S, c->min_faces, c->trial_budget, gates, c->batch, c->keep_permille, nullptr, 0, r);
+            // confirmation at the audit views (generate.cpp:456-562)
+            GateRef refs[4];
+            PlanKey keys[4];
+            resolve_gates(S, gates, refs, keys);
+            DevMesh state = S.state.view;
+            state.nf = S.state_faces;
+            const DevMesh& prev = S.previous_is_source ? S.source.view : S.previous.view;
+            const Measurement ms = evaluate_full(S, S.source.view, state, &gates[2], refs[2].g);
+            const Measurement mt = evaluate_full(S, prev, state, &gates[3], refs[3].g);
+            B200_CUDA(cudaStreamSynchronize(S.stream));
+            if (out) {
+                blitz_chain_level& l = out[level - 1];
+                std::memset(&l, 0, sizeof l);
+                l.struct_size = sizeof l;
+                l.level = level;
+                l.pixels = pixels, l.transition = delta, l.source_bound = bound;
+                l.faces = S.state_faces, l.commits = r.commits, l.trials = r.trials;
+                l.stop_reason = r.stop_reason;
+                l.confirmed = measurement_accepted(ms) && measurement_accepted(mt);
+                std::memcpy(&l.source_audit, &ms, sizeof ms);
+                std::memcpy(&l.transition_audit, &mt, sizeof mt);
+                l.seconds = double(now_ns() - t0) * 1e-9;
+            }
+            if (emit) {
+                const DevMesh& m = S.state.view;
+                idx.resize(size_t(S.state_faces) * 3);
+                pos.resize(size_t(m.nv) * 3);
+                B200_CUDA(cudaMemcpyAsync(idx.data(), m.idx, idx.size() * 4, cudaMemcpyDeviceToHost, S.stream));
+                B200_CUDA(cudaMemcpyAsync(pos.data(), m.pos, pos.size() * 4, cudaMemcpyDeviceToHost, S.stream));
+                B200_CUDA(cudaStreamSynchronize(S.stream));
+                emit(user, level, idx.data(), S.state_faces, pos.data(), m.nv);
+            }
+        }
+        bind_previous_source();
+    });
+}

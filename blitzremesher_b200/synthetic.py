@@ -326,3 +326,36 @@ def batched_set(count: int = 64, seed: int = 2, lo: int = 2000, hi: int = 200000
         else:
             meshes.append(seamed_heightfield(faces, s, charts))
     return meshes
+
+
+def ridged_noise(p: np.ndarray, seed: int, octaves: int = 6, frequency: float = 1.5) -> np.ndarray:
+    """Ridged multifractal sum: per octave (1 - |n|)^2 of value noise, amplitude
+    halving and frequency doubling, normalised to [0, 1]."""
+    total = np.zeros(p.shape[0])
+    amp, norm = 1.0, 0.0
+    for o in range(octaves):
+        n = value_noise(p * (2 ** o), seed + 104729 * o, octaves=1, frequency=frequency)
+        total += amp * (1.0 - np.abs(n)) ** 2
+        norm += amp
+        amp *= 0.5
+    return total / norm
+
+
+def rock(level: int, seed: int = 3, relief: float = 0.25) -> Mesh:
+    """A rock: icosphere (20 * 4^level faces) displaced radially by 6-octave
+    ridged noise, with FP32 UVs on 8 charts (one per octant of the face
+    centroid; vertices shared across charts are duplicated)."""
+    p, f = icosphere(level)
+    r = 1.0 + relief * (ridged_noise(p, seed) - 0.5)
+    pos = (p * r[:, None]).astype(np.float32)
+    cent = p[f].mean(1)
+    chart = (cent[:, 0] > 0).astype(np.int64) | ((cent[:, 1] > 0) << 1) | ((cent[:, 2] > 0) << 2)
+    key = f * 8 + chart[:, None]
+    uniq, inv = np.unique(key.reshape(-1), return_inverse=True)
+    slot_vertex, slot_chart = uniq // 8, uniq % 8
+    d = p[slot_vertex]
+    u = (np.arctan2(d[:, 1], d[:, 0]) / (2 * np.pi) + 0.5) * 0.24 + 0.25 * (slot_chart % 4)
+    v = (np.arcsin(np.clip(d[:, 2], -1, 1)) / np.pi + 0.5) * 0.49 + 0.5 * (slot_chart // 4)
+    faces = inv.reshape(-1, 3).astype(np.uint32)
+    return Mesh(pos[slot_vertex], faces.reshape(-1), uv=np.stack([u, v], 1).astype(np.float32),
+                name=f"rock{level}-seed{seed}", meta={"kind": "rock", "level": level, "charts": 8, "seed": seed})

@@ -351,6 +351,57 @@ blitz_status blitz_audit_batch_candidates(blitz_audit_batch*, const blitz_collap
                                           char* error, size_t error_capacity);
 blitz_status blitz_audit_batch_read_info(const blitz_audit_batch*, blitz_audit_batch_info* out);
 
+/* ---- LOD chain -------------------------------------------------------------
+ * Levels 1..levels-1 from the source: per level the schedule of chain.cpp
+ * (schedule 101-118, Curve::at 25-36: pixels S_i = base (last/base)^(i/(levels-1)),
+ * transition d_i from the curve, LOD0 bound B_i = min(B_{i-1} S_i/S_{i-1} + d_i,
+ * max_lod0_delta_px)), the four gates of eval_config (179-199: search views and
+ * max_changed_area 1, audit views and max_changed_area), the previous level
+ * bound as the adjacent reference, the executor (blitz_audit_execute_ex) down
+ * to `min_faces`, then the confirmation of the emitted level at the audit
+ * views against the source (B_i) and the previous level (d_i)
+ * (generate.cpp:456-562, hooks.confirm). The session's state ends as the last
+ * level. */
+typedef struct blitz_chain_settings {
+    uint32_t struct_size;
+    uint32_t levels;               /* 2..32, LOD0 included */
+    double base_pixels;            /* S_0 */
+    double last_pixels;            /* S_{levels-1} */
+    double max_lod0_delta_px;      /* 0: no cap */
+    float transition_curve[16];    /* (x, y) pairs, x ascending */
+    uint32_t transition_points;    /* 1..8 */
+    uint16_t search_orthographic, search_perspective;
+    uint32_t search_seed;
+    uint16_t audit_orthographic, audit_perspective;
+    uint32_t audit_seed;
+    uint8_t search_supersample, audit_supersample, max_supersample, force_two_sided;
+    double max_changed_area;       /* audit gates; search gates use 1 */
+    uint32_t batch;                /* 1..64 */
+    uint32_t keep_permille;        /* surrogate pruning (attached model), 0 off */
+    uint32_t trial_budget;         /* per level */
+    uint32_t min_faces;            /* per-level target faces (1: as far as the gates allow) */
+    uint32_t reserved[4];
+} blitz_chain_settings;
+void blitz_chain_settings_init(blitz_chain_settings*);
+typedef struct blitz_chain_level {
+    uint32_t struct_size;
+    uint32_t level;
+    double pixels, transition, source_bound;
+    uint32_t faces, commits, trials;
+    uint8_t stop_reason;           /* as blitz_audit_execution */
+    uint8_t confirmed;             /* both confirmation audits passed */
+    uint8_t reserved[2];
+    blitz_measurement source_audit, transition_audit;
+    double seconds;                /* executor + confirmation */
+} blitz_chain_level;
+/* Called once per level with the level's compacted indices and every vertex
+ * slot's position (host memory valid during the call). */
+typedef void (*blitz_chain_emit)(void* user, uint32_t level, const uint32_t* indices, uint32_t face_count,
+                                 const float* positions, uint32_t vertex_count);
+blitz_status blitz_audit_chain(blitz_audit_session*, const blitz_chain_settings* settings,
+                               blitz_chain_level* levels, size_t capacity, blitz_chain_emit emit, void* user,
+                               char* error, size_t error_capacity);
+
 /* Current state: compacted indices (3 per face) and every vertex slot's position. */
 blitz_status blitz_audit_state(blitz_audit_session*, uint32_t* indices, size_t index_capacity, float* positions,
                                size_t position_capacity, uint32_t* face_count, char* error, size_t error_capacity);

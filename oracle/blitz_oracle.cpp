@@ -1132,14 +1132,28 @@ int bo_execute_batched(const bo_mesh* source, const bo_mesh* previous, uint32_t 
                        const bo_eval_settings gates[4], int preserve_uv, uint32_t batch,
                        uint32_t* commits_from_to, uint32_t capacity, uint32_t* commits, uint32_t* trials,
                        uint32_t* out_indices, uint32_t* out_faces, float* out_positions, uint8_t* stop) {
+    return bo_execute_from(source, previous, nullptr, target, budget, gates, preserve_uv, batch, commits_from_to,
+                           capacity, commits, trials, out_indices, out_faces, out_positions, stop);
+}
+
+// The same walk starting from `start` (a later state of `source`: same vertex
+// slots, fewer faces) instead of from the source itself; the geometric
+// classes stay those welded on the source (a chain's levels continue one
+// state, generate.cpp:456-562).
+int bo_execute_from(const bo_mesh* source, const bo_mesh* previous, const bo_mesh* start, uint32_t target,
+                    uint32_t budget, const bo_eval_settings gates[4], int preserve_uv, uint32_t batch,
+                    uint32_t* commits_from_to, uint32_t capacity, uint32_t* commits, uint32_t* trials,
+                    uint32_t* out_indices, uint32_t* out_faces, float* out_positions, uint8_t* stop) {
     if (!batch || batch > 64) return 1;
+    if (start && start->vertex_count != source->vertex_count) return 1;
     return guarded([&] {
         ExecState st;
-        st.pos.assign(source->positions, source->positions + size_t(source->vertex_count) * 3);
-        st.idx.assign(source->indices, source->indices + size_t(source->face_count) * 3);
-        if (source->materials) st.mat.assign(source->materials, source->materials + source->face_count);
+        const bo_mesh& from = start ? *start : *source;
+        st.pos.assign(from.positions, from.positions + size_t(from.vertex_count) * 3);
+        st.idx.assign(from.indices, from.indices + size_t(from.face_count) * 3);
+        if (from.materials) st.mat.assign(from.materials, from.materials + from.face_count);
         if (source->double_sided) st.sided.assign(source->double_sided, source->double_sided + source->double_sided_count);
-        if (source->uv) st.uv.assign(source->uv, source->uv + size_t(source->vertex_count) * 2);
+        if (from.uv) st.uv.assign(from.uv, from.uv + size_t(from.vertex_count) * 2);
         bo_bounds b{};
         bo_bounds_of(source, &b);
         const double diameter = std::max(1e-20, b.radius * 2);

@@ -143,25 +143,29 @@ class Oracle:
         assert self.lib.bo_bounds_of(C.byref(h.c), C.byref(b)) == 0
         return b
 
-    def execute(self, source, target: int, budget: int, gates, previous=None, preserve_uv=True, batch=1) -> dict:
+    def execute(self, source, target: int, budget: int, gates, previous=None, preserve_uv=True, batch=1,
+                start=None) -> dict:
         """Greedy executor (ShortestEdge, midpoint placement), batches of up to
-        `batch` independent collapses audited as one trial."""
+        `batch` independent collapses audited as one trial, from `start` (a
+        later state of `source`; default the source)."""
         L = self.lib
         P = C.POINTER
-        L.bo_execute_batched.argtypes = [P(BoMesh), P(BoMesh), C.c_uint32, C.c_uint32, P(BoEvalSettings), C.c_int,
-                                         C.c_uint32, C.c_void_p, C.c_uint32, P(C.c_uint32), P(C.c_uint32),
-                                         C.c_void_p, P(C.c_uint32), C.c_void_p, P(C.c_uint8)]
+        L.bo_execute_from.argtypes = [P(BoMesh), P(BoMesh), P(BoMesh), C.c_uint32, C.c_uint32, P(BoEvalSettings),
+                                      C.c_int, C.c_uint32, C.c_void_p, C.c_uint32, P(C.c_uint32),
+                                      P(C.c_uint32), C.c_void_p, P(C.c_uint32), C.c_void_p, P(C.c_uint8)]
         hs = _MeshHold(source)
         hp = None if previous is None else _MeshHold(previous)
+        hst = None if start is None else _MeshHold(start)
         cap = source.face_count
         ft = np.zeros(2 * cap, np.uint32)
         idx = np.zeros(source.face_count * 3, np.uint32)
         pos = np.zeros((source.vertex_count, 3), np.float32)
         commits, trials, faces, stop = C.c_uint32(), C.c_uint32(), C.c_uint32(), C.c_uint8()
         g = (BoEvalSettings * 4)(*gates)
-        st = L.bo_execute_batched(C.byref(hs.c), None if hp is None else C.byref(hp.c), target, budget, g,
-                                  int(preserve_uv), batch, ft.ctypes.data, cap, C.byref(commits), C.byref(trials),
-                                  idx.ctypes.data, C.byref(faces), pos.ctypes.data, C.byref(stop))
+        st = L.bo_execute_from(C.byref(hs.c), None if hp is None else C.byref(hp.c),
+                               None if hst is None else C.byref(hst.c), target, budget, g, int(preserve_uv), batch,
+                               ft.ctypes.data, cap, C.byref(commits), C.byref(trials), idx.ctypes.data,
+                               C.byref(faces), pos.ctypes.data, C.byref(stop))
         assert st == 0
         n = commits.value
         return {"commits": ft[: 2 * n].reshape(-1, 2), "trials": trials.value, "stop": stop.value,

@@ -159,3 +159,35 @@ def test_giant_regions_match_oracle(gpu_lib, oracle):
         stop = 4 if want.failed_gate == 0 else (want.failed_gate if want.failed_gate <= 4 else 0)
         for g in range(stop):
             assert measurement_fields(meas[i, g]) == measurement_fields(want.gates[g]), (i, g)
+
+
+def _oracle_chain(oracle, mesh, levels, base, last, curve, lod0, search, audit, ss, batch, budget):
+    p, t, b = oracle.schedule(base, last, levels, [v for xy in curve for v in xy], lod0)
+    state, prev, out = None, None, []
+    for i in range(1, levels):
+        gates = [oracle_settings(p[i], b[i], search, ss, ss, 1.0), oracle_settings(p[i], t[i], search, ss, ss, 1.0),
+                 oracle_settings(p[i], b[i], audit, ss, ss, 1.0), oracle_settings(p[i], t[i], audit, ss, ss, 1.0)]
+        r = oracle.execute(mesh, 1, budget, gates, previous=prev, batch=batch, start=state)
+        state = syn.Mesh(r["positions"], r["indices"])
+        prev = state
+        out.append(r)
+    return out
+
+
+@pytest.mark.parametrize("batch", [1, 8])
+def test_chain_matches_oracle(gpu_lib, oracle, batch):
+    """A 4-level chain (48 -> 12 px, transition 1 -> 3 px, LOD0 bound capped at
+    2 px): each level's executor against the bound previous level, then the
+    confirmation; every emitted level equals the oracle chain's."""
+    mesh = syn.noisy_icosphere(3, 21)
+    curve, search, audit = ((0.0, 1.0), (1.0, 3.0)), (6, 0, 5), (8, 0, 7)
+    want = _oracle_chain(oracle, mesh, 4, 48.0, 12.0, curve, 2.0, search, audit, 4, batch, 120)
+    settings = br.chain_settings(4, 48.0, 12.0, curve, 2.0, search, audit, 4, 4, 4, 1.0, batch, 0, 120, 1)
+    with br.AuditSession(mesh) as s:
+        levels, meshes = s.chain(settings)
+    assert len(levels) == 3 and len(meshes) == 3
+    for lv, (idx, pos), w in zip(levels, meshes, want):
+        assert lv["trials"] == w["trials"] and lv["stop_reason"] == w["stop"]
+        assert np.array_equal(idx, w["indices"]) and np.array_equal(pos, w["positions"])
+        assert lv["confirmed"] == 1
+    assert levels[-1]["faces"] < levels[0]["faces"] < mesh.face_count
