@@ -171,7 +171,7 @@ class Execution(C.Structure):
 
 class ExecuteOptions(C.Structure):
     _fields_ = [("struct_size", C.c_uint32), ("batch", C.c_uint32), ("keep_permille", C.c_uint32),
-                ("reserved", C.c_uint32 * 5)]
+                ("ranking", C.c_uint32), ("reserved", C.c_uint32 * 4)]
 
 
 class ChainSettings(C.Structure):
@@ -182,7 +182,8 @@ class ChainSettings(C.Structure):
                 ("audit_perspective", C.c_uint16), ("audit_seed", C.c_uint32), ("search_supersample", C.c_uint8),
                 ("audit_supersample", C.c_uint8), ("max_supersample", C.c_uint8), ("force_two_sided", C.c_uint8),
                 ("max_changed_area", C.c_double), ("batch", C.c_uint32), ("keep_permille", C.c_uint32),
-                ("trial_budget", C.c_uint32), ("min_faces", C.c_uint32), ("reserved", C.c_uint32 * 4)]
+                ("trial_budget", C.c_uint32), ("min_faces", C.c_uint32), ("ranking", C.c_uint32),
+                ("reserved", C.c_uint32 * 3)]
 
 
 class ChainLevel(C.Structure):
@@ -201,7 +202,7 @@ def chain_settings(levels: int, base_pixels: float, last_pixels: float, curve=((
                    max_lod0_delta_px: float = 2.0, search_views=(42, 12, 0xB1172024), audit_views=(642, 64, 0xB1172026),
                    search_supersample: int = 4, audit_supersample: int = 8, max_supersample: int = 32,
                    max_changed_area: float = 1.0, batch: int = 64, keep_permille: int = 0,
-                   trial_budget: int = 1 << 30, min_faces: int = 1) -> ChainSettings:
+                   trial_budget: int = 1 << 30, min_faces: int = 1, ranking: int = 3) -> ChainSettings:
     c = ChainSettings()
     load().blitz_chain_settings_init(C.byref(c))
     c.levels, c.base_pixels, c.last_pixels, c.max_lod0_delta_px = levels, base_pixels, last_pixels, max_lod0_delta_px
@@ -212,7 +213,7 @@ def chain_settings(levels: int, base_pixels: float, last_pixels: float, curve=((
     c.audit_orthographic, c.audit_perspective, c.audit_seed = audit_views
     c.search_supersample, c.audit_supersample, c.max_supersample = search_supersample, audit_supersample, max_supersample
     c.max_changed_area, c.batch, c.keep_permille = max_changed_area, batch, keep_permille
-    c.trial_budget, c.min_faces = trial_budget, min_faces
+    c.trial_budget, c.min_faces, c.ranking = trial_budget, min_faces, ranking
     return c
 
 
@@ -404,7 +405,7 @@ class AuditSession:
                                                       measurements_ptr or None, stream or None, err, 512), err)
 
     def execute(self, target_faces: int, trial_budget: int, gates: Sequence[EvalSettings], batch: int = 1,
-                keep_permille: int = 0) -> dict:
+                keep_permille: int = 0, ranking: int = 3) -> dict:
         """Greedy LOD step on the current state (ShortestEdge ranking), with
         batches of up to `batch` independent collapses per audited trial; with
         `keep_permille` the attached surrogate prunes the ranked edits first."""
@@ -413,7 +414,7 @@ class AuditSession:
         out.struct_size = C.sizeof(Execution)
         g = (EvalSettings * 4)(*gates)
         err = C.create_string_buffer(512)
-        if batch == 1 and not keep_permille:
+        if batch == 1 and not keep_permille and ranking == 3:
             _check(self.lib.blitz_audit_execute(self.handle, target_faces, trial_budget, g, commits.ctypes.data,
                                                 commits.size // 2, C.byref(out), err, 512), err)
         else:
@@ -421,6 +422,7 @@ class AuditSession:
             self.lib.blitz_execute_options_init(C.byref(opts))
             opts.batch = batch
             opts.keep_permille = keep_permille
+            opts.ranking = ranking
             _check(self.lib.blitz_audit_execute_ex(self.handle, target_faces, trial_budget, g, C.byref(opts),
                                                    commits.ctypes.data, commits.size // 2, C.byref(out), err, 512),
                    err)

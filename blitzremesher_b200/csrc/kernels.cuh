@@ -143,10 +143,11 @@ void launch_batch_trial(const DevMesh& m, const DevTopology& t, const Edit* edit
                         uint32_t count, uint32_t* remap, uint32_t* owner, float* placements, uint32_t* keep,
                         uint32_t* offsets, uint32_t* out_idx, uint16_t* out_mat, float* out_pos, uint32_t* table,
                         uint32_t table_cap, uint32_t* info, uint32_t* scan_scratch, cudaStream_t s);
-// ShortestEdge scores of the legal edits (action_gpu.cu:822-825), keys for a
-// stable descending sort.
-void launch_rank_shortest(const DevMesh& m, const Edit* edits, const uint32_t* count, uint32_t capacity,
-                          double diameter, float* scores, uint32_t* order, cudaStream_t s);
+// Ranking scores of the legal edits (rank_actions, action_gpu.cu:809-844),
+// keys for a stable descending sort. ranking: 1 Constant, 3 ShortestEdge,
+// 4 CurrentPlane (neural.hpp:9).
+void launch_rank(const DevMesh& m, const DevTopology& t, const Edit* edits, const uint32_t* count, uint32_t capacity,
+                 double diameter, int ranking, float* scores, uint32_t* order, cudaStream_t s);
 void launch_gather_window(const Edit* edits, const uint32_t* order, uint32_t first, uint32_t n, void* collapses,
                           cudaStream_t s);
 cudaError_t sort_scores_desc(const float* keys_in, float* keys_out, const uint32_t* vals_in, uint32_t* vals_out,

@@ -1088,6 +1088,32 @@ static void commit_collapse(Session& S, const blitz_collapse& col) {
     rebuild_topology(S);
 }
 
+static void prune_ranked(Session& S, uint32_t actions, uint32_t keep, float px, float px2);
+
+// Ranking scores of the state's legal edits: 1 Constant, 3 ShortestEdge,
+// 4 CurrentPlane (rank_actions, action_gpu.cu:809-844), or 0 Learned: the
+// attached surrogate's acceptance logits.
+static void rank_edits(Session& S, uint32_t actions, double diameter, int ranking, const blitz_eval_settings* gates,
+                       float* scores, uint32_t* order, cudaStream_t st) {
+    Topology& t = S.topo;
+    if (ranking != 0) {
+        launch_rank(S.state.view, t.view, t.edits.p, t.offsets.p + t.total_nbrs, actions, diameter, ranking, scores,
+                    order, st);
+        return;
+    }
+    if (!S.surrogate) throw Failure(BLITZ_INVALID_ARGUMENT, "learned ranking needs an attached surrogate");
+    const float px = float(gates[0].screen_size / std::max(1e-20, 2 * S.bounds.radius));
+    const float px2 = float(gates[2].screen_size / std::max(1e-20, 2 * S.bounds.radius));
+    const size_t cap = 6ull * S.source.view.nf + 1;
+    S.sur_features.ensure(S.pool, cap * kSurrogateIn);
+    S.sur_out.ensure(S.pool, 2 * cap);
+    launch_features(S.state.view, t.view, t.edits.p, t.offsets.p + t.total_nbrs, actions, px, px2,
+                    S.sur_features.p, st);
+    B200_CUDA(launch_mlp(S.surrogate->dev(), S.sur_features.p, actions, S.sur_out.p, nullptr, 0.f, nullptr,
+                         S.surrogate->error.p, 148, st));
+    launch_prune_prepare(S.sur_out.p, actions, scores, order, st);
+}
+
 static void reset_state(Session& S) {
     cudaStream_t st = S.stream;
     const DevMesh& src = S.source.view;
@@ -1316,7 +1342,7 @@ static void prune_ranked(Session& S, uint32_t actions, uint32_t keep, float px, 
 
 static void execute_batched(Session& S, uint32_t target, uint32_t budget, const blitz_eval_settings gates_in[4],
                             uint32_t batch, uint32_t keep_permille, uint32_t* commits_out, size_t capacity,
-                            blitz_audit_execution& out) {
+                            blitz_audit_execution& out, int ranking = 3) {
     target = std::max<uint32_t>(1, target);
     cudaStream_t st = S.stream;
     Topology& t = S.topo;
@@ -1371,8 +1397,7 @@ static void execute_batched(Session& S, uint32_t target, uint32_t budget, const 
             reason = 2;
             break;
         }
-        launch_rank_shortest(S.state.view, t.edits.p, t.offsets.p + t.total_nbrs, actions, diameter, S.scores.p,
-                             S.order.p, st);
+        rank_edits(S, actions, diameter, ranking, gates_in, S.scores.p, S.order.p, st);
         size_t bytes = S.sort_bytes;
         B200_CUDA(sort_scores_desc(S.scores.p, S.sorted_scores.p, S.order.p, S.sorted_order.p, actions, S.sort_temp.p,
                                    bytes, st));
@@ -1477,7 +1502,7 @@ static void execute_batched(Session& S, uint32_t target, uint32_t budget, const 
 // speculatively in ranked windows (one batched launch each) and replayed in
 // order on the host; the result equals the serial loop trial for trial.
 static void execute(Session& S, uint32_t target, uint32_t budget, const blitz_eval_settings gates[4],
-                    uint32_t* commits_out, size_t capacity, blitz_audit_execution& out) {
+                    uint32_t* commits_out, size_t capacity, blitz_audit_execution& out, int ranking = 3) {
     target = std::max<uint32_t>(1, target);
     cudaStream_t st = S.stream;
     Topology& t = S.topo;
@@ -1514,8 +1539,7 @@ static void execute(Session& S, uint32_t target, uint32_t budget, const blitz_ev
             reason = 2;
             break;
         }
-        launch_rank_shortest(S.state.view, t.edits.p, t.offsets.p + t.total_nbrs, actions, diameter, S.scores.p,
-                             S.order.p, st);
+        rank_edits(S, actions, diameter, ranking, gates, S.scores.p, S.order.p, st);
         size_t bytes = S.sort_bytes;
         B200_CUDA(sort_scores_desc(S.scores.p, S.sorted_scores.p, S.order.p, S.sorted_order.p, actions, S.sort_temp.p,
                                    bytes, st));
@@ -1910,6 +1934,7 @@ void blitz_execute_options_init(blitz_execute_options* o) {
     std::memset(o, 0, sizeof(*o));
     o->struct_size = sizeof(*o);
     o->batch = 1;
+    o->ranking = 3;
 }
 
 blitz_status blitz_audit_execute_ex(blitz_audit_session* s, uint32_t target_faces, uint32_t trial_budget,
@@ -1922,10 +1947,14 @@ blitz_status blitz_audit_execute_ex(blitz_audit_session* s, uint32_t target_face
             throw Failure(BLITZ_INVALID_ARGUMENT, "null argument or bad execution descriptor");
         if (options->batch < 1 || options->batch > 64)
             throw Failure(BLITZ_INVALID_ARGUMENT, "action batch outside 1..64");
+        if (options->ranking != 0 && options->ranking != 1 && options->ranking != 3 && options->ranking != 4)
+            throw Failure(BLITZ_INVALID_ARGUMENT, "ranking must be learned (0), constant (1), shortest edge (3) or "
+                                                  "current plane (4)");
+        if (options->ranking == 0 && !s->s.surrogate)
+            throw Failure(BLITZ_INVALID_ARGUMENT, "learned ranking needs an attached surrogate");
         if (options->keep_permille > 1000)
             throw Failure(BLITZ_INVALID_ARGUMENT, "surrogate keep share above 1000 permille");
-        if (options->keep_permille && options->batch == 1)
-            throw Failure(BLITZ_INVALID_ARGUMENT, "surrogate pruning needs the batched executor (batch > 1)");
+
         if (options->keep_permille && !s->s.surrogate)
             throw Failure(BLITZ_INVALID_ARGUMENT, "no surrogate attached to the session");
         for (uint32_t r : options->reserved)
@@ -1938,11 +1967,11 @@ blitz_status blitz_audit_execute_ex(blitz_audit_session* s, uint32_t target_face
         uint64_t t0 = now_ns();
         blitz_audit_execution r{};
         r.struct_size = sizeof(r);
-        if (options->batch == 1)
-            execute(S, target_faces, trial_budget, gates, commits_from_to, capacity, r);
+        if (options->batch == 1 && !options->keep_permille)
+            execute(S, target_faces, trial_budget, gates, commits_from_to, capacity, r, int(options->ranking));
         else
             execute_batched(S, target_faces, trial_budget, gates, options->batch, options->keep_permille,
-                            commits_from_to, capacity, r);
+                            commits_from_to, capacity, r, int(options->ranking));
         *out = r;
         S.info.gpu_audit_ns += now_ns() - t0;
         S.info.legal_collapses += r.commits;
@@ -2535,6 +2564,7 @@ void blitz_chain_settings_init(blitz_chain_settings* c) {
     c->batch = 64;
     c->trial_budget = 1u << 30;
     c->min_faces = 1;
+    c->ranking = 3;
 }
 
 blitz_status blitz_audit_chain(blitz_audit_session* s, const blitz_chain_settings* c, blitz_chain_level* out,
@@ -2547,6 +2577,9 @@ blitz_status blitz_audit_chain(blitz_audit_session* s, const blitz_chain_setting
         if (c->transition_points < 1 || c->transition_points > 8)
             throw Failure(BLITZ_INVALID_ARGUMENT, "transition curve needs 1..8 points");
         if (c->batch < 1 || c->batch > 64) throw Failure(BLITZ_INVALID_ARGUMENT, "action batch outside 1..64");
+        if (c->ranking != 0 && c->ranking != 1 && c->ranking != 3 && c->ranking != 4)
+            throw Failure(BLITZ_INVALID_ARGUMENT, "unknown ranking");
+        if (c->ranking == 0 && !s->s.surrogate) throw Failure(BLITZ_INVALID_ARGUMENT, "learned ranking needs a surrogate");
         if (out && capacity < c->levels - 1) throw Failure(BLITZ_INVALID_ARGUMENT, "level output too small");
         Session& S = s->s;
         DeviceScope scope(S.device);
@@ -2600,9 +2633,10 @@ blitz_status blitz_audit_chain(blitz_audit_session* s, const blitz_chain_setting
             blitz_audit_execution r{};
             r.struct_size = sizeof(r);
             if (c->batch == 1 && !c->keep_permille)
-                execute(S, c->min_faces, c->trial_budget, gates, nullptr, 0, r);
+                execute(S, c->min_faces, c->trial_budget, gates, nullptr, 0, r, int(c->ranking));
             else
-                execute_batched(S, c->min_faces, c->trial_budget, gates, c->batch, c->keep_permille, nullptr, 0, r);
+                execute_batched(S, c->min_faces, c->trial_budget, gates, c->batch, c->keep_permille, nullptr, 0, r,
+                                int(c->ranking));
             // confirmation at the audit views (generate.cpp:456-562)
             GateRef refs[4];
             PlanKey keys[4];

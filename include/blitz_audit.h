@@ -243,8 +243,10 @@ typedef struct blitz_execute_options {
     uint32_t struct_size;
     uint32_t batch;         /* 1..64 independent collapses audited as one combined trial */
     uint32_t keep_permille; /* 0: no surrogate; else the share of ranked edits the attached surrogate
-                               keeps (250 = top 25%), with the full order as fallback; batch > 1 only */
-    uint32_t reserved[5];   /* zero */
+                               keeps (250 = top 25%), with the full order as fallback */
+    uint32_t ranking;       /* NeuralRanking (neural.hpp:9): 0 learned = the attached surrogate's acceptance
+                               logits, 1 constant, 3 shortest edge (default), 4 current plane */
+    uint32_t reserved[4];   /* zero */
 } blitz_execute_options;
 void blitz_execute_options_init(blitz_execute_options*);
 
@@ -380,7 +382,8 @@ typedef struct blitz_chain_settings {
     uint32_t keep_permille;        /* surrogate pruning (attached model), 0 off */
     uint32_t trial_budget;         /* per level */
     uint32_t min_faces;            /* per-level target faces (1: as far as the gates allow) */
-    uint32_t reserved[4];
+    uint32_t ranking;              /* as blitz_execute_options.ranking */
+    uint32_t reserved[3];
 } blitz_chain_settings;
 void blitz_chain_settings_init(blitz_chain_settings*);
 typedef struct blitz_chain_level {

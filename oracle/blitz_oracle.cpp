@@ -928,6 +928,32 @@ float shortest_edge_score(const bo_mesh& m, const bo_edit& e, double diameter) {
     return -float(length(d));
 }
 
+// CurrentPlane ranking of rank_actions (action_gpu.cu:826-840): minus the sum,
+// over the faces of the `from` class, of the face's area weight times the
+// squared distance of `to` to its plane, all over the diameter.
+float current_plane_score(const bo_mesh& m, const Topology& t, const bo_edit& e, double diameter) {
+    const double scale = std::max(1e-20, diameter);
+    double cost = 0;
+    for (uint32_t k = t.face_offsets[e.from]; k < t.face_offsets[e.from + 1]; ++k) {
+        const uint32_t f = t.faces[k];
+        V3 p = load3(m.positions, m.indices[3 * f]), q = load3(m.positions, m.indices[3 * f + 1]),
+           r = load3(m.positions, m.indices[3 * f + 2]);
+        V3 normal = cross(sub(q, p), sub(r, p));
+        const double weight = length(normal);
+        const V3 unit = weight > 0 ? scale3(normal, 1 / weight) : V3{0, 0, 0};
+        const double distance = dot(unit, sub(load3(m.positions, e.to), p)) / scale;
+        cost += distance * distance * weight / (scale * scale);
+    }
+    return float(-cost);
+}
+// Scores of the rankings the executor supports (neural.hpp:9): 1 Constant,
+// 3 ShortestEdge, 4 CurrentPlane.
+float rank_score(int ranking, const bo_mesh& m, const Topology& t, const bo_edit& e, double diameter) {
+    if (ranking == 1) return 0.f;
+    if (ranking == 4) return current_plane_score(m, t, e, diameter);
+    return shortest_edge_score(m, e, diameter);
+}
+
 template <class F> int guarded(F f) {
     try {
         f();
@@ -1132,7 +1158,7 @@ int bo_execute_batched(const bo_mesh* source, const bo_mesh* previous, uint32_t 
                        const bo_eval_settings gates[4], int preserve_uv, uint32_t batch,
                        uint32_t* commits_from_to, uint32_t capacity, uint32_t* commits, uint32_t* trials,
                        uint32_t* out_indices, uint32_t* out_faces, float* out_positions, uint8_t* stop) {
-    return bo_execute_from(source, previous, nullptr, target, budget, gates, preserve_uv, batch, commits_from_to,
+    return bo_execute_from(source, previous, nullptr, target, budget, gates, preserve_uv, batch, 3, commits_from_to,
                            capacity, commits, trials, out_indices, out_faces, out_positions, stop);
 }
 
@@ -1141,10 +1167,10 @@ int bo_execute_batched(const bo_mesh* source, const bo_mesh* previous, uint32_t 
 // classes stay those welded on the source (a chain's levels continue one
 // state, generate.cpp:456-562).
 int bo_execute_from(const bo_mesh* source, const bo_mesh* previous, const bo_mesh* start, uint32_t target,
-                    uint32_t budget, const bo_eval_settings gates[4], int preserve_uv, uint32_t batch,
+                    uint32_t budget, const bo_eval_settings gates[4], int preserve_uv, uint32_t batch, int ranking,
                     uint32_t* commits_from_to, uint32_t capacity, uint32_t* commits, uint32_t* trials,
                     uint32_t* out_indices, uint32_t* out_faces, float* out_positions, uint8_t* stop) {
-    if (!batch || batch > 64) return 1;
+    if (!batch || batch > 64 || (ranking != 1 && ranking != 3 && ranking != 4)) return 1;
     if (start && start->vertex_count != source->vertex_count) return 1;
     return guarded([&] {
         ExecState st;
@@ -1180,7 +1206,7 @@ int bo_execute_from(const bo_mesh* source, const bo_mesh* previous, const bo_mes
                 break;
             }
             std::vector<float> scores(edits.size());
-            for (size_t i = 0; i < edits.size(); ++i) scores[i] = shortest_edge_score(m, edits[i], diameter);
+            for (size_t i = 0; i < edits.size(); ++i) scores[i] = rank_score(ranking, m, t, edits[i], diameter);
             std::vector<uint32_t> order(edits.size());
             std::iota(order.begin(), order.end(), 0);
             std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t c) { return scores[a] > scores[c]; });

@@ -144,14 +144,14 @@ class Oracle:
         return b
 
     def execute(self, source, target: int, budget: int, gates, previous=None, preserve_uv=True, batch=1,
-                start=None) -> dict:
+                start=None, ranking=3) -> dict:
         """Greedy executor (ShortestEdge, midpoint placement), batches of up to
         `batch` independent collapses audited as one trial, from `start` (a
         later state of `source`; default the source)."""
         L = self.lib
         P = C.POINTER
         L.bo_execute_from.argtypes = [P(BoMesh), P(BoMesh), P(BoMesh), C.c_uint32, C.c_uint32, P(BoEvalSettings),
-                                      C.c_int, C.c_uint32, C.c_void_p, C.c_uint32, P(C.c_uint32),
+                                      C.c_int, C.c_uint32, C.c_int, C.c_void_p, C.c_uint32, P(C.c_uint32),
                                       P(C.c_uint32), C.c_void_p, P(C.c_uint32), C.c_void_p, P(C.c_uint8)]
         hs = _MeshHold(source)
         hp = None if previous is None else _MeshHold(previous)
@@ -164,6 +164,7 @@ class Oracle:
         g = (BoEvalSettings * 4)(*gates)
         st = L.bo_execute_from(C.byref(hs.c), None if hp is None else C.byref(hp.c),
                                None if hst is None else C.byref(hst.c), target, budget, g, int(preserve_uv), batch,
+                               ranking,
                                ft.ctypes.data, cap, C.byref(commits), C.byref(trials), idx.ctypes.data,
                                C.byref(faces), pos.ctypes.data, C.byref(stop))
         assert st == 0

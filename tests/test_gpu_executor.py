@@ -191,3 +191,37 @@ def test_chain_matches_oracle(gpu_lib, oracle, batch):
         assert np.array_equal(idx, w["indices"]) and np.array_equal(pos, w["positions"])
         assert lv["confirmed"] == 1
     assert levels[-1]["faces"] < levels[0]["faces"] < mesh.face_count
+
+
+@pytest.mark.parametrize("ranking,batch", [(4, 1), (4, 8), (1, 8)])
+def test_rankings_match_oracle(gpu_lib, oracle, ranking, batch):
+    """CurrentPlane (4) and Constant (1) rankings of rank_actions: the same walk
+    as the oracle's executor with that ranking."""
+    make, views, screen, ss, budget = CASES["sphere2_96"]
+    mesh = make()
+    args = _gates(screen, views, ss)
+    target = mesh.face_count // 2
+    want = oracle.execute(mesh, target, budget, [oracle_settings(*a) for a in args], batch=batch, ranking=ranking)
+    with br.AuditSession(mesh) as s:
+        got = s.execute(target, budget, [br.eval_settings(*a) for a in args], batch=batch, ranking=ranking)
+        idx, pos = s.state()
+    assert len(want["commits"]) > 5
+    assert np.array_equal(got["commits"], want["commits"])
+    assert got["trials"] == want["trials"] and got["stop"] == want["stop"]
+    assert np.array_equal(idx, want["indices"]) and np.array_equal(pos, want["positions"])
+
+
+def test_learned_ranking_passes_the_exact_audit(gpu_lib):
+    """Learned ranking (the attached surrogate's logits) reorders the walk; the
+    exact audit still judges every committed batch."""
+    mesh = syn.noisy_icosphere(3, 8)
+    args = _gates(64.0, (8, 0, 0xB1172026), 8)
+    gates = [br.eval_settings(*a) for a in args]
+    with br.AuditSession(mesh) as s:
+        s.attach_surrogate(br.Surrogate(seed=3))
+        r = s.execute(mesh.face_count // 3, 300, gates, batch=16, ranking=0)
+        idx, pos = s.state()
+        assert len(r["commits"]) > 0
+        for g in gates:
+            m = br.evaluate(mesh, syn.Mesh(pos, idx), g, session=s)
+            assert m.passed == 1
