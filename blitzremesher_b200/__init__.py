@@ -158,6 +158,7 @@ EXPORTS = {
     "blitz_audit_batch_read_info": ([C.c_void_p, C.c_void_p], C.c_int),
     "blitz_audit_state": ([C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p, C.c_size_t, C.POINTER(C.c_uint32),
                            C.c_char_p, C.c_size_t], C.c_int),
+    "blitz_audit_state_uv": ([C.c_void_p, C.c_void_p, C.c_size_t, C.c_char_p, C.c_size_t], C.c_int),
     "blitz_audit_reset": ([C.c_void_p, C.c_char_p, C.c_size_t], C.c_int),
     "blitz_audit_profile_read": ([C.c_void_p, C.c_void_p], C.c_int),
 }
@@ -486,6 +487,13 @@ class AuditSession:
         _check(self.lib.blitz_audit_state(self.handle, idx.ctypes.data, idx.size, pos.ctypes.data, pos.size,
                                           C.byref(faces), err, 512), err)
         return idx, pos
+
+    def state_uv(self) -> np.ndarray:
+        """Current state's uv per vertex slot (uv transported by commits)."""
+        err = C.create_string_buffer(512)
+        uv = np.zeros((self._source.pos.shape[0], 2), np.float32)
+        _check(self.lib.blitz_audit_state_uv(self.handle, uv.ctypes.data, uv.size, err, 512), err)
+        return uv
 
     def reset(self) -> None:
         err = C.create_string_buffer(512)

@@ -36,6 +36,20 @@ struct Edit {
     uint8_t wedges, removed, valid, pad;
 };
 
+// Attribute charts for uv transport (place_vertices): the session's source
+// mesh and, per canonical class of the source (position + uv weld with
+// preserve_uv, the geometric classes without), its source faces in
+// ascending order, each face once. uv == null: the mesh has no uv. flip:
+// preserve_uv, which adds the uv orientation check of validate_placement.
+struct UvSource {
+    const float* pos;
+    const float* uv;
+    const uint32_t* idx;
+    const uint32_t* offsets; // canonical class -> range in faces (nv + 1)
+    const uint32_t* faces;
+    bool flip;
+};
+
 constexpr int kMaxAffected = 32; // faces in faces(from) U faces(to) handled on the fast path
 constexpr int kMaxLocal = 31;    // distinct vertex slots of those faces; local index 31 = placement
 constexpr uint8_t kPlacementLocal = 31;
@@ -100,7 +114,8 @@ void launch_position_table(const DevMesh& m, const DevTopology& t, uint32_t* tab
                            cudaStream_t s);
 void launch_prepare(const DevMesh& m, const DevTopology& t, const DevMesh& original, const DevTopology& ot,
                     const void* collapses, uint32_t n, const uint32_t* table, uint32_t capacity,
-                    const uint32_t* flat_total, bool preserve_uv, CandidateRecord* out, cudaStream_t s);
+                    const uint32_t* flat_total, bool preserve_uv, CandidateRecord* out, cudaStream_t s,
+                    const UvSource* uv = nullptr);
 void launch_raster(const DevMesh& m, const Camera* cam_host, const float* center, uint32_t ss, uint32_t size,
                    bool force_two, bool cpu_semantics, uint32_t* bits, uint8_t* counts, uint32_t* state,
                    cudaStream_t s);
@@ -142,7 +157,8 @@ cudaError_t launch_select_batch(const DevTopology& t, const Edit* edits, const u
 void launch_batch_trial(const DevMesh& m, const DevTopology& t, const Edit* edits, const uint32_t* selected,
                         uint32_t count, uint32_t* remap, uint32_t* owner, float* placements, uint32_t* keep,
                         uint32_t* offsets, uint32_t* out_idx, uint16_t* out_mat, float* out_pos, uint32_t* table,
-                        uint32_t table_cap, uint32_t* info, uint32_t* scan_scratch, cudaStream_t s);
+                        uint32_t table_cap, uint32_t* info, uint32_t* scan_scratch, cudaStream_t s,
+                        const UvSource* uv = nullptr, float* out_uv = nullptr);
 // Ranking scores of the legal edits (rank_actions, action_gpu.cu:809-844),
 // keys for a stable descending sort. ranking: 1 Constant, 3 ShortestEdge,
 // 4 CurrentPlane (neural.hpp:9).
@@ -210,8 +226,9 @@ struct TrialInfo {
     float placement[3];
     uint32_t ok;
 };
+// out_uv (with uv): the trial's uv per vertex slot, transported for moved slots.
 void launch_trial(const DevMesh& m, const DevTopology& t, const void* collapse, TrialInfo* info, uint32_t* keep,
                   uint32_t* offsets, uint32_t* out_idx, uint16_t* out_mat, float* out_pos, uint32_t* scan_scratch,
-                  cudaStream_t s);
+                  cudaStream_t s, const UvSource* uv = nullptr, float* out_uv = nullptr);
 
 } // namespace b200

@@ -278,6 +278,10 @@ struct Topology {
     Buf<uint32_t> positions; // live position table
     uint32_t table_cap = 0, pos_cap = 0, total_nbrs = 0, actions = 0;
     DevTopology view{};
+    // uv transport: source faces per canonical class
+    Buf<uint32_t> uv_offsets, uv_faces;
+    UvSource uvs{};
+    const UvSource* uv() const { return uvs.uv ? &uvs : nullptr; }
 };
 
 static uint32_t pow2_at_least(uint64_t n) {
@@ -489,7 +493,52 @@ static void init_topology(Session& S) {
     t.flat = Buf<uint32_t>(P, 1);
     t.pos_cap = pow2_at_least(4ull * n);
     t.positions = Buf<uint32_t>(P, t.pos_cap);
-    t.view = DevTopology{t.geometry.p, t.geometry.p, t.face_offsets.p, t.faces.p, t.nbr_offsets.p, t.neighbors.p,
+    const uint32_t* canonical = t.geometry.p;
+    if (m.uv) {
+        // Attribute charts (action_gpu.cu:1520-1525): with preserve_uv the
+        // position + uv weld, else the geometric classes; then each class's
+        // source faces in ascending order for place_vertices.
+        if (S.options.preserve_uv) {
+            t.canonical = Buf<uint32_t>(P, n);
+            launch_weld(m, t.table.p, t.table_cap, true, t.canonical.p, S.stream);
+            canonical = t.canonical.p;
+        }
+        std::vector<uint32_t> cls(n), offsets(size_t(n) + 1, 0), faces;
+        B200_CUDA(cudaMemcpyAsync(cls.data(), canonical, size_t(n) * 4, cudaMemcpyDeviceToHost, S.stream));
+        B200_CUDA(cudaStreamSynchronize(S.stream));
+        const std::vector<uint32_t>& idx = S.source_h.idx;
+        auto corners = [&](uint32_t f, uint32_t* c) {
+            for (int j = 0; j < 3; ++j) c[j] = cls[idx[3 * f + j]];
+            if (c[1] == c[0]) c[1] = kNone;
+            if (c[2] == c[0] || c[2] == c[1]) c[2] = kNone;
+        };
+        for (uint32_t f = 0; f < nf; ++f) {
+            uint32_t c[3];
+            corners(f, c);
+            for (uint32_t k : c)
+                if (k != kNone) ++offsets[k + 1];
+        }
+        for (uint32_t v = 0; v < n; ++v) offsets[v + 1] += offsets[v];
+        faces.resize(offsets[n]);
+        std::vector<uint32_t> fill(offsets.begin(), offsets.end() - 1);
+        for (uint32_t f = 0; f < nf; ++f) {
+            uint32_t c[3];
+            corners(f, c);
+            for (uint32_t k : c)
+                if (k != kNone) faces[fill[k]++] = f;
+        }
+        t.uv_offsets = Buf<uint32_t>(P, offsets.size());
+        t.uv_faces = Buf<uint32_t>(P, std::max<size_t>(1, faces.size()));
+        B200_CUDA(cudaMemcpyAsync(t.uv_offsets.p, offsets.data(), offsets.size() * 4, cudaMemcpyHostToDevice,
+                                  S.stream));
+        if (!faces.empty())
+            B200_CUDA(cudaMemcpyAsync(t.uv_faces.p, faces.data(), faces.size() * 4, cudaMemcpyHostToDevice,
+                                      S.stream));
+        B200_CUDA(cudaStreamSynchronize(S.stream));
+        const DevMesh& src = S.source.view;
+        t.uvs = UvSource{src.pos, src.uv, src.idx, t.uv_offsets.p, t.uv_faces.p, S.options.preserve_uv != 0};
+    }
+    t.view = DevTopology{t.geometry.p, canonical, t.face_offsets.p, t.faces.p, t.nbr_offsets.p, t.neighbors.p,
                          t.nbr_count.p, t.boundary.p, t.invalid.p, t.slot_offsets.p, t.slots.p};
 }
 
@@ -789,6 +838,7 @@ static void ensure_trial_buffers(Session& S) {
     S.trial.pos = Buf<float>(S.pool, 3ull * src.nv);
     S.trial.idx = Buf<uint32_t>(S.pool, 3ull * src.nf);
     if (src.mat) S.trial.mat = Buf<uint16_t>(S.pool, src.nf);
+    if (src.uv) S.trial.uv = Buf<float>(S.pool, 2ull * src.nv);
     S.trial_keep = Buf<uint32_t>(S.pool, src.nf + 1);
     S.trial_offsets = Buf<uint32_t>(S.pool, src.nf + 1);
     S.trial_info = Buf<TrialInfo>(S.pool, 1);
@@ -901,7 +951,7 @@ static void exact_candidate(Session& S, const blitz_collapse& col, const GateRef
     ensure_trial_buffers(S);
     B200_CUDA(cudaMemcpyAsync(S.trial_collapse.p, &col, sizeof(col), cudaMemcpyHostToDevice, S.stream));
     launch_trial(m, t.view, S.trial_collapse.p, S.trial_info.p, S.trial_keep.p, S.trial_offsets.p, S.trial.idx.p, S.trial.mat.p,
-                 S.trial.pos.p, t.scan.p, S.stream);
+                 S.trial.pos.p, t.scan.p, S.stream, t.uv(), S.trial.uv.p);
     uint32_t faces = 0;
     B200_CUDA(cudaMemcpyAsync(&faces, S.trial_offsets.p + m.nf, 4, cudaMemcpyDeviceToHost, S.stream));
     B200_CUDA(cudaStreamSynchronize(S.stream));
@@ -1025,7 +1075,7 @@ static void audit_candidates(Session& S, const blitz_collapse* cands_dev, const 
         B200_CUDA(cudaEventRecord(S.ev[0], st));
     }
     launch_prepare(S.state.view, t.view, S.state.view, t.view, cands_dev, nn, t.positions.p, t.pos_cap, t.flat.p,
-                   S.options.preserve_uv != 0, S.records.p, st);
+                   S.options.preserve_uv != 0, S.records.p, st, t.uv());
     if (prof) B200_CUDA(cudaEventRecord(S.ev[1], st));
     S.profile.launches += nn ? 1 : 0;
     upload_verdict_tables(S, a, nn, st);
@@ -1073,7 +1123,7 @@ static void commit_collapse(Session& S, const blitz_collapse& col) {
     cudaStream_t st = S.stream;
     B200_CUDA(cudaMemcpyAsync(S.trial_collapse.p, &col, sizeof(col), cudaMemcpyHostToDevice, st));
     launch_trial(m, S.topo.view, S.trial_collapse.p, S.trial_info.p, S.trial_keep.p, S.trial_offsets.p, S.trial.idx.p,
-                 S.trial.mat.p, S.trial.pos.p, S.topo.scan.p, st);
+                 S.trial.mat.p, S.trial.pos.p, S.topo.scan.p, st, S.topo.uv(), S.trial.uv.p);
     uint32_t faces = 0;
     B200_CUDA(cudaMemcpyAsync(&faces, S.trial_offsets.p + m.nf, 4, cudaMemcpyDeviceToHost, st));
     B200_CUDA(cudaStreamSynchronize(st));
@@ -1081,6 +1131,7 @@ static void commit_collapse(Session& S, const blitz_collapse& col) {
     B200_CUDA(cudaMemcpyAsync(S.state.idx.p, S.trial.idx.p, size_t(faces) * 12, cudaMemcpyDeviceToDevice, st));
     B200_CUDA(cudaMemcpyAsync(S.state.pos.p, S.trial.pos.p, size_t(m.nv) * 12, cudaMemcpyDeviceToDevice, st));
     if (m.mat) B200_CUDA(cudaMemcpyAsync(S.state.mat.p, S.trial.mat.p, size_t(faces) * 2, cudaMemcpyDeviceToDevice, st));
+    if (m.uv) B200_CUDA(cudaMemcpyAsync(S.state.uv.p, S.trial.uv.p, size_t(m.nv) * 8, cudaMemcpyDeviceToDevice, st));
     m.nf = faces;
     S.state_faces = faces;
     ++S.state_revision;
@@ -1120,6 +1171,7 @@ static void reset_state(Session& S) {
     B200_CUDA(cudaMemcpyAsync(S.state.idx.p, src.idx, size_t(src.nf) * 12, cudaMemcpyDeviceToDevice, st));
     B200_CUDA(cudaMemcpyAsync(S.state.pos.p, src.pos, size_t(src.nv) * 12, cudaMemcpyDeviceToDevice, st));
     if (src.mat) B200_CUDA(cudaMemcpyAsync(S.state.mat.p, src.mat, size_t(src.nf) * 2, cudaMemcpyDeviceToDevice, st));
+    if (src.uv) B200_CUDA(cudaMemcpyAsync(S.state.uv.p, src.uv, size_t(src.nv) * 8, cudaMemcpyDeviceToDevice, st));
     S.state.view.nf = src.nf;
     S.state_faces = src.nf;
     ++S.state_revision;
@@ -1245,6 +1297,7 @@ static void commit_trial(Session& S, uint32_t faces, uint64_t tag) {
     B200_CUDA(cudaMemcpyAsync(S.state.idx.p, S.trial.idx.p, size_t(faces) * 12, cudaMemcpyDeviceToDevice, st));
     B200_CUDA(cudaMemcpyAsync(S.state.pos.p, S.trial.pos.p, size_t(m.nv) * 12, cudaMemcpyDeviceToDevice, st));
     if (m.mat) B200_CUDA(cudaMemcpyAsync(S.state.mat.p, S.trial.mat.p, size_t(faces) * 2, cudaMemcpyDeviceToDevice, st));
+    if (m.uv) B200_CUDA(cudaMemcpyAsync(S.state.uv.p, S.trial.uv.p, size_t(m.nv) * 8, cudaMemcpyDeviceToDevice, st));
     m.nf = faces;
     S.state_faces = faces;
     ++S.state_revision;
@@ -1292,7 +1345,8 @@ static uint32_t build_batch_trial(Session& S, uint32_t count, bool& invalid) {
     cudaStream_t st = S.stream;
     launch_batch_trial(m, t.view, t.edits.p, S.batch_selected.p, count, S.batch_remap.p, S.batch_owner.p,
                        S.batch_placements.p, S.trial_keep.p, S.trial_offsets.p, S.trial.idx.p, S.trial.mat.p,
-                       S.trial.pos.p, S.batch_table.p, S.batch_table_cap, S.batch_info.p, t.scan.p, st);
+                       S.trial.pos.p, S.batch_table.p, S.batch_table_cap, S.batch_info.p, t.scan.p, st, t.uv(),
+                       S.trial.uv.p);
     uint32_t host[2] = {0, 0};
     B200_CUDA(cudaMemcpyAsync(&host[0], S.trial_offsets.p + m.nf, 4, cudaMemcpyDeviceToHost, st));
     B200_CUDA(cudaMemcpyAsync(&host[1], S.batch_info.p, 4, cudaMemcpyDeviceToHost, st));
@@ -1867,8 +1921,6 @@ blitz_status blitz_audit_candidates_device(blitz_audit_session* s, const blitz_c
             throw Failure(BLITZ_INVALID_ARGUMENT, "null argument");
         Session& S = s->s;
         DeviceScope scope(S.device);
-        if (S.options.preserve_uv && !S.source_h.uv.empty())
-            throw Failure(BLITZ_UNAVAILABLE, "uv transport on the candidate path is not implemented");
         uint64_t t0 = now_ns();
         cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : S.stream;
         audit_candidates(S, candidates_device, nullptr, n, gates, out_device,
@@ -1884,8 +1936,6 @@ blitz_status blitz_audit_candidates(blitz_audit_session* s, const blitz_collapse
         if (!s || !gates || (n && (!candidates || !out))) throw Failure(BLITZ_INVALID_ARGUMENT, "null argument");
         Session& S = s->s;
         DeviceScope scope(S.device);
-        if (S.options.preserve_uv && !S.source_h.uv.empty())
-            throw Failure(BLITZ_UNAVAILABLE, "uv transport on the candidate path is not implemented");
         uint64_t t0 = now_ns();
         S.collapse_dev.ensure(S.pool, std::max<size_t>(n, 1));
         S.verdict_dev.ensure(S.pool, std::max<size_t>(n, 1) * sizeof(blitz_candidate_verdict));
@@ -1915,8 +1965,6 @@ blitz_status blitz_audit_execute(blitz_audit_session* s, uint32_t target_faces, 
             throw Failure(BLITZ_INVALID_ARGUMENT, "null argument or bad execution descriptor");
         Session& S = s->s;
         DeviceScope scope(S.device);
-        if (S.options.preserve_uv && !S.source_h.uv.empty())
-            throw Failure(BLITZ_UNAVAILABLE, "uv transport on the candidate path is not implemented");
         for (int g = 0; g < 4; ++g) gate_of(&gates[g], S.bounds);
         uint64_t t0 = now_ns();
         blitz_audit_execution r{};
@@ -1961,8 +2009,6 @@ blitz_status blitz_audit_execute_ex(blitz_audit_session* s, uint32_t target_face
             if (r) throw Failure(BLITZ_INVALID_ARGUMENT, "reserved execution options must be zero");
         Session& S = s->s;
         DeviceScope scope(S.device);
-        if (S.options.preserve_uv && !S.source_h.uv.empty())
-            throw Failure(BLITZ_UNAVAILABLE, "uv transport on the candidate path is not implemented");
         for (int g = 0; g < 4; ++g) gate_of(&gates[g], S.bounds);
         uint64_t t0 = now_ns();
         blitz_audit_execution r{};
@@ -1991,6 +2037,19 @@ blitz_status blitz_audit_state(blitz_audit_session* s, uint32_t* indices, size_t
             B200_CUDA(cudaMemcpyAsync(indices, m.idx, size_t(S.state_faces) * 12, cudaMemcpyDeviceToHost, S.stream));
         if (positions && position_capacity >= size_t(m.nv) * 3)
             B200_CUDA(cudaMemcpyAsync(positions, m.pos, size_t(m.nv) * 12, cudaMemcpyDeviceToHost, S.stream));
+        B200_CUDA(cudaStreamSynchronize(S.stream));
+    });
+}
+
+blitz_status blitz_audit_state_uv(blitz_audit_session* s, float* uv, size_t uv_capacity, char* error, size_t cap) {
+    return guarded(error, cap, [&] {
+        if (!s || !uv) throw Failure(BLITZ_INVALID_ARGUMENT, "null argument");
+        Session& S = s->s;
+        DeviceScope scope(S.device);
+        const DevMesh& m = S.state.view;
+        if (!m.uv) throw Failure(BLITZ_INVALID_ARGUMENT, "the session's mesh has no uv");
+        if (uv_capacity < size_t(m.nv) * 2) throw Failure(BLITZ_INVALID_ARGUMENT, "uv capacity below 2 per vertex");
+        B200_CUDA(cudaMemcpyAsync(uv, m.uv, size_t(m.nv) * 8, cudaMemcpyDeviceToHost, S.stream));
         B200_CUDA(cudaStreamSynchronize(S.stream));
     });
 }
@@ -2395,7 +2454,7 @@ blitz_status blitz_audit_batch_candidates(blitz_audit_batch* b, const blitz_coll
                 Topology& t = S.topo;
                 launch_prepare(S.state.view, t.view, S.state.view, t.view, cands + off[i], uint32_t(counts[i]),
                                t.positions.p, t.pos_cap, t.flat.p, S.options.preserve_uv != 0, b->records.p + off[i],
-                               st);
+                               st, t.uv());
             }
             if (profile) {
                 cudaMemsetAsync(b->stats.p, 0, 32, st);
@@ -2584,8 +2643,6 @@ blitz_status blitz_audit_chain(blitz_audit_session* s, const blitz_chain_setting
         Session& S = s->s;
         DeviceScope scope(S.device);
         if (c->keep_permille && !S.surrogate) throw Failure(BLITZ_INVALID_ARGUMENT, "no surrogate attached");
-        if (S.options.preserve_uv && !S.source_h.uv.empty())
-            throw Failure(BLITZ_UNAVAILABLE, "uv transport on the candidate path is not implemented");
         reset_state(S);
         auto bind_previous_source = [&] {
             S.previous_is_source = true;

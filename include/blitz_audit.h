@@ -408,6 +408,11 @@ blitz_status blitz_audit_chain(blitz_audit_session*, const blitz_chain_settings*
 /* Current state: compacted indices (3 per face) and every vertex slot's position. */
 blitz_status blitz_audit_state(blitz_audit_session*, uint32_t* indices, size_t index_capacity, float* positions,
                                size_t position_capacity, uint32_t* face_count, char* error, size_t error_capacity);
+/* Current state's uv, 2 per vertex slot (the uv stream of GpuActionState's
+ * mesh, transported by place_vertices, action_gpu.cu:962-1067). Invalid
+ * argument when the session's mesh has no uv. */
+blitz_status blitz_audit_state_uv(blitz_audit_session*, float* uv, size_t uv_capacity, char* error,
+                                  size_t error_capacity);
 /* Restores the state to the source (GpuActionState::reset, action_gpu.cu:1884-1906). */
 blitz_status blitz_audit_reset(blitz_audit_session*, char* error, size_t error_capacity);
 

@@ -1159,7 +1159,7 @@ int bo_execute_batched(const bo_mesh* source, const bo_mesh* previous, uint32_t 
                        uint32_t* commits_from_to, uint32_t capacity, uint32_t* commits, uint32_t* trials,
                        uint32_t* out_indices, uint32_t* out_faces, float* out_positions, uint8_t* stop) {
     return bo_execute_from(source, previous, nullptr, target, budget, gates, preserve_uv, batch, 3, commits_from_to,
-                           capacity, commits, trials, out_indices, out_faces, out_positions, stop);
+                           capacity, commits, trials, out_indices, out_faces, out_positions, stop, nullptr);
 }
 
 // The same walk starting from `start` (a later state of `source`: same vertex
@@ -1169,7 +1169,8 @@ int bo_execute_batched(const bo_mesh* source, const bo_mesh* previous, uint32_t 
 int bo_execute_from(const bo_mesh* source, const bo_mesh* previous, const bo_mesh* start, uint32_t target,
                     uint32_t budget, const bo_eval_settings gates[4], int preserve_uv, uint32_t batch, int ranking,
                     uint32_t* commits_from_to, uint32_t capacity, uint32_t* commits, uint32_t* trials,
-                    uint32_t* out_indices, uint32_t* out_faces, float* out_positions, uint8_t* stop) {
+                    uint32_t* out_indices, uint32_t* out_faces, float* out_positions, uint8_t* stop,
+                    float* out_uv) {
     if (!batch || batch > 64 || (ranking != 1 && ranking != 3 && ranking != 4)) return 1;
     if (start && start->vertex_count != source->vertex_count) return 1;
     return guarded([&] {
@@ -1251,6 +1252,7 @@ int bo_execute_from(const bo_mesh* source, const bo_mesh* previous, const bo_mes
         *out_faces = uint32_t(st.idx.size() / 3);
         std::copy(st.idx.begin(), st.idx.end(), out_indices);
         std::copy(st.pos.begin(), st.pos.end(), out_positions);
+        if (out_uv) std::copy(st.uv.begin(), st.uv.end(), out_uv);
         *stop = reason;
     });
 }

@@ -137,12 +137,14 @@ int bo_execute_batched(const bo_mesh* source, const bo_mesh* previous, uint32_t 
                        uint32_t* commits_from_to, uint32_t capacity, uint32_t* commits, uint32_t* trials,
                        uint32_t* out_indices, uint32_t* out_faces, float* out_positions, uint8_t* stop);
 /* The batched walk from `start` (a later state of `source`, same vertex
- * slots; NULL = the source) against the source and `previous`. */
+ * slots; NULL = the source) against the source and `previous`; out_uv
+ * receives the final state's uv when the meshes have uv. */
 /* ranking: 1 Constant, 3 ShortestEdge, 4 CurrentPlane (neural.hpp:9). */
 int bo_execute_from(const bo_mesh* source, const bo_mesh* previous, const bo_mesh* start, uint32_t target,
                     uint32_t budget, const bo_eval_settings gates[4], int preserve_uv, uint32_t batch, int ranking,
                     uint32_t* commits_from_to, uint32_t capacity, uint32_t* commits, uint32_t* trials,
-                    uint32_t* out_indices, uint32_t* out_faces, float* out_positions, uint8_t* stop);
+                    uint32_t* out_indices, uint32_t* out_faces, float* out_positions, uint8_t* stop,
+                    float* out_uv /* 2 per vertex, or NULL */);
 
 #ifdef __cplusplus
 }

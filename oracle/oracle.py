@@ -152,7 +152,8 @@ class Oracle:
         P = C.POINTER
         L.bo_execute_from.argtypes = [P(BoMesh), P(BoMesh), P(BoMesh), C.c_uint32, C.c_uint32, P(BoEvalSettings),
                                       C.c_int, C.c_uint32, C.c_int, C.c_void_p, C.c_uint32, P(C.c_uint32),
-                                      P(C.c_uint32), C.c_void_p, P(C.c_uint32), C.c_void_p, P(C.c_uint8)]
+                                      P(C.c_uint32), C.c_void_p, P(C.c_uint32), C.c_void_p, P(C.c_uint8),
+                                      C.c_void_p]
         hs = _MeshHold(source)
         hp = None if previous is None else _MeshHold(previous)
         hst = None if start is None else _MeshHold(start)
@@ -160,17 +161,19 @@ class Oracle:
         ft = np.zeros(2 * cap, np.uint32)
         idx = np.zeros(source.face_count * 3, np.uint32)
         pos = np.zeros((source.vertex_count, 3), np.float32)
+        uv = np.zeros((source.vertex_count, 2), np.float32)
         commits, trials, faces, stop = C.c_uint32(), C.c_uint32(), C.c_uint32(), C.c_uint8()
         g = (BoEvalSettings * 4)(*gates)
         st = L.bo_execute_from(C.byref(hs.c), None if hp is None else C.byref(hp.c),
                                None if hst is None else C.byref(hst.c), target, budget, g, int(preserve_uv), batch,
                                ranking,
                                ft.ctypes.data, cap, C.byref(commits), C.byref(trials), idx.ctypes.data,
-                               C.byref(faces), pos.ctypes.data, C.byref(stop))
+                               C.byref(faces), pos.ctypes.data, C.byref(stop), uv.ctypes.data)
         assert st == 0
         n = commits.value
         return {"commits": ft[: 2 * n].reshape(-1, 2), "trials": trials.value, "stop": stop.value,
-                "indices": idx[: 3 * faces.value].copy(), "positions": pos}
+                "indices": idx[: 3 * faces.value].copy(), "positions": pos,
+                "uv": uv if source.uv is not None else None}
 
     def cameras(self, b: BoBounds, screen: float, views: tuple) -> list:
         n = views[0] + views[1]
