@@ -56,7 +56,7 @@ constexpr int kLargeWarps = 3; // warps per block of the large tier
 struct LimitsHuge {
     static constexpr int kRegionWords = 32;
     static constexpr int kRegionRows = 1024;
-    static constexpr int kDeltaSamples = 1 << 20;
+    static constexpr int kDeltaSamples = 16384; // direct-test units only
     static constexpr int kQueue = 65536;
     static constexpr int kAffected = 64;
 };
@@ -66,7 +66,7 @@ constexpr int kHugeWarps = 8;
 struct LimitsGiant {
     static constexpr int kRegionWords = 136;
     static constexpr int kRegionRows = 4160;
-    static constexpr int kDeltaSamples = 4352 * 4160;
+    static constexpr int kDeltaSamples = 16384;
     static constexpr int kQueue = 65536;
     static constexpr int kAffected = 64;
 };
@@ -77,10 +77,56 @@ template <class L> struct alignas(16) WarpScratch {
     FaceSetup faces[kMaxOk];       // old faces carry pad = -1, new faces pad = +1
     uint32_t work[kMaxOk];         // exclusive prefix of bbox samples per face
     uint32_t affected[L::kAffected];
-    uint32_t region[L::kRegionRows * L::kRegionWords];
+    uint32_t qcount[4];            // [0]: flipped samples queued
+    uint32_t region[L::kRegionRows * L::kRegionWords]; // candidate XOR state coverage
     uint32_t delta[L::kDeltaSamples / 4]; // per-sample count delta + 128, one byte each
     uint32_t queue[L::kQueue];
 };
+
+// Covered samples [lo, hi] of row py - .5 of face s (lo > hi: none), from
+// s's bbox columns: each edge term of face_covers is monotone in x, so a
+// binary search per edge finds the interval's ends with the same FP64
+// expressions.
+__device__ __forceinline__ void face_interval(const FaceSetup& s, double py, int& lo, int& hi) {
+    lo = s.x0, hi = s.x1;
+    // edge (d, e), edge (e, a), edge (a, d) of face_covers
+    const double ax3[3] = {s.dx, s.ex, s.ax}, ay3[3] = {s.dy, s.ey, s.ay};
+    const double bx3[3] = {s.ex, s.ax, s.dx}, by3[3] = {s.ey, s.ay, s.dy};
+    const double r3[3] = {s.r0, s.r1, s.r2};
+    for (int e = 0; e < 3 && lo <= hi; ++e) {
+        const double ax = ax3[e], ay = ay3[e], r = r3[e];
+        const double t1 = (bx3[e] - ax) * (py - ay), c = by3[e] - ay;
+        // covered(x) = !((t1 - c * (x + .5 - ax)) + r < 0)
+        auto ok = [&](int x) { return !((t1 - c * ((double(x) + .5) - ax)) + r < 0); };
+        if (c > 0) { // true then false: last covered x
+            if (!ok(lo)) {
+                hi = lo - 1;
+                break;
+            }
+            int a = lo, b = hi;
+            while (a < b) {
+                const int m = a + (b - a + 1) / 2;
+                if (ok(m)) a = m;
+                else b = m - 1;
+            }
+            hi = a;
+        } else if (c < 0) { // false then true: first covered x
+            if (!ok(hi)) {
+                hi = lo - 1;
+                break;
+            }
+            int a = lo, b = hi;
+            while (a < b) {
+                const int m = a + (b - a) / 2;
+                if (ok(m)) b = m;
+                else a = m + 1;
+            }
+            lo = a;
+        } else if (!ok(lo)) {
+            hi = lo - 1;
+        }
+    }
+}
 
 __device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31; }
 
@@ -99,14 +145,16 @@ __device__ __forceinline__ uint32_t chunk_global(const uint32_t* bits, uint32_t 
     return v & size_mask(size, chunk);
 }
 
+// The candidate's coverage: the state's, with the region's flipped samples
+// (region words: candidate XOR state) applied.
 struct CandMask {
-    const uint32_t* state; // state coverage outside the region
+    const uint32_t* state;
     const uint32_t* region;
     uint32_t size, y0, y1, c0, words;
     __device__ uint32_t chunk(uint32_t row, uint32_t c) const {
-        if (row >= y0 && row <= y1 && c >= c0 && c < c0 + words)
-            return region[(row - y0) * words + (c - c0)] & size_mask(size, c);
-        return chunk_global(state, size, row, c);
+        const uint32_t w = chunk_global(state, size, row, c);
+        if (row >= y0 && row <= y1 && c >= c0 && c < c0 + words) return w ^ region[(row - y0) * words + (c - c0)];
+        return w;
     }
 };
 struct RefMask {
@@ -286,7 +334,7 @@ __device__ void audit_unit(const CandidateRecord* __restrict__ rec, const PlanDe
     }
     __syncwarp();
     int dchg = 0, dtot = 0, dcov = 0;
-    uint32_t qn = 0, region_changed = 0;
+    uint32_t qn = 0, region_changed = 0, nflips = 0;
     int region_words = 0;
     bool fallback = false;
     CandMask cmask;
@@ -306,48 +354,71 @@ __device__ void audit_unit(const CandidateRecord* __restrict__ rec, const PlanDe
         cmask.y0 = uint32_t(ry0), cmask.y1 = uint32_t(ry1), cmask.c0 = uint32_t(wx0 >> 5), cmask.words = uint32_t(words);
         const int bw = x1 - x0 + 1, bh = y1 - y0 + 1;
         const int bws = (bw + 15) & ~15; // delta map row stride: whole 16-byte vectors
-        if (words > kRegionWords || rows > kRegionRows || bws * bh > kDeltaSamples) {
+        // Sum of the faces' bbox areas: small units test every (face, sample
+        // of its bbox) into a byte difference map; the others sweep rows.
+        uint32_t area = 0;
+        if (lane < nok) area += uint32_t(ws.faces[lane].x1 - ws.faces[lane].x0 + 1) * uint32_t(ws.faces[lane].y1 - ws.faces[lane].y0 + 1);
+        if (lane + 32 < nok)
+            area += uint32_t(ws.faces[lane + 32].x1 - ws.faces[lane + 32].x0 + 1) *
+                    uint32_t(ws.faces[lane + 32].y1 - ws.faces[lane + 32].y0 + 1);
+        for (int o = 16; o; o >>= 1) area += __shfl_xor_sync(0xffffffffu, area, o);
+        const bool direct = area <= kDirectTests && uint32_t(bws) * uint32_t(bh) <= uint32_t(kDeltaSamples);
+        if (words > kRegionWords || rows > kRegionRows) {
             fallback = true;
         } else {
-            samples = uint64_t(rows) * words * 32;
-            // Phase 1: per (face, row) the covered samples form one interval:
-            // each edge term of the reference's test is monotone in x (IEEE
-            // rounding is monotone), so three binary searches over the same
-            // FP64 expressions find its ends exactly. Intervals are added to a
-            // per-sample byte difference map (biased by 128: at most 32 old
-            // and 32 new faces), which a per-row prefix scan turns into the
-            // candidate's count delta (new faces +1, old faces -1).
-            const uint32_t delta_words = uint32_t(bws * bh) >> 2;
-            for (uint32_t k = lane; k < delta_words; k += 32) ws.delta[k] = 0x80808080u;
-            // Small units test every (face, sample in its bbox) directly; large
-            // ones take the interval route below. Both give the same map.
-            uint32_t area = 0;
-            if (lane < nok) area += uint32_t(ws.faces[lane].x1 - ws.faces[lane].x0 + 1) * uint32_t(ws.faces[lane].y1 - ws.faces[lane].y0 + 1);
-            if (lane + 32 < nok)
-                area += uint32_t(ws.faces[lane + 32].x1 - ws.faces[lane + 32].x0 + 1) *
-                        uint32_t(ws.faces[lane + 32].y1 - ws.faces[lane + 32].y0 + 1);
-            for (int o = 16; o; o >>= 1) area += __shfl_xor_sync(0xffffffffu, area, o);
-            // (the small tier's regions are too small for intervals to pay)
-            const bool direct = L::kDeltaSamples <= 2048 || area <= kDirectTests;
-            uint32_t c0 = 0, c1 = 0;
-            if (lane < nok)
-                c0 = direct ? uint32_t(ws.faces[lane].x1 - ws.faces[lane].x0 + 1) * uint32_t(ws.faces[lane].y1 - ws.faces[lane].y0 + 1)
-                            : uint32_t(ws.faces[lane].y1 - ws.faces[lane].y0 + 1);
-            if (lane + 32 < nok)
-                c1 = direct ? uint32_t(ws.faces[lane + 32].x1 - ws.faces[lane + 32].x0 + 1) *
-                                  uint32_t(ws.faces[lane + 32].y1 - ws.faces[lane + 32].y0 + 1)
-                            : uint32_t(ws.faces[lane + 32].y1 - ws.faces[lane + 32].y0 + 1);
-            uint32_t i0 = c0, i1 = c1;
-            for (int o = 1; o < 32; o <<= 1) {
-                const uint32_t a = __shfl_up_sync(0xffffffffu, i0, o), b = __shfl_up_sync(0xffffffffu, i1, o);
-                if (lane >= uint32_t(o)) i0 += a, i1 += b;
-            }
-            const uint32_t tot0 = __shfl_sync(0xffffffffu, i0, 31);
-            if (lane < nok) ws.work[lane] = i0 - c0;
-            if (lane + 32 < nok) ws.work[lane + 32] = tot0 + i1 - c1;
-            const uint32_t items = tot0 + __shfl_sync(0xffffffffu, i1, 31);
+            samples = uint64_t(rows) * uint64_t(words) * 32;
+            // ws.region holds the candidate's coverage words XOR the state's
+            // over the region (its flipped samples).
+            const int nwords = rows * words;
+            for (int k = int(lane); k < nwords; k += 32) ws.region[k] = 0;
+            if (lane == 0) ws.qcount[0] = 0;
             __syncwarp();
+            bool negative = false;
+            int flips = 0;
+            // A sample whose count changes by dv (state count pc): it flips
+            // where covered-ness changes; each flip moves the popcounts
+            // against the reference by one sample. With the state equal to
+            // the reference every changed sample of the region is a flip, and
+            // flips go to the queue for the distance phase (bit 31: covered by
+            // the candidate).
+            auto visit = [&](int x, int y, int dv, int pc, bool shared_rows) {
+                const int cc = pc + dv;
+                negative |= cc < 0;
+                if ((cc > 0) == (pc > 0)) return;
+                const bool P = pc > 0, C = !P;
+                const bool R = same_ref ? P : pv_ref_bit(pv.ref_bits, size_t(y) * size + size_t(x));
+                dcov += C ? 1 : -1;
+                dchg += int(C != R) - int(P != R);
+                dtot += int(C || R) - int(P || R);
+                const uint32_t xr = uint32_t(x - wx0), yr = uint32_t(y - ry0);
+                uint32_t* word = &ws.region[yr * uint32_t(words) + (xr >> 5)];
+                if (shared_rows) atomicXor(word, 1u << (xr & 31));
+                else *word ^= 1u << (xr & 31);
+                ++flips;
+                if (same_ref) {
+                    const uint32_t pos = atomicAdd(&ws.qcount[0], 1u);
+                    if (pos < uint32_t(kQueue)) ws.queue[pos] = xr | (yr << 15) | (C ? 0x80000000u : 0u);
+                }
+            };
             if (direct) {
+                const uint32_t delta_words = uint32_t(bws * bh) >> 2;
+                for (uint32_t k = lane; k < delta_words; k += 32) ws.delta[k] = 0x80808080u;
+                uint32_t c0 = 0, c1 = 0;
+                if (lane < nok)
+                    c0 = uint32_t(ws.faces[lane].x1 - ws.faces[lane].x0 + 1) * uint32_t(ws.faces[lane].y1 - ws.faces[lane].y0 + 1);
+                if (lane + 32 < nok)
+                    c1 = uint32_t(ws.faces[lane + 32].x1 - ws.faces[lane + 32].x0 + 1) *
+                         uint32_t(ws.faces[lane + 32].y1 - ws.faces[lane + 32].y0 + 1);
+                uint32_t i0 = c0, i1 = c1;
+                for (int o = 1; o < 32; o <<= 1) {
+                    const uint32_t a = __shfl_up_sync(0xffffffffu, i0, o), b = __shfl_up_sync(0xffffffffu, i1, o);
+                    if (lane >= uint32_t(o)) i0 += a, i1 += b;
+                }
+                const uint32_t tot0 = __shfl_sync(0xffffffffu, i0, 31);
+                if (lane < nok) ws.work[lane] = i0 - c0;
+                if (lane + 32 < nok) ws.work[lane + 32] = tot0 + i1 - c1;
+                const uint32_t items = tot0 + __shfl_sync(0xffffffffu, i1, 31);
+                __syncwarp();
                 for (uint32_t t = lane; t < items; t += 32) {
                     uint32_t f = 0; // last face whose prefix is <= t
                     for (uint32_t step = 32; step; step >>= 1)
@@ -362,140 +433,82 @@ __device__ void audit_unit(const CandidateRecord* __restrict__ rec, const PlanDe
                         else atomicSub(&ws.delta[d >> 2], unit);
                     }
                 }
-            }
-            uint32_t f = 0;
-            for (uint32_t t = direct ? items : lane; t < items; t += 32) {
-                while (f + 1 < nok && ws.work[f + 1] <= t) ++f;
-                const FaceSetup& s = ws.faces[f];
-                const int fy = s.y0 + int(t - ws.work[f]);
-                int lo = s.x0, hi = s.x1;
-                const double py = double(fy) + .5;
-                // edge (d, e), edge (e, a), edge (a, d) of face_covers
-                const double ax3[3] = {s.dx, s.ex, s.ax}, ay3[3] = {s.dy, s.ey, s.ay};
-                const double bx3[3] = {s.ex, s.ax, s.dx}, by3[3] = {s.ey, s.ay, s.dy};
-                const double r3[3] = {s.r0, s.r1, s.r2};
-                for (int e = 0; e < 3 && lo <= hi; ++e) {
-                    const double ax = ax3[e], ay = ay3[e], r = r3[e];
-                    const double t1 = (bx3[e] - ax) * (py - ay), c = by3[e] - ay;
-                    // covered(x) = !((t1 - c * (x + .5 - ax)) + r < 0)
-                    auto ok = [&](int x) { return !((t1 - c * ((double(x) + .5) - ax)) + r < 0); };
-                    if (c > 0) { // true then false: last covered x
-                        if (!ok(lo)) { hi = lo - 1; break; }
-                        int a = lo, b = hi;
-                        while (a < b) {
-                            const int m = a + (b - a + 1) / 2;
-                            if (ok(m)) a = m;
-                            else b = m - 1;
-                        }
-                        hi = a;
-                    } else if (c < 0) { // false then true: first covered x
-                        if (!ok(hi)) { hi = lo - 1; break; }
-                        int a = lo, b = hi;
-                        while (a < b) {
-                            const int m = a + (b - a) / 2;
-                            if (ok(m)) b = m;
-                            else a = m + 1;
-                        }
-                        lo = a;
-                    } else if (!ok(lo)) {
-                        hi = lo - 1;
+                __syncwarp();
+                const float inv_bws = 1.0f / float(bws);
+                for (uint32_t k = lane; k < delta_words; k += 32) {
+                    const uint32_t dw = ws.delta[k];
+                    if (dw == 0x80808080u) continue;
+                    for (uint32_t j = 0; j < 4; ++j) {
+                        const int dv = int((dw >> (8 * j)) & 0xffu) - 128;
+                        const uint32_t d = 4 * k + j;
+                        if (!dv) continue;
+                        uint32_t q = uint32_t(float(d) * inv_bws); // row in the bbox, corrected below
+                        while (q * uint32_t(bws) > d) --q;
+                        while ((q + 1) * uint32_t(bws) <= d) ++q;
+                        if (d - q * uint32_t(bws) >= uint32_t(bw)) continue; // row padding
+                        const int y = y0 + int(q), x = x0 + int(d - q * uint32_t(bws));
+                        visit(x, y, dv, int(pv.state_count[size_t(y) * size + size_t(x)]), true);
                     }
                 }
-                if (lo <= hi) {
-                    const uint32_t row = uint32_t(fy - y0) * uint32_t(bws);
-                    const uint32_t d0 = row + uint32_t(lo - x0);
-                    const uint32_t u0 = 1u << (8 * (d0 & 3));
-                    if (s.pad > 0) atomicAdd(&ws.delta[d0 >> 2], u0);
-                    else atomicSub(&ws.delta[d0 >> 2], u0);
-                    if (hi < x1) {
-                        const uint32_t d1 = row + uint32_t(hi + 1 - x0);
-                        const uint32_t u1 = 1u << (8 * (d1 & 3));
-                        if (s.pad > 0) atomicSub(&ws.delta[d1 >> 2], u1);
-                        else atomicAdd(&ws.delta[d1 >> 2], u1);
-                    }
-                }
-            }
-            __syncwarp();
-            // Row prefix sums: difference map -> per-sample delta (bias kept).
-            if (!direct) {
-                // one row per lane, 16 samples per vector load
-                for (int ry = int(lane); ry < bh; ry += 32) {
-                    uint4* rowp = reinterpret_cast<uint4*>(ws.delta) + size_t(ry) * uint32_t(bws >> 4);
-                    int carry = 0;
-                    for (int c = 0; c < (bws >> 4); ++c) {
-                        uint4 v = rowp[c];
-                        uint32_t* w4 = reinterpret_cast<uint32_t*>(&v);
-                        for (int q = 0; q < 4; ++q) {
-                            uint32_t out = 0;
-                            for (int b = 0; b < 4; ++b) {
-                                carry += int((w4[q] >> (8 * b)) & 0xffu) - 128;
-                                out |= uint32_t(carry + 128) << (8 * b);
-                            }
-                            w4[q] = out;
+            } else {
+                // Row sweep, one bbox row per lane. Per face crossing the row
+                // the covered samples form one interval: each edge term of
+                // the reference's test is monotone in x (IEEE rounding is
+                // monotone), so binary searches over the same FP64
+                // expressions find its ends exactly. The sorted interval ends
+                // (+1 at a new face's start and an old face's end, -1 at the
+                // others) give the count delta piecewise; only samples of
+                // pieces with a non-zero delta read their state count (four
+                // per load).
+                for (int y = y0 + int(lane); y <= y1; y += 32) {
+                    uint32_t ev[2 * kMaxOk];
+                    int n = 0;
+                    auto insert = [&](uint32_t e) {
+                        int i = n++;
+                        while (i > 0 && ev[i - 1] > e) {
+                            ev[i] = ev[i - 1];
+                            --i;
                         }
-                        rowp[c] = v;
+                        ev[i] = e;
+                    };
+                    const double py = double(y) + .5;
+                    for (uint32_t f = 0; f < nok; ++f) {
+                        const FaceSetup& s = ws.faces[f];
+                        if (y < s.y0 || y > s.y1) continue;
+                        int lo, hi;
+                        face_interval(s, py, lo, hi);
+                        if (lo > hi) continue;
+                        const uint32_t up = s.pad > 0 ? 1u : 0u;
+                        insert((uint32_t(lo) << 1) | up);
+                        insert((uint32_t(hi + 1) << 1) | (up ^ 1u));
                     }
-                }
-            }
-            __syncwarp();
-            // Phase 2: the candidate's coverage words over the region start as
-            // the state's words (independent word loads, 32 per warp
-            // iteration); only samples with a non-zero count delta read their
-            // state count, and their bit flips where covered-ness changes.
-            const int nwords = rows * words;
-            const uint32_t cbase = uint32_t(wx0 >> 5);
-            for (int k = int(lane); k < nwords; k += 32)
-                ws.region[k] = chunk_global(pv.state_bits, size, uint32_t(ry0 + k / words), cbase + uint32_t(k % words));
-            __syncwarp();
-            const float inv_bws = 1.0f / float(bws);
-            bool negative = false;
-            for (uint32_t k = lane; k < delta_words; k += 32) {
-                const uint32_t dw = ws.delta[k];
-                if (dw == 0x80808080u) continue;
-                for (uint32_t j = 0; j < 4; ++j) {
-                    const int dv = int((dw >> (8 * j)) & 0xffu) - 128;
-                    const uint32_t d = 4 * k + j;
-                    if (!dv) continue;
-                    uint32_t q = uint32_t(float(d) * inv_bws); // row in the bbox, corrected below
-                    while (q * uint32_t(bws) > d) --q;
-                    while ((q + 1) * uint32_t(bws) <= d) ++q;
-                    if (d - q * uint32_t(bws) >= uint32_t(bw)) continue; // row padding
-                    const int y = y0 + int(q), x = x0 + int(d - q * uint32_t(bws));
-                    const int pc = int(pv.state_count[size_t(y) * size + size_t(x)]);
-                    const int cc = pc + dv;
-                    negative |= cc < 0;
-                    if ((cc > 0) != (pc > 0))
-                        atomicXor(&ws.region[(y - ry0) * words + ((x - wx0) >> 5)], 1u << ((x - wx0) & 31));
+                    int acc = 0;
+                    for (int i = 0; i < n; ++i) {
+                        acc += (ev[i] & 1u) ? 1 : -1;
+                        if (!acc) continue;
+                        const int xa = int(ev[i] >> 1), xb = i + 1 < n ? int(ev[i + 1] >> 1) : x1 + 1;
+                        for (int x = xa; x < xb;) {
+                            // the aligned 4-byte word of counts holding x (view
+                            // buffers start 4-aligned and are padded to 4)
+                            const size_t at = size_t(y) * size + size_t(x);
+                            const uint32_t w4 = *reinterpret_cast<const uint32_t*>(pv.state_count + (at & ~size_t(3)));
+                            for (uint32_t j = uint32_t(at & 3); j < 4 && x < xb; ++j, ++x)
+                                visit(x, y, acc, int((w4 >> (8 * j)) & 0xffu), false);
+                        }
+                    }
                 }
             }
             if (__any_sync(0xffffffffu, negative)) fallback = true;
-            __syncwarp();
-            // Popcount deltas against the reference, one region word per lane;
-            // the distance phase walks the same words for the changed samples.
-            region_words = nwords;
-            for (int base = 0; base < nwords; base += 32) {
-                const int k = base + int(lane);
-                uint32_t Cw = 0, Rw = 0;
-                int ry = 0, cw = 0;
-                if (k < nwords) {
-                    ry = ry0 + k / words, cw = k % words;
-                    const uint32_t Pw = chunk_global(pv.state_bits, size, uint32_t(ry), cbase + uint32_t(cw));
-                    Cw = ws.region[k];
-                    Rw = same_ref ? Pw : chunk_global(pv.ref_bits, size, uint32_t(ry), cbase + uint32_t(cw));
-                    if (Cw != Pw) {
-                        dchg += __popc(Cw ^ Rw) - __popc(Pw ^ Rw);
-                        dtot += __popc(Cw | Rw) - __popc(Pw | Rw);
-                        dcov += __popc(Cw) - __popc(Pw);
-                    }
-                }
-                region_changed += __popc(Cw ^ Rw);
-            }
             for (int o = 16; o; o >>= 1) {
                 dchg += __shfl_xor_sync(0xffffffffu, dchg, o);
                 dtot += __shfl_xor_sync(0xffffffffu, dtot, o);
                 dcov += __shfl_xor_sync(0xffffffffu, dcov, o);
-                region_changed += __shfl_xor_sync(0xffffffffu, region_changed, o);
+                flips += __shfl_xor_sync(0xffffffffu, flips, o);
             }
+            __syncwarp();
+            region_words = nwords;
+            nflips = uint32_t(flips);
+            region_changed = nflips;
             // A unit with many changed samples goes to the next tier when
             // that one runs more warps per SM.
             if (spill && region_changed > heavy) fallback = true;
@@ -591,56 +604,77 @@ __device__ void audit_unit(const CandidateRecord* __restrict__ rec, const PlanDe
             }
         }
         __syncwarp();
-        // Changed samples of the region, straight from its coverage words, 32
-        // words per round: the round's masks and a prefix of their counts go
-        // to shared memory and every lane takes samples by rank.
-        // Candidate-only samples measure to the reference (resident field or
-        // search), reference-only samples search the candidate.
-        const uint32_t cbase = uint32_t(wx0 >> 5);
-        uint32_t* rmask_s = ws.queue;       // 32 xor masks (the queue is consumed)
-        uint32_t* cmask_s = ws.queue + 32;  // 32 candidate words
-        uint32_t* pre = ws.work;            // 33 prefix counts
-        for (int base = 0; base < region_words; base += 32) {
-            const int k = base + int(lane);
-            uint32_t xm = 0, Cw = 0;
-            if (k < region_words) {
-                Cw = ws.region[k];
-                xm = Cw ^ chunk_global(same_ref ? pv.state_bits : pv.ref_bits, size, uint32_t(ry0 + k / words),
-                                       cbase + uint32_t(k % words));
+        const uint32_t queued = same_ref ? nflips : 0;
+        if (same_ref && queued <= uint32_t(kQueue)) {
+            // The region's changed samples are its flips, queued in phase 2.
+            // Candidate-only samples measure to the reference (resident field
+            // or search), reference-only samples search the candidate.
+            for (uint32_t base = 0; base < queued; base += 32) {
+                const uint32_t k = base + lane;
+                if (k < queued) {
+                    const uint32_t e = ws.queue[k];
+                    const uint32_t x = uint32_t(wx0) + (e & 0x7fffu), y = uint32_t(ry0) + ((e >> 15) & 0x7fffu);
+                    uint32_t d;
+                    if (e >> 31) d = pv.ref_field ? pv.ref_field[size_t(y) * size + x] : nearest_d2(rmask, x, y, best);
+                    else d = nearest_d2(cmask, x, y, best);
+                    best = d > best ? d : best;
+                }
+                for (int o = 16; o; o >>= 1) {
+                    const uint32_t y = __shfl_xor_sync(0xffffffffu, best, o);
+                    best = y > best ? y : best;
+                }
             }
-            if (!__any_sync(0xffffffffu, xm != 0)) continue; // no changed sample in these 32 words
-            const uint32_t cnt = __popc(xm);
-            uint32_t incl = cnt;
-            for (int o = 1; o < 32; o <<= 1) {
-                const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
-                if (lane >= uint32_t(o)) incl += t;
+        } else {
+            // Changed samples of the region from its coverage words, 32 words
+            // per round: the round's masks and a prefix of their counts go to
+            // shared memory and every lane takes samples by rank.
+            const uint32_t cbase = uint32_t(wx0 >> 5);
+            uint32_t* rmask_s = ws.queue;       // 32 xor masks (the queue is consumed)
+            uint32_t* cmask_s = ws.queue + 32;  // 32 candidate words
+            uint32_t* pre = ws.work;            // 33 prefix counts
+            for (int base = 0; base < region_words; base += 32) {
+                const int k = base + int(lane);
+                uint32_t xm = 0, Cw = 0;
+                if (k < region_words) {
+                    const uint32_t row = uint32_t(ry0 + k / words), cw = cbase + uint32_t(k % words);
+                    const uint32_t Sw = chunk_global(pv.state_bits, size, row, cw);
+                    Cw = Sw ^ ws.region[k];
+                    xm = Cw ^ (same_ref ? Sw : chunk_global(pv.ref_bits, size, row, cw));
+                }
+                if (!__any_sync(0xffffffffu, xm != 0)) continue; // no changed sample in these 32 words
+                const uint32_t cnt = __popc(xm);
+                uint32_t incl = cnt;
+                for (int o = 1; o < 32; o <<= 1) {
+                    const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+                    if (lane >= uint32_t(o)) incl += t;
+                }
+                rmask_s[lane] = xm;
+                cmask_s[lane] = Cw;
+                pre[lane + 1] = incl;
+                if (lane == 0) pre[0] = 0;
+                const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
+                __syncwarp();
+                for (uint32_t j = lane; j < total; j += 32) {
+                    uint32_t w = 0; // last word whose prefix is <= j
+                    for (uint32_t step = 16; step; step >>= 1)
+                        if (pre[w + step] <= j) w += step;
+                    const uint32_t m = rmask_s[w];
+                    const uint32_t bit = __fns(m, 0, int(j - pre[w]) + 1);
+                    const int kw = base + int(w);
+                    const uint32_t ry = uint32_t(ry0 + kw / words), cw = uint32_t(kw % words);
+                    const uint32_t x = uint32_t(wx0) + 32 * cw + bit;
+                    uint32_t d;
+                    if ((cmask_s[w] >> bit) & 1u)
+                        d = pv.ref_field ? pv.ref_field[size_t(ry) * size + x] : nearest_d2(rmask, x, ry, best);
+                    else d = nearest_d2(cmask, x, ry, best);
+                    best = d > best ? d : best;
+                }
+                for (int o = 16; o; o >>= 1) {
+                    const uint32_t y = __shfl_xor_sync(0xffffffffu, best, o);
+                    best = y > best ? y : best;
+                }
+                __syncwarp();
             }
-            rmask_s[lane] = xm;
-            cmask_s[lane] = Cw;
-            pre[lane + 1] = incl;
-            if (lane == 0) pre[0] = 0;
-            const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
-            __syncwarp();
-            for (uint32_t j = lane; j < total; j += 32) {
-                uint32_t w = 0; // last word whose prefix is <= j
-                for (uint32_t step = 16; step; step >>= 1)
-                    if (pre[w + step] <= j) w += step;
-                const uint32_t m = rmask_s[w];
-                const uint32_t bit = __fns(m, 0, int(j - pre[w]) + 1);
-                const int kw = base + int(w);
-                const uint32_t ry = uint32_t(ry0 + kw / words), cw = uint32_t(kw % words);
-                const uint32_t x = uint32_t(wx0) + 32 * cw + bit;
-                uint32_t d;
-                if ((cmask_s[w] >> bit) & 1u)
-                    d = pv.ref_field ? pv.ref_field[size_t(ry) * size + x] : nearest_d2(rmask, x, ry, best);
-                else d = nearest_d2(cmask, x, ry, best);
-                best = d > best ? d : best;
-            }
-            for (int o = 16; o; o >>= 1) {
-                const uint32_t y = __shfl_xor_sync(0xffffffffu, best, o);
-                best = y > best ? y : best;
-            }
-            __syncwarp();
         }
     }
     r.max_d2 = best;
