@@ -461,6 +461,11 @@ def run_icosphere(args, rank: int, world: int, local: int) -> dict:
     return line
 
 
+def _shares(values) -> list:
+    total = float(sum(values))
+    return [round(v / total, 4) if total else 0.0 for v in values]
+
+
 def _barrier(world: int) -> None:
     if world > 1:
         import torch.distributed as dist
@@ -578,7 +583,14 @@ def run_batched(args, rank: int, world: int, local: int) -> dict:
                          "kernel": "k_audit (+ large and huge tiers)", "kernel_ms": info["audit_ms"],
                          "algorithmic_bytes": alg_bytes, "units_per_launch": info["units"],
                          "samples_per_launch": info["region_samples"],
-                         "peak_source": pk["source"] + " hbm_gbs (burst)"},
+                         "peak_source": pk["source"] + " hbm_gbs (burst)",
+                         "tiers": {"units": dict(zip(("warp", "large", "huge", "giant"), info["tier_units"])),
+                                   "warp_busy_share": dict(zip(("warp", "large", "huge", "giant"),
+                                                               _shares(info["tier_cycles"]))),
+                                   "phase_share": dict(zip(("setup", "region", "distance"),
+                                                           _shares(info["phase_cycles"]))),
+                                   "flipped_samples": info["flipped_samples"],
+                                   "note": "SM cycles of each unit's warp, summed per tier and per phase"}},
             "clocks": clocks.summary(),
             "e2e": {"value": n * world * args.steps / e2e_s, "unit": "collapses/s",
                     "h2d_bytes_per_step": int(n * br.COLLAPSE_DTYPE.itemsize),

@@ -222,7 +222,9 @@ class BatchInfo(C.Structure):
     _fields_ = [("struct_size", C.c_uint32), ("sessions", C.c_uint32), ("tier", C.c_uint32), ("tuned", C.c_uint32),
                 ("graph_captured", C.c_uint32), ("tune_ms", C.c_float * 4), ("graph_launches", C.c_uint64),
                 ("exact_candidates", C.c_uint64), ("audit_ms", C.c_float), ("units", C.c_uint64),
-                ("region_samples", C.c_uint64), ("changed_samples", C.c_uint64)]
+                ("region_samples", C.c_uint64), ("changed_samples", C.c_uint64),
+                ("tier_units", C.c_uint64 * 4), ("tier_cycles", C.c_uint64 * 4), ("phase_cycles", C.c_uint64 * 3),
+                ("flipped_samples", C.c_uint64)]
 
 
 BATCH_GRAPH, BATCH_AUTOTUNE, BATCH_PROFILE = 1, 2, 4
@@ -563,7 +565,8 @@ class AuditBatch:
         i.struct_size = C.sizeof(BatchInfo)
         assert self.lib.blitz_audit_batch_read_info(self.handle, C.byref(i)) == BLITZ_OK
         d = {k: getattr(i, k) for k, _ in i._fields_ if k != "struct_size"}
-        d["tune_ms"] = list(i.tune_ms)
+        for k in ("tune_ms", "tier_units", "tier_cycles", "phase_cycles"):
+            d[k] = list(getattr(i, k))
         return d
 
 

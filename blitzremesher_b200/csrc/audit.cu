@@ -164,65 +164,92 @@ struct RefMask {
 };
 
 // Smallest |dx| <= maxdx with a covered sample at (x+dx, row); kNone if none.
+// The two sides are scanned one chunk each per step, outward, so the scan
+// ends near the nearest covered sample instead of at a row end.
 template <class M> __device__ uint32_t nearest_in_row(const M& mask, uint32_t row, uint32_t x, uint32_t maxdx) {
-    uint32_t cx = x >> 5, bx = x & 31, best = kNone;
-    uint32_t w = mask.chunk(row, cx);
-    uint32_t left = w & (bx == 31 ? 0xffffffffu : ((2u << bx) - 1u));
-    uint32_t right = w & (0xffffffffu << bx);
+    const uint32_t cx = x >> 5, bx = x & 31;
+    uint32_t best = kNone;
+    const uint32_t w = mask.chunk(row, cx);
+    const uint32_t left = w & (bx == 31 ? 0xffffffffu : ((2u << bx) - 1u));
+    const uint32_t right = w & (0xffffffffu << bx);
     if (left) best = bx - (31 - __clz(left));
     if (right) {
-        uint32_t d = (__ffs(right) - 1) - bx;
+        const uint32_t d = (__ffs(right) - 1) - bx;
         best = d < best ? d : best;
     }
     if (best == 0) return 0;
-    for (uint32_t c = cx; c-- > 0;) {
-        uint32_t nearest = x - (c * 32 + 31);
-        if (nearest > maxdx || nearest >= best) break;
-        uint32_t v = mask.chunk(row, c);
-        if (v) {
-            uint32_t d = x - (c * 32 + (31 - __clz(v)));
-            best = d < best ? d : best;
-            break;
+    const uint32_t chunks = (mask.size + 31) >> 5;
+    bool go_left = cx > 0, go_right = cx + 1 < chunks;
+    for (uint32_t k = 1; go_left || go_right; ++k) {
+        if (go_left) {
+            const uint32_t c = cx - k;
+            const uint32_t nearest = x - (c * 32 + 31);
+            if (nearest > maxdx || nearest >= best) {
+                go_left = false;
+            } else {
+                const uint32_t v = mask.chunk(row, c);
+                if (v) {
+                    const uint32_t d = x - (c * 32 + (31 - __clz(v)));
+                    best = d < best ? d : best;
+                    go_left = false;
+                } else if (c == 0) {
+                    go_left = false;
+                }
+            }
         }
-    }
-    uint32_t chunks = (mask.size + 31) >> 5;
-    for (uint32_t c = cx + 1; c < chunks; ++c) {
-        uint32_t nearest = c * 32 - x;
-        if (nearest > maxdx || nearest >= best) break;
-        uint32_t v = mask.chunk(row, c);
-        if (v) {
-            uint32_t d = c * 32 + (__ffs(v) - 1) - x;
-            best = d < best ? d : best;
-            break;
+        if (go_right) {
+            const uint32_t c = cx + k;
+            const uint32_t nearest = c * 32 - x;
+            if (nearest > maxdx || nearest >= best) {
+                go_right = false;
+            } else {
+                const uint32_t v = mask.chunk(row, c);
+                if (v) {
+                    const uint32_t d = c * 32 + (__ffs(v) - 1) - x;
+                    best = d < best ? d : best;
+                    go_right = false;
+                } else if (c + 1 >= chunks) {
+                    go_right = false;
+                }
+            }
         }
     }
     return best <= maxdx ? best : kNone;
 }
 
-// Exact squared Euclidean distance from (x, y) to the nearest covered sample,
-// or any value <= `enough` once a covered sample that close is found (the
-// caller only needs distances above `enough`: the running maximum).
+// Exact squared Euclidean distance from (x, y) to the nearest covered sample
+// (kNone: none), or any value <= `enough` once a covered sample that close is
+// found (the caller only needs distances above `enough`: the running
+// maximum). The search runs in boxes of half-width R = 32, 128, ...: rows
+// are scanned up to R columns until a covered sample is found, and then
+// within its distance; a result <= R^2 (or <= enough) is final, since every
+// sample left out of the box is farther than R.
 template <class M> __device__ uint32_t nearest_d2(const M& mask, uint32_t x, uint32_t y, uint32_t enough = 0) {
     const uint32_t size = mask.size;
-    uint32_t best = kNone;
-    for (uint32_t dy = 0;; ++dy) {
-        uint64_t dy2 = uint64_t(dy) * dy;
-        if (best != kNone && (dy2 >= best || best <= enough)) break;
-        bool any = false;
-        for (int side = 0; side < (dy ? 2 : 1); ++side) {
-            int64_t row = side ? int64_t(y) + dy : int64_t(y) - dy;
-            if (row < 0 || row >= int64_t(size)) continue;
-            any = true;
-            uint32_t maxdx = best == kNone ? size : uint32_t(sqrtf(float(best - dy2))) + 1;
-            uint32_t dx = nearest_in_row(mask, uint32_t(row), x, maxdx);
-            if (dx != kNone) {
-                uint64_t d = uint64_t(dx) * dx + dy2;
-                if (d < best) best = uint32_t(d);
+    for (uint32_t R = 32;; R *= 4) {
+        const bool last = R >= size;
+        uint32_t best = kNone;
+        for (uint32_t dy = 0;; ++dy) {
+            const uint64_t dy2 = uint64_t(dy) * dy;
+            if (best != kNone && (dy2 >= best || best <= enough)) break;
+            if (best == kNone && !last && dy > R) break;
+            bool any = false;
+            for (int side = 0; side < (dy ? 2 : 1); ++side) {
+                const int64_t row = side ? int64_t(y) + dy : int64_t(y) - dy;
+                if (row < 0 || row >= int64_t(size)) continue;
+                any = true;
+                const uint32_t maxdx =
+                    best == kNone ? (last ? size : R) : uint32_t(sqrtf(float(best - dy2))) + 1;
+                const uint32_t dx = nearest_in_row(mask, uint32_t(row), x, maxdx);
+                if (dx != kNone) {
+                    const uint64_t d = uint64_t(dx) * dx + dy2;
+                    if (d < best) best = uint32_t(d);
+                }
             }
+            if (!any) break;
         }
-        if (!any) break;
+        if (last || (best != kNone && (best <= enough || uint64_t(best) <= uint64_t(R) * R))) return best;
     }
-    return best;
 }
 
 __device__ __forceinline__ bool pv_ref_bit(const uint32_t* bits, size_t i) { return (bits[i >> 5] >> (i & 31)) & 1u; }
@@ -240,6 +267,7 @@ __device__ void audit_unit(const CandidateRecord* __restrict__ rec, const PlanDe
     constexpr int kRegionWords = L::kRegionWords, kRegionRows = L::kRegionRows;
     constexpr int kDeltaSamples = L::kDeltaSamples, kQueue = L::kQueue, kAffected = L::kAffected;
     const uint32_t lane = lane_id();
+    const long long t_start = stats ? clock64() : 0;
     const PlanView pv = plan.views[v];
     const uint32_t size = plan.size;
     ViewRecord r;
@@ -333,6 +361,7 @@ __device__ void audit_unit(const CandidateRecord* __restrict__ rec, const PlanDe
         y1 = max(y1, __shfl_xor_sync(0xffffffffu, y1, o));
     }
     __syncwarp();
+    const long long t_setup = stats ? clock64() : 0;
     int dchg = 0, dtot = 0, dcov = 0;
     uint32_t qn = 0, region_changed = 0, nflips = 0;
     int region_words = 0;
@@ -579,6 +608,7 @@ __device__ void audit_unit(const CandidateRecord* __restrict__ rec, const PlanDe
         }
         __syncwarp();
     }
+    const long long t_region = stats ? clock64() : 0;
     r.changed = uint32_t(int64_t(pv.changed) + dchg);
     r.total = uint32_t(int64_t(pv.total) + dtot);
     r.cb = int64_t(pv.cov_state) + dcov > 0;
@@ -684,9 +714,20 @@ __device__ void audit_unit(const CandidateRecord* __restrict__ rec, const PlanDe
         if (fallback && spill) spill[1 + atomicAdd(spill, 1u)] = u;
         *out = r;
         if (stats) {
+            // profiling counters (kAuditStats slots): units, region samples,
+            // searched samples; per tier units and SM cycles; SM cycles of the
+            // face setup, the region phases and the distance phase; flips
+            const long long t_end = clock64();
+            constexpr int tier = L::kRegionRows <= 128 ? 0 : L::kRegionRows <= 256 ? 1 : L::kRegionRows <= 1024 ? 2 : 3;
             atomicAdd(stats, 1ull);
             atomicAdd(stats + 1, (unsigned long long)samples);
             atomicAdd(stats + 2, (unsigned long long)(qn + region_changed));
+            atomicAdd(stats + 3 + tier, 1ull);
+            atomicAdd(stats + 7 + tier, (unsigned long long)(t_end - t_start));
+            atomicAdd(stats + 11, (unsigned long long)(t_setup - t_start));
+            atomicAdd(stats + 12, (unsigned long long)(t_region - t_setup));
+            atomicAdd(stats + 13, (unsigned long long)(t_end - t_region));
+            atomicAdd(stats + 14, (unsigned long long)nflips);
         }
     }
     __syncwarp();

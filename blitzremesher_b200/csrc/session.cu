@@ -1070,8 +1070,8 @@ static void audit_candidates(Session& S, const blitz_collapse* cands_dev, const 
     S.records.ensure(S.pool, nn);
     const bool prof = S.profiling && nn;
     if (prof) {
-        S.stats.ensure(S.pool, 4);
-        B200_CUDA(cudaMemsetAsync(S.stats.p, 0, 32, st));
+        S.stats.ensure(S.pool, kAuditStats);
+        B200_CUDA(cudaMemsetAsync(S.stats.p, 0, kAuditStats * 8, st));
         B200_CUDA(cudaEventRecord(S.ev[0], st));
     }
     launch_prepare(S.state.view, t.view, S.state.view, t.view, cands_dev, nn, t.positions.p, t.pos_cap, t.flat.p,
@@ -2330,7 +2330,7 @@ struct blitz_audit_batch {
     Buf<unsigned long long> stats;
     cudaEvent_t ev[2] = {nullptr, nullptr};
     float audit_ms = 0;
-    unsigned long long prof[3] = {0, 0, 0};
+    unsigned long long prof[kAuditStats] = {};
     ~blitz_audit_batch() {
         for (auto e : ev)
             if (e) cudaEventDestroy(e);
@@ -2443,7 +2443,7 @@ blitz_status blitz_audit_batch_candidates(blitz_audit_batch* b, const blitz_coll
         // The launch sequence: per-session records, one audit job per plan
         // slot over all sessions, per-session verdicts.
         if (profile && !b->stats.p) {
-            b->stats = Buf<unsigned long long>(b->pool, 4);
+            b->stats = Buf<unsigned long long>(b->pool, kAuditStats);
             B200_CUDA(cudaEventCreate(&b->ev[0]));
             B200_CUDA(cudaEventCreate(&b->ev[1]));
         }
@@ -2457,7 +2457,7 @@ blitz_status blitz_audit_batch_candidates(blitz_audit_batch* b, const blitz_coll
                                st, t.uv());
             }
             if (profile) {
-                cudaMemsetAsync(b->stats.p, 0, 32, st);
+                cudaMemsetAsync(b->stats.p, 0, kAuditStats * 8, st);
                 cudaEventRecord(b->ev[0], st);
             }
             for (size_t j = 0; j < slots; ++j) {
@@ -2570,6 +2570,9 @@ blitz_status blitz_audit_batch_read_info(const blitz_audit_batch* b, blitz_audit
     out->units = b->prof[0];
     out->region_samples = b->prof[1];
     out->changed_samples = b->prof[2];
+    for (int k = 0; k < 4; ++k) out->tier_units[k] = b->prof[3 + k], out->tier_cycles[k] = b->prof[7 + k];
+    for (int k = 0; k < 3; ++k) out->phase_cycles[k] = b->prof[11 + k];
+    out->flipped_samples = b->prof[14];
     return BLITZ_OK;
 }
 

@@ -339,6 +339,10 @@ typedef struct blitz_audit_batch_info {
      * samples measured */
     float audit_ms;
     uint64_t units, region_samples, changed_samples;
+    /* the same call, per tier (warp, large, huge, giant): units audited and
+     * the SM cycles their warps spent; SM cycles of all units' face setup,
+     * region phases and distance phase; samples whose coverage flipped */
+    uint64_t tier_units[4], tier_cycles[4], phase_cycles[3], flipped_samples;
 } blitz_audit_batch_info;
 blitz_status blitz_audit_batch_create(blitz_audit_session* const* sessions, size_t count, blitz_audit_batch** out,
                                       char* error, size_t error_capacity);
