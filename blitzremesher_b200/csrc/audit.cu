@@ -263,7 +263,10 @@ __device__ __forceinline__ void record_write(ViewRecord* out, const ViewRecord& 
 template <class L>
 __device__ void audit_unit(const CandidateRecord* __restrict__ rec, const PlanDev& plan, uint32_t v,
                            WarpScratch<L>& ws, ViewRecord* out, unsigned long long* stats, uint32_t u,
-                           uint32_t* spill, uint32_t heavy = 0xffffffffu) {
+                           uint32_t* spill, uint32_t heavy = 0xffffffffu, FaceSetup* face_table = nullptr) {
+    // The face setups: in the warp's scratch, or in shared memory for the
+    // tiers whose scratch is global (the row sweep reads them every row).
+    FaceSetup* const faces = face_table ? face_table : ws.faces;
     constexpr int kRegionWords = L::kRegionWords, kRegionRows = L::kRegionRows;
     constexpr int kDeltaSamples = L::kDeltaSamples, kQueue = L::kQueue, kAffected = L::kAffected;
     const uint32_t lane = lane_id();
@@ -295,7 +298,7 @@ __device__ void audit_unit(const CandidateRecord* __restrict__ rec, const PlanDe
     }
     __syncwarp();
     // Face setups, old faces first, then the candidate's faces; the rasterized
-    // ones are compacted into ws.faces (old carry -1, new +1).
+    // ones are compacted into faces (old carry -1, new +1).
     const uint32_t below = (1u << lane) - 1u;
     const uint8_t fl = lane < nfaces ? rec->flags[lane] : 0;
     const bool two = plan.force_two || (fl & kFaceTwo);
@@ -321,7 +324,7 @@ __device__ void audit_unit(const CandidateRecord* __restrict__ rec, const PlanDe
         const uint32_t slot = __popc(m & below);
         if (ok && slot < uint32_t(kMaxOk)) {
             s.pad = -1;
-            ws.faces[slot] = s;
+            faces[slot] = s;
             x0 = s.x0, x1 = s.x1, y0 = s.y0, y1 = s.y1;
         }
     }
@@ -344,7 +347,7 @@ __device__ void audit_unit(const CandidateRecord* __restrict__ rec, const PlanDe
         const uint32_t slot = n_old + __popc(m & below);
         if (ok && slot < uint32_t(kMaxOk)) {
             s.pad = 1;
-            ws.faces[slot] = s;
+            faces[slot] = s;
             x0 = min(x0, s.x0), x1 = max(x1, s.x1), y0 = min(y0, s.y0), y1 = max(y1, s.y1);
         }
     }
@@ -386,10 +389,10 @@ __device__ void audit_unit(const CandidateRecord* __restrict__ rec, const PlanDe
         // Sum of the faces' bbox areas: small units test every (face, sample
         // of its bbox) into a byte difference map; the others sweep rows.
         uint32_t area = 0;
-        if (lane < nok) area += uint32_t(ws.faces[lane].x1 - ws.faces[lane].x0 + 1) * uint32_t(ws.faces[lane].y1 - ws.faces[lane].y0 + 1);
+        if (lane < nok) area += uint32_t(faces[lane].x1 - faces[lane].x0 + 1) * uint32_t(faces[lane].y1 - faces[lane].y0 + 1);
         if (lane + 32 < nok)
-            area += uint32_t(ws.faces[lane + 32].x1 - ws.faces[lane + 32].x0 + 1) *
-                    uint32_t(ws.faces[lane + 32].y1 - ws.faces[lane + 32].y0 + 1);
+            area += uint32_t(faces[lane + 32].x1 - faces[lane + 32].x0 + 1) *
+                    uint32_t(faces[lane + 32].y1 - faces[lane + 32].y0 + 1);
         for (int o = 16; o; o >>= 1) area += __shfl_xor_sync(0xffffffffu, area, o);
         const bool direct = area <= kDirectTests && uint32_t(bws) * uint32_t(bh) <= uint32_t(kDeltaSamples);
         if (words > kRegionWords || rows > kRegionRows) {
@@ -434,10 +437,10 @@ __device__ void audit_unit(const CandidateRecord* __restrict__ rec, const PlanDe
                 for (uint32_t k = lane; k < delta_words; k += 32) ws.delta[k] = 0x80808080u;
                 uint32_t c0 = 0, c1 = 0;
                 if (lane < nok)
-                    c0 = uint32_t(ws.faces[lane].x1 - ws.faces[lane].x0 + 1) * uint32_t(ws.faces[lane].y1 - ws.faces[lane].y0 + 1);
+                    c0 = uint32_t(faces[lane].x1 - faces[lane].x0 + 1) * uint32_t(faces[lane].y1 - faces[lane].y0 + 1);
                 if (lane + 32 < nok)
-                    c1 = uint32_t(ws.faces[lane + 32].x1 - ws.faces[lane + 32].x0 + 1) *
-                         uint32_t(ws.faces[lane + 32].y1 - ws.faces[lane + 32].y0 + 1);
+                    c1 = uint32_t(faces[lane + 32].x1 - faces[lane + 32].x0 + 1) *
+                         uint32_t(faces[lane + 32].y1 - faces[lane + 32].y0 + 1);
                 uint32_t i0 = c0, i1 = c1;
                 for (int o = 1; o < 32; o <<= 1) {
                     const uint32_t a = __shfl_up_sync(0xffffffffu, i0, o), b = __shfl_up_sync(0xffffffffu, i1, o);
@@ -452,7 +455,7 @@ __device__ void audit_unit(const CandidateRecord* __restrict__ rec, const PlanDe
                     uint32_t f = 0; // last face whose prefix is <= t
                     for (uint32_t step = 32; step; step >>= 1)
                         if (f + step < nok && ws.work[f + step] <= t) f += step;
-                    const FaceSetup& s = ws.faces[f];
+                    const FaceSetup& s = faces[f];
                     const uint32_t fw = uint32_t(s.x1 - s.x0 + 1), r = t - ws.work[f];
                     const int fy = s.y0 + int(r / fw), fx = s.x0 + int(r % fw);
                     if (face_covers(s, fx, fy)) {
@@ -502,7 +505,7 @@ __device__ void audit_unit(const CandidateRecord* __restrict__ rec, const PlanDe
                     };
                     const double py = double(y) + .5;
                     for (uint32_t f = 0; f < nok; ++f) {
-                        const FaceSetup& s = ws.faces[f];
+                        const FaceSetup& s = faces[f];
                         if (y < s.y0 || y > s.y1) continue;
                         int lo, hi;
                         face_interval(s, py, lo, hi);
@@ -511,20 +514,41 @@ __device__ void audit_unit(const CandidateRecord* __restrict__ rec, const PlanDe
                         insert((uint32_t(lo) << 1) | up);
                         insert((uint32_t(hi + 1) << 1) | (up ^ 1u));
                     }
+                    // Pieces with a non-zero delta go in groups of four: the
+                    // groups' first count words are loaded together. A count
+                    // word is the aligned 4-byte word holding x (view buffers
+                    // start 4-aligned and are padded to 4).
+                    const size_t row_at = size_t(y) * size;
+                    auto count_word = [&](int x) {
+                        return *reinterpret_cast<const uint32_t*>(pv.state_count + ((row_at + size_t(x)) & ~size_t(3)));
+                    };
+                    int pa[4], pb[4], pd[4], np = 0;
+                    auto flush = [&]() {
+                        uint32_t w[4];
+#pragma unroll
+                        for (int q = 0; q < 4; ++q) w[q] = q < np ? count_word(pa[q]) : 0u;
+#pragma unroll
+                        for (int q = 0; q < 4; ++q) {
+                            if (q >= np) break;
+                            uint32_t w4 = w[q];
+                            for (int x = pa[q]; x < pb[q];) {
+                                for (uint32_t j = uint32_t((row_at + size_t(x)) & 3); j < 4 && x < pb[q]; ++j, ++x)
+                                    visit(x, y, pd[q], int((w4 >> (8 * j)) & 0xffu), false);
+                                if (x < pb[q]) w4 = count_word(x);
+                            }
+                        }
+                        np = 0;
+                    };
                     int acc = 0;
                     for (int i = 0; i < n; ++i) {
                         acc += (ev[i] & 1u) ? 1 : -1;
                         if (!acc) continue;
                         const int xa = int(ev[i] >> 1), xb = i + 1 < n ? int(ev[i + 1] >> 1) : x1 + 1;
-                        for (int x = xa; x < xb;) {
-                            // the aligned 4-byte word of counts holding x (view
-                            // buffers start 4-aligned and are padded to 4)
-                            const size_t at = size_t(y) * size + size_t(x);
-                            const uint32_t w4 = *reinterpret_cast<const uint32_t*>(pv.state_count + (at & ~size_t(3)));
-                            for (uint32_t j = uint32_t(at & 3); j < 4 && x < xb; ++j, ++x)
-                                visit(x, y, acc, int((w4 >> (8 * j)) & 0xffu), false);
-                        }
+                        if (xa >= xb) continue;
+                        pa[np] = xa, pb[np] = xb, pd[np] = acc;
+                        if (++np == 4) flush();
                     }
+                    flush();
                 }
             }
             if (__any_sync(0xffffffffu, negative)) fallback = true;
@@ -813,9 +837,10 @@ __global__ void __launch_bounds__(kLargeWarps * 32, 1)
 // own slot of global scratch (`scratch`, one WarpScratch<L> per resident
 // warp); what overflows goes to `spill_next` (may be null).
 template <class L, int kWarps>
-__global__ void __launch_bounds__(kWarps * 32, 1)
+__global__ void __launch_bounds__(kWarps * 32, 2)
     k_audit_global(const __grid_constant__ AuditJob job, unsigned long long* stats, const uint32_t* spill,
                    uint32_t* cursor, unsigned char* scratch, uint32_t* spill_next) {
+    __shared__ FaceSetup face_table[kWarps][kMaxOk];
     const uint32_t lane = lane_id();
     const uint32_t slot = blockIdx.x * kWarps + (threadIdx.x >> 5);
     WarpScratch<L>& ws = reinterpret_cast<WarpScratch<L>*>(scratch)[slot];
@@ -832,7 +857,8 @@ __global__ void __launch_bounds__(kWarps * 32, 1)
         uint32_t lu;
         resolve_unit(job, u, plan, recs, out, lu);
         const uint32_t c = lu / plan->nviews, v = lu - c * plan->nviews;
-        audit_unit(recs + c, *plan, v, ws, out + lu, stats, u, spill_next);
+        audit_unit(recs + c, *plan, v, ws, out + lu, stats, u, spill_next, 0xffffffffu,
+                   face_table[threadIdx.x >> 5]);
     }
 }
 
