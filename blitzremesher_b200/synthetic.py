@@ -359,3 +359,59 @@ def rock(level: int, seed: int = 3, relief: float = 0.25) -> Mesh:
     faces = inv.reshape(-1, 3).astype(np.uint32)
     return Mesh(pos[slot_vertex], faces.reshape(-1), uv=np.stack([u, v], 1).astype(np.float32),
                 name=f"rock{level}-seed{seed}", meta={"kind": "rock", "level": level, "charts": 8, "seed": seed})
+
+
+def ribbons(count: int = 2000, seed: int = 5, height: float = 2.0, quads: int = 10) -> Mesh:
+    """Ribbon cards (foliage / hair cards): `count` two-sided quad strips of
+    quads x quads cells (2 * quads^2 triangles each), length 0.5-3% of the
+    scene height (`height`, cards based in [-1, 1]^2 x [-height/2, height/2]),
+    width a quarter of the length, random orientation, a seeded bend (arc of
+    up to 90 degrees along the length) and twist (up to 90 degrees). Each card
+    is its own uv chart, one cell of a square atlas."""
+    n = quads + 1
+    u = uniform(seed, 12 * count, 0.0, 1.0).reshape(12, count)
+    base = np.stack([2 * u[0] - 1, height * (u[1] - 0.5), 2 * u[2] - 1], 1)
+    length = height * (0.005 + 0.025 * u[3])
+    width = 0.25 * length
+    # orthonormal frame per card: strip axis a, bending normal b, binormal c
+    z = 2 * u[4] - 1
+    phi = 2 * np.pi * u[5]
+    a = np.stack([np.sqrt(1 - z * z) * np.cos(phi), np.sqrt(1 - z * z) * np.sin(phi), z], 1)
+    helper = np.where(np.abs(a[:, 0:1]) < 0.9, np.array([[1.0, 0, 0]]), np.array([[0, 1.0, 0]]))
+    b = np.cross(a, helper)
+    b /= np.linalg.norm(b, axis=1, keepdims=True)
+    rot = 2 * np.pi * u[6]
+    c0 = np.cross(a, b)
+    b, c = np.cos(rot)[:, None] * b + np.sin(rot)[:, None] * c0, -np.sin(rot)[:, None] * b + np.cos(rot)[:, None] * c0
+    bend = (u[7] - 0.5) * np.pi  # total arc angle, -90..90 degrees
+    twist = (u[8] - 0.5) * np.pi
+    t = np.linspace(0.0, 1.0, n)                       # along the length
+    s = np.linspace(-0.5, 0.5, n)                      # across the width
+    theta = bend[:, None] * t[None, :]                 # (count, n)
+    safe = np.where(np.abs(bend) < 1e-9, 1.0, bend)
+    along = np.where(np.abs(bend)[:, None] < 1e-9, t[None, :], np.sin(theta) / safe[:, None])
+    side = np.where(np.abs(bend)[:, None] < 1e-9, 0.0, (1 - np.cos(theta)) / safe[:, None])
+    center = (base[:, None, :] + length[:, None, None] * (along[..., None] * a[:, None, :] +
+                                                           side[..., None] * b[:, None, :]))
+    tangent = np.cos(theta)[..., None] * a[:, None, :] + np.sin(theta)[..., None] * b[:, None, :]
+    tw = twist[:, None] * t[None, :]
+    cross_tc = np.cross(tangent, np.broadcast_to(c[:, None, :], tangent.shape))
+    wdir = np.cos(tw)[..., None] * c[:, None, :] + np.sin(tw)[..., None] * cross_tc
+    pos = center[:, :, None, :] + (width[:, None, None, None] * s[None, None, :, None]) * wdir[:, :, None, :]
+    pos = pos.reshape(count * n * n, 3).astype(np.float32)
+    # faces: cell (i, j) of card k -> two triangles, the same winding on every card
+    i, j = np.meshgrid(np.arange(quads), np.arange(quads), indexing="ij")
+    v00 = (i * n + j).reshape(-1)
+    v01, v10, v11 = v00 + 1, v00 + n, v00 + n + 1
+    cell = np.stack([np.stack([v00, v10, v11], 1), np.stack([v00, v11, v01], 1)], 1).reshape(-1, 3)
+    faces = (cell[None, :, :] + (np.arange(count) * n * n)[:, None, None]).reshape(-1)
+    # uv: card k in cell (k % side, k // side) of a side x side atlas, 10% margin
+    side_cells = int(np.ceil(np.sqrt(count)))
+    k = np.arange(count)
+    cu, cv = (k % side_cells).astype(np.float64), (k // side_cells).astype(np.float64)
+    uu = (cu[:, None, None] + 0.05 + 0.9 * (s[None, None, :] + 0.5)) / side_cells
+    vv = (cv[:, None, None] + 0.05 + 0.9 * t[None, :, None]) / side_cells
+    uv = np.stack(np.broadcast_arrays(uu, vv), -1).reshape(count * n * n, 2).astype(np.float32)
+    return Mesh(pos, faces.astype(np.uint32), uv=uv, double_sided=np.array([1], np.uint8),
+                name=f"ribbons{count}-seed{seed}",
+                meta={"kind": "ribbons", "cards": count, "quads": quads, "seed": seed})
