@@ -466,6 +466,18 @@ def _shares(values) -> list:
     return [round(v / total, 4) if total else 0.0 for v in values]
 
 
+def _region_split(r) -> dict:
+    """Region-phase sub-phases of a profiled batch (SM cycles, per unit)."""
+    zero, dcyc, dunits, scyc, sunits, sev, spc, srows = [float(x) for x in r]
+    units = dunits + sunits
+    return {"zeroing_cycles_per_unit": zero / units if units else 0.0,
+            "direct": {"units": int(dunits), "cycles_per_unit": dcyc / dunits if dunits else 0.0},
+            "sweep": {"units": int(sunits), "cycles_per_unit": scyc / sunits if sunits else 0.0,
+                      "event_cycles_per_unit": sev / sunits if sunits else 0.0,
+                      "piece_cycles_per_unit": spc / sunits if sunits else 0.0,
+                      "rows_per_unit": srows / sunits if sunits else 0.0}}
+
+
 def _barrier(world: int) -> None:
     if world > 1:
         import torch.distributed as dist
@@ -590,6 +602,7 @@ def run_batched(args, rank: int, world: int, local: int) -> dict:
                                    "phase_share": dict(zip(("setup", "region", "distance"),
                                                            _shares(info["phase_cycles"]))),
                                    "flipped_samples": info["flipped_samples"],
+                                   "region_split": _region_split(info["region_split"]),
                                    "note": "SM cycles of each unit's warp, summed per tier and per phase"}},
             "clocks": clocks.summary(),
             "e2e": {"value": n * world * args.steps / e2e_s, "unit": "collapses/s",

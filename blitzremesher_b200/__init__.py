@@ -224,7 +224,7 @@ class BatchInfo(C.Structure):
                 ("exact_candidates", C.c_uint64), ("audit_ms", C.c_float), ("units", C.c_uint64),
                 ("region_samples", C.c_uint64), ("changed_samples", C.c_uint64),
                 ("tier_units", C.c_uint64 * 4), ("tier_cycles", C.c_uint64 * 4), ("phase_cycles", C.c_uint64 * 3),
-                ("flipped_samples", C.c_uint64)]
+                ("flipped_samples", C.c_uint64), ("region_split", C.c_uint64 * 8)]
 
 
 BATCH_GRAPH, BATCH_AUTOTUNE, BATCH_PROFILE = 1, 2, 4
@@ -565,7 +565,7 @@ class AuditBatch:
         i.struct_size = C.sizeof(BatchInfo)
         assert self.lib.blitz_audit_batch_read_info(self.handle, C.byref(i)) == BLITZ_OK
         d = {k: getattr(i, k) for k, _ in i._fields_ if k != "struct_size"}
-        for k in ("tune_ms", "tier_units", "tier_cycles", "phase_cycles"):
+        for k in ("tune_ms", "tier_units", "tier_cycles", "phase_cycles", "region_split"):
             d[k] = list(getattr(i, k))
         return d
 

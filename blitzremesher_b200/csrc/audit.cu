@@ -365,6 +365,10 @@ __device__ void audit_unit(const CandidateRecord* __restrict__ rec, const PlanDe
     }
     __syncwarp();
     const long long t_setup = stats ? clock64() : 0;
+    // profiling only: region sub-phases (zeroing, direct path or row sweep,
+    // the sweep's per-lane event and piece cycles, max over lanes)
+    long long st_zero = 0, st_path = 0, st_events = 0, st_pieces = 0;
+    int st_kind = -1, st_rows = 0;
     int dchg = 0, dtot = 0, dcov = 0;
     uint32_t qn = 0, region_changed = 0, nflips = 0;
     int region_words = 0;
@@ -405,6 +409,8 @@ __device__ void audit_unit(const CandidateRecord* __restrict__ rec, const PlanDe
             for (int k = int(lane); k < nwords; k += 32) ws.region[k] = 0;
             if (lane == 0) ws.qcount[0] = 0;
             __syncwarp();
+            const long long t_zero = stats ? clock64() : 0;
+            long long c_events = 0, c_pieces = 0;
             bool negative = false;
             int flips = 0;
             // A sample whose count changes by dv (state count pc): it flips
@@ -493,6 +499,7 @@ __device__ void audit_unit(const CandidateRecord* __restrict__ rec, const PlanDe
                 // pieces with a non-zero delta read their state count (four
                 // per load).
                 for (int y = y0 + int(lane); y <= y1; y += 32) {
+                    const long long r0 = stats ? clock64() : 0;
                     uint32_t ev[2 * kMaxOk];
                     int n = 0;
                     auto insert = [&](uint32_t e) {
@@ -514,6 +521,8 @@ __device__ void audit_unit(const CandidateRecord* __restrict__ rec, const PlanDe
                         insert((uint32_t(lo) << 1) | up);
                         insert((uint32_t(hi + 1) << 1) | (up ^ 1u));
                     }
+                    const long long r1 = stats ? clock64() : 0;
+                    c_events += r1 - r0;
                     // Pieces with a non-zero delta go in groups of four: the
                     // groups' first count words are loaded together. A count
                     // word is the aligned 4-byte word holding x (view buffers
@@ -549,9 +558,21 @@ __device__ void audit_unit(const CandidateRecord* __restrict__ rec, const PlanDe
                         if (++np == 4) flush();
                     }
                     flush();
+                    if (stats) c_pieces += clock64() - r1;
                 }
             }
+            if (stats) {
+                st_zero = t_zero - t_setup;
+                st_path = clock64() - t_zero;
+                st_kind = direct ? 0 : 1;
+                st_rows = bh;
+            }
             if (__any_sync(0xffffffffu, negative)) fallback = true;
+            for (int o = 16; o; o >>= 1) {
+                c_events = max(c_events, __shfl_xor_sync(0xffffffffu, c_events, o));
+                c_pieces = max(c_pieces, __shfl_xor_sync(0xffffffffu, c_pieces, o));
+            }
+            st_events = c_events, st_pieces = c_pieces;
             for (int o = 16; o; o >>= 1) {
                 dchg += __shfl_xor_sync(0xffffffffu, dchg, o);
                 dtot += __shfl_xor_sync(0xffffffffu, dtot, o);
@@ -740,7 +761,9 @@ __device__ void audit_unit(const CandidateRecord* __restrict__ rec, const PlanDe
         if (stats) {
             // profiling counters (kAuditStats slots): units, region samples,
             // searched samples; per tier units and SM cycles; SM cycles of the
-            // face setup, the region phases and the distance phase; flips
+            // face setup, the region phases and the distance phase; flips;
+            // region sub-phases (zeroing; direct path cycles and units; row
+            // sweep cycles and units, its event and piece cycles, rows)
             const long long t_end = clock64();
             constexpr int tier = L::kRegionRows <= 128 ? 0 : L::kRegionRows <= 256 ? 1 : L::kRegionRows <= 1024 ? 2 : 3;
             atomicAdd(stats, 1ull);
@@ -752,6 +775,17 @@ __device__ void audit_unit(const CandidateRecord* __restrict__ rec, const PlanDe
             atomicAdd(stats + 12, (unsigned long long)(t_region - t_setup));
             atomicAdd(stats + 13, (unsigned long long)(t_end - t_region));
             atomicAdd(stats + 14, (unsigned long long)nflips);
+            atomicAdd(stats + 15, (unsigned long long)st_zero);
+            if (st_kind == 0) {
+                atomicAdd(stats + 16, (unsigned long long)st_path);
+                atomicAdd(stats + 17, 1ull);
+            } else if (st_kind == 1) {
+                atomicAdd(stats + 18, (unsigned long long)st_path);
+                atomicAdd(stats + 19, 1ull);
+                atomicAdd(stats + 20, (unsigned long long)st_events);
+                atomicAdd(stats + 21, (unsigned long long)st_pieces);
+                atomicAdd(stats + 22, (unsigned long long)st_rows);
+            }
         }
     }
     __syncwarp();

@@ -2573,6 +2573,7 @@ blitz_status blitz_audit_batch_read_info(const blitz_audit_batch* b, blitz_audit
     for (int k = 0; k < 4; ++k) out->tier_units[k] = b->prof[3 + k], out->tier_cycles[k] = b->prof[7 + k];
     for (int k = 0; k < 3; ++k) out->phase_cycles[k] = b->prof[11 + k];
     out->flipped_samples = b->prof[14];
+    for (int k = 0; k < 8; ++k) out->region_split[k] = b->prof[15 + k];
     return BLITZ_OK;
 }
 

@@ -343,6 +343,11 @@ typedef struct blitz_audit_batch_info {
      * the SM cycles their warps spent; SM cycles of all units' face setup,
      * region phases and distance phase; samples whose coverage flipped */
     uint64_t tier_units[4], tier_cycles[4], phase_cycles[3], flipped_samples;
+    /* region phases split: SM cycles zeroing the region words; direct-test
+     * path cycles and units; row-sweep path cycles and units; the sweep's
+     * cycles building sorted interval ends and visiting pieces (each the max
+     * over a warp's lanes); rows swept */
+    uint64_t region_split[8];
 } blitz_audit_batch_info;
 blitz_status blitz_audit_batch_create(blitz_audit_session* const* sessions, size_t count, blitz_audit_batch** out,
                                       char* error, size_t error_capacity);
