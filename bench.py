@@ -623,11 +623,13 @@ ROCK_CHAIN = {"levels": 6, "base": 240.0, "last": 7.5, "curve": ((0.0, 1.0), (1.
               "views": 32, "ss": 8, "batch": 64, "budget": 300}
 
 
-def run_rock_chain(args, local: int) -> dict:
+def run_rock_chain(args, local: int, preserve_uv: int = 0) -> dict:
     """Multi-level LOD chain of a ridged-noise rock (81,920 faces, 8 UV charts):
     6 levels scheduled 240 -> 7.5 px (the 1024 -> 32 px ratio of the 1M-face
     configuration), transition 1 -> 3 px, LOD0 bound 2 px, 32 ortho views at
-    ss 8, batches of 64, 300 trials per level, each level confirmed."""
+    ss 8, batches of 64, 300 trials per level, each level confirmed. With
+    preserve_uv the collapses carry the transported uv and placements that
+    fold a uv triangle are rejected."""
     import torch
 
     import blitzremesher_b200 as br
@@ -635,7 +637,7 @@ def run_rock_chain(args, local: int) -> dict:
 
     c = ROCK_CHAIN
     mesh = syn.rock(6, 3)
-    session = br.AuditSession(mesh, br.neural_options(device=local, preserve_uv=0))
+    session = br.AuditSession(mesh, br.neural_options(device=local, preserve_uv=preserve_uv))
     settings = br.chain_settings(c["levels"], c["base"], c["last"], c["curve"], c["lod0"], (c["views"], 0, 0xB1172024),
                                  (c["views"], 0, 0xB1172026), c["ss"], c["ss"], c["ss"], 1.0, c["batch"], 0,
                                  c["budget"], 1)
@@ -647,7 +649,7 @@ def run_rock_chain(args, local: int) -> dict:
     session.close()
     return {"metric": "LOD-chain s/mesh", "seconds": seconds, "unit": "s/mesh",
             "mesh": f"rock: icosphere level 6 ({mesh.face_count} faces), 6-octave ridged noise, 8 UV charts "
-                    "(uv not preserved)",
+                    + ("(preserve_uv: uv transported, uv flips rejected)" if preserve_uv else "(uv not preserved)"),
             "schedule": c, "levels": [{k: (round(v, 4) if isinstance(v, float) else v) for k, v in l.items()
                                        if k not in ("source_audit", "transition_audit")}
                                       | {"source_error": l["source_audit"].error,
@@ -673,6 +675,10 @@ def run_gpu(args) -> None:
         line = run_batched(args, rank, world, local)
         if not args.no_rock:
             line["lod_chain_rock"] = run_rock_chain(args, local)
+            try:
+                line["lod_chain_rock_preserve_uv"] = run_rock_chain(args, local, preserve_uv=1)
+            except Exception as e:  # recorded in the line; the headline stands
+                line["lod_chain_rock_preserve_uv"] = {"error": f"{type(e).__name__}: {e}"}
         if not args.no_icosphere:
             ico = run_icosphere(args, rank, world, local)
             for k in ("metric", "n_gpus", "steps", "warmup", "higher_is_better", "scaling", "vs_baseline", "data"):
