@@ -599,6 +599,9 @@ def run_batched(args, rank: int, world: int, local: int) -> dict:
                          "tiers": {"units": dict(zip(("warp", "large", "huge", "giant"), info["tier_units"])),
                                    "warp_busy_share": dict(zip(("warp", "large", "huge", "giant"),
                                                                _shares(info["tier_cycles"]))),
+                                   "cycles_per_unit": dict(zip(("warp", "large", "huge", "giant"),
+                                                               [c / u if u else 0.0 for c, u in
+                                                                zip(info["tier_cycles"], info["tier_units"])])),
                                    "phase_share": dict(zip(("setup", "region", "distance"),
                                                            _shares(info["phase_cycles"]))),
                                    "flipped_samples": info["flipped_samples"],
