@@ -11,6 +11,7 @@
 // sample by a row scan over coverage words. The result equals a full
 // re-raster of the candidate (evaluate.cpp:125-209) sample for sample.
 #include "kernels.cuh"
+#include "nearest.cuh"
 
 namespace b200 {
 namespace {
@@ -83,51 +84,6 @@ template <class L> struct alignas(16) WarpScratch {
     uint32_t queue[L::kQueue];
 };
 
-// Covered samples [lo, hi] of row py - .5 of face s (lo > hi: none), from
-// s's bbox columns: each edge term of face_covers is monotone in x, so a
-// binary search per edge finds the interval's ends with the same FP64
-// expressions.
-__device__ __forceinline__ void face_interval(const FaceSetup& s, double py, int& lo, int& hi) {
-    lo = s.x0, hi = s.x1;
-    // edge (d, e), edge (e, a), edge (a, d) of face_covers
-    const double ax3[3] = {s.dx, s.ex, s.ax}, ay3[3] = {s.dy, s.ey, s.ay};
-    const double bx3[3] = {s.ex, s.ax, s.dx}, by3[3] = {s.ey, s.ay, s.dy};
-    const double r3[3] = {s.r0, s.r1, s.r2};
-    for (int e = 0; e < 3 && lo <= hi; ++e) {
-        const double ax = ax3[e], ay = ay3[e], r = r3[e];
-        const double t1 = (bx3[e] - ax) * (py - ay), c = by3[e] - ay;
-        // covered(x) = !((t1 - c * (x + .5 - ax)) + r < 0)
-        auto ok = [&](int x) { return !((t1 - c * ((double(x) + .5) - ax)) + r < 0); };
-        if (c > 0) { // true then false: last covered x
-            if (!ok(lo)) {
-                hi = lo - 1;
-                break;
-            }
-            int a = lo, b = hi;
-            while (a < b) {
-                const int m = a + (b - a + 1) / 2;
-                if (ok(m)) a = m;
-                else b = m - 1;
-            }
-            hi = a;
-        } else if (c < 0) { // false then true: first covered x
-            if (!ok(hi)) {
-                hi = lo - 1;
-                break;
-            }
-            int a = lo, b = hi;
-            while (a < b) {
-                const int m = a + (b - a) / 2;
-                if (ok(m)) b = m;
-                else a = m + 1;
-            }
-            lo = a;
-        } else if (!ok(lo)) {
-            hi = lo - 1;
-        }
-    }
-}
-
 __device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31; }
 
 __device__ __forceinline__ uint32_t size_mask(uint32_t size, uint32_t chunk) {
@@ -162,95 +118,6 @@ struct RefMask {
     uint32_t size;
     __device__ uint32_t chunk(uint32_t row, uint32_t c) const { return chunk_global(bits, size, row, c); }
 };
-
-// Smallest |dx| <= maxdx with a covered sample at (x+dx, row); kNone if none.
-// The two sides are scanned one chunk each per step, outward, so the scan
-// ends near the nearest covered sample instead of at a row end.
-template <class M> __device__ uint32_t nearest_in_row(const M& mask, uint32_t row, uint32_t x, uint32_t maxdx) {
-    const uint32_t cx = x >> 5, bx = x & 31;
-    uint32_t best = kNone;
-    const uint32_t w = mask.chunk(row, cx);
-    const uint32_t left = w & (bx == 31 ? 0xffffffffu : ((2u << bx) - 1u));
-    const uint32_t right = w & (0xffffffffu << bx);
-    if (left) best = bx - (31 - __clz(left));
-    if (right) {
-        const uint32_t d = (__ffs(right) - 1) - bx;
-        best = d < best ? d : best;
-    }
-    if (best == 0) return 0;
-    const uint32_t chunks = (mask.size + 31) >> 5;
-    bool go_left = cx > 0, go_right = cx + 1 < chunks;
-    for (uint32_t k = 1; go_left || go_right; ++k) {
-        if (go_left) {
-            const uint32_t c = cx - k;
-            const uint32_t nearest = x - (c * 32 + 31);
-            if (nearest > maxdx || nearest >= best) {
-                go_left = false;
-            } else {
-                const uint32_t v = mask.chunk(row, c);
-                if (v) {
-                    const uint32_t d = x - (c * 32 + (31 - __clz(v)));
-                    best = d < best ? d : best;
-                    go_left = false;
-                } else if (c == 0) {
-                    go_left = false;
-                }
-            }
-        }
-        if (go_right) {
-            const uint32_t c = cx + k;
-            const uint32_t nearest = c * 32 - x;
-            if (nearest > maxdx || nearest >= best) {
-                go_right = false;
-            } else {
-                const uint32_t v = mask.chunk(row, c);
-                if (v) {
-                    const uint32_t d = c * 32 + (__ffs(v) - 1) - x;
-                    best = d < best ? d : best;
-                    go_right = false;
-                } else if (c + 1 >= chunks) {
-                    go_right = false;
-                }
-            }
-        }
-    }
-    return best <= maxdx ? best : kNone;
-}
-
-// Exact squared Euclidean distance from (x, y) to the nearest covered sample
-// (kNone: none), or any value <= `enough` once a covered sample that close is
-// found (the caller only needs distances above `enough`: the running
-// maximum). The search runs in boxes of half-width R = 32, 128, ...: rows
-// are scanned up to R columns until a covered sample is found, and then
-// within its distance; a result <= R^2 (or <= enough) is final, since every
-// sample left out of the box is farther than R.
-template <class M> __device__ uint32_t nearest_d2(const M& mask, uint32_t x, uint32_t y, uint32_t enough = 0) {
-    const uint32_t size = mask.size;
-    for (uint32_t R = 32;; R *= 4) {
-        const bool last = R >= size;
-        uint32_t best = kNone;
-        for (uint32_t dy = 0;; ++dy) {
-            const uint64_t dy2 = uint64_t(dy) * dy;
-            if (best != kNone && (dy2 >= best || best <= enough)) break;
-            if (best == kNone && !last && dy > R) break;
-            bool any = false;
-            for (int side = 0; side < (dy ? 2 : 1); ++side) {
-                const int64_t row = side ? int64_t(y) + dy : int64_t(y) - dy;
-                if (row < 0 || row >= int64_t(size)) continue;
-                any = true;
-                const uint32_t maxdx =
-                    best == kNone ? (last ? size : R) : uint32_t(sqrtf(float(best - dy2))) + 1;
-                const uint32_t dx = nearest_in_row(mask, uint32_t(row), x, maxdx);
-                if (dx != kNone) {
-                    const uint64_t d = uint64_t(dx) * dx + dy2;
-                    if (d < best) best = uint32_t(d);
-                }
-            }
-            if (!any) break;
-        }
-        if (last || (best != kNone && (best <= enough || uint64_t(best) <= uint64_t(R) * R))) return best;
-    }
-}
 
 __device__ __forceinline__ bool pv_ref_bit(const uint32_t* bits, size_t i) { return (bits[i >> 5] >> (i & 31)) & 1u; }
 

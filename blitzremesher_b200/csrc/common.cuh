@@ -124,6 +124,51 @@ BH bool face_covers(const FaceSetup& s, int x, int y) {
     return !(w + s.r2 < 0);
 }
 
+// Covered samples [lo, hi] of row py - .5 of face s (lo > hi: none), from
+// s's bbox columns: each edge term of face_covers is monotone in x, so a
+// binary search per edge finds the interval's ends with the same FP64
+// expressions.
+BH void face_interval(const FaceSetup& s, double py, int& lo, int& hi) {
+    lo = s.x0, hi = s.x1;
+    // edge (d, e), edge (e, a), edge (a, d) of face_covers
+    const double ax3[3] = {s.dx, s.ex, s.ax}, ay3[3] = {s.dy, s.ey, s.ay};
+    const double bx3[3] = {s.ex, s.ax, s.dx}, by3[3] = {s.ey, s.ay, s.dy};
+    const double r3[3] = {s.r0, s.r1, s.r2};
+    for (int e = 0; e < 3 && lo <= hi; ++e) {
+        const double ax = ax3[e], ay = ay3[e], r = r3[e];
+        const double t1 = (bx3[e] - ax) * (py - ay), c = by3[e] - ay;
+        // covered(x) = !((t1 - c * (x + .5 - ax)) + r < 0)
+        auto ok = [&](int x) { return !((t1 - c * ((double(x) + .5) - ax)) + r < 0); };
+        if (c > 0) { // true then false: last covered x
+            if (!ok(lo)) {
+                hi = lo - 1;
+                break;
+            }
+            int a = lo, b = hi;
+            while (a < b) {
+                const int m = a + (b - a + 1) / 2;
+                if (ok(m)) a = m;
+                else b = m - 1;
+            }
+            hi = a;
+        } else if (c < 0) { // false then true: first covered x
+            if (!ok(hi)) {
+                hi = lo - 1;
+                break;
+            }
+            int a = lo, b = hi;
+            while (a < b) {
+                const int m = a + (b - a) / 2;
+                if (ok(m)) b = m;
+                else a = m + 1;
+            }
+            lo = a;
+        } else if (!ok(lo)) {
+            hi = lo - 1;
+        }
+    }
+}
+
 // Raw per-(candidate, view) audit record consumed by finish_view.
 struct ViewRecord {
     uint32_t max_d2;  // max squared distance over XOR samples (exact integer)
