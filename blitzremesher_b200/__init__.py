@@ -436,13 +436,16 @@ class AuditSession:
 
     def chain(self, settings: ChainSettings, meshes: bool = True):
         """LOD chain from the source (blitz_audit_chain): per-level records and,
-        with `meshes`, each level's (indices, positions)."""
+        with `meshes`, each level's (indices, positions), plus its uv when the
+        source has uv (read inside the callback, where the state is the level)."""
         out = (ChainLevel * (settings.levels - 1))()
         emitted = []
+        with_uv = self._source.uv is not None
 
         def on_level(user, level, idx, faces, pos, nv):
-            emitted.append((np.ctypeslib.as_array(idx, shape=(faces * 3,)).copy(),
-                            np.ctypeslib.as_array(pos, shape=(nv * 3,)).reshape(-1, 3).copy()))
+            mesh = (np.ctypeslib.as_array(idx, shape=(faces * 3,)).copy(),
+                    np.ctypeslib.as_array(pos, shape=(nv * 3,)).reshape(-1, 3).copy())
+            emitted.append(mesh + (self.state_uv(),) if with_uv else mesh)
 
         cb = CHAIN_EMIT(on_level) if meshes else None
         err = C.create_string_buffer(512)

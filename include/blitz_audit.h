@@ -407,7 +407,8 @@ typedef struct blitz_chain_level {
     double seconds;                /* executor + confirmation */
 } blitz_chain_level;
 /* Called once per level with the level's compacted indices and every vertex
- * slot's position (host memory valid during the call). */
+ * slot's position (host memory valid during the call). During the call the
+ * session's state is that level: blitz_audit_state_uv returns its uv. */
 typedef void (*blitz_chain_emit)(void* user, uint32_t level, const uint32_t* indices, uint32_t face_count,
                                  const float* positions, uint32_t vertex_count);
 blitz_status blitz_audit_chain(blitz_audit_session*, const blitz_chain_settings* settings,
