@@ -74,6 +74,28 @@ def test_descriptor_layouts_match_python(tmp_path):
     assert int(lay["blitz_candidate_verdict"]) == C.sizeof(br.Verdict) == br.VERDICT_DTYPE.itemsize
 
 
+def test_batch_chain_profile_layouts_match_python(tmp_path):
+    """The batch info, chain settings / level and profile records: sizes and
+    the offsets of their last fields equal the ctypes mirrors'."""
+    extra = ("S(blitz_audit_batch_info) S(blitz_chain_settings) S(blitz_chain_level) S(blitz_audit_profile) "
+             "O(blitz_audit_batch_info, changed_samples) O(blitz_audit_batch_info, tier_cycles) "
+             "O(blitz_audit_batch_info, flipped_samples) O(blitz_audit_batch_info, region_split) "
+             "O(blitz_chain_settings, ranking) O(blitz_chain_level, transition_audit) "
+             "O(blitz_audit_profile, record_bytes)")
+    lay = _c_layout(LAYOUT_SRC % ("blitz_audit.h", extra), ROOT / "include", tmp_path)
+    for c_name, py in [("blitz_audit_batch_info", br.BatchInfo), ("blitz_chain_settings", br.ChainSettings),
+                       ("blitz_chain_level", br.ChainLevel), ("blitz_audit_profile", br.AuditProfile)]:
+        assert int(lay[c_name]) == C.sizeof(py), c_name
+    for c_name, py, field in [("blitz_audit_batch_info", br.BatchInfo, "changed_samples"),
+                              ("blitz_audit_batch_info", br.BatchInfo, "tier_cycles"),
+                              ("blitz_audit_batch_info", br.BatchInfo, "flipped_samples"),
+                              ("blitz_audit_batch_info", br.BatchInfo, "region_split"),
+                              ("blitz_chain_settings", br.ChainSettings, "ranking"),
+                              ("blitz_chain_level", br.ChainLevel, "transition_audit"),
+                              ("blitz_audit_profile", br.AuditProfile, "record_bytes")]:
+        assert int(lay[f"{c_name}.{field}"]) == getattr(py, field).offset, (c_name, field)
+
+
 @pytest.mark.skipif(not REFERENCE_HEADER.exists(), reason="reference headers absent")
 def test_abi5_descriptors_identical_to_reference(tmp_path):
     ours = _c_layout(LAYOUT_SRC % ("blitz_audit.h", ""), ROOT / "include", tmp_path)
