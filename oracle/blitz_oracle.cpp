@@ -969,6 +969,13 @@ template <class F> int guarded(F f) {
 extern "C" {
 
 // mesh.cpp:12-20
+int bo_barycentric(const float p[3], const float a[3], const float b[3], const float c[3], float w[3]) {
+    if (!p || !a || !b || !c || !w) return 1;
+    const V3 r = barycentric({p[0], p[1], p[2]}, {a[0], a[1], a[2]}, {b[0], b[1], b[2]}, {c[0], c[1], c[2]});
+    w[0] = r.x, w[1] = r.y, w[2] = r.z;
+    return 0;
+}
+
 int bo_bounds_of(const bo_mesh* m, bo_bounds* out) {
     if (!m || !out || !m->vertex_count) return 1;
     V3 lo = load3(m->positions, 0), hi = lo;

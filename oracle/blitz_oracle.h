@@ -83,6 +83,9 @@ typedef struct bo_verdict {
 } bo_verdict;
 
 /* status: 0 ok, 1 invalid argument, 2 length/resource error */
+/* Closest point of triangle (a, b, c) to p as barycentric weights
+ * (action_gpu.cu:919-952), the uv transport's projection. */
+int bo_barycentric(const float p[3], const float a[3], const float b[3], const float c[3], float w[3]);
 int bo_bounds_of(const bo_mesh* m, bo_bounds* out);
 int bo_cameras(const bo_bounds* b, double screen, uint16_t ortho, uint16_t persp, uint32_t seed,
                bo_camera* out);

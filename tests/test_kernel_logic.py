@@ -23,3 +23,26 @@ def test_intervals_and_nearest_search(tmp_path):
     assert rows > 20_000 and queries == 12_000
     assert bad_rows == 0 and bad_queries == 0
     assert r.returncode == 0
+
+
+CUDA_INCLUDE = Path("/usr/local/cuda/include")
+
+
+@pytest.mark.skipif(shutil.which("g++") is None or not (CUDA_INCLUDE / "vector_types.h").exists(),
+                    reason="needs g++ and the CUDA vector-type headers")
+def test_uv_projection_matches_oracle_and_definition(tmp_path):
+    """The uv transport's closest-point weights (csrc/placement.cuh) equal
+    the oracle's bit for bit on 20,000 random cases (collinear and repeated
+    corners included) and are the closest point of the triangle."""
+    from oracle.oracle import HERE as ORACLE, build
+
+    if not (ORACLE / "liboracle.so").exists():
+        build(ref=False)
+    exe = tmp_path / "placement_logic"
+    subprocess.run(["g++", "-O2", "-std=c++17", "-ffp-contract=off", "-fno-fast-math", f"-I{CUDA_INCLUDE}",
+                    str(HERE / "placement_logic.cpp"), f"-L{ORACLE}", "-loracle", f"-Wl,-rpath,{ORACLE}",
+                    "-o", str(exe)], check=True)
+    r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=600)
+    cases, mismatch, not_closest = map(int, r.stdout.split()[1:4])
+    assert cases == 20_000 and mismatch == 0 and not_closest == 0
+    assert r.returncode == 0
