@@ -158,6 +158,8 @@ EXPORTS = {
     "blitz_audit_batch_read_info": ([C.c_void_p, C.c_void_p], C.c_int),
     "blitz_audit_state": ([C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p, C.c_size_t, C.POINTER(C.c_uint32),
                            C.c_char_p, C.c_size_t], C.c_int),
+    "blitz_chain_schedule": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t, C.c_char_p, C.c_size_t],
+                             C.c_int),
     "blitz_audit_state_uv": ([C.c_void_p, C.c_void_p, C.c_size_t, C.c_char_p, C.c_size_t], C.c_int),
     "blitz_audit_reset": ([C.c_void_p, C.c_char_p, C.c_size_t], C.c_int),
     "blitz_audit_profile_read": ([C.c_void_p, C.c_void_p], C.c_int),
@@ -216,6 +218,17 @@ def chain_settings(levels: int, base_pixels: float, last_pixels: float, curve=((
     c.max_changed_area, c.batch, c.keep_permille = max_changed_area, batch, keep_permille
     c.trial_budget, c.min_faces, c.ranking = trial_budget, min_faces, ranking
     return c
+
+
+def chain_schedule(settings: ChainSettings):
+    """The chain's per-level (pixels, transition bound, LOD0 bound), index 0
+    the source (blitz_chain_schedule; no GPU needed)."""
+    n = settings.levels
+    p, t, b = (np.zeros(n) for _ in range(3))
+    err = C.create_string_buffer(512)
+    _check(load().blitz_chain_schedule(C.byref(settings), p.ctypes.data, t.ctypes.data, b.ctypes.data, n, err, 512),
+           err)
+    return p, t, b
 
 
 class BatchInfo(C.Structure):

@@ -2592,6 +2592,32 @@ double curve_at(const blitz_chain_settings& c, double t) {
         }
     return xy[2 * n - 1];
 }
+// The schedule's part of the settings checks (levels, pixels, curve).
+void check_schedule(const blitz_chain_settings* c) {
+    if (!c || c->struct_size != sizeof(*c)) throw Failure(BLITZ_INVALID_ARGUMENT, "bad chain settings");
+    if (c->levels < 2 || c->levels > 32) throw Failure(BLITZ_INVALID_ARGUMENT, "level count must be 2..32");
+    if (!(c->base_pixels >= c->last_pixels) || !(c->last_pixels > 0) || c->base_pixels > 16384)
+        throw Failure(BLITZ_INVALID_ARGUMENT, "base pixels must be >= last pixels and <= 16384");
+    if (c->transition_points < 1 || c->transition_points > 8)
+        throw Failure(BLITZ_INVALID_ARGUMENT, "transition curve needs 1..8 points");
+}
+// schedule (chain.cpp:101-118): for levels 1..levels-1 the audited screen
+// size S_i = S_0 (S_last / S_0)^(i / (levels - 1)), the transition bound
+// delta_i = curve(t_i), and the LOD0 bound B_i = B_(i-1) S_i / S_(i-1) +
+// delta_i, capped at max_lod0_delta_px when that is positive. Index 0 is the
+// source: base pixels, bounds 0.
+void chain_schedule(const blitz_chain_settings& c, double* pixels, double* transition, double* source) {
+    pixels[0] = c.base_pixels, transition[0] = source[0] = 0;
+    double cumulative = 0;
+    for (uint32_t level = 1; level < c.levels; ++level) {
+        const double p = c.base_pixels * std::pow(c.last_pixels / c.base_pixels, double(level) / (c.levels - 1));
+        const double delta = curve_at(c, c.levels == 2 ? 0 : double(level - 1) / (c.levels - 2));
+        cumulative = cumulative * p / pixels[level - 1] + delta;
+        pixels[level] = p;
+        transition[level] = delta;
+        source[level] = c.max_lod0_delta_px > 0 ? std::min(cumulative, c.max_lod0_delta_px) : cumulative;
+    }
+}
 blitz_eval_settings chain_gate(const blitz_chain_settings& c, double pixels, double limit, bool audit) {
     blitz_eval_settings e;
     std::memset(&e, 0, sizeof e);
@@ -2630,15 +2656,21 @@ void blitz_chain_settings_init(blitz_chain_settings* c) {
     c->ranking = 3;
 }
 
+blitz_status blitz_chain_schedule(const blitz_chain_settings* c, double* pixels, double* transition,
+                                  double* source_bound, size_t capacity, char* error, size_t cap) {
+    return guarded(error, cap, [&] {
+        check_schedule(c);
+        if (!pixels || !transition || !source_bound || capacity < c->levels)
+            throw Failure(BLITZ_INVALID_ARGUMENT, "schedule output needs `levels` entries");
+        chain_schedule(*c, pixels, transition, source_bound);
+    });
+}
+
 blitz_status blitz_audit_chain(blitz_audit_session* s, const blitz_chain_settings* c, blitz_chain_level* out,
                                size_t capacity, blitz_chain_emit emit, void* user, char* error, size_t cap) {
     return guarded(error, cap, [&] {
-        if (!s || !c || c->struct_size != sizeof(*c)) throw Failure(BLITZ_INVALID_ARGUMENT, "bad chain settings");
-        if (c->levels < 2 || c->levels > 32) throw Failure(BLITZ_INVALID_ARGUMENT, "level count must be 2..32");
-        if (!(c->base_pixels >= c->last_pixels) || !(c->last_pixels > 0) || c->base_pixels > 16384)
-            throw Failure(BLITZ_INVALID_ARGUMENT, "base pixels must be >= last pixels and <= 16384");
-        if (c->transition_points < 1 || c->transition_points > 8)
-            throw Failure(BLITZ_INVALID_ARGUMENT, "transition curve needs 1..8 points");
+        if (!s) throw Failure(BLITZ_INVALID_ARGUMENT, "null session");
+        check_schedule(c);
         if (c->batch < 1 || c->batch > 64) throw Failure(BLITZ_INVALID_ARGUMENT, "action batch outside 1..64");
         if (c->ranking != 0 && c->ranking != 1 && c->ranking != 3 && c->ranking != 4)
             throw Failure(BLITZ_INVALID_ARGUMENT, "unknown ranking");
@@ -2656,18 +2688,13 @@ blitz_status blitz_audit_chain(blitz_audit_session* s, const blitz_chain_setting
                 it = it->first.reference == 1 ? S.plans.erase(it) : std::next(it);
         };
         bind_previous_source();
-        double prev_pixels = c->base_pixels, cumulative = 0;
+        double sched_pixels[32], sched_delta[32], sched_bound[32];
+        chain_schedule(*c, sched_pixels, sched_delta, sched_bound);
         std::vector<uint32_t> idx;
         std::vector<float> pos;
         for (uint32_t level = 1; level < c->levels; ++level) {
             const uint64_t t0 = now_ns();
-            // schedule (chain.cpp:101-118)
-            const double pixels =
-                c->base_pixels * std::pow(c->last_pixels / c->base_pixels, double(level) / (c->levels - 1));
-            const double delta = curve_at(*c, c->levels == 2 ? 0 : double(level - 1) / (c->levels - 2));
-            cumulative = cumulative * pixels / prev_pixels + delta;
-            const double bound = c->max_lod0_delta_px > 0 ? std::min(cumulative, c->max_lod0_delta_px) : cumulative;
-            prev_pixels = pixels;
+            const double pixels = sched_pixels[level], delta = sched_delta[level], bound = sched_bound[level];
             blitz_eval_settings gates[4] = {chain_gate(*c, pixels, bound, false), chain_gate(*c, pixels, delta, false),
                                             chain_gate(*c, pixels, bound, true), chain_gate(*c, pixels, delta, true)};
             for (int g = 0; g < 4; ++g) gate_of(&gates[g], S.bounds);

@@ -411,6 +411,11 @@ typedef struct blitz_chain_level {
  * session's state is that level: blitz_audit_state_uv returns its uv. */
 typedef void (*blitz_chain_emit)(void* user, uint32_t level, const uint32_t* indices, uint32_t face_count,
                                  const float* positions, uint32_t vertex_count);
+/* The chain's schedule alone (blitz::schedule, chain.cpp:101-118; no GPU):
+ * per level (0 = the source) the audited screen size, the transition bound
+ * and the LOD0 bound that blitz_audit_chain uses. `capacity` >= levels. */
+blitz_status blitz_chain_schedule(const blitz_chain_settings* settings, double* pixels, double* transition,
+                                  double* source_bound, size_t capacity, char* error, size_t error_capacity);
 blitz_status blitz_audit_chain(blitz_audit_session*, const blitz_chain_settings* settings,
                                blitz_chain_level* levels, size_t capacity, blitz_chain_emit emit, void* user,
                                char* error, size_t error_capacity);
