@@ -158,6 +158,9 @@ EXPORTS = {
     "blitz_audit_batch_read_info": ([C.c_void_p, C.c_void_p], C.c_int),
     "blitz_audit_state": ([C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p, C.c_size_t, C.POINTER(C.c_uint32),
                            C.c_char_p, C.c_size_t], C.c_int),
+    "blitz_mesh_bounds": ([C.c_void_p, C.c_void_p, C.POINTER(C.c_double), C.c_char_p, C.c_size_t], C.c_int),
+    "blitz_view_cameras": ([C.c_void_p, C.c_double, C.c_double, C.c_uint16, C.c_uint16, C.c_uint32, C.c_void_p,
+                           C.c_size_t, C.c_char_p, C.c_size_t], C.c_int),
     "blitz_chain_schedule": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t, C.c_char_p, C.c_size_t],
                              C.c_int),
     "blitz_audit_state_uv": ([C.c_void_p, C.c_void_p, C.c_size_t, C.c_char_p, C.c_size_t], C.c_int),
@@ -218,6 +221,34 @@ def chain_settings(levels: int, base_pixels: float, last_pixels: float, curve=((
     c.max_changed_area, c.batch, c.keep_permille = max_changed_area, batch, keep_permille
     c.trial_budget, c.min_faces, c.ranking = trial_budget, min_faces, ranking
     return c
+
+
+class ViewCamera(C.Structure):
+    _fields_ = [("right", C.c_float * 3), ("up", C.c_float * 3), ("forward", C.c_float * 3),
+                ("distance", C.c_double), ("focal", C.c_double), ("scale", C.c_double),
+                ("perspective", C.c_uint32), ("pad", C.c_uint32)]
+
+
+def mesh_bounds(mesh):
+    """(center float32[3], radius) of a mesh, as every audit projects with
+    (blitz_mesh_bounds; no GPU needed)."""
+    h = _MeshHold(mesh)
+    center = np.zeros(3, np.float32)
+    radius = C.c_double()
+    err = C.create_string_buffer(512)
+    _check(load().blitz_mesh_bounds(C.byref(h.c), center.ctypes.data, C.byref(radius), err, 512), err)
+    return center, radius.value
+
+
+def view_cameras(center, radius: float, screen: float, views: tuple) -> list:
+    """The camera set (ortho, persp, seed) at `screen` (blitz_view_cameras)."""
+    ortho, persp, seed = views
+    c = np.ascontiguousarray(center, np.float32)
+    out = (ViewCamera * max(1, ortho + persp))()
+    err = C.create_string_buffer(512)
+    _check(load().blitz_view_cameras(c.ctypes.data, radius, screen, ortho, persp, seed, out, ortho + persp, err, 512),
+           err)
+    return list(out[: ortho + persp])
 
 
 def chain_schedule(settings: ChainSettings):

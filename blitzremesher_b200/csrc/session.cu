@@ -2656,6 +2656,38 @@ void blitz_chain_settings_init(blitz_chain_settings* c) {
     c->ranking = 3;
 }
 
+blitz_status blitz_mesh_bounds(const blitz_mesh* mesh, float center[3], double* radius, char* error, size_t cap) {
+    return guarded(error, cap, [&] {
+        if (!mesh || !center || !radius) throw Failure(BLITZ_INVALID_ARGUMENT, "null argument");
+        const HostMesh h = import_mesh(mesh);
+        const Bounds b = bounds_of(h);
+        for (int k = 0; k < 3; ++k) center[k] = b.center[k];
+        *radius = b.radius;
+    });
+}
+
+blitz_status blitz_view_cameras(const float center[3], double radius, double screen, uint16_t ortho, uint16_t persp,
+                                uint32_t seed, blitz_view_camera* out, size_t capacity, char* error, size_t cap) {
+    return guarded(error, cap, [&] {
+        if (!center || !out) throw Failure(BLITZ_INVALID_ARGUMENT, "null argument");
+        if (capacity < size_t(ortho) + persp) throw Failure(BLITZ_INVALID_ARGUMENT, "camera output too small");
+        if (!(screen > 0) || !std::isfinite(screen) || !(radius > 0) || !std::isfinite(radius))
+            throw Failure(BLITZ_INVALID_ARGUMENT, "screen and radius must be positive and finite");
+        Bounds b{};
+        for (int k = 0; k < 3; ++k) b.center[k] = center[k];
+        b.radius = radius;
+        const std::vector<Camera> cams = make_cameras(b, screen, ortho, persp, seed);
+        static_assert(sizeof(blitz_view_camera) == sizeof(Camera), "camera layouts");
+        for (size_t i = 0; i < cams.size(); ++i) {
+            blitz_view_camera& o = out[i];
+            std::memcpy(o.right, cams[i].right, 12), std::memcpy(o.up, cams[i].up, 12);
+            std::memcpy(o.forward, cams[i].forward, 12);
+            o.distance = cams[i].distance, o.focal = cams[i].focal, o.scale = cams[i].scale;
+            o.perspective = cams[i].perspective, o.pad = 0;
+        }
+    });
+}
+
 blitz_status blitz_chain_schedule(const blitz_chain_settings* c, double* pixels, double* transition,
                                   double* source_bound, size_t capacity, char* error, size_t cap) {
     return guarded(error, cap, [&] {

@@ -148,6 +148,23 @@ blitz_status blitz_audit_evaluate(blitz_audit_session*, const blitz_mesh* refere
                                   const blitz_mesh* candidate, const blitz_eval_settings* settings,
                                   blitz_measurement* out, char* error, size_t error_capacity);
 
+/* One view of a camera set: blitz::Camera (evaluate.hpp:46). */
+typedef struct blitz_view_camera {
+    float right[3], up[3], forward[3];
+    double distance, focal, scale;
+    uint32_t perspective, pad;
+} blitz_view_camera;
+/* Host only, no session or GPU: the bounds every audit projects with
+ * (blitz::bounds, mesh.cpp:12-20: bbox centre, largest distance to it) and
+ * the camera set of (ortho, persp, seed) at `screen` (blitz::cameras,
+ * evaluate.cpp:108-124, with this platform's libm as the reference uses its
+ * own). `capacity` >= ortho + persp cameras. */
+blitz_status blitz_mesh_bounds(const blitz_mesh* mesh, float center[3], double* radius, char* error,
+                               size_t error_capacity);
+blitz_status blitz_view_cameras(const float center[3], double radius, double screen, uint16_t ortho, uint16_t persp,
+                                uint32_t seed, blitz_view_camera* out, size_t capacity, char* error,
+                                size_t error_capacity);
+
 /* Packed coverage mask of `mesh` in camera `view` of the camera set
  * (ortho, persp, seed) at `screen` x `supersample`, with the session's bounds:
  * the twin of blitz::detail::rasterize_coverage (evaluate.cpp:193-195).
