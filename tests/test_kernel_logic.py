@@ -46,3 +46,25 @@ def test_uv_projection_matches_oracle_and_definition(tmp_path):
     cases, mismatch, not_closest = map(int, r.stdout.split()[1:4])
     assert cases == 20_000 and mismatch == 0 and not_closest == 0
     assert r.returncode == 0
+
+
+@pytest.mark.skipif(shutil.which("g++") is None, reason="needs g++")
+def test_view_measurement_matches_oracle(tmp_path):
+    """finish_view and bounded_refinement (csrc/common.cuh, run by the verdict
+    kernel) equal the oracle's restatements bit for bit on 200,000 random view
+    records (clipped, empty-side, same-mask, conservative-screen cases) and
+    11,628 refinement bounds."""
+    from oracle.oracle import HERE as ORACLE, build
+
+    if not (ORACLE / "liboracle.so").exists():
+        build(ref=False)
+    exe = tmp_path / "verdict_logic"
+    subprocess.run(["g++", "-O2", "-std=c++17", "-ffp-contract=off", "-fno-fast-math",
+                    str(HERE / "verdict_logic.cpp"), f"-L{ORACLE}", "-loracle", f"-Wl,-rpath,{ORACLE}",
+                    "-o", str(exe)], check=True)
+    r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=600)
+    lines = dict(l.split(" ", 1) for l in r.stdout.strip().splitlines())
+    cases, bad = map(int, lines["finish_view"].split())
+    rcases, rbad = map(int, lines["refinement"].split())
+    assert cases == 200_000 and bad == 0 and rcases > 10_000 and rbad == 0
+    assert r.returncode == 0
