@@ -265,8 +265,14 @@ __device__ void audit_unit(const CandidateRecord* __restrict__ rec, const PlanDe
             area += uint32_t(faces[lane + 32].x1 - faces[lane + 32].x0 + 1) *
                     uint32_t(faces[lane + 32].y1 - faces[lane + 32].y0 + 1);
         for (int o = 16; o; o >>= 1) area += __shfl_xor_sync(0xffffffffu, area, o);
-        const bool direct = area <= kDirectTests && uint32_t(bws) * uint32_t(bh) <= uint32_t(kDeltaSamples);
-        if (words > kRegionWords || rows > kRegionRows) {
+        // The small tier (regions of at most 128 x 64 samples) always tests
+        // every sample; a unit whose delta map does not fit goes on to the
+        // next tier.
+        constexpr bool kSweep = kDeltaSamples > 2048;
+        const bool direct =
+            !kSweep || (area <= kDirectTests && uint32_t(bws) * uint32_t(bh) <= uint32_t(kDeltaSamples));
+        if (words > kRegionWords || rows > kRegionRows ||
+            (!kSweep && uint32_t(bws) * uint32_t(bh) > uint32_t(kDeltaSamples))) {
             fallback = true;
         } else {
             samples = uint64_t(rows) * uint64_t(words) * 32;
@@ -355,7 +361,7 @@ __device__ void audit_unit(const CandidateRecord* __restrict__ rec, const PlanDe
                         visit(x, y, dv, int(pv.state_count[size_t(y) * size + size_t(x)]), true);
                     }
                 }
-            } else {
+            } else if constexpr (kSweep) {
                 // Row sweep, one bbox row per lane. Per face crossing the row
                 // the covered samples form one interval: each edge term of
                 // the reference's test is monotone in x (IEEE rounding is
