@@ -144,3 +144,32 @@ def test_midpoint_trial_properties(oracle):
         assert np.array_equal(pos[e.to], mid)
         assert idx.size // 3 == mesh.face_count - e.removed
         assert not np.any(idx == e.from_)
+
+
+def test_oracle_matches_reference_live_ribbons(oracle, reference):
+    """Two-sided open cards (the ribbon workload's mesh): bounds, cameras,
+    masks (the mesh's own double-sided flag and forced two-sided), action sets
+    and evaluate Measurements of endpoint trials equal the reference's."""
+    mesh = syn.ribbons(40, seed=6)
+    bo, br = oracle.bounds(mesh), reference.bounds(mesh)
+    assert bytes(bo) == bytes(br)
+    co = oracle.cameras(bo, 48.0, (5, 3, 0xB1172026))
+    cr = reference.cameras(br, 48.0, (5, 3, 0xB1172026))
+    assert all(bytes(a) == bytes(b) for a, b in zip(co, cr))
+    covered = 0
+    for cam in co:
+        for ss in (1, 4):
+            for two in (False, True):
+                wo, clo, _ = oracle.rasterize(mesh, bo, cam, 48.0, ss, two)
+                wr, clr, _ = reference.rasterize(mesh, bo, cam, 48.0, ss, two)
+                assert np.array_equal(wo, wr) and clo == clr
+                covered += int(np.unpackbits(wo.view(np.uint8)).sum())
+    assert covered > 0
+    acts = reference.actions(mesh)
+    mine = np.array([(e.from_, e.to) for e in oracle.actions(mesh, placement=False)], np.uint32).reshape(-1, 2)
+    assert len(acts) > 0 and np.array_equal(mine, acts)
+    s = settings(48.0, 1.0, (5, 3, 3), 2, 8, 0.5)
+    for frm, to in acts[:: max(1, len(acts) // 6)]:
+        idx = reference.trial_endpoint(mesh, int(frm), int(to))
+        cand = syn.Mesh(mesh.positions, idx, double_sided=mesh.double_sided)
+        assert bytes(oracle.evaluate(mesh, cand, bo, s)) == bytes(reference.evaluate(mesh, cand, bo, s))
