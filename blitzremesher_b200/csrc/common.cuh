@@ -169,6 +169,32 @@ BH void face_interval(const FaceSetup& s, double py, int& lo, int& hi) {
     }
 }
 
+// CPU float value of the field where the exact distance reaches 2^24: the
+// row pass rounds g^2 to float, the column pass rounds (dy^2 + f) to float;
+// the lower envelope of the reference picks the smallest such value. `g`:
+// per row the distance to its nearest covered sample in column x (kNone:
+// none), row stride `width`.
+BH float cpu_field_value(const uint32_t* g, uint32_t width, uint32_t height, uint32_t x, uint32_t y) {
+    float best = INFINITY;
+    for (uint32_t q = 0; q < height; ++q) {
+        uint32_t gq = g[size_t(q) * width + x];
+        if (gq == kNone) continue;
+#if defined(__CUDA_ARCH__)
+        float f = __uint2float_rn(gq * gq);
+#else
+        float f = float(gq * gq);
+#endif
+        double dy = double(y) - double(q);
+#if defined(__CUDA_ARCH__)
+        float val = __double2float_rn(dy * dy + double(f));
+#else
+        float val = float(dy * dy + double(f));
+#endif
+        best = val < best ? val : best;
+    }
+    return best;
+}
+
 // Raw per-(candidate, view) audit record consumed by finish_view.
 struct ViewRecord {
     uint32_t max_d2;  // max squared distance over XOR samples (exact integer)

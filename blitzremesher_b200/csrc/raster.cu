@@ -177,21 +177,6 @@ __device__ void k_column_envelope_body(const uint32_t* g, uint32_t width, uint32
     }
 }
 
-// CPU float value of the field where the exact distance reaches 2^24: the
-// row pass rounds g^2 to float, the column pass rounds (dy^2 + f) to float.
-__device__ float cpu_field_value(const uint32_t* g, uint32_t width, uint32_t height, uint32_t x, uint32_t y) {
-    float best = INFINITY;
-    for (uint32_t q = 0; q < height; ++q) {
-        uint32_t gq = g[size_t(q) * width + x];
-        if (gq == kNone) continue;
-        float f = __uint2float_rn(gq * gq);
-        double dy = double(y) - double(q);
-        float val = __double2float_rn(dy * dy + double(f));
-        best = val < best ? val : best;
-    }
-    return best;
-}
-
 // Max over samples covered by `from` and not by `to` of the field of `to`, as
 // float bit patterns (non-negative floats order like their bits).
 __global__ void k_directed_max(const uint32_t* from, const uint32_t* to, const uint32_t* d2, const uint32_t* g,

@@ -68,3 +68,22 @@ def test_view_measurement_matches_oracle(tmp_path):
     rcases, rbad = map(int, lines["refinement"].split())
     assert cases == 200_000 and bad == 0 and rcases > 10_000 and rbad == 0
     assert r.returncode == 0
+
+
+@pytest.mark.skipif(shutil.which("g++") is None, reason="needs g++")
+def test_distance_field_values_match_oracle(tmp_path):
+    """On a 4160 x 4160 raster: exact integer squared distances below 2^24,
+    and cpu_field_value's float roundings from 2^24 up (csrc/common.cuh, the
+    audit's full-raster path), equal the oracle's float distance field."""
+    from oracle.oracle import HERE as ORACLE, build
+
+    if not (ORACLE / "liboracle.so").exists():
+        build(ref=False)
+    exe = tmp_path / "field_logic"
+    subprocess.run(["g++", "-O2", "-std=c++17", "-ffp-contract=off", "-fno-fast-math",
+                    str(HERE / "field_logic.cpp"), f"-L{ORACLE}", "-loracle", f"-Wl,-rpath,{ORACLE}",
+                    "-o", str(exe)], check=True)
+    r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=600)
+    n, bad_exact, bad_round, rounded = map(int, r.stdout.split()[1:5])
+    assert n == 3000 and rounded > 500 and bad_exact == 0 and bad_round == 0
+    assert r.returncode == 0
