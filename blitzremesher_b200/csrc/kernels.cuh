@@ -1,6 +1,7 @@
 // Device data layouts and kernel launchers of the candidate-audit engine.
 #pragma once
 #include "common.cuh"
+#include "legality.cuh"
 #include <cuda_runtime.h>
 
 namespace b200 {
@@ -30,11 +31,11 @@ struct DevTopology {
     const uint32_t* slots;        // vertex slots per class, ascending
 };
 
-// One directed collapse edit (action_gpu.cu:129-132).
-struct Edit {
-    uint32_t from, to, source[2], target[2];
-    uint8_t wedges, removed, valid, pad;
-};
+// The legality view of a mesh state and its topology.
+__host__ __device__ inline ClassRing class_ring(const DevMesh& m, const DevTopology& t) {
+    return ClassRing{m.idx, m.mat, t.geometry, t.face_offsets, t.faces, t.nbr_offsets, t.neighbors, t.nbr_count,
+                     t.boundary, t.invalid, m.nv, m.nf};
+}
 
 // Attribute charts for uv transport (place_vertices): the session's source
 // mesh and, per canonical class of the source (position + uv weld with
@@ -107,8 +108,8 @@ size_t scan_scratch_words(uint32_t n);
 void launch_topology(const DevMesh& m, uint32_t* geometry, uint32_t* face_offsets, uint32_t* faces,
                      uint32_t* cursor, uint32_t* entry_offsets, uint32_t* entries, uint32_t* nbr_offsets,
                      uint32_t* neighbors, uint8_t* nbr_count, uint8_t* boundary, uint8_t* invalid,
-                     uint8_t* visited, uint32_t* slot_offsets, uint32_t* slots, uint32_t* scan_scratch,
-                     uint32_t* host_counts, cudaStream_t s);
+                     uint32_t* slot_offsets, uint32_t* slots, uint32_t* scan_scratch, uint32_t* host_counts,
+                     cudaStream_t s);
 void launch_enumerate(const DevMesh& m, const DevTopology& t, uint32_t* edge_base, uint8_t* valid,
                       Edit* slots, uint32_t* offsets, Edit* out, uint32_t* scan_scratch, uint32_t total_nbrs,
                       bool preserve_uv, cudaStream_t s);
@@ -122,8 +123,10 @@ void launch_prepare(const DevMesh& m, const DevTopology& t, const DevMesh& origi
 void launch_raster(const DevMesh& m, const Camera* cam_host, const float* center, uint32_t ss, uint32_t size,
                    bool force_two, bool cpu_semantics, uint32_t* bits, uint8_t* counts, uint32_t* state,
                    cudaStream_t s);
+// Popcounts {a^b, a|b, a, b} over `words` u32 words; samples != 0 counts
+// only the first `samples` bits (bits past the last sample are ignored).
 void launch_popcounts(const uint32_t* a, const uint32_t* b, uint32_t words, unsigned long long* out,
-                      cudaStream_t s);
+                      cudaStream_t s, uint64_t samples = 0);
 void launch_distance(const uint32_t* from, const uint32_t* to, uint32_t width, uint32_t height, uint32_t* g,
                      uint32_t* d2, int32_t* stack_v, long long* stack_num, long long* stack_den, uint32_t* out_max,
                      cudaStream_t s);

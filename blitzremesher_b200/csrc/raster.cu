@@ -76,10 +76,17 @@ __global__ void k_raster_fill(RasterArgs a, uint32_t* bits, uint8_t* counts, uin
         }
 }
 
-__global__ void k_popcounts(const uint32_t* a, const uint32_t* b, uint32_t words, unsigned long long* out) {
+__global__ void k_popcounts(const uint32_t* a, const uint32_t* b, uint32_t words, uint64_t samples,
+                            unsigned long long* out) {
     unsigned long long changed = 0, total = 0, ca = 0, cb = 0;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < words; i += gridDim.x * blockDim.x) {
         uint32_t x = a[i], y = b[i];
+        // samples != 0: bits at or past `samples` are not samples and do not count.
+        if (samples && uint64_t(i + 1) * 32 > samples) {
+            const uint64_t first = uint64_t(i) * 32;
+            const uint32_t keep = samples > first ? uint32_t((1ull << (samples - first)) - 1) : 0u;
+            x &= keep, y &= keep;
+        }
         changed += __popc(x ^ y);
         total += __popc(x | y);
         ca += __popc(x);
@@ -445,12 +452,12 @@ void launch_raster(const DevMesh& m, const Camera* cam_host, const float* center
 }
 
 void launch_popcounts(const uint32_t* a, const uint32_t* b, uint32_t words, unsigned long long* out,
-                      cudaStream_t s) {
+                      cudaStream_t s, uint64_t samples) {
     cudaMemsetAsync(out, 0, 4 * sizeof(unsigned long long), s);
     uint32_t grid = blocks_for(words);
     if (grid > 1184) grid = 1184;
     if (!grid) grid = 1;
-    k_popcounts<<<grid, kThreads, 0, s>>>(a, b, words, out);
+    k_popcounts<<<grid, kThreads, 0, s>>>(a, b, words, samples, out);
 }
 
 // Field of `to`, max over from \ to (as float bits) into out_max.

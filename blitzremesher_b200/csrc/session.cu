@@ -271,7 +271,7 @@ static bool identical(const HostMesh& a, const HostMesh& b) {
 struct Topology {
     Buf<uint32_t> geometry, canonical, face_offsets, faces, cursor, entries, nbr_offsets, neighbors, slot_offsets,
         slots, scan, table;
-    Buf<uint8_t> nbr_count, boundary, invalid, visited;
+    Buf<uint8_t> nbr_count, boundary, invalid;
     Buf<uint32_t> edge_base, offsets, flat;
     Buf<uint8_t> valid;
     Buf<Edit> edit_slots, edits;
@@ -480,7 +480,6 @@ static void init_topology(Session& S) {
     t.nbr_count = Buf<uint8_t>(P, 6ull * nf);
     t.boundary = Buf<uint8_t>(P, n);
     t.invalid = Buf<uint8_t>(P, n);
-    t.visited = Buf<uint8_t>(P, 6ull * nf);
     t.slot_offsets = Buf<uint32_t>(P, n + 1);
     t.slots = Buf<uint32_t>(P, n);
     size_t scan_words = std::max(scan_scratch_words(n + 1), scan_scratch_words(uint32_t(6ull * nf + 1)));
@@ -550,7 +549,7 @@ static void rebuild_topology(Session& S) {
     const uint32_t n = m.nv;
     cudaStream_t st = S.stream;
     launch_topology(m, t.geometry.p, t.face_offsets.p, t.faces.p, t.cursor.p, nullptr, t.entries.p, t.nbr_offsets.p,
-                    t.neighbors.p, t.nbr_count.p, t.boundary.p, t.invalid.p, t.visited.p, t.slot_offsets.p,
+                    t.neighbors.p, t.nbr_count.p, t.boundary.p, t.invalid.p, t.slot_offsets.p,
                     t.slots.p, t.scan.p, nullptr, st);
     B200_CUDA(cudaMemcpyAsync(&t.total_nbrs, t.nbr_offsets.p + n, 4, cudaMemcpyDeviceToHost, st));
     B200_CUDA(cudaStreamSynchronize(st));

@@ -34,8 +34,12 @@ constexpr size_t kStaticBytes = kOffMax + align256(2 * 4);
 
 static __device__ __align__(256) unsigned char g_distance_scratch[kStaticBytes];
 
-// Device address of g_distance_scratch per device ordinal; taken once per
-// device with that device current.
+// Device address of g_distance_scratch per device ordinal, looked up with
+// that device current. Outside stream capture every call looks it up again
+// (a context torn down and created anew, e.g. after cudaDeviceReset, loads
+// the module at a new address); during capture the address of the last call
+// outside capture is used, so the first call on a device must come before
+// any capture.
 std::mutex g_setup_mutex;
 void* g_scratch_address[64] = {};
 
@@ -87,10 +91,23 @@ extern "C" blitz_status blitz_audit_coverage_distance_static(const uint64_t* a_d
         message(error, error_capacity, "no current CUDA device");
         return BLITZ_UNAVAILABLE;
     }
+    // An error left by the caller's earlier work stays theirs: report it
+    // without consuming it, and enqueue nothing.
+    if (cudaPeekAtLastError() != cudaSuccess) {
+        message(error, error_capacity, "a CUDA error from earlier work is pending on this thread; nothing enqueued");
+        return BLITZ_INTERNAL_ERROR;
+    }
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    cudaStreamCaptureStatus capture = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(st, &capture) != cudaSuccess) {
+        cudaGetLastError();
+        message(error, error_capacity, "cudaStreamIsCapturing failed on the given stream");
+        return BLITZ_INVALID_ARGUMENT;
+    }
     unsigned char* base = nullptr;
     {
         std::lock_guard<std::mutex> lock(g_setup_mutex);
-        if (!g_scratch_address[device]) {
+        if (capture == cudaStreamCaptureStatusNone) {
             void* ptr = nullptr;
             cudaError_t e = cudaGetSymbolAddress(&ptr, g_distance_scratch);
             if (e != cudaSuccess || !ptr) {
@@ -99,10 +116,13 @@ extern "C" blitz_status blitz_audit_coverage_distance_static(const uint64_t* a_d
                 return BLITZ_UNAVAILABLE;
             }
             g_scratch_address[device] = ptr;
+        } else if (!g_scratch_address[device]) {
+            message(error, error_capacity,
+                    "first call on this device during stream capture: call once outside capture first");
+            return BLITZ_INVALID_ARGUMENT;
         }
         base = static_cast<unsigned char*>(g_scratch_address[device]);
     }
-    cudaStream_t st = static_cast<cudaStream_t>(stream);
     auto* g = reinterpret_cast<uint32_t*>(base + kOffG);
     auto* d2 = reinterpret_cast<uint32_t*>(base + kOffD2);
     auto* sv = reinterpret_cast<int32_t*>(base + kOffV);
@@ -115,7 +135,8 @@ extern "C" blitz_status blitz_audit_coverage_distance_static(const uint64_t* a_d
     const uint32_t words = uint32_t(((uint64_t(width) * height + 63) / 64) * 2);
     // The counters keep the previous call's contents: clear them first.
     k_static_clear<<<1, 32, 0, st>>>(pop, maxes);
-    launch_popcounts(a, b, words, pop, st);
+    // Bits at or past width x height are not samples: they do not count.
+    launch_popcounts(a, b, words, pop, st, uint64_t(width) * height);
     launch_distance(a, b, width, height, g, d2, sv, sn, sd, maxes, st);
     launch_distance(b, a, width, height, g, d2, sv, sn, sd, maxes + 1, st);
     k_static_finish<<<1, 32, 0, st>>>(pop, maxes, supersample, out_device);

@@ -194,12 +194,17 @@ blitz_status blitz_audit_coverage_distance(blitz_audit_session*, const uint64_t*
  * about 7 MiB, held by every GPU that loads the library until the process
  * exits; masks are limited to 512 x 512 = 262144 samples (larger masks return
  * BLITZ_INVALID_ARGUMENT). Inputs are device masks (layout of
- * blitz_audit_raster, no padding needed) and the result is written to the
- * device double `out_device`, all enqueued on `stream` (a cudaStream_t, NULL =
- * default stream) on the current device; the call does not synchronise. The
- * first call on a device looks up the array's device address (once per
- * device); make that first call before any stream capture. All calls share
- * the one array, so calls that overlap on the GPU race: serialise them. */
+ * blitz_audit_raster, no padding needed; bits at or past width x height are
+ * ignored) and the result is written to the device double `out_device`, all
+ * enqueued on `stream` (a cudaStream_t, NULL = default stream) on the current
+ * device; the call does not synchronise. Each call outside stream capture
+ * looks up the array's device address on the current device (so a context
+ * created anew after cudaDeviceReset is followed); a call during capture
+ * reuses the address of the last call outside it, so make the first call on a
+ * device before any stream capture. A CUDA error already pending on the
+ * calling thread is left in place and reported as BLITZ_INTERNAL_ERROR with
+ * nothing enqueued. All calls share the one array, so calls that overlap on
+ * the GPU race: serialise them. */
 blitz_status blitz_audit_coverage_distance_static(const uint64_t* a_device, const uint64_t* b_device,
                                                   uint32_t width, uint32_t height, uint8_t supersample,
                                                   double* out_device, void* stream, char* error,

@@ -49,13 +49,14 @@ def _bind(lib):
     fn.restype = C.c_int
 
 
-def test_static_scratch_matches_session_entry_point(gpu_lib):
+def test_static_scratch_matches_session_entry_point(gpu_lib, oracle):
     lib = br.load()
     _bind(lib)
     rng = np.random.default_rng(23)
     with br.AuditSession(syn.noisy_icosphere(1, 1)) as s:
         # Two calls in a row on different shapes: the second must not see the
-        # first call's leftovers in the shared scratch.
+        # first call's leftovers in the shared scratch. Each result is also
+        # the oracle's (the reference's coverage distance restated on the CPU).
         for width, height, ss, blobs in ((257, 190, 1, 4), (512, 512, 8, 3), (13, 11, 2, 1)):
             a = _blob_mask(rng, width, height, blobs)
             b = _blob_mask(rng, width, height, blobs + 1)
@@ -63,6 +64,7 @@ def test_static_scratch_matches_session_entry_point(gpu_lib):
             st, got, msg = _static_distance(lib, a, b, width, height, ss)
             assert st == br.BLITZ_OK, msg
             assert got == want, (width, height, ss, got, want)
+            assert got == oracle.coverage_distance(a, b, width, height, ss)
         # Equal masks and one empty mask keep the session's semantics.
         a = _blob_mask(rng, 64, 64, 2)
         empty = np.zeros_like(a)
@@ -77,3 +79,26 @@ def test_static_scratch_rejects_oversized_masks(gpu_lib):
     st, got, msg = _static_distance(lib, a, a, 513, 512, 1)
     assert st == br.BLITZ_INVALID_ARGUMENT and "512 x 512" in msg
     assert got == -1.0
+
+
+def test_static_scratch_ignores_bits_past_the_last_sample(gpu_lib):
+    """Bits set at or past width x height in the last word are not samples:
+    the result equals that of the same masks with those bits cleared."""
+    lib = br.load()
+    _bind(lib)
+    rng = np.random.default_rng(5)
+    width, height, ss = 13, 11, 1  # 143 samples: the last u64 word holds 49 non-samples
+    a = _blob_mask(rng, width, height, 2)
+    b = _blob_mask(rng, width, height, 3)
+    tail = ~np.uint64((1 << (width * height - 64 * (a.size - 1))) - 1)
+    dirty_a, dirty_b = a.copy(), b.copy()
+    dirty_a[-1] |= tail
+    dirty_b[-1] |= tail & np.uint64(0x5555555555555555)
+    st, clean, msg = _static_distance(lib, a, b, width, height, ss)
+    assert st == br.BLITZ_OK, msg
+    st, dirty, msg = _static_distance(lib, dirty_a, dirty_b, width, height, ss)
+    assert st == br.BLITZ_OK, msg
+    assert dirty == clean
+    # Equal samples with different tails are still equal masks: distance 0.
+    st, same, msg = _static_distance(lib, a, dirty_a, width, height, ss)
+    assert st == br.BLITZ_OK and same == 0.0, msg
