@@ -272,6 +272,19 @@ class Oracle:
         return v
 
 
+def reference_root() -> Path | None:
+    """The reference source tree: $BLITZ_REFERENCE, else the tree that
+    oracle/Makefile compiled oracle/_ref from; None when neither exists."""
+    env = os.environ.get("BLITZ_REFERENCE")
+    if env:
+        return Path(env) if Path(env).is_dir() else None
+    rec = HERE / "_ref" / "source_root.txt"
+    if rec.exists():
+        p = Path(rec.read_text().strip())
+        return p if p.is_dir() else None
+    return None
+
+
 class Reference:
     """The reference's own CPU sources (oracle/_ref/libblitz_ref.so)."""
 

@@ -9,10 +9,12 @@ import numpy as np
 import pytest
 
 import blitzremesher_b200 as br
+from oracle.oracle import reference_root
 
 ROOT = Path(__file__).resolve().parents[1]
 HEADER = ROOT / "include" / "blitz_audit.h"
-REFERENCE_HEADER = Path("/root/reference/include/blitz/blitz.h")
+_REF_ROOT = reference_root()
+REFERENCE_HEADER = (_REF_ROOT / "include" / "blitz" / "blitz.h") if _REF_ROOT else None
 
 
 def declared_functions():
@@ -96,7 +98,8 @@ def test_batch_chain_profile_layouts_match_python(tmp_path):
         assert int(lay[f"{c_name}.{field}"]) == getattr(py, field).offset, (c_name, field)
 
 
-@pytest.mark.skipif(not REFERENCE_HEADER.exists(), reason="reference headers absent")
+@pytest.mark.skipif(REFERENCE_HEADER is None or not REFERENCE_HEADER.exists(),
+                    reason="reference headers absent (set BLITZ_REFERENCE to the reference tree)")
 def test_abi5_descriptors_identical_to_reference(tmp_path):
     ours = _c_layout(LAYOUT_SRC % ("blitz_audit.h", ""), ROOT / "include", tmp_path)
     (tmp_path / "ref").mkdir()
