@@ -554,16 +554,16 @@ def run_batched(args, rank: int, world: int, local: int) -> dict:
     alg_bytes = n * 624 * 1 + info["region_samples"] * (1 + 1 / 8) + info["units"] * 16
     achieved_gbs = alg_bytes / (info["audit_ms"] * 1e-3) / 1e9
     pk = peaks()
-    # End to end: pinned host candidates in, verdicts out, every step.
+    # End to end through the host C ABI (blitz_audit_batch_candidates_host):
+    # pinned host candidates in, host verdicts out, copies inside every step.
     pinned = torch.empty(n * br.COLLAPSE_DTYPE.itemsize, dtype=torch.uint8, pin_memory=True)
     pinned.numpy()[:] = cat.view(np.uint8)
+    host_cands = pinned.numpy().view(br.COLLAPSE_DTYPE)
     out_pinned = torch.empty(n * br.VERDICT_DTYPE.itemsize, dtype=torch.uint8, pin_memory=True)
+    host_out = out_pinned.numpy().view(br.VERDICT_DTYPE)
 
     def e2e_step():
-        cand_dev.copy_(pinned, non_blocking=True)
-        step()
-        out_pinned.copy_(verdict_dev, non_blocking=True)
-        torch.cuda.current_stream(device).synchronize()
+        batch.candidates_host(host_cands, counts, gates, host_out, br.BATCH_GRAPH)
 
     for _ in range(2):
         e2e_step()
@@ -572,7 +572,7 @@ def run_batched(args, rank: int, world: int, local: int) -> dict:
     for _ in range(args.steps):
         e2e_step()
     e2e_s = _max_over_ranks(time.perf_counter() - t1, world, device)
-    assert np.array_equal(out_pinned.numpy().view(br.VERDICT_DTYPE), verdicts)
+    assert np.array_equal(host_out, verdicts)
     faces = [m.face_count for m in meshes]
     line = {"metric": METRIC, "value": n * world * args.steps / (max_ms * 1e-3), "unit": "collapses/s",
             "n_gpus": world, "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": max_ms / args.steps,

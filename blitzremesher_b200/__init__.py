@@ -155,6 +155,8 @@ EXPORTS = {
     "blitz_audit_batch_destroy": ([C.c_void_p], None),
     "blitz_audit_batch_candidates": ([C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(EvalSettings), C.c_void_p,
                                       C.c_uint32, C.c_void_p, C.c_char_p, C.c_size_t], C.c_int),
+    "blitz_audit_batch_candidates_host": ([C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(EvalSettings), C.c_void_p,
+                                           C.c_uint32, C.c_char_p, C.c_size_t], C.c_int),
     "blitz_audit_batch_read_info": ([C.c_void_p, C.c_void_p], C.c_int),
     "blitz_audit_state": ([C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p, C.c_size_t, C.POINTER(C.c_uint32),
                            C.c_char_p, C.c_size_t], C.c_int),
@@ -606,6 +608,18 @@ class AuditBatch:
         self.candidates_device(dev.data_ptr(), counts, gates, out.data_ptr(), flags)
         v = out.cpu().numpy().view(VERDICT_DTYPE)[: cat.size]
         return np.split(v, np.cumsum(counts)[:-1])
+
+    def candidates_host(self, collapses: np.ndarray, counts: Sequence[int], gates: Sequence[EvalSettings],
+                        out: np.ndarray, flags: int = 0) -> np.ndarray:
+        """Host entry point: concatenated collapses (COLLAPSE_DTYPE) in, verdicts
+        (VERDICT_DTYPE, same length) written to `out`; pinned arrays copy fastest."""
+        assert collapses.dtype == COLLAPSE_DTYPE and out.dtype == VERDICT_DTYPE and out.size >= collapses.size
+        cnt = (C.c_size_t * len(counts))(*counts)
+        g = (EvalSettings * 4)(*gates)
+        err = C.create_string_buffer(512)
+        _check(self.lib.blitz_audit_batch_candidates_host(self.handle, collapses.ctypes.data, cnt, g,
+                                                          out.ctypes.data, flags, err, 512), err)
+        return out
 
     def info(self) -> dict:
         i = BatchInfo()

@@ -2311,6 +2311,8 @@ struct blitz_audit_batch {
     cudaStream_t stream = nullptr;
     Pool pool;
     Buf<CandidateRecord> records;
+    Buf<blitz_collapse> host_cands;         // device copies for the host entry point
+    Buf<blitz_candidate_verdict> host_out;
     std::vector<Buf<AuditEntry>> entries; // per plan slot
     std::vector<uint32_t> nentries;
     std::vector<uint64_t> units;
@@ -2337,6 +2339,7 @@ struct blitz_audit_batch {
         if (exec) cudaGraphExecDestroy(exec);
         if (graph) cudaGraphDestroy(graph);
         records.release(), queue.release(), spill.release(), spill_huge.release(), exact.release(), huge.release();
+        host_cands.release(), host_out.release();
         spill_giant.release(), giant.release();
         entries.clear();
         if (stream) cudaStreamDestroy(stream);
@@ -2372,15 +2375,15 @@ void blitz_audit_batch_destroy(blitz_audit_batch* b) {
     cudaSetDevice(previous);
 }
 
-blitz_status blitz_audit_batch_candidates(blitz_audit_batch* b, const blitz_collapse* cands, const size_t* counts,
-                                          const blitz_eval_settings gates_in[4], blitz_candidate_verdict* out,
-                                          uint32_t flags, void* stream, char* error, size_t cap) {
-    return guarded(error, cap, [&] {
+// One batched audit of device candidates into device verdicts on `st`
+// (blitz_audit_batch_candidates without the status wrapper); synchronises.
+static void batch_candidates(blitz_audit_batch* b, const blitz_collapse* cands, const size_t* counts,
+                             const blitz_eval_settings gates_in[4], blitz_candidate_verdict* out, uint32_t flags,
+                             cudaStream_t st) {
+    {
         if (!b || !counts || !gates_in || flags > 7) throw Failure(BLITZ_INVALID_ARGUMENT, "bad batch arguments");
         const bool profile = (flags & 4u) != 0;
         if (profile && (flags & 1u)) throw Failure(BLITZ_INVALID_ARGUMENT, "profiling runs without graph replay");
-        DeviceScope scope(b->device);
-        cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : b->stream;
         const size_t ns = b->sessions.size();
         std::vector<uint64_t> off(ns + 1, 0);
         for (size_t i = 0; i < ns; ++i) {
@@ -2553,6 +2556,41 @@ blitz_status blitz_audit_batch_candidates(blitz_audit_batch* b, const blitz_coll
                           st);
         }
         for (size_t i = 0; i < ns; ++i) b->sessions[i]->s.info.decoded += counts[i];
+    }
+}
+
+blitz_status blitz_audit_batch_candidates(blitz_audit_batch* b, const blitz_collapse* cands, const size_t* counts,
+                                          const blitz_eval_settings gates_in[4], blitz_candidate_verdict* out,
+                                          uint32_t flags, void* stream, char* error, size_t cap) {
+    return guarded(error, cap, [&] {
+        if (!b) throw Failure(BLITZ_INVALID_ARGUMENT, "null batch");
+        DeviceScope scope(b->device);
+        batch_candidates(b, cands, counts, gates_in, out, flags, stream ? static_cast<cudaStream_t>(stream) : b->stream);
+    });
+}
+
+blitz_status blitz_audit_batch_candidates_host(blitz_audit_batch* b, const blitz_collapse* cands,
+                                               const size_t* counts, const blitz_eval_settings gates_in[4],
+                                               blitz_candidate_verdict* out, uint32_t flags, char* error,
+                                               size_t cap) {
+    return guarded(error, cap, [&] {
+        if (!b || !counts) throw Failure(BLITZ_INVALID_ARGUMENT, "bad batch arguments");
+        DeviceScope scope(b->device);
+        size_t n = 0;
+        for (size_t i = 0; i < b->sessions.size(); ++i) n += counts[i];
+        if (n && (!cands || !out)) throw Failure(BLITZ_INVALID_ARGUMENT, "null candidate or verdict array");
+        // Batch-owned device buffers: their addresses stay fixed from call to
+        // call, so a captured graph of the launch sequence keeps replaying.
+        b->host_cands.ensure(b->pool, std::max<size_t>(1, n));
+        b->host_out.ensure(b->pool, std::max<size_t>(1, n));
+        cudaStream_t st = b->stream;
+        if (n)
+            B200_CUDA(cudaMemcpyAsync(b->host_cands.p, cands, n * sizeof(blitz_collapse), cudaMemcpyHostToDevice, st));
+        batch_candidates(b, b->host_cands.p, counts, gates_in, b->host_out.p, flags, st);
+        if (n)
+            B200_CUDA(cudaMemcpyAsync(out, b->host_out.p, n * sizeof(blitz_candidate_verdict), cudaMemcpyDeviceToHost,
+                                      st));
+        B200_CUDA(cudaStreamSynchronize(st));
     });
 }
 

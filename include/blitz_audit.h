@@ -382,6 +382,17 @@ blitz_status blitz_audit_batch_candidates(blitz_audit_batch*, const blitz_collap
                                           const size_t* counts, const blitz_eval_settings gates[4],
                                           blitz_candidate_verdict* verdicts_device, uint32_t flags, void* stream,
                                           char* error, size_t error_capacity);
+/* The same batched audit from host memory: the sessions' candidates
+ * concatenated in session order are copied in, the verdicts copied out
+ * (through device buffers the batch owns, so a captured graph keeps
+ * replaying), on the batch's stream. The host-buffer counterpart of
+ * blitz_audit_candidates (the reference's audit takes host meshes:
+ * AuditCuda::evaluate, src/neural/internal.hpp:131-175) for many sessions.
+ * Synchronises before returning. */
+blitz_status blitz_audit_batch_candidates_host(blitz_audit_batch*, const blitz_collapse* candidates,
+                                               const size_t* counts, const blitz_eval_settings gates[4],
+                                               blitz_candidate_verdict* verdicts, uint32_t flags, char* error,
+                                               size_t error_capacity);
 blitz_status blitz_audit_batch_read_info(const blitz_audit_batch*, blitz_audit_batch_info* out);
 
 /* ---- LOD chain -------------------------------------------------------------

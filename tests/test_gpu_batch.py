@@ -1,7 +1,7 @@
 """Several sessions audited in one persistent launch: the verdicts equal each
 session's own blitz_audit_candidates, with and without graph replay and after
-autotuning, for meshes at LOD0, after commits, and at rasters above 256 x 256
-(large and huge tiers)."""
+autotuning, through the device and the host entry points, for meshes at LOD0,
+after commits, and at rasters above 256 x 256 (large and huge tiers)."""
 import numpy as np
 import pytest
 
@@ -48,6 +48,13 @@ def test_batch_equals_per_session(gpu_lib, screen):
             assert np.array_equal(out.cpu().numpy().view(br.VERDICT_DTYPE), expect), flags
         info = batch.info()
         assert info["tuned"] == 1 and info["graph_captured"] == 1 and info["graph_launches"] >= 2
+        # host entry point: host collapses in, host verdicts out, graph replayed
+        host_out = np.zeros(cat.size, br.VERDICT_DTYPE)
+        for flags in (0, br.BATCH_GRAPH, br.BATCH_GRAPH):
+            host_out[:] = 0
+            batch.candidates_host(cat, counts, gates, host_out, flags)
+            assert np.array_equal(host_out, expect), flags
+        assert batch.info()["graph_launches"] > info["graph_launches"]
         batch.close()
     finally:
         for s in sessions:
