@@ -206,7 +206,7 @@ CHAIN_EMIT = C.CFUNCTYPE(None, C.c_void_p, C.c_uint32, C.POINTER(C.c_uint32), C.
                          C.c_uint32)
 
 
-def chain_settings(levels: int, base_pixels: float, last_pixels: float, curve=((0.0, 1.0),),
+def chain_settings(levels: int, base_pixels: float, last_pixels: float, curve=((0.0, 2.0), (1.0, 3.0)),
                    max_lod0_delta_px: float = 2.0, search_views=(42, 12, 0xB1172024), audit_views=(642, 64, 0xB1172026),
                    search_supersample: int = 4, audit_supersample: int = 8, max_supersample: int = 32,
                    max_changed_area: float = 1.0, batch: int = 64, keep_permille: int = 0,

@@ -2637,6 +2637,19 @@ void check_schedule(const blitz_chain_settings* c) {
         throw Failure(BLITZ_INVALID_ARGUMENT, "base pixels must be >= last pixels and <= 16384");
     if (c->transition_points < 1 || c->transition_points > 8)
         throw Failure(BLITZ_INVALID_ARGUMENT, "transition curve needs 1..8 points");
+    if (!(c->max_lod0_delta_px >= 0) || !std::isfinite(c->max_lod0_delta_px))
+        throw Failure(BLITZ_INVALID_ARGUMENT, "invalid optional pixel limit");
+    // The curve rules of the reference's settings validation (chain.cpp:67-77).
+    const float* xy = c->transition_curve;
+    const uint32_t n = c->transition_points;
+    if (xy[0] != 0 || xy[2 * (n - 1)] != 1) throw Failure(BLITZ_INVALID_ARGUMENT, "curves must span [0,1]");
+    double last = -1;
+    for (uint32_t i = 0; i < n; ++i) {
+        const float x = xy[2 * i], y = xy[2 * i + 1];
+        if (!std::isfinite(x) || !std::isfinite(y) || x <= last || x > 1 || y < 0 || y > 1e6)
+            throw Failure(BLITZ_INVALID_ARGUMENT, "curve points must be ordered, finite and in 0..1e6");
+        last = x;
+    }
 }
 // schedule (chain.cpp:101-118): for levels 1..levels-1 the audited screen
 // size S_i = S_0 (S_last / S_0)^(i / (levels - 1)), the transition bound
@@ -2681,8 +2694,9 @@ void blitz_chain_settings_init(blitz_chain_settings* c) {
     c->levels = 2;
     c->base_pixels = c->last_pixels = 24;
     c->max_lod0_delta_px = 2;
-    c->transition_curve[0] = 0, c->transition_curve[1] = 1;
-    c->transition_points = 1;
+    // the reference's default transition curve {(0, 2), (1, 3)} (remesher.hpp:12-13)
+    c->transition_curve[0] = 0, c->transition_curve[1] = 2, c->transition_curve[2] = 1, c->transition_curve[3] = 3;
+    c->transition_points = 2;
     c->search_orthographic = 42, c->search_perspective = 12, c->search_seed = 0xB1172024u;
     c->audit_orthographic = 642, c->audit_perspective = 64, c->audit_seed = 0xB1172026u;
     c->search_supersample = 4, c->audit_supersample = 8, c->max_supersample = 32;

@@ -1173,11 +1173,42 @@ int bo_execute_batched(const bo_mesh* source, const bo_mesh* previous, uint32_t 
 // slots, fewer faces) instead of from the source itself; the geometric
 // classes stay those welded on the source (a chain's levels continue one
 // state, generate.cpp:456-562).
-int bo_execute_from(const bo_mesh* source, const bo_mesh* previous, const bo_mesh* start, uint32_t target,
-                    uint32_t budget, const bo_eval_settings gates[4], int preserve_uv, uint32_t batch, int ranking,
-                    uint32_t* commits_from_to, uint32_t capacity, uint32_t* commits, uint32_t* trials,
-                    uint32_t* out_indices, uint32_t* out_faces, float* out_positions, uint8_t* stop,
-                    float* out_uv) {
+}
+namespace {
+// Endpoint trial of the reference CPU executor (ActionState::trial(span),
+// action.cpp:308-345): the wedge remap of every edit, faces that become
+// degenerate in classes dropped, positions unchanged.
+Trial make_endpoint_trial(const bo_mesh& m, const Topology& t, const std::vector<bo_edit>& batch) {
+    Trial out;
+    std::vector<uint32_t> remap(m.vertex_count, kNone);
+    for (const bo_edit& e : batch)
+        for (unsigned j = 0; j < e.wedges; ++j) remap[e.source[j]] = e.target[j];
+    for (uint32_t f = 0; f < m.face_count; ++f) {
+        uint32_t ids[3];
+        bool changed = false;
+        for (int j = 0; j < 3; ++j) {
+            ids[j] = m.indices[3 * f + j];
+            if (remap[ids[j]] != kNone) ids[j] = remap[ids[j]], changed = true;
+        }
+        if (changed && (t.geometry[ids[0]] == t.geometry[ids[1]] || t.geometry[ids[1]] == t.geometry[ids[2]] ||
+                        t.geometry[ids[0]] == t.geometry[ids[2]]))
+            continue;
+        out.indices.insert(out.indices.end(), ids, ids + 3);
+        if (m.materials) out.materials.push_back(m.materials[f]);
+    }
+    out.positions.assign(m.positions, m.positions + size_t(m.vertex_count) * 3);
+    if (m.uv) out.uv.assign(m.uv, m.uv + size_t(m.vertex_count) * 2);
+    return out;
+}
+
+// The greedy walk of execute_actions (action.cpp:453-525) over midpoint
+// collapses (legality with placement, make_trial) or, with `endpoint`, over
+// the reference CPU executor's endpoint collapses (legality without
+// placement, make_endpoint_trial).
+int execute_walk(const bo_mesh* source, const bo_mesh* previous, const bo_mesh* start, uint32_t target,
+                 uint32_t budget, const bo_eval_settings gates[4], int preserve_uv, uint32_t batch, int ranking,
+                 bool endpoint, uint32_t* commits_from_to, uint32_t capacity, uint32_t* commits, uint32_t* trials,
+                 uint32_t* out_indices, uint32_t* out_faces, float* out_positions, uint8_t* stop, float* out_uv) {
     if (!batch || batch > 64 || (ranking != 1 && ranking != 3 && ranking != 4)) return 1;
     if (start && start->vertex_count != source->vertex_count) return 1;
     return guarded([&] {
@@ -1208,7 +1239,7 @@ int bo_execute_from(const bo_mesh* source, const bo_mesh* previous, const bo_mes
                 break;
             }
             Topology t = build_topology(m, preserve_uv != 0, &classes);
-            std::vector<bo_edit> edits = enumerate(m, t, true, preserve_uv != 0);
+            std::vector<bo_edit> edits = enumerate(m, t, !endpoint, preserve_uv != 0);
             if (edits.empty()) {
                 reason = 2;
                 break;
@@ -1227,7 +1258,8 @@ int bo_execute_from(const bo_mesh* source, const bo_mesh* previous, const bo_mes
                 while (n_trials < budget) {
                     std::vector<bo_edit> chosen;
                     for (size_t k : picked) chosen.push_back(edits[order[k]]);
-                    Trial tr = make_trial(m, t, original, classes, chosen, preserve_uv != 0);
+                    Trial tr = endpoint ? make_endpoint_trial(m, t, chosen)
+                                        : make_trial(m, t, original, classes, chosen, preserve_uv != 0);
                     ++n_trials;
                     if (tr.valid && audit_gates(trial_view(m, tr), *source, prev, b, gates, nullptr)) {
                         for (const bo_edit& e : chosen) {
@@ -1262,6 +1294,26 @@ int bo_execute_from(const bo_mesh* source, const bo_mesh* previous, const bo_mes
         if (out_uv) std::copy(st.uv.begin(), st.uv.end(), out_uv);
         *stop = reason;
     });
+}
+} // namespace
+extern "C" {
+
+int bo_execute_from(const bo_mesh* source, const bo_mesh* previous, const bo_mesh* start, uint32_t target,
+                    uint32_t budget, const bo_eval_settings gates[4], int preserve_uv, uint32_t batch, int ranking,
+                    uint32_t* commits_from_to, uint32_t capacity, uint32_t* commits, uint32_t* trials,
+                    uint32_t* out_indices, uint32_t* out_faces, float* out_positions, uint8_t* stop,
+                    float* out_uv) {
+    return execute_walk(source, previous, start, target, budget, gates, preserve_uv, batch, ranking, false,
+                        commits_from_to, capacity, commits, trials, out_indices, out_faces, out_positions, stop,
+                        out_uv);
+}
+
+int bo_execute_endpoint(const bo_mesh* source, uint32_t target, uint32_t budget, const bo_eval_settings gates[4],
+                        uint32_t batch, uint32_t* commits_from_to, uint32_t capacity, uint32_t* commits,
+                        uint32_t* trials, uint32_t* out_indices, uint32_t* out_faces, uint8_t* stop) {
+    std::vector<float> positions(size_t(source->vertex_count) * 3);
+    return execute_walk(source, nullptr, nullptr, target, budget, gates, 0, batch, 3, true, commits_from_to,
+                        capacity, commits, trials, out_indices, out_faces, positions.data(), stop, nullptr);
 }
 
 // Four-gate acceptance of one candidate (generate.cpp:365-388, chain.cpp:470-483):

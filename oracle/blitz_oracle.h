@@ -149,6 +149,14 @@ int bo_execute_from(const bo_mesh* source, const bo_mesh* previous, const bo_mes
                     uint32_t* out_indices, uint32_t* out_faces, float* out_positions, uint8_t* stop,
                     float* out_uv /* 2 per vertex, or NULL */);
 
+/* The same walk over the reference CPU executor's endpoint collapses
+ * (legality without placement, ActionState::trial: wedge remap, positions
+ * unchanged), ShortestEdge ranking, previous = source: the restatement of
+ * neural::execute_actions (action.cpp:453-525) that oracle/_ref runs itself. */
+int bo_execute_endpoint(const bo_mesh* source, uint32_t target, uint32_t budget, const bo_eval_settings gates[4],
+                        uint32_t batch, uint32_t* commits_from_to, uint32_t capacity, uint32_t* commits,
+                        uint32_t* trials, uint32_t* out_indices, uint32_t* out_faces, uint8_t* stop);
+
 #ifdef __cplusplus
 }
 #endif

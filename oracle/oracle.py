@@ -175,6 +175,27 @@ class Oracle:
                 "indices": idx[: 3 * faces.value].copy(), "positions": pos,
                 "uv": uv if source.uv is not None else None}
 
+    def execute_endpoint(self, source, target: int, budget: int, gates, batch=1) -> dict:
+        """The walk over endpoint collapses (the reference CPU executor's),
+        ShortestEdge ranking, previous = source."""
+        L = self.lib
+        P = C.POINTER
+        L.bo_execute_endpoint.argtypes = [P(BoMesh), C.c_uint32, C.c_uint32, P(BoEvalSettings), C.c_uint32,
+                                          C.c_void_p, C.c_uint32, P(C.c_uint32), P(C.c_uint32), C.c_void_p,
+                                          P(C.c_uint32), P(C.c_uint8)]
+        hs = _MeshHold(source)
+        cap = source.face_count
+        ft = np.zeros(2 * cap, np.uint32)
+        idx = np.zeros(source.face_count * 3, np.uint32)
+        commits, trials, faces, stop = C.c_uint32(), C.c_uint32(), C.c_uint32(), C.c_uint8()
+        g = (BoEvalSettings * 4)(*gates)
+        st = L.bo_execute_endpoint(C.byref(hs.c), target, budget, g, batch, ft.ctypes.data, cap, C.byref(commits),
+                                   C.byref(trials), idx.ctypes.data, C.byref(faces), C.byref(stop))
+        assert st == 0
+        n = commits.value
+        return {"commits": ft[: 2 * n].reshape(-1, 2), "trials": trials.value, "stop": stop.value,
+                "indices": idx[: 3 * faces.value].copy()}
+
     def cameras(self, b: BoBounds, screen: float, views: tuple) -> list:
         n = views[0] + views[1]
         out = (BoCamera * n)()
@@ -312,6 +333,25 @@ class Reference:
         L.br_precision_masks.argtypes = [C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p]
         L.br_trial_endpoint.argtypes = [P(BoMesh), C.c_uint32, C.c_uint32, C.c_void_p]
         L.br_trial_endpoint.restype = C.c_int64
+
+    def execute_actions(self, source, target: int, budget: int, gates, batch=1) -> dict:
+        """neural::execute_actions itself (action.cpp:453-525): endpoint
+        collapses, ShortestEdge ranking, the four gates over blitz::evaluate."""
+        L = self.lib
+        P = C.POINTER
+        L.br_execute_actions.argtypes = [P(BoMesh), C.c_uint32, C.c_uint32, P(BoEvalSettings), C.c_uint32,
+                                         C.c_void_p, P(C.c_uint32), P(C.c_uint64), P(C.c_uint64), P(C.c_uint64),
+                                         P(C.c_uint8)]
+        h = _MeshHold(source)
+        idx = np.zeros(source.face_count * 3, np.uint32)
+        faces, stop = C.c_uint32(), C.c_uint8()
+        trials, accepted, rejected = C.c_uint64(), C.c_uint64(), C.c_uint64()
+        g = (BoEvalSettings * 4)(*gates)
+        st = L.br_execute_actions(C.byref(h.c), target, budget, g, batch, idx.ctypes.data, C.byref(faces),
+                                  C.byref(trials), C.byref(accepted), C.byref(rejected), C.byref(stop))
+        assert st == 0
+        return {"trials": trials.value, "accepted": accepted.value, "rejected": rejected.value, "stop": stop.value,
+                "indices": idx[: 3 * faces.value].copy()}
 
     def trial_endpoint(self, mesh, frm: int, to: int) -> np.ndarray:
         h = _MeshHold(mesh)

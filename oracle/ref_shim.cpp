@@ -8,6 +8,7 @@
 #include "blitz/evaluate.hpp"
 #include "coverage.hpp"
 #include "neural/action.hpp"
+#include "neural/audit_measurement.hpp"
 #include "neural/internal.hpp"
 
 #include <cstring>
@@ -182,6 +183,49 @@ int64_t br_trial_endpoint(const br_mesh* m, uint32_t from, uint32_t to, uint32_t
         faces = int64_t(lod.data.indices.size() / 3);
     });
     return status ? -1 : faces;
+}
+// The reference CPU executor itself (neural::execute_actions,
+// action.cpp:453-525): endpoint collapses, batches of 1..64, a ShortestEdge
+// ranker (minus the edge length over the source diameter, each component of
+// the scaled delta rounded to float: the formula of rank_actions,
+// action_gpu.cu:822-825) and the four-gate ActionGate over blitz::evaluate
+// (source and previous are both the input; each gate's max_supersample
+// pre-bounded, graph.cpp:5-18; pass = audit_measurement_passed). Writes the
+// final indices; stop: 0 target reached, 1 trial budget, 2 no legal actions,
+// 3 no accepted action.
+int br_execute_actions(const br_mesh* m, uint32_t target, uint32_t budget, const br_eval_settings gates[4],
+                       uint32_t batch, uint32_t* out_indices, uint32_t* out_faces, uint64_t* trials,
+                       uint64_t* accepted, uint64_t* rejected, uint8_t* stop) {
+    return guarded([&] {
+        const MeshView input = view(*m);
+        const Bounds b = bounds(input);
+        const double diameter = std::max(1e-20, b.radius * 2);
+        neural::ActionRanker rank = [&](const neural::ActionState& state,
+                                        std::span<const neural::ActionRecord> rows) {
+            std::vector<float> scores(rows.size());
+            const MeshView v = state.view();
+            for (size_t i = 0; i < rows.size(); ++i) {
+                const Vec3 d = (v.positions[rows[i].action.to] - v.positions[rows[i].action.from]) * (1 / diameter);
+                scores[i] = -float(length(d));
+            }
+            return scores;
+        };
+        neural::ActionGate gate = [&](MeshView candidate) {
+            for (int g = 0; g < 4; ++g) {
+                EvalSettings s = settings_of(gates[g]);
+                s.max_supersample = neural::bounded_refinement(s);
+                if (!neural::audit_measurement_passed(evaluate(input, candidate, b, s))) return false;
+            }
+            return true;
+        };
+        std::array<float, neural::conditions> c{};
+        neural::ActionStats stats;
+        Lod lod = neural::execute_actions(input, c, target, budget, rank, gate, &stats, {}, batch);
+        std::memcpy(out_indices, lod.data.indices.data(), lod.data.indices.size() * 4);
+        *out_faces = uint32_t(lod.data.indices.size() / 3);
+        *trials = stats.trials, *accepted = stats.accepted, *rejected = stats.rejected;
+        *stop = uint8_t(stats.stop_reason);
+    });
 }
 // The random mask pairs of tests/precision.cpp:82-91 (mt19937 seed 2921, 13x11).
 void br_precision_masks(uint32_t seed, uint32_t trials, uint64_t* a_out, uint64_t* b_out) {

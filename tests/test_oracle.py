@@ -173,3 +173,24 @@ def test_oracle_matches_reference_live_ribbons(oracle, reference):
         idx = reference.trial_endpoint(mesh, int(frm), int(to))
         cand = syn.Mesh(mesh.positions, idx, double_sided=mesh.double_sided)
         assert bytes(oracle.evaluate(mesh, cand, bo, s)) == bytes(reference.evaluate(mesh, cand, bo, s))
+
+
+@pytest.mark.parametrize("level,seed,screen,limit,batch,budget", [
+    (2, 1, 24.0, 1.0, 1, 120), (2, 3, 24.0, 0.6, 8, 100), (3, 2, 24.0, 1.0, 64, 40), (3, 5, 48.0, 0.5, 16, 60)])
+def test_endpoint_walk_matches_reference_executor(oracle, reference, level, seed, screen, limit, batch, budget):
+    """The oracle's executor walk (rank, disjoint batches, halving on
+    rejection, stop reasons), run over endpoint collapses, equals the
+    reference's own neural::execute_actions (action.cpp:453-525) with the same
+    ShortestEdge ranking and four blitz::evaluate gates: trial count, accepted
+    collapses, stop reason and final indices. The GPU executor is compared
+    with the same walk over midpoint collapses (tests/test_gpu_executor.py)."""
+    mesh = syn.noisy_icosphere(level, seed)
+    views = (8, 0, 0xB1172026)
+    gates = [settings(screen, 2.0, views, 4, 8, 1.0), settings(screen, limit, views, 4, 8, 1.0),
+             settings(screen, 2.0, views, 8, 8, 0.5), settings(screen, limit, views, 8, 8, 0.5)]
+    mine = oracle.execute_endpoint(mesh, mesh.face_count // 2, budget, gates, batch)
+    ref = reference.execute_actions(mesh, mesh.face_count // 2, budget, gates, batch)
+    assert mine["trials"] == ref["trials"] and len(mine["commits"]) == ref["accepted"]
+    assert mine["stop"] == ref["stop"]
+    assert np.array_equal(mine["indices"], ref["indices"])
+    assert ref["accepted"] > 0
