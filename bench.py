@@ -61,7 +61,6 @@ BATCH_GATE_ARGS = [(BATCH_SCREEN, SOURCE_LIMIT, BATCH_VIEWS, SS, SS, 1.0),
                    (BATCH_SCREEN, TRANSITION_LIMIT, BATCH_VIEWS, SS, SS, 1.0),
                    (BATCH_SCREEN, SOURCE_LIMIT, BATCH_VIEWS, SS, SS, 1.0),
                    (BATCH_SCREEN, TRANSITION_LIMIT, BATCH_VIEWS, SS, SS, 1.0)]
-CPU_SAMPLE_VIEWS = 4  # views of the bounded reference sample, scaled to 64
 
 
 def peaks() -> dict:
@@ -174,60 +173,131 @@ def _reference_audit(job):
     return time.perf_counter() - t0, int(ok)
 
 
-def _reference_batched_audit(job):
-    """Four-gate reference audit (blitz::evaluate, evaluate.cpp:353) of one
-    midpoint collapse of a batched-set mesh on CPU_SAMPLE_VIEWS views."""
-    mesh = job
+def host_cpu() -> dict:
+    """The host's CPU model and the threads this process may use."""
+    model = "unknown"
+    try:
+        for line in Path("/proc/cpuinfo").read_text().splitlines():
+            if line.startswith("model name"):
+                model = line.split(":", 1)[1].strip()
+                break
+    except OSError:
+        pass
+    try:
+        usable = len(os.sched_getaffinity(0))
+    except AttributeError:
+        usable = os.cpu_count() or 1
+    return {"model": model, "nproc": usable}
+
+
+def _reference_gate(job):
+    """One gate of the reference's four-gate audit: blitz::evaluate
+    (evaluate.cpp:353) of a midpoint trial against the source on all 64 views
+    at 512 px x ss 8. Returns (busy seconds, passed)."""
+    pos, idx, trial_idx, trial_pos, gate = job
     sys.path.insert(0, str(ROOT))
     from blitzremesher_b200 import synthetic as syn
-    from oracle.oracle import BoEdit, Oracle, Reference, settings
+    from oracle.oracle import Reference, settings
 
-    O, R = Oracle(), Reference()
-    first = O.actions(mesh, placement=True, preserve_uv=False)[0]  # the GPU's first pick of this mesh
-    e = BoEdit()
-    e.from_, e.to = first.from_, first.to
-    idx, pos, _, valid = O.trial_midpoint(mesh, e, preserve_uv=False)
-    b = R.bounds(mesh)
-    cand = syn.Mesh(pos, idx)
-    views = (CPU_SAMPLE_VIEWS, 0, BATCH_VIEWS[2])
+    R = Reference()
+    src, cand = syn.Mesh(pos, idx), syn.Mesh(trial_pos, trial_idx)
+    a = BATCH_GATE_ARGS[gate]
     t0 = time.perf_counter()
-    ok = valid
-    if valid:
-        for a in BATCH_GATE_ARGS:
-            m = R.evaluate(mesh, cand, b, settings(a[0], a[1], views, a[3], a[4], a[5]))
-            if not (m.complete and m.passed and not m.resource_limited):
-                ok = False
-                break
-    return time.perf_counter() - t0, int(ok)
+    m = R.evaluate(src, cand, R.bounds(src), settings(*a))
+    return time.perf_counter() - t0, bool(m.complete and m.passed and not m.resource_limited)
 
 
-def cpu_reference_batched(meshes, threads: int, per_thread: int = 1) -> dict:
-    """The reference CPU audit on a bounded sample of the batched workload:
-    the first candidate of the meshes nearest the median face count, each on
-    CPU_SAMPLE_VIEWS of the 64 views, the time scaled to 64 views."""
-    from concurrent.futures import ProcessPoolExecutor
-    import multiprocessing as mp
+def _noop(_):
+    return 0
 
-    order = np.argsort([m.face_count for m in meshes])
-    mid = len(order) // 2
-    n = max(1, threads * per_thread)
-    chosen = [int(order[(mid + k) % len(order)]) for k in range(n)]
-    jobs = [meshes[i] for i in chosen]
-    t0 = time.perf_counter()
-    if threads <= 1:
-        results = [_reference_batched_audit(j) for j in jobs]
-    else:
-        with ProcessPoolExecutor(max_workers=threads, mp_context=mp.get_context("spawn")) as ex:
-            results = list(ex.map(_reference_batched_audit, jobs))
-    wall = time.perf_counter() - t0
-    scale = BATCH_VIEWS[0] / CPU_SAMPLE_VIEWS
-    busy = sum(r[0] for r in results)
-    value = len(jobs) / (scale * (wall if threads > 1 else busy))
-    faces = [meshes[i].face_count for i in chosen]
-    return {"value": value, "wall_s": wall, "busy_s": busy, "candidates": len(jobs),
-            "sample": f"{len(jobs)} midpoint collapse(s) of meshes with {faces} faces, reference blitz::evaluate "
-                      f"over the four gates with early exit on {CPU_SAMPLE_VIEWS} of the 64 views at 512 px x ss8 "
-                      f"({busy:.1f} s busy), time scaled x{scale:.0f} to 64 views"}
+
+class ReferenceSampler:
+    """The reference CPU audit on a bounded sample of the batched workload.
+
+    Sample: one mesh from each face-count quartile of the 64 (the quartile's
+    median), several of the benchmark's own candidates per mesh, every
+    candidate audited in full: the four gates (blitz::evaluate each, all 64
+    views at 512 px x ss 8, no scaling) as independent jobs on a pool of
+    host processes. A step audits `per_step` candidates (four gate jobs each)
+    round-robin over the quartiles; its wall time is the step time. The
+    midpoint trials come from the oracle, outside the timed part (the
+    reference has midpoint placement only in CUDA)."""
+
+    def __init__(self, meshes, picks_of, threads: int):
+        from concurrent.futures import ProcessPoolExecutor
+        import multiprocessing as mp
+
+        from oracle.oracle import BoEdit, Oracle
+
+        order = np.argsort([m.face_count for m in meshes], kind="stable")
+        q = len(order) // 4
+        self.quartile_meshes = [int(order[min(len(order) - 1, k * q + q // 2)]) for k in range(4)]
+        self.threads = max(1, threads)
+        self.per_step = max(1, self.threads // 4)
+        O = Oracle()
+        self.meshes = meshes
+        self.items = []  # (mesh index, pick position, trial job payload, placement valid)
+        for slot in range(16):
+            mi = self.quartile_meshes[slot % 4]
+            picks = picks_of(mi)
+            pick = (slot // 4 * 21) % len(picks)
+            e = BoEdit()
+            e.from_, e.to = int(picks[pick]["from"]), int(picks[pick]["to"])
+            tidx, tpos, _, valid = O.trial_midpoint(meshes[mi], e, preserve_uv=False)
+            self.items.append((mi, pick, (meshes[mi].positions, meshes[mi].indices, tidx, tpos), bool(valid)))
+        self.pool = ProcessPoolExecutor(max_workers=self.threads, mp_context=mp.get_context("spawn"))
+        list(self.pool.map(_noop, range(self.threads)))
+        self.cursor = 0
+        self.results = []  # (mesh index, pick, faces, sequential seconds, accepted)
+
+    def step(self) -> float:
+        chosen = [self.items[(self.cursor + k) % len(self.items)] for k in range(self.per_step)]
+        self.cursor += self.per_step
+        jobs, owners = [], []
+        for n, (mi, pick, payload, valid) in enumerate(chosen):
+            if not valid:
+                continue
+            for g in range(4):
+                jobs.append((*payload, g))
+                owners.append(n)
+        t0 = time.perf_counter()
+        out = list(self.pool.map(_reference_gate, jobs))
+        wall = time.perf_counter() - t0
+        for n, (mi, pick, _, valid) in enumerate(chosen):
+            gates = [r for r, o in zip(out, owners) if o == n]
+            seq, ok = 0.0, valid
+            for busy, passed in gates:  # the reference's sequential audit stops at the first failing gate
+                seq += busy
+                if not passed:
+                    ok = False
+                    break
+            self.results.append((mi, pick, self.meshes[mi].face_count, seq, ok))
+        return wall
+
+    def close(self):
+        self.pool.shutdown()
+
+    def summary(self, wall_s: float, steps: int) -> dict:
+        per_mesh = {}
+        for mi, pick, faces, seq, ok in self.results:
+            d = per_mesh.setdefault(mi, {"faces": faces, "candidates": 0, "seconds": 0.0, "accepted": 0})
+            d["candidates"] += 1
+            d["seconds"] += seq
+            d["accepted"] += int(ok)
+        for d in per_mesh.values():
+            d["collapses_per_s_1thread"] = d["candidates"] / d["seconds"] if d["seconds"] else None
+        total_faces = sum(d["faces"] * d["candidates"] for d in per_mesh.values())
+        weighted = sum(d["faces"] * d["candidates"] / d["seconds"] for d in per_mesh.values() if d["seconds"])
+        n = len(self.results)
+        return {"value": n / wall_s if wall_s else 0.0, "candidates": n, "wall_s": wall_s,
+                "ms_per_step": 1e3 * wall_s / max(1, steps),
+                "collapses_per_s_1thread_face_weighted": weighted / total_faces if total_faces else None,
+                "per_mesh": {self.meshes[k].name: v for k, v in per_mesh.items()},
+                "sample": f"{n} of the benchmark's midpoint collapses, {self.per_step} per step, on 4 meshes "
+                          f"(one per face-count quartile: {[self.meshes[k].face_count for k in self.quartile_meshes]} "
+                          f"faces), each audited in full by the reference's blitz::evaluate: four gates, all 64 "
+                          f"views at 512 px x ss8, no scaling; the four gate evaluations of a candidate run as "
+                          f"parallel jobs on {self.threads} host processes"}
 
 
 def run_reference(args) -> None:
@@ -237,21 +307,34 @@ def run_reference(args) -> None:
     threads = os.cpu_count() or 1
     if args.config == "batched":
         from blitzremesher_b200 import synthetic as syn
+        from oracle.oracle import Oracle
 
         meshes = syn.batched_set(BATCH_MESHES, seed=2)
-        vals, samples = [], ""
-        for _ in range(args.steps):
-            r = cpu_reference_batched(meshes, min(threads, 64))
-            vals.append(r["value"])
-            samples = r["sample"]
-        value = float(np.mean(vals))
+        cpu = host_cpu()
+        threads = min(cpu["nproc"], 64)
+        oracle = Oracle()
+
+        def picks_of(mi):
+            acts = oracle.actions(meshes[mi], placement=True, preserve_uv=False)
+            idx = np.linspace(0, len(acts) - 1, min(BATCH_PER_MESH, len(acts))).astype(np.int64)
+            return [{"from": acts[i].from_, "to": acts[i].to} for i in idx]
+
+        sampler = ReferenceSampler(meshes, picks_of, threads)
+        for _ in range(args.warmup):  # warm-up: pool round trips (the trials are prepared untimed above)
+            list(sampler.pool.map(_noop, range(sampler.threads)))
+        wall = sum(sampler.step() for _ in range(args.steps))
+        r = sampler.summary(wall, args.steps)
+        sampler.close()
+        value = r["value"]
         line = {"metric": METRIC, "value": value, "unit": "collapses/s", "n_gpus": args.gpus, "steps": args.steps,
-                "warmup": args.warmup, "ms_per_step": 1e3 * BATCH_MESHES * BATCH_PER_MESH / value,
-                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-                "data": "synthetic", "impl": "reference",
-                "config": {"workload": BATCH_WORKLOAD, "threads": min(threads, 64)},
-                "cpu_baseline": {"value": value, "unit": "collapses/s", "cores": min(threads, 64),
-                                 "kind": "reference", "sample": samples},
+                "warmup": args.warmup, "ms_per_step": r["ms_per_step"], "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+                "config": {"workload": BATCH_WORKLOAD, "threads": threads, "cpu": cpu,
+                           "step": f"{sampler.per_step} candidate audits (4 gate jobs each) on {threads} processes"},
+                "cpu_baseline": {"value": value, "unit": "collapses/s", "cores": threads, "kind": "reference",
+                                 "sample": r["sample"], "cpu_model": cpu["model"], "nproc": cpu["nproc"],
+                                 "collapses_per_s_1thread_face_weighted": r["collapses_per_s_1thread_face_weighted"],
+                                 "per_mesh": r["per_mesh"]},
                 "e2e": {"value": value, "unit": "collapses/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line), flush=True)
         return
@@ -330,14 +413,20 @@ def run_icosphere(args, rank: int, world: int, local: int) -> dict:
     verdicts = verdict_dev.cpu().numpy().view(br.VERDICT_DTYPE)
     accepted = int(verdicts["accepted"].sum())
 
-    # Kernel profile: audit-kernel device time and the samples it touched.
-    session.profile(True)
+    # Kernel profile: the samples the audit kernel touched (counting replay),
+    # and its device time from a replay whose kernels run without counters.
+    session.profile(1)
     for _ in range(args.steps):
         step()
     torch.cuda.synchronize(device)
     prof = session.profile()
-    session.profile(False)
-    audit_ms = prof["audit_ms"] / max(1, prof["audit_launches"])
+    session.profile(2)
+    for _ in range(args.steps):
+        step()
+    torch.cuda.synchronize(device)
+    timing = session.profile()
+    session.profile(0)
+    audit_ms = timing["audit_ms"] / max(1, timing["audit_launches"])
     # Algorithmic bytes per audit launch: candidate records, per sample one
     # state-count byte plus one reference-mask bit, one 16-byte view record out.
     launches = max(1, prof["audit_launches"])
@@ -398,8 +487,9 @@ def run_icosphere(args, rank: int, world: int, local: int) -> dict:
                     "h2d_bytes_per_step": int(n * br.COLLAPSE_DTYPE.itemsize + 4 * 64),
                     "d2h_bytes_per_step": int(n * br.VERDICT_DTYPE.itemsize + 4)},
             "gpu_launches": int(prof["launches"] // max(1, args.steps) * args.steps),
-            "kernel_ms": {"prepare": prof["prepare_ms"] / args.steps, "audit": prof["audit_ms"] / args.steps,
-                          "verdicts": prof["verdict_ms"] / args.steps}}
+            "kernel_ms": {"prepare": timing["prepare_ms"] / args.steps, "audit": timing["audit_ms"] / args.steps,
+                          "verdicts": timing["verdict_ms"] / args.steps,
+                          "note": "CUDA events around each launch of a replay without counters"}}
     # Learned surrogate: trained on exact-audit labels of the icosphere family
     # (seeds 2..9, states at 100/70/50/35/25% faces), judged on 16 held-out
     # seeds (1001..1016): pruning to the top 25% and whole LOD steps.
@@ -546,13 +636,17 @@ def run_batched(args, rank: int, world: int, local: int) -> dict:
     _barrier(world)
     max_ms = _max_over_ranks(start.elapsed_time(end), world, device)
     verdicts = verdict_dev.cpu().numpy().view(br.VERDICT_DTYPE).copy()
-    # Audit kernels: device time and work counters of one profiled batch.
+    # Audit kernels: work counters of one counting batch, device time of one
+    # batch whose kernels run without counters (as in the graph replays).
     step(br.BATCH_PROFILE)
     torch.cuda.synchronize(device)
     info = batch.info()
     assert np.array_equal(verdict_dev.cpu().numpy().view(br.VERDICT_DTYPE), verdicts)
+    step(br.BATCH_TIMING)
+    torch.cuda.synchronize(device)
+    audit_ms = batch.info()["audit_ms"]
     alg_bytes = n * 624 * 1 + info["region_samples"] * (1 + 1 / 8) + info["units"] * 16
-    achieved_gbs = alg_bytes / (info["audit_ms"] * 1e-3) / 1e9
+    achieved_gbs = alg_bytes / (audit_ms * 1e-3) / 1e9
     pk = peaks()
     # End to end through the host C ABI (blitz_audit_batch_candidates_host):
     # pinned host candidates in, host verdicts out, copies inside every step.
@@ -592,7 +686,8 @@ def run_batched(args, rank: int, world: int, local: int) -> dict:
                        "parallelism": f"dp{world} (64 meshes per rank)"},
             "roofline": {"bound": "hbm", "achieved": achieved_gbs, "peak": pk["hbm_gbs"], "unit": "GB/s",
                          "frac": achieved_gbs / pk["hbm_gbs"], "traffic": None,
-                         "kernel": "k_audit (+ large and huge tiers)", "kernel_ms": info["audit_ms"],
+                         "kernel": "k_audit (+ large and huge tiers)", "kernel_ms": audit_ms,
+                         "kernel_ms_counting": info["audit_ms"],
                          "algorithmic_bytes": alg_bytes, "units_per_launch": info["units"],
                          "samples_per_launch": info["region_samples"],
                          "peak_source": pk["source"] + " hbm_gbs (burst)",
@@ -612,10 +707,25 @@ def run_batched(args, rank: int, world: int, local: int) -> dict:
                     "h2d_bytes_per_step": int(n * br.COLLAPSE_DTYPE.itemsize),
                     "d2h_bytes_per_step": int(n * br.VERDICT_DTYPE.itemsize)},
             "gpu_launches": int((2 * len(meshes) + 3 + 3) * args.steps)}
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        r = cpu_reference_batched(meshes, 1)
-        line["cpu_baseline"] = {"value": r["value"], "unit": "collapses/s", "cores": 1, "kind": "reference",
-                                "sample": r["sample"]}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and len(meshes) == BATCH_MESHES:
+        # The reference CPU audit of some of the same candidates, on all host
+        # cores for one bounded step; its verdicts must equal the GPU's.
+        cpu = host_cpu()
+        sampler = ReferenceSampler(meshes, lambda mi: picks[mi], min(cpu["nproc"], 64))
+        wall = sampler.step()
+        r = sampler.summary(wall, 1)
+        sampler.close()
+        offsets = np.concatenate([[0], np.cumsum(counts)])
+        checked = [(mi, pick, ok) for mi, pick, _, _, ok in sampler.results]
+        mismatches = [(mi, pick) for mi, pick, ok in checked if bool(verdicts[offsets[mi] + pick]["accepted"]) != ok]
+        assert not mismatches, f"reference and GPU verdicts differ: {mismatches}"
+        line["parity_checked"] = len(checked)
+        line["cpu_baseline"] = {"value": r["value"], "unit": "collapses/s", "cores": sampler.threads,
+                                "kind": "reference", "sample": r["sample"], "cpu_model": cpu["model"],
+                                "nproc": cpu["nproc"], "wall_s": wall,
+                                "collapses_per_s_1thread_face_weighted": r["collapses_per_s_1thread_face_weighted"],
+                                "per_mesh": r["per_mesh"],
+                                "parity": f"{len(checked)} reference verdicts equal the GPU's"}
     batch.close()
     for s_ in sessions:
         s_.close()

@@ -273,7 +273,7 @@ class BatchInfo(C.Structure):
                 ("flipped_samples", C.c_uint64), ("region_split", C.c_uint64 * 8)]
 
 
-BATCH_GRAPH, BATCH_AUTOTUNE, BATCH_PROFILE = 1, 2, 4
+BATCH_GRAPH, BATCH_AUTOTUNE, BATCH_PROFILE, BATCH_TIMING = 1, 2, 4, 8
 
 
 class AuditProfile(C.Structure):
@@ -550,8 +550,10 @@ class AuditSession:
         err = C.create_string_buffer(512)
         _check(self.lib.blitz_audit_reset(self.handle, err, 512), err)
 
-    def profile(self, enable: Optional[bool] = None) -> dict:
-        """Enables/disables kernel profiling (resetting counters) or reads it."""
+    def profile(self, enable: Optional[int] = None) -> dict:
+        """Enables kernel profiling (1 or True: device times and work counters;
+        2: device times only, kernels without counters), disables it (0), or
+        reads it (None). Enabling resets the totals."""
         if enable is not None:
             assert self.lib.blitz_audit_profile_enable(self.handle, int(enable)) == BLITZ_OK
         p = AuditProfile()

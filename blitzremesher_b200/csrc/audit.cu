@@ -125,15 +125,117 @@ __device__ __forceinline__ void record_write(ViewRecord* out, const ViewRecord& 
     if (lane_id() == 0) *out = r;
 }
 
+// Rows of interval ends kept per pass of the word-row region phase.
+constexpr int kPassRows = 8;
+
+// Region phase over coverage words (the global tiers): lanes own 32-sample
+// words of the region's rows (several rows per pass when the region is
+// narrow). Per (face, row) the covered samples are one interval (exact
+// FP64 binary searches, face_interval), computed once per pass by the lanes
+// together and kept in `iv` (shared memory); each lane turns the intervals
+// crossing its word into masks: the union of the new faces' masks (B) and
+// a bit-sliced count of the old faces covering each sample (A). Because the
+// state's count pc includes every old face (pc >= A), the candidate's count
+// pc - A + B is positive wherever B > 0, and where B = 0 it is pc - A. So a
+// sample flips iff it is newly covered (B > 0 on a state-empty sample, from
+// the state's coverage word alone) or it loses its last faces (B = 0, A > 0
+// and pc == A: the only samples whose state count is read). Flipped samples
+// are written to the region words (candidate XOR state) and counted into the
+// popcount deltas against the reference.
+__device__ void region_word_rows(const FaceSetup* faces, uint32_t nok, int wx0, int ry0, int ry1, int words,
+                                 const PlanView& pv, uint32_t size, bool same_ref, uint32_t* region, short2* iv,
+                                 int& dchg, int& dtot, int& dcov, int& flips, bool& negative) {
+    const uint32_t lane = lane_id();
+    // Lanes per row: the region's words rounded up to a power of two (at
+    // most 32); rows per pass: 32 / that, at most kPassRows.
+    uint32_t span = 1;
+    while (span < uint32_t(words) && span < 32) span <<= 1;
+    const uint32_t rows_per_pass = min(uint32_t(kPassRows), 32u / span);
+    const uint32_t my_row = lane / span, my_word = lane % span;
+    for (int ybase = ry0; ybase <= ry1; ybase += int(rows_per_pass)) {
+        const uint32_t pass_rows = min(rows_per_pass, uint32_t(ry1 - ybase + 1));
+        // Interval ends of every (row, face) of this pass.
+        const uint32_t items = pass_rows * nok;
+        for (uint32_t t = lane; t < items; t += 32) {
+            const uint32_t r = t / nok, f = t - r * nok;
+            const int y = ybase + int(r);
+            const FaceSetup& fs = faces[f];
+            int lo = 1, hi = 0;
+            if (y >= fs.y0 && y <= fs.y1) face_interval(fs, double(y) + .5, lo, hi);
+            iv[r * kMaxOk + f] = make_short2(short(lo), short(hi));
+        }
+        __syncwarp();
+        const int y = ybase + int(my_row);
+        const bool row_ok = my_row < pass_rows;
+        for (uint32_t w = my_word; row_ok && w < uint32_t(words); w += span) {
+            const int xb = wx0 + 32 * int(w); // first sample of the word
+            uint32_t bnew = 0, a0 = 0, a1 = 0, a2 = 0, a3 = 0, a4 = 0, a5 = 0;
+            for (uint32_t f = 0; f < nok; ++f) {
+                const short2 e = iv[my_row * kMaxOk + f];
+                const int lo = max(int(e.x), xb), hi = min(int(e.y), xb + 31);
+                if (lo > hi) continue;
+                const uint32_t m = (hi - xb == 31 ? 0xffffffffu : ((2u << (hi - xb)) - 1u)) & ~((1u << (lo - xb)) - 1u);
+                if (faces[f].pad > 0) {
+                    bnew |= m;
+                } else { // bit-sliced count of the old faces (at most 48 < 64)
+                    uint32_t c = m, t;
+                    t = a0 & c, a0 ^= c, c = t;
+                    t = a1 & c, a1 ^= c, c = t;
+                    t = a2 & c, a2 ^= c, c = t;
+                    t = a3 & c, a3 ^= c, c = t;
+                    t = a4 & c, a4 ^= c, c = t;
+                    a5 ^= c;
+                }
+            }
+            const uint32_t aany = a0 | a1 | a2 | a3 | a4 | a5;
+            if (!(bnew | aany)) {
+                region[uint32_t(y - ry0) * uint32_t(words) + w] = 0;
+                continue;
+            }
+            const uint32_t cw = uint32_t(xb) >> 5;
+            const uint32_t S = chunk_global(pv.state_bits, size, uint32_t(y), cw);
+            const uint32_t R = same_ref ? S : chunk_global(pv.ref_bits, size, uint32_t(y), cw);
+            const uint32_t grown = bnew & ~S;   // newly covered
+            uint32_t lost_cand = aany & ~bnew;  // covered only if other faces cover it
+            negative |= (lost_cand & ~S) != 0;  // pc >= A > 0 must hold
+            lost_cand &= S;
+            uint32_t lost = 0;
+            const size_t row_at = size_t(y) * size;
+            while (lost_cand) {
+                const int i = __ffs(lost_cand) - 1;
+                lost_cand &= lost_cand - 1;
+                const uint32_t A = ((a0 >> i) & 1u) | (((a1 >> i) & 1u) << 1) | (((a2 >> i) & 1u) << 2) |
+                                   (((a3 >> i) & 1u) << 3) | (((a4 >> i) & 1u) << 4) | (((a5 >> i) & 1u) << 5);
+                const uint32_t pc = pv.state_count[row_at + size_t(xb + i)];
+                negative |= pc < A;
+                if (pc == A) lost |= 1u << i;
+            }
+            const uint32_t fl = grown | lost;
+            region[uint32_t(y - ry0) * uint32_t(words) + w] = fl;
+            if (!fl) continue;
+            flips += __popc(fl);
+            dcov += __popc(grown) - __popc(lost);
+            const uint32_t X = S ^ R;
+            dchg += __popc(fl & ~X) - __popc(fl & X);
+            dtot += __popc(fl & ~R & ~S) - __popc(fl & ~R & S);
+        }
+        __syncwarp();
+    }
+}
+
 // `spill` (small tier only): units that overflow the tier's limits append
 // their unit index `u` there for the large tier instead of falling back.
 template <class L>
 __device__ void audit_unit(const CandidateRecord* __restrict__ rec, const PlanDev& plan, uint32_t v,
                            WarpScratch<L>& ws, ViewRecord* out, unsigned long long* stats, uint32_t u,
-                           uint32_t* spill, uint32_t heavy = 0xffffffffu, FaceSetup* face_table = nullptr) {
+                           uint32_t* spill, uint32_t heavy = 0xffffffffu, FaceSetup* face_table = nullptr,
+                           short2* iv_table = nullptr) {
     // The face setups: in the warp's scratch, or in shared memory for the
     // tiers whose scratch is global (the row sweep reads them every row).
     FaceSetup* const faces = face_table ? face_table : ws.faces;
+    // With an interval table the region phase runs over coverage words
+    // (region_word_rows) and the distance phase walks the region words.
+    const bool word_rows = iv_table != nullptr;
     constexpr int kRegionWords = L::kRegionWords, kRegionRows = L::kRegionRows;
     constexpr int kDeltaSamples = L::kDeltaSamples, kQueue = L::kQueue, kAffected = L::kAffected;
     const uint32_t lane = lane_id();
@@ -277,9 +379,11 @@ __device__ void audit_unit(const CandidateRecord* __restrict__ rec, const PlanDe
         } else {
             samples = uint64_t(rows) * uint64_t(words) * 32;
             // ws.region holds the candidate's coverage words XOR the state's
-            // over the region (its flipped samples).
+            // over the region (its flipped samples). The word-row pass writes
+            // every word itself; the other paths flip bits of zeroed words.
             const int nwords = rows * words;
-            for (int k = int(lane); k < nwords; k += 32) ws.region[k] = 0;
+            if (!word_rows)
+                for (int k = int(lane); k < nwords; k += 32) ws.region[k] = 0;
             if (lane == 0) ws.qcount[0] = 0;
             __syncwarp();
             const long long t_zero = stats ? clock64() : 0;
@@ -311,7 +415,10 @@ __device__ void audit_unit(const CandidateRecord* __restrict__ rec, const PlanDe
                     if (pos < uint32_t(kQueue)) ws.queue[pos] = xr | (yr << 15) | (C ? 0x80000000u : 0u);
                 }
             };
-            if (direct) {
+            if (word_rows) {
+                region_word_rows(faces, nok, wx0, ry0, ry1, words, pv, size, same_ref, ws.region, iv_table, dchg, dtot,
+                                 dcov, flips, negative);
+            } else if (direct) {
                 const uint32_t delta_words = uint32_t(bws * bh) >> 2;
                 for (uint32_t k = lane; k < delta_words; k += 32) ws.delta[k] = 0x80808080u;
                 uint32_t c0 = 0, c1 = 0;
@@ -437,7 +544,7 @@ __device__ void audit_unit(const CandidateRecord* __restrict__ rec, const PlanDe
             if (stats) {
                 st_zero = t_zero - t_setup;
                 st_path = clock64() - t_zero;
-                st_kind = direct ? 0 : 1;
+                st_kind = direct && !word_rows ? 0 : 1;
                 st_rows = bh;
             }
             if (__any_sync(0xffffffffu, negative)) fallback = true;
@@ -553,7 +660,7 @@ __device__ void audit_unit(const CandidateRecord* __restrict__ rec, const PlanDe
         }
         __syncwarp();
         const uint32_t queued = same_ref ? nflips : 0;
-        if (same_ref && queued <= uint32_t(kQueue)) {
+        if (same_ref && !word_rows && queued <= uint32_t(kQueue)) {
             // The region's changed samples are its flips, queued in phase 2.
             // Candidate-only samples measure to the reference (resident field
             // or search), reference-only samples search the candidate.
@@ -748,6 +855,7 @@ __global__ void __launch_bounds__(kWarps * 32, 2)
     k_audit_global(const __grid_constant__ AuditJob job, unsigned long long* stats, const uint32_t* spill,
                    uint32_t* cursor, unsigned char* scratch, uint32_t* spill_next) {
     __shared__ FaceSetup face_table[kWarps][kMaxOk];
+    __shared__ short2 iv_table[kWarps][kPassRows * kMaxOk];
     const uint32_t lane = lane_id();
     const uint32_t slot = blockIdx.x * kWarps + (threadIdx.x >> 5);
     WarpScratch<L>& ws = reinterpret_cast<WarpScratch<L>*>(scratch)[slot];
@@ -765,7 +873,7 @@ __global__ void __launch_bounds__(kWarps * 32, 2)
         resolve_unit(job, u, plan, recs, out, lu);
         const uint32_t c = lu / plan->nviews, v = lu - c * plan->nviews;
         audit_unit(recs + c, *plan, v, ws, out + lu, stats, u, spill_next, 0xffffffffu,
-                   face_table[threadIdx.x >> 5]);
+                   face_table[threadIdx.x >> 5], iv_table[threadIdx.x >> 5]);
     }
 }
 

@@ -437,8 +437,9 @@ struct Session {
     size_t sort_bytes = 0;
     blitz_neural_info info{};
     uint64_t internal_errors = 0;
-    // profiling
-    bool profiling = false;
+    // profiling: device times of candidate calls; work counters as well
+    // (per-unit clock and counter atomics in the audit kernels) when counting
+    bool profiling = false, counting = false;
     blitz_audit_profile profile{};
     Buf<unsigned long long> stats;
     cudaEvent_t ev[6] = {};
@@ -1067,7 +1068,7 @@ static void audit_candidates(Session& S, const blitz_collapse* cands_dev, const 
     const uint32_t nn = uint32_t(n);
     Topology& t = S.topo;
     S.records.ensure(S.pool, nn);
-    const bool prof = S.profiling && nn;
+    const bool prof = S.profiling && nn, counted = prof && S.counting;
     if (prof) {
         S.stats.ensure(S.pool, kAuditStats);
         B200_CUDA(cudaMemsetAsync(S.stats.p, 0, kAuditStats * 8, st));
@@ -1079,7 +1080,7 @@ static void audit_candidates(Session& S, const blitz_collapse* cands_dev, const 
     S.profile.launches += nn ? 1 : 0;
     upload_verdict_tables(S, a, nn, st);
     for (Plan* pp : a.plans) {
-        run_audit(S, *pp, nn, prof ? S.stats.p : nullptr, st);
+        run_audit(S, *pp, nn, counted ? S.stats.p : nullptr, st);
         if (nn) S.profile.launches += 1, S.profile.audit_launches += 1;
     }
     if (prof) B200_CUDA(cudaEventRecord(S.ev[4], st));
@@ -1103,6 +1104,7 @@ static void audit_candidates(Session& S, const blitz_collapse* cands_dev, const 
         S.profile.prepare_ms += ta;
         S.profile.audit_ms += tb;
         S.profile.verdict_ms += tc;
+        if (!counted) h[0] = h[1] = h[2] = 0;
         S.profile.units += h[0];
         S.profile.region_samples += h[1];
         S.profile.changed_samples += h[2];
@@ -2069,7 +2071,9 @@ blitz_status blitz_audit_profile_enable(blitz_audit_session* s, int enable) {
         DeviceScope scope(S.device);
         if (enable && !S.ev[0])
             for (auto& e : S.ev) B200_CUDA(cudaEventCreate(&e));
+        if (enable < 0 || enable > 2) throw Failure(BLITZ_INVALID_ARGUMENT, "profile mode is 0, 1 or 2");
         S.profiling = enable != 0;
+        S.counting = enable == 1;
         S.profile = blitz_audit_profile{};
     });
 }
@@ -2381,8 +2385,8 @@ static void batch_candidates(blitz_audit_batch* b, const blitz_collapse* cands, 
                              const blitz_eval_settings gates_in[4], blitz_candidate_verdict* out, uint32_t flags,
                              cudaStream_t st) {
     {
-        if (!b || !counts || !gates_in || flags > 7) throw Failure(BLITZ_INVALID_ARGUMENT, "bad batch arguments");
-        const bool profile = (flags & 4u) != 0;
+        if (!b || !counts || !gates_in || flags > 15) throw Failure(BLITZ_INVALID_ARGUMENT, "bad batch arguments");
+        const bool counting = (flags & 4u) != 0, profile = counting || (flags & 8u) != 0;
         if (profile && (flags & 1u)) throw Failure(BLITZ_INVALID_ARGUMENT, "profiling runs without graph replay");
         const size_t ns = b->sessions.size();
         std::vector<uint64_t> off(ns + 1, 0);
@@ -2466,7 +2470,7 @@ static void batch_candidates(blitz_audit_batch* b, const blitz_collapse* cands, 
                 if (!b->units[j]) continue;
                 AuditJob job{};
                 job.entries = b->entries[j].p, job.nentries = b->nentries[j], job.total = b->units[j];
-                launch_audit(job, profile ? b->stats.p : nullptr, b->queue.p, b->spill.p,
+                launch_audit(job, counting ? b->stats.p : nullptr, b->queue.p, b->spill.p,
                              big ? b->spill_huge.p : nullptr, big ? b->huge.p : nullptr, big ? b->huge_blocks : 0,
                              st, variant, giant ? &giant_tier : nullptr);
             }
@@ -2547,7 +2551,7 @@ static void batch_candidates(blitz_audit_batch* b, const blitz_collapse* cands, 
         B200_CUDA(cudaGetLastError());
         if (profile && off[ns]) {
             B200_CUDA(cudaEventElapsedTime(&b->audit_ms, b->ev[0], b->ev[1]));
-            B200_CUDA(cudaMemcpy(b->prof, b->stats.p, sizeof(b->prof), cudaMemcpyDeviceToHost));
+            if (counting) B200_CUDA(cudaMemcpy(b->prof, b->stats.p, sizeof(b->prof), cudaMemcpyDeviceToHost));
         }
         for (size_t i = 0; i < ns; ++i) {
             if (!exact[i]) continue;

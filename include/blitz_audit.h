@@ -347,6 +347,8 @@ typedef struct blitz_audit_batch blitz_audit_batch;
                                    verdict buffers, counts, gates, stream and session states are unchanged */
 #define BLITZ_BATCH_AUTOTUNE 2u /* time the audit variants on this call and keep the fastest */
 #define BLITZ_BATCH_PROFILE 4u  /* record the audit launches' device time and work counters (no graph) */
+#define BLITZ_BATCH_TIMING 8u   /* record the audit launches' device time only: the kernels run without
+                                   their per-unit counters (no graph) */
 typedef struct blitz_audit_batch_info {
     uint32_t struct_size;
     uint32_t sessions;
@@ -465,9 +467,12 @@ blitz_status blitz_audit_state_uv(blitz_audit_session*, float* uv, size_t uv_cap
 blitz_status blitz_audit_reset(blitz_audit_session*, char* error, size_t error_capacity);
 
 /* Device-side profile of the session's own kernels (no reference
- * counterpart; the reference exposes NVTX ranges, timeline.hpp:6-19). When
- * enabled, every candidate call times its kernels with CUDA events on the
- * launching stream and counts the samples the audit kernel touched. */
+ * counterpart; the reference exposes NVTX ranges, timeline.hpp:6-19). With
+ * enable = 1 every candidate call times its kernels with CUDA events on the
+ * launching stream and counts the samples the audit kernel touched (per-unit
+ * clock reads and counter atomics inside the kernel); with enable = 2 it only
+ * times them (the kernels run as in production, the counters stay zero);
+ * 0 disables. */
 typedef struct blitz_audit_profile {
     uint32_t struct_size, enabled;
     uint64_t launches;         /* kernels launched by candidate calls */

@@ -115,23 +115,31 @@ def test_large_regions_match_oracle(gpu_lib, oracle, commit):
             assert measurement_fields(meas[i, g]) == measurement_fields(want.gates[g]), (i, g)
 
 
-def test_huge_regions_match_oracle(gpu_lib, oracle):
+@pytest.mark.parametrize("commit", [False, True])
+def test_huge_regions_match_oracle(gpu_lib, oracle, commit):
     """An 80-face sphere at 64 px x ss 8: 1-ring regions of about 300 x 300
     samples overflow the large tier and are audited by the huge tier (global
-    scratch); verdicts and gate Measurements equal the oracle's."""
+    scratch, the word-row region phase); verdicts and gate Measurements equal
+    the oracle's, at LOD0 and after commits (state unlike its references:
+    tile maxima, region widened to whole tiles)."""
     mesh = syn.noisy_icosphere(1, 5)
     views = (6, 0, 91)
     args = _gates(64.0, views, 8)
     with br.AuditSession(mesh) as s:
+        if commit:  # loose 6 px gates so that a few collapses commit
+            s.execute(mesh.face_count - 12, 60, [br.eval_settings(64.0, 6.0, views, 8, 8, 1.0)] * 4, batch=4)
+        idx, pos = s.state()
         cands = br.midpoint_collapses(s.actions())
         picks = cands[:: max(1, cands.size // 30)]
         verdicts, meas = s.candidates(picks, [br.eval_settings(*a) for a in args], measurements=True)
-    assert np.mean(verdicts["exact_path"]) < 0.25
+    assert np.mean(verdicts["exact_path"]) < (0.5 if commit else 0.25)
+    state = syn.Mesh(pos, idx)
+    assert not commit or state.face_count < mesh.face_count
     b = oracle.bounds(mesh)
     for i, c in enumerate(picks):
         e = BoEdit()
         e.from_, e.to = int(c["from"]), int(c["to"])
-        want = oracle.audit_candidate(mesh, e, mesh, mesh, b, [oracle_settings(*a) for a in args])
+        want = oracle.audit_candidate(state, e, mesh, mesh, b, [oracle_settings(*a) for a in args])
         assert verdicts[i]["accepted"] == want.accepted and verdicts[i]["failed_gate"] == want.failed_gate, i
         stop = 4 if want.failed_gate == 0 else (want.failed_gate if want.failed_gate <= 4 else 0)
         for g in range(stop):
