@@ -21,7 +21,6 @@ constexpr int kAuditWarps = 8;
 #define B200_AUDIT_MIN_BLOCKS 3 // resident blocks per SM the register budget targets
 #endif
 constexpr int kMaxOk = 48;          // rasterized (unculled, unclipped) old + new faces
-constexpr int kMaxTileSide = 32;    // tile-maxima path for rasters up to 1024 x 1024
 constexpr uint32_t kDirectTests = 4096; // bbox samples up to which phase 1 tests every sample
 constexpr uint32_t kHeavyUnit = 512;    // changed samples above which a warp-tier unit may spill
 
@@ -248,7 +247,7 @@ __device__ void audit_unit(const CandidateRecord* __restrict__ rec, const PlanDe
     r.ca = pv.cov_ref > 0;
     r.max_d2 = 0, r.changed = 0, r.total = 0, r.cb = 0;
     const bool same_ref = plan.state_is_ref != 0; // state words equal reference words
-    if (!same_ref && (!pv.tile_t1 || plan.size > 32 * kMaxTileSide)) {
+    if (!same_ref && !pv.tile_t1) {
         // Without tile maxima a state that differs from the reference needs
         // the full distance field.
         r.flags |= kRecFallback;

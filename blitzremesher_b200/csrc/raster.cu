@@ -108,24 +108,45 @@ __global__ void k_popcounts(const uint32_t* a, const uint32_t* b, uint32_t words
 
 __device__ __forceinline__ bool bit_at(const uint32_t* bits, size_t i) { return (bits[i >> 5] >> (i & 31)) & 1u; }
 
-// Horizontal distance to the nearest covered sample of each row (INF if none).
-__device__ void k_row_nearest_body(const uint32_t* to, uint32_t width, uint32_t y, uint32_t* g);
-__global__ void k_row_nearest(const uint32_t* to, uint32_t width, uint32_t height, uint32_t* g) {
-    uint32_t y = blockIdx.x * blockDim.x + threadIdx.x;
-    if (y < height) k_row_nearest_body(to, width, y, g);
+// Horizontal distance to the nearest covered sample of row y (kNone when the
+// row has none), one warp per row: per group of 32 samples each lane takes
+// one sample, the group's coverage word is read once by all lanes, and the
+// nearest covered sample at or after / at or before the lane comes from the
+// word's bits or, when they hold none, from the groups already passed (the
+// same for all lanes). Writes are 32 consecutive words per group.
+__device__ void row_nearest_warp(const uint32_t* bits, uint32_t width, uint32_t y, uint32_t* g) {
+    const uint32_t lane = threadIdx.x & 31;
+    const size_t row = size_t(y) * width, row_end = row + width;
+    const uint32_t groups = (width + 31) / 32;
+    auto word_of = [&](uint32_t k) {
+        const size_t b = row + size_t(k) * 32;
+        const uint32_t sh = uint32_t(b & 31);
+        const size_t w = b >> 5;
+        uint32_t v = bits[w] >> sh;
+        if (sh && (w + 1) * 32 < row_end) v |= bits[w + 1] << (32 - sh); // only words holding samples of the row
+        const uint32_t rem = width - k * 32;
+        return rem >= 32 ? v : (v & ((1u << rem) - 1u));
+    };
+    uint32_t next = kNone; // first covered sample after the groups to the right
+    for (uint32_t k = groups; k-- > 0;) {
+        const uint32_t w = word_of(k), x = k * 32 + lane;
+        const uint32_t m = w & ~((1u << lane) - 1u); // covered samples at or after x in this group
+        const uint32_t at = m ? k * 32 + uint32_t(__ffs(m)) - 1 : next;
+        if (x < width) g[row + x] = at == kNone ? kNone : at - x;
+        if (w) next = k * 32 + uint32_t(__ffs(w)) - 1;
+    }
+    uint32_t last = kNone; // last covered sample of the groups to the left
+    for (uint32_t k = 0; k < groups; ++k) {
+        const uint32_t w = word_of(k), x = k * 32 + lane;
+        const uint32_t m = lane == 31 ? w : (w & ((2u << lane) - 1u)); // covered samples at or before x
+        const uint32_t at = m ? k * 32 + 31 - uint32_t(__clz(m)) : last;
+        if (x < width && at != kNone && x - at < g[row + x]) g[row + x] = x - at;
+        if (w) last = k * 32 + 31 - uint32_t(__clz(w));
+    }
 }
-__device__ void k_row_nearest_body(const uint32_t* to, uint32_t width, uint32_t y, uint32_t* g) {
-    size_t row = size_t(y) * width;
-    uint32_t last = kNone;
-    for (uint32_t x = 0; x < width; ++x) {
-        if (bit_at(to, row + x)) last = x;
-        g[row + x] = last == kNone ? kNone : x - last;
-    }
-    last = kNone;
-    for (uint32_t x = width; x-- > 0;) {
-        if (bit_at(to, row + x)) last = x;
-        if (last != kNone && last - x < g[row + x]) g[row + x] = last - x;
-    }
+__global__ void k_row_nearest(const uint32_t* to, uint32_t width, uint32_t height, uint32_t* g) {
+    const uint32_t y = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (y < height) row_nearest_warp(to, width, y, g);
 }
 
 // Lower envelope of the parabolas (y-q)^2 + g(x,q)^2 over rows q with a site
@@ -141,9 +162,20 @@ __global__ void k_column_envelope(const uint32_t* g, uint32_t width, uint32_t he
 __device__ void k_column_envelope_body(const uint32_t* g, uint32_t width, uint32_t height, uint32_t x, uint32_t* d2,
                                        int32_t* sv, long long* snum, long long* sden) {
     const uint32_t size = width; // row stride of g and d2
-    int32_t* v = sv + size_t(x) * height;
-    long long* zn = snum + size_t(x) * height;
-    long long* zd = sden + size_t(x) * height;
+    // Stack entry k of column x lives at k * width + x: neighbouring columns'
+    // entries are neighbours in memory.
+    struct Col {
+        int32_t* p;
+        size_t s;
+        __device__ int32_t& operator[](int k) const { return p[size_t(k) * s]; }
+    };
+    struct ColL {
+        long long* p;
+        size_t s;
+        __device__ long long& operator[](int k) const { return p[size_t(k) * s]; }
+    };
+    const Col v{sv + x, width};
+    const ColL zn{snum + x, width}, zd{sden + x, width};
     int k = -1;
     for (uint32_t q = 0; q < height; ++q) {
         uint32_t gq = g[size_t(q) * size + x];
@@ -301,10 +333,10 @@ __global__ void k_counts_to_bits_views(const uint8_t* counts, size_t cstride, si
     bits[size_t(wstride) * v + w] = out;
 }
 __global__ void k_row_nearest_views(const uint32_t* bits, uint32_t wstride, uint32_t size, uint32_t* g) {
-    const uint32_t y = blockIdx.x * blockDim.x + threadIdx.x, v = blockIdx.y;
+    const uint32_t y = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, v = blockIdx.y;
     if (y >= size) return;
     const size_t samples = size_t(size) * size;
-    k_row_nearest_body(bits + size_t(wstride) * v, size, y, g + samples * v);
+    row_nearest_warp(bits + size_t(wstride) * v, size, y, g + samples * v);
 }
 __global__ void k_column_envelope_views(const uint32_t* g, uint32_t size, uint32_t* d2, int32_t* sv, long long* sn,
                                         long long* sd) {
@@ -373,7 +405,8 @@ void launch_refresh_views(const DevMesh& m, const Camera* cams_dev, uint32_t nvi
         k_counts_to_bits_views<<<dim3(blocks_for(words), nviews), kThreads, 0, s>>>(counts, cstride, samples,
                                                                                      state_bits, wstride, words);
         if (state_field) {
-            k_row_nearest_views<<<dim3(blocks_for(size, 64), nviews), 64, 0, s>>>(state_bits, wstride, size, g);
+            k_row_nearest_views<<<dim3(blocks_for(uint64_t(size) * 32, 128), nviews), 128, 0, s>>>(state_bits, wstride,
+                                                                                                 size, g);
             k_column_envelope_views<<<dim3(blocks_for(size, 64), nviews), 64, 0, s>>>(g, size, state_field, sv, sn,
                                                                                        sd);
             const uint32_t tiles = ((size + 31) / 32) * ((size + 31) / 32);
@@ -433,7 +466,7 @@ void launch_tile_maxima(const uint32_t* ref_bits, const uint32_t* state_bits, co
 // Exact squared distance field of `bits` (d2 = kNone where the mask is empty).
 void launch_field(const uint32_t* bits, uint32_t width, uint32_t height, uint32_t* g, uint32_t* d2, int32_t* stack_v,
                   long long* stack_num, long long* stack_den, cudaStream_t s) {
-    k_row_nearest<<<blocks_for(height, 64), 64, 0, s>>>(bits, width, height, g);
+    k_row_nearest<<<blocks_for(uint64_t(height) * 32, 128), 128, 0, s>>>(bits, width, height, g);
     k_column_envelope<<<blocks_for(width, 64), 64, 0, s>>>(g, width, height, d2, stack_v, stack_num, stack_den);
 }
 
@@ -464,7 +497,7 @@ void launch_popcounts(const uint32_t* a, const uint32_t* b, uint32_t words, unsi
 void launch_distance(const uint32_t* from, const uint32_t* to, uint32_t width, uint32_t height, uint32_t* g,
                      uint32_t* d2, int32_t* stack_v, long long* stack_num, long long* stack_den, uint32_t* out_max,
                      cudaStream_t s) {
-    k_row_nearest<<<blocks_for(height, 64), 64, 0, s>>>(to, width, height, g);
+    k_row_nearest<<<blocks_for(uint64_t(height) * 32, 128), 128, 0, s>>>(to, width, height, g);
     k_column_envelope<<<blocks_for(width, 64), 64, 0, s>>>(g, width, height, d2, stack_v, stack_num, stack_den);
     size_t n = size_t(width) * height;
     uint32_t grid = uint32_t((n + kThreads - 1) / kThreads);

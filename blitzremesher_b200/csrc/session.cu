@@ -305,16 +305,18 @@ struct PlanKey {
 
 // A plan keeps, per view, the reference mask (CPU semantics) and the current
 // state's per-sample face counts, coverage and popcounts against the
-// reference. Plans of rasters up to 1024 x 1024 also keep both exact distance
-// fields and 32x32 tile maxima, so candidates of a state that differs from the
-// reference stay on the incremental path.
+// reference. Once the state differs from the reference, a plan also keeps the
+// reference's exact distance field (built then, not before) and the state's
+// 32x32 tile maxima (from a field computed per refresh and not kept), so
+// candidates of such a state stay on the incremental path at every raster
+// size up to 4160 x 4160.
 struct Plan {
     PlanKey key{};
     uint32_t size = 0, views = 0, words = 0;
     bool resource_limited = false, tiled = false, ref_box_clip = false;
     Buf<Camera> cameras;
     std::vector<Camera> hcams;
-    Buf<uint32_t> ref_bits, state_bits, ref_field, state_field;
+    Buf<uint32_t> ref_bits, state_bits, ref_field;
     Buf<int32_t> t1, t2;
     Buf<uint8_t> state_count;
     Buf<PlanView> dviews;
@@ -329,7 +331,7 @@ struct Plan {
     // The last combined trial evaluated on this plan, laid out like the state
     // data (so a commit of that trial swaps it in).
     Buf<uint8_t> trial_count;
-    Buf<uint32_t> trial_bits, trial_field, trial_state;
+    Buf<uint32_t> trial_bits, trial_state;
     Buf<int32_t> trial_t1, trial_t2, trial_max;
     Buf<unsigned long long> trial_pop;
     std::vector<uint32_t> trial_hstate;
@@ -345,8 +347,9 @@ struct Scratch {
     Buf<long long> sn, sd;
     Buf<unsigned long long> pop;
     size_t samples = 0;
-    // per-view field scratch of the batched state refresh
-    Buf<uint32_t> vg;
+    // per-view field scratch of the batched state refresh (vfield: the state
+    // or trial field of the chunk, only used to build the tile maxima)
+    Buf<uint32_t> vg, vfield;
     Buf<int32_t> vsv;
     Buf<long long> vsn, vsd;
     size_t view_entries = 0;
@@ -579,8 +582,46 @@ static void ensure_scratch(Session& S, uint32_t size);
 
 static size_t count_stride(size_t samples) { return (samples + 3) & ~size_t(3); }
 
-// Brings the plan's state data (counts, coverage, fields, tile maxima,
-// popcounts) up to the session's current state.
+// The reference's exact distance field and the tile-maxima arrays of a plan,
+// built the first time its state differs from the reference.
+static void ensure_tile_data(Session& S, Plan& p) {
+    if (p.ref_field.p) return;
+    const size_t samples = size_t(p.size) * p.size;
+    const uint32_t tiles = ((p.size + 31) / 32) * ((p.size + 31) / 32);
+    cudaStream_t st = S.stream;
+    ensure_scratch(S, p.size);
+    p.ref_field = Buf<uint32_t>(S.pool, samples * p.views);
+    p.t1 = Buf<int32_t>(S.pool, size_t(tiles) * p.views);
+    p.t2 = Buf<int32_t>(S.pool, size_t(tiles) * p.views);
+    B200_CUDA(cudaMemsetAsync(p.t1.p, 0xff, size_t(tiles) * p.views * 4, st));
+    B200_CUDA(cudaMemsetAsync(p.t2.p, 0xff, size_t(tiles) * p.views * 4, st));
+    for (uint32_t v = 0; v < p.views; ++v)
+        launch_field(p.ref_bits.p + size_t(p.words) * v, p.size, p.size, S.scratch.g.p, p.ref_field.p + samples * v,
+                     S.scratch.sv.p, S.scratch.sn.p, S.scratch.sd.p, st);
+}
+
+// Views per refresh launch so that the chunk's field scratch (row distances,
+// envelope stacks, the field itself: 28 bytes a sample) stays within 256 MiB;
+// sizes the scratch for it.
+static uint32_t field_chunk(Session& S, const Plan& p) {
+    const size_t samples = size_t(p.size) * p.size;
+    const uint32_t chunk =
+        uint32_t(std::max<size_t>(1, std::min<size_t>(p.views, (size_t(256) << 20) / (samples * 28))));
+    Scratch& x = S.scratch;
+    const size_t entries = samples * chunk;
+    if (x.view_entries < entries) {
+        x.vg = Buf<uint32_t>(S.pool, entries);
+        x.vfield = Buf<uint32_t>(S.pool, entries);
+        x.vsv = Buf<int32_t>(S.pool, entries);
+        x.vsn = Buf<long long>(S.pool, entries);
+        x.vsd = Buf<long long>(S.pool, entries);
+        x.view_entries = entries;
+    }
+    return chunk;
+}
+
+// Brings the plan's state data (counts, coverage, tile maxima, popcounts)
+// up to the session's current state.
 static void refresh_state(Session& S, Plan& p) {
     const PlanKey& key = p.key;
     const size_t samples = size_t(p.size) * p.size, cstride = count_stride(samples);
@@ -604,28 +645,16 @@ static void refresh_state(Session& S, Plan& p) {
     const uint32_t* sbits = own_bits ? p.state_bits.p : p.ref_bits.p;
     const bool fields = p.tiled && !p.state_is_ref;
     const uint32_t tiles = ((p.size + 31) / 32) * ((p.size + 31) / 32);
+    if (fields) ensure_tile_data(S, p);
     // Views per launch: the field scratch of one chunk stays within 256 MiB.
-    uint32_t chunk = p.views;
-    if (fields) {
-        const size_t per_view = samples * 24;
-        chunk = uint32_t(std::max<size_t>(1, std::min<size_t>(p.views, (size_t(256) << 20) / per_view)));
-        Scratch& x = S.scratch;
-        const size_t entries = samples * chunk;
-        if (x.view_entries < entries) {
-            x.vg = Buf<uint32_t>(S.pool, entries);
-            x.vsv = Buf<int32_t>(S.pool, entries);
-            x.vsn = Buf<long long>(S.pool, entries);
-            x.vsd = Buf<long long>(S.pool, entries);
-            x.view_entries = entries;
-        }
-    }
+    const uint32_t chunk = fields ? field_chunk(S, p) : p.views;
     for (uint32_t v0 = 0; v0 < p.views; v0 += chunk) {
         const uint32_t n = std::min(chunk, p.views - v0);
         const size_t w0 = size_t(p.words) * v0, s0 = samples * v0, t0 = size_t(tiles) * v0;
         launch_refresh_views(live, p.cameras.p + v0, n, S.bounds.center, key.ss, p.size, key.force_two,
                              p.state_count.p + cstride * v0, cstride, p.raster_state.p + 4 * v0,
                              own_bits ? p.state_bits.p + w0 : nullptr, p.ref_bits.p + w0, p.words, p.pop.p + 4 * v0,
-                             fields ? p.ref_field.p + s0 : nullptr, fields ? p.state_field.p + s0 : nullptr,
+                             fields ? p.ref_field.p + s0 : nullptr, fields ? S.scratch.vfield.p : nullptr,
                              S.scratch.vg.p, S.scratch.vsv.p, S.scratch.vsn.p, S.scratch.vsd.p,
                              fields ? p.t1.p + t0 : nullptr, fields ? p.t2.p + t0 : nullptr, st);
     }
@@ -640,8 +669,9 @@ static void refresh_state(Session& S, Plan& p) {
         PlanView& pv = p.hviews[v];
         pv.state_bits = sbits + size_t(v) * p.words;
         pv.state_count = p.state_count.p + cstride * v;
-        pv.tile_t1 = p.tiled ? p.t1.p + tiles * v : nullptr;
-        pv.tile_t2 = p.tiled ? p.t2.p + tiles * v : nullptr;
+        pv.tile_t1 = p.t1.p ? p.t1.p + tiles * v : nullptr;
+        pv.tile_t2 = p.t2.p ? p.t2.p + tiles * v : nullptr;
+        pv.ref_field = p.ref_field.p ? p.ref_field.p + samples * v : nullptr;
         pv.changed = uint32_t(hpop[4 * v]);
         pv.total = uint32_t(hpop[4 * v + 1]);
         pv.cov_ref = uint32_t(hpop[4 * v + 2]);
@@ -671,7 +701,7 @@ static Plan& plan_for(Session& S, const PlanKey& key) {
         return *(S.plans[key] = std::move(plan));
     }
     p.words = mask_words(p.size);
-    p.tiled = p.size <= 1024;
+    p.tiled = p.size <= 4160;
     p.hcams = make_cameras(S.bounds, key.screen, key.ortho, key.persp, key.seed);
     p.cameras = Buf<Camera>(S.pool, p.hcams.size());
     cudaStream_t st = S.stream;
@@ -693,21 +723,6 @@ static Plan& plan_for(Session& S, const PlanKey& key) {
         p.ref_box_clip |= hstate[4 * v] != kNone;
         p.hviews[v].ref_bits = p.ref_bits.p + size_t(v) * p.words;
         p.hviews[v].clipped_ref = hstate[4 * v + 1];
-    }
-    if (p.tiled) {
-        ensure_scratch(S, p.size);
-        const uint32_t tiles = ((p.size + 31) / 32) * ((p.size + 31) / 32);
-        p.ref_field = Buf<uint32_t>(S.pool, samples * p.views);
-        p.state_field = Buf<uint32_t>(S.pool, samples * p.views);
-        p.t1 = Buf<int32_t>(S.pool, size_t(tiles) * p.views);
-        p.t2 = Buf<int32_t>(S.pool, size_t(tiles) * p.views);
-        B200_CUDA(cudaMemsetAsync(p.t1.p, 0xff, size_t(tiles) * p.views * 4, st));
-        B200_CUDA(cudaMemsetAsync(p.t2.p, 0xff, size_t(tiles) * p.views * 4, st));
-        for (uint32_t v = 0; v < p.views; ++v) {
-            launch_field(p.ref_bits.p + size_t(p.words) * v, p.size, p.size, S.scratch.g.p, p.ref_field.p + samples * v,
-                         S.scratch.sv.p, S.scratch.sn.p, S.scratch.sd.p, st);
-            p.hviews[v].ref_field = p.ref_field.p + samples * v;
-        }
     }
     p.dviews = Buf<PlanView>(S.pool, p.views);
     p.dev.cameras = p.cameras.p;
@@ -1209,7 +1224,6 @@ static void trial_views(Session& S, Plan& p, const DevMesh& cand, uint64_t tag) 
         p.trial_count = Buf<uint8_t>(S.pool, cstride * p.views);
         p.trial_bits = Buf<uint32_t>(S.pool, size_t(p.words) * p.views);
         B200_CUDA(cudaMemsetAsync(p.trial_bits.p, 0, size_t(p.words) * p.views * 4, st));
-        p.trial_field = Buf<uint32_t>(S.pool, samples * p.views);
         p.trial_state = Buf<uint32_t>(S.pool, 4 * size_t(p.views));
         p.trial_t1 = Buf<int32_t>(S.pool, size_t(tiles) * p.views);
         p.trial_t2 = Buf<int32_t>(S.pool, size_t(tiles) * p.views);
@@ -1219,23 +1233,16 @@ static void trial_views(Session& S, Plan& p, const DevMesh& cand, uint64_t tag) 
         p.trial_hpop.assign(4 * size_t(p.views), 0);
         p.trial_hmax.assign(2 * size_t(p.views), 0);
     }
-    const uint32_t chunk =
-        uint32_t(std::max<size_t>(1, std::min<size_t>(p.views, (size_t(256) << 20) / (samples * 24))));
+    ensure_tile_data(S, p);
+    const uint32_t chunk = field_chunk(S, p);
     Scratch& x = S.scratch;
-    if (x.view_entries < samples * chunk) {
-        x.vg = Buf<uint32_t>(S.pool, samples * chunk);
-        x.vsv = Buf<int32_t>(S.pool, samples * chunk);
-        x.vsn = Buf<long long>(S.pool, samples * chunk);
-        x.vsd = Buf<long long>(S.pool, samples * chunk);
-        x.view_entries = samples * chunk;
-    }
     for (uint32_t v0 = 0; v0 < p.views; v0 += chunk) {
         const uint32_t n = std::min(chunk, p.views - v0);
         const size_t w0 = size_t(p.words) * v0, s0 = samples * v0, t0 = size_t(tiles) * v0;
         launch_refresh_views(cand, p.cameras.p + v0, n, S.bounds.center, p.key.ss, p.size, p.key.force_two,
                              p.trial_count.p + cstride * v0, cstride, p.trial_state.p + 4 * v0, p.trial_bits.p + w0,
                              p.ref_bits.p + w0, p.words, p.trial_pop.p + 4 * v0, p.ref_field.p + s0,
-                             p.trial_field.p + s0, x.vg.p, x.vsv.p, x.vsn.p, x.vsd.p, p.trial_t1.p + t0,
+                             x.vfield.p, x.vg.p, x.vsv.p, x.vsn.p, x.vsd.p, p.trial_t1.p + t0,
                              p.trial_t2.p + t0, st);
     }
     launch_view_maxima(p.trial_t1.p, p.trial_t2.p, tiles, p.views, p.trial_max.p, st);
@@ -1308,7 +1315,6 @@ static void commit_trial(Session& S, uint32_t faces, uint64_t tag) {
         if (p.resource_limited || !p.tiled || p.trial_tag != tag || !p.state_bits.p) continue;
         std::swap(p.state_count, p.trial_count);
         std::swap(p.state_bits, p.trial_bits);
-        std::swap(p.state_field, p.trial_field);
         std::swap(p.t1, p.trial_t1);
         std::swap(p.t2, p.trial_t2);
         std::swap(p.raster_state, p.trial_state);
@@ -1325,6 +1331,7 @@ static void commit_trial(Session& S, uint32_t faces, uint64_t tag) {
             pv.state_count = p.state_count.p + cstride * v;
             pv.tile_t1 = p.t1.p + size_t(tiles) * v;
             pv.tile_t2 = p.t2.p + size_t(tiles) * v;
+            pv.ref_field = p.ref_field.p + samples * v;
             pv.changed = uint32_t(p.hpop[4 * v]);
             pv.total = uint32_t(p.hpop[4 * v + 1]);
             pv.cov_ref = uint32_t(p.hpop[4 * v + 2]);
