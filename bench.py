@@ -734,22 +734,25 @@ def run_batched(args, rank: int, world: int, local: int) -> dict:
 
 ROCK_CHAIN = {"levels": 6, "base": 240.0, "last": 7.5, "curve": ((0.0, 1.0), (1.0, 3.0)), "lod0": 2.0,
               "views": 32, "ss": 8, "batch": 64, "budget": 300}
+# The 1M-face rock of the full LOD-chain workload: 6 levels scheduled 1024 ->
+# 32 px (audits at 512 ... 32 px x ss 8), transition 1 px at LOD1 rising to
+# 3 px, LOD0 bound 2 px, 128 search and 128 audit views, uv preserved.
+ROCK_1M_CHAIN = {"levels": 6, "base": 1024.0, "last": 32.0, "curve": ((0.0, 1.0), (1.0, 3.0)), "lod0": 2.0,
+                 "views": 128, "ss": 8, "batch": 64, "budget": 40}
+# The thin-structure workload: 2,000 ribbon cards (400k faces), 256 views at
+# 512 px, 6-level chain (512 -> 16 px, the same 32:1 ratio).
+RIBBON_CHAIN = {"levels": 6, "base": 512.0, "last": 16.0, "curve": ((0.0, 1.0), (1.0, 3.0)), "lod0": 2.0,
+                "views": 256, "ss": 8, "batch": 64, "budget": 40}
 
 
-def run_rock_chain(args, local: int, preserve_uv: int = 0) -> dict:
-    """Multi-level LOD chain of a ridged-noise rock (81,920 faces, 8 UV charts):
-    6 levels scheduled 240 -> 7.5 px (the 1024 -> 32 px ratio of the 1M-face
-    configuration), transition 1 -> 3 px, LOD0 bound 2 px, 32 ortho views at
-    ss 8, batches of 64, 300 trials per level, each level confirmed. With
-    preserve_uv the collapses carry the transported uv and placements that
-    fold a uv triangle are rejected."""
+def run_chain(args, local: int, mesh, c: dict, preserve_uv: int = 0, label: str = "") -> dict:
+    """One LOD chain (blitz_audit_chain: schedule, four gates per level,
+    previous-level binding, batched executor, confirmation of every emitted
+    level) of `mesh` under the chain settings `c`; wall clock around it."""
     import torch
 
     import blitzremesher_b200 as br
-    from blitzremesher_b200 import synthetic as syn
 
-    c = ROCK_CHAIN
-    mesh = syn.rock(6, 3)
     session = br.AuditSession(mesh, br.neural_options(device=local, preserve_uv=preserve_uv))
     settings = br.chain_settings(c["levels"], c["base"], c["last"], c["curve"], c["lod0"], (c["views"], 0, 0xB1172024),
                                  (c["views"], 0, 0xB1172026), c["ss"], c["ss"], c["ss"], 1.0, c["batch"], 0,
@@ -759,16 +762,55 @@ def run_rock_chain(args, local: int, preserve_uv: int = 0) -> dict:
     levels, _ = session.chain(settings, meshes=False)
     torch.cuda.synchronize()
     seconds = time.perf_counter() - t0
+    info = session.info()
     session.close()
-    return {"metric": "LOD-chain s/mesh", "seconds": seconds, "unit": "s/mesh",
-            "mesh": f"rock: icosphere level 6 ({mesh.face_count} faces), 6-octave ridged noise, 8 UV charts "
-                    + ("(preserve_uv: uv transported, uv flips rejected)" if preserve_uv else "(uv not preserved)"),
-            "schedule": c, "levels": [{k: (round(v, 4) if isinstance(v, float) else v) for k, v in l.items()
-                                       if k not in ("source_audit", "transition_audit")}
-                                      | {"source_error": l["source_audit"].error,
-                                         "transition_error": l["transition_audit"].error} for l in levels],
+    return {"metric": "LOD-chain s/mesh", "seconds": seconds, "unit": "s/mesh", "mesh": label,
+            "faces": int(mesh.face_count), "schedule": c,
+            "levels": [{k: (round(v, 4) if isinstance(v, float) else v) for k, v in l.items()
+                        if k not in ("source_audit", "transition_audit")}
+                       | {"source_error": l["source_audit"].error, "transition_error": l["transition_audit"].error}
+                       for l in levels],
             "all_confirmed": all(l["confirmed"] for l in levels),
+            "audited_collapses": int(info["decoded"]),
             "timing": "wall clock around blitz_audit_chain (executor, previous-level binding, confirmation)"}
+
+
+def run_rock_chain(args, local: int, preserve_uv: int = 0) -> dict:
+    """Multi-level LOD chain of a ridged-noise rock (81,920 faces, 8 UV charts):
+    6 levels scheduled 240 -> 7.5 px (the 1024 -> 32 px ratio of the 1M-face
+    configuration), transition 1 -> 3 px, LOD0 bound 2 px, 32 ortho views at
+    ss 8, batches of 64, 300 trials per level, each level confirmed. With
+    preserve_uv the collapses carry the transported uv and placements that
+    fold a uv triangle are rejected."""
+    from blitzremesher_b200 import synthetic as syn
+
+    mesh = syn.rock(6, 3)
+    label = (f"rock: icosphere level 6 ({mesh.face_count} faces), 6-octave ridged noise, 8 UV charts "
+             + ("(preserve_uv: uv transported, uv flips rejected)" if preserve_uv else "(uv not preserved)"))
+    return run_chain(args, local, mesh, ROCK_CHAIN, preserve_uv, label)
+
+
+def run_rock_1m(args, local: int) -> dict:
+    """The full LOD-chain workload: the 1,310,720-face rock (icosphere level 8,
+    6-octave ridged noise, 8 UV charts, uv preserved), 128 views, 1024 -> 32 px."""
+    from blitzremesher_b200 import synthetic as syn
+
+    mesh = syn.rock(8, 3)
+    label = f"rock: icosphere level 8 ({mesh.face_count} faces), 6-octave ridged noise, 8 UV charts, preserve_uv"
+    out = run_chain(args, local, mesh, ROCK_1M_CHAIN, 1, label)
+    out["note"] = f"trial budget {ROCK_1M_CHAIN['budget']} batches of up to 64 collapses per level"
+    return out
+
+
+def run_ribbons(args, local: int) -> dict:
+    """The thin-structure workload: 2,000 two-sided ribbon cards (400k faces),
+    256 views at 512 px, 6-level chain."""
+    from blitzremesher_b200 import synthetic as syn
+
+    mesh = syn.ribbons(2000, seed=5)
+    out = run_chain(args, local, mesh, RIBBON_CHAIN, 0, f"2,000 ribbon cards ({mesh.face_count} faces), two-sided")
+    out["note"] = f"trial budget {RIBBON_CHAIN['budget']} batches of up to 64 collapses per level"
+    return out
 
 
 def run_gpu(args) -> None:
@@ -797,6 +839,10 @@ def run_gpu(args) -> None:
             for k in ("metric", "n_gpus", "steps", "warmup", "higher_is_better", "scaling", "vs_baseline", "data"):
                 ico.pop(k, None)
             line["icosphere_20480"] = ico
+    elif args.config == "rock1m":
+        line = run_rock_1m(args, local)
+    elif args.config == "ribbons":
+        line = run_ribbons(args, local)
     else:
         line = run_icosphere(args, rank, world, local)
     if rank == 0:
@@ -817,7 +863,7 @@ def main() -> None:
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-chain", action="store_true")
     ap.add_argument("--no-surrogate", action="store_true")
-    ap.add_argument("--config", default="batched", choices=["batched", "icosphere"])
+    ap.add_argument("--config", default="batched", choices=["batched", "icosphere", "rock1m", "ribbons"])
     ap.add_argument("--no-icosphere", action="store_true")
     ap.add_argument("--no-rock", action="store_true")
     ap.add_argument("--meshes", type=int, default=BATCH_MESHES, help="meshes of the batched set (64 = the workload)")

@@ -62,6 +62,61 @@ class NeuralInfo(C.Structure):
                 ("reference_rejections", C.c_uint64), ("fallback_levels", C.c_uint32)]
 
 
+class CurvePoint(C.Structure):
+    _fields_ = [("x", C.c_float), ("y", C.c_float)]
+
+
+class Settings(C.Structure):
+    """blitz_settings (blitz.h:38-63)."""
+    _fields_ = [("struct_size", C.c_uint32), ("abi_version", C.c_uint32), ("levels", C.c_uint8),
+                ("profile", C.c_uint8), ("triangle_overhead_bps", C.c_uint16),
+                ("max_added_vertex_bytes_bps", C.c_uint32), ("objective", C.c_uint8), ("beam_width", C.c_uint8),
+                ("search_supersample", C.c_uint8), ("audit_supersample", C.c_uint8), ("max_supersample", C.c_uint8),
+                ("prune", C.c_uint8), ("force_scalar", C.c_uint8), ("coupled_wedges", C.c_uint8),
+                ("candidate_budget", C.c_uint16), ("search_ortho", C.c_uint16), ("search_perspective", C.c_uint16),
+                ("audit_ortho", C.c_uint16), ("audit_perspective", C.c_uint16), ("search_seed", C.c_uint32),
+                ("audit_seed", C.c_uint32), ("pixels_per_meter", C.c_double), ("meters_per_unit", C.c_double),
+                ("base_pixels", C.c_double), ("last_pixels", C.c_double), ("max_lod0_delta_px", C.c_double),
+                ("normal_weight", C.c_double), ("color_weight", C.c_double), ("material_weight", C.c_double),
+                ("max_changed_area", C.c_double), ("transition", C.c_void_p), ("transition_count", C.c_size_t),
+                ("normal_importance", C.c_void_p), ("normal_importance_count", C.c_size_t),
+                ("attribute_importance", C.c_void_p), ("attribute_importance_count", C.c_size_t),
+                ("cancelled", C.c_void_p), ("user_data", C.c_void_p)]
+
+
+class LodInfo(C.Structure):
+    """blitz_lod_info (blitz.h:64-73)."""
+    _fields_ = [("struct_size", C.c_uint32), ("mesh", BlitzMesh), ("screen_pixels", C.c_double),
+                ("transition_limit", C.c_double), ("source_limit", C.c_double), ("transition_error", C.c_double),
+                ("source_error", C.c_double), ("transition_worst_view", C.c_uint32), ("source_worst_view", C.c_uint32),
+                ("shared_vertices", C.c_uint8), ("passed", C.c_uint8), ("reference_triangles", C.c_uint32),
+                ("transition_changed_area", C.c_double), ("source_changed_area", C.c_double),
+                ("transition_changed_area_worst_view", C.c_uint32), ("source_changed_area_worst_view", C.c_uint32)]
+
+
+class StorageInfo(C.Structure):
+    _fields_ = [("struct_size", C.c_uint32), ("source_vertex_bytes", C.c_uint64), ("added_vertex_bytes", C.c_uint64),
+                ("index_bytes", C.c_uint64), ("total_bytes", C.c_uint64), ("added_vertex_budget_bytes", C.c_uint64),
+                ("max_added_vertex_bytes_bps", C.c_uint32)]
+
+
+class RuntimeLodStorage(C.Structure):
+    _fields_ = [("struct_size", C.c_uint32), ("scheduled_index", C.c_uint8), ("added_vertex_bytes", C.c_uint64),
+                ("index_bytes", C.c_uint64), ("cumulative_added_vertex_bytes", C.c_uint64)]
+
+
+class NeuralOptionsV1(C.Structure):
+    _fields_ = [("struct_size", C.c_uint32), ("version", C.c_uint32), ("device", C.c_int32),
+                ("memory_mib", C.c_uint32), ("overdraw_tiebreak", C.c_uint8), ("reserved", C.c_uint8 * 3)]
+
+
+class ActionProposal(C.Structure):
+    _fields_ = [("struct_size", C.c_uint32), ("version", C.c_uint32), ("start_triangles", C.c_uint32),
+                ("target_triangles", C.c_uint32), ("final_triangles", C.c_uint32), ("trial_budget", C.c_uint32),
+                ("trials", C.c_uint32), ("accepted_batches", C.c_uint32), ("screen_pixels", C.c_double),
+                ("origin", C.c_uint8), ("output", C.c_uint8), ("stop_reason", C.c_uint8), ("reserved", C.c_uint8 * 5)]
+
+
 class EvalSettings(C.Structure):
     _fields_ = [("struct_size", C.c_uint32), ("profile", C.c_uint8), ("supersample", C.c_uint8),
                 ("max_supersample", C.c_uint8), ("force_two_sided", C.c_uint8), ("conservative_screen", C.c_uint8),
@@ -158,6 +213,29 @@ EXPORTS = {
     "blitz_audit_batch_candidates_host": ([C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(EvalSettings), C.c_void_p,
                                            C.c_uint32, C.c_char_p, C.c_size_t], C.c_int),
     "blitz_audit_batch_read_info": ([C.c_void_p, C.c_void_p], C.c_int),
+    "blitz_settings_init": ([C.POINTER(Settings), C.c_size_t], C.c_int),
+    "blitz_generate": ([C.c_void_p, C.c_void_p, C.POINTER(C.c_void_p), C.c_char_p, C.c_size_t], C.c_int),
+    "blitz_neural_options_init": ([C.POINTER(NeuralOptionsV1), C.c_size_t], C.c_int),
+    "blitz_neural_model_load": ([C.c_char_p, C.POINTER(NeuralOptionsV1), C.POINTER(C.c_void_p), C.c_char_p,
+                                 C.c_size_t], C.c_int),
+    "blitz_neural_model_load_v2": ([C.c_char_p, C.POINTER(NeuralOptionsV2), C.POINTER(C.c_void_p), C.c_char_p,
+                                    C.c_size_t], C.c_int),
+    "blitz_neural_model_destroy": ([C.c_void_p], None),
+    "blitz_neural_model_sha256": ([C.c_void_p], C.c_char_p),
+    "blitz_generate_neural": ([C.POINTER(BlitzMesh), C.POINTER(Settings), C.c_void_p, C.POINTER(C.c_void_p),
+                               C.c_char_p, C.c_size_t], C.c_int),
+    "blitz_result_lod_count": ([C.c_void_p], C.c_size_t),
+    "blitz_result_runtime_lod_count": ([C.c_void_p], C.c_size_t),
+    "blitz_result_runtime_lod_index": ([C.c_void_p, C.c_size_t], C.c_size_t),
+    "blitz_result_lod": ([C.c_void_p, C.c_size_t, C.POINTER(LodInfo)], C.c_int),
+    "blitz_result_storage": ([C.c_void_p, C.POINTER(StorageInfo)], C.c_int),
+    "blitz_result_runtime_lod_storage": ([C.c_void_p, C.c_size_t, C.POINTER(RuntimeLodStorage)], C.c_int),
+    "blitz_result_destroy": ([C.c_void_p], None),
+    "blitz_result_neural_info": ([C.c_void_p, C.POINTER(NeuralInfo)], C.c_int),
+    "blitz_result_neural_action_proposal_count": ([C.c_void_p], C.c_size_t),
+    "blitz_result_neural_action_proposal": ([C.c_void_p, C.c_size_t, C.POINTER(ActionProposal)], C.c_int),
+    "blitz_audit_state_materials": ([C.c_void_p, C.c_void_p, C.c_size_t, C.POINTER(C.c_uint32), C.c_char_p,
+                                     C.c_size_t], C.c_int),
     "blitz_audit_state": ([C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p, C.c_size_t, C.POINTER(C.c_uint32),
                            C.c_char_p, C.c_size_t], C.c_int),
     "blitz_mesh_bounds": ([C.c_void_p, C.c_void_p, C.POINTER(C.c_double), C.c_char_p, C.c_size_t], C.c_int),
@@ -734,3 +812,88 @@ def four_gates(search: EvalSettings, audit: EvalSettings, source_limit: float, t
                 g.max_changed_area = 1.0
             gates.append(g)
     return gates
+
+
+def settings(**kw) -> Settings:
+    """blitz_settings with the reference's defaults, fields overridden by `kw`
+    (`transition` as a sequence of (x, y) points)."""
+    c = Settings()
+    if load().blitz_settings_init(C.byref(c), C.sizeof(c)) != BLITZ_OK:
+        raise BlitzError(BLITZ_INVALID_ARGUMENT, "blitz_settings_init")
+    curve = kw.pop("transition", None)
+    for k, v in kw.items():
+        setattr(c, k, v)
+    if curve is not None:
+        pts = (CurvePoint * len(curve))(*[CurvePoint(float(x), float(y)) for x, y in curve])
+        c._curve = pts  # kept alive with the settings
+        c.transition, c.transition_count = C.cast(pts, C.c_void_p), len(curve)
+    return c
+
+
+class NeuralModel:
+    """A BLZNET policy file loaded through blitz_neural_model_load_v2."""
+
+    def __init__(self, path, options: Optional[NeuralOptionsV2] = None):
+        self.lib = load()
+        self.handle = C.c_void_p()
+        opts = options if options is not None else neural_options()
+        err = C.create_string_buffer(512)
+        _check(self.lib.blitz_neural_model_load_v2(str(path).encode(), C.byref(opts), C.byref(self.handle), err, 512),
+               err)
+
+    @property
+    def sha256(self) -> str:
+        return self.lib.blitz_neural_model_sha256(self.handle).decode()
+
+    def close(self) -> None:
+        if self.handle:
+            self.lib.blitz_neural_model_destroy(self.handle)
+            self.handle = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def generate_neural(mesh, config: Settings, model: NeuralModel) -> dict:
+    """blitz_generate_neural: every scheduled level (0 = the source) with its
+    lod info, indices and positions; runtime levels, storage, diagnostics and
+    per-level action proposals."""
+    lib = load()
+    hold = _MeshHold(mesh)
+    res = C.c_void_p()
+    err = C.create_string_buffer(512)
+    _check(lib.blitz_generate_neural(C.byref(hold.c), C.byref(config), model.handle, C.byref(res), err, 512), err)
+    try:
+        lods = []
+        for i in range(lib.blitz_result_lod_count(res)):
+            info = LodInfo()
+            info.struct_size = C.sizeof(LodInfo)
+            assert lib.blitz_result_lod(res, i, C.byref(info)) == BLITZ_OK
+            m = info.mesh
+            idx = np.ctypeslib.as_array(C.cast(m.indices, C.POINTER(C.c_uint32)), shape=(m.index_count,)).copy()
+            pos = np.ctypeslib.as_array(C.cast(m.positions.data, C.POINTER(C.c_float)),
+                                        shape=(m.positions.count * 3,)).reshape(-1, 3).copy()
+            d = {k: getattr(info, k) for k, _ in info._fields_ if k not in ("struct_size", "mesh")}
+            d["indices"], d["positions"] = idx, pos
+            lods.append(d)
+        runtime = [lib.blitz_result_runtime_lod_index(res, i) for i in range(lib.blitz_result_runtime_lod_count(res))]
+        st = StorageInfo()
+        st.struct_size = C.sizeof(StorageInfo)
+        assert lib.blitz_result_storage(res, C.byref(st)) == BLITZ_OK
+        ni = NeuralInfo()
+        ni.struct_size = C.sizeof(NeuralInfo)
+        assert lib.blitz_result_neural_info(res, C.byref(ni)) == BLITZ_OK
+        props = []
+        for i in range(lib.blitz_result_neural_action_proposal_count(res)):
+            a = ActionProposal()
+            a.struct_size, a.version = C.sizeof(ActionProposal), 1
+            assert lib.blitz_result_neural_action_proposal(res, i, C.byref(a)) == BLITZ_OK
+            props.append({k: getattr(a, k) for k, _ in a._fields_ if k not in ("struct_size", "reserved")})
+        return {"lods": lods, "runtime": runtime,
+                "storage": {k: getattr(st, k) for k, _ in st._fields_ if k != "struct_size"},
+                "info": {k: getattr(ni, k) for k, _ in ni._fields_ if k != "struct_size"}, "proposals": props}
+    finally:
+        lib.blitz_result_destroy(res)

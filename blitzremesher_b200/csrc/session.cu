@@ -2062,6 +2062,22 @@ blitz_status blitz_audit_state_uv(blitz_audit_session* s, float* uv, size_t uv_c
     });
 }
 
+blitz_status blitz_audit_state_materials(blitz_audit_session* s, uint16_t* materials, size_t capacity,
+                                         uint32_t* face_count, char* error, size_t cap) {
+    return guarded(error, cap, [&] {
+        if (!s || !face_count) throw Failure(BLITZ_INVALID_ARGUMENT, "null argument");
+        Session& S = s->s;
+        DeviceScope scope(S.device);
+        const DevMesh& m = S.state.view;
+        *face_count = S.state_faces;
+        if (!m.mat) throw Failure(BLITZ_INVALID_ARGUMENT, "the session's mesh has no materials");
+        if (materials && capacity >= S.state_faces) {
+            B200_CUDA(cudaMemcpyAsync(materials, m.mat, size_t(S.state_faces) * 2, cudaMemcpyDeviceToHost, S.stream));
+            B200_CUDA(cudaStreamSynchronize(S.stream));
+        }
+    });
+}
+
 blitz_status blitz_audit_reset(blitz_audit_session* s, char* error, size_t cap) {
     return guarded(error, cap, [&] {
         if (!s) throw Failure(BLITZ_INVALID_ARGUMENT, "null session");
@@ -2792,6 +2808,9 @@ blitz_status blitz_audit_chain(blitz_audit_session* s, const blitz_chain_setting
             blitz_eval_settings gates[4] = {chain_gate(*c, pixels, bound, false), chain_gate(*c, pixels, delta, false),
                                             chain_gate(*c, pixels, bound, true), chain_gate(*c, pixels, delta, true)};
             for (int g = 0; g < 4; ++g) gate_of(&gates[g], S.bounds);
+            // Plans of earlier levels' screen sizes are not used again.
+            for (auto it = S.plans.begin(); it != S.plans.end();)
+                it = it->first.screen != pixels ? S.plans.erase(it) : std::next(it);
             // previous level = the state now (the source for level 1)
             if (level >= 2) {
                 HostMesh h;

@@ -78,6 +78,123 @@ typedef struct blitz_neural_info {
 uint32_t blitz_abi_version(void);
 /* c_api.cpp:228-245 — defaults of blitz::NeuralOptions. */
 blitz_status blitz_neural_options_v2_init(blitz_neural_options_v2*, size_t);
+
+/* ---- The rest of blitz.h (blitz.h:22-27, 38-88, 95-171), same layouts ----
+ * Generation here is the neural path only: blitz_generate_neural routes every
+ * audit of the LOD chain to this engine (blitz_audit_chain: the schedule of
+ * chain.cpp:101-118, the four gates of generate.cpp:365-388, the executor's
+ * collapses with midpoint placement, the confirmation of generate.cpp:456-562
+ * at the audit views). blitz_generate (the classical CPU reducer) and the
+ * normals/attributes profiles return BLITZ_UNAVAILABLE. */
+typedef struct blitz_color_rgba8 {
+    uint8_t r, g, b, a;
+} blitz_color_rgba8;
+typedef struct blitz_curve_point {
+    float x, y;
+} blitz_curve_point;
+typedef struct blitz_settings {
+    uint32_t struct_size, abi_version;
+    uint8_t levels, profile;
+    uint16_t triangle_overhead_bps;
+    uint32_t max_added_vertex_bytes_bps;
+    uint8_t objective, beam_width, search_supersample, audit_supersample;
+    uint8_t max_supersample, prune, force_scalar, coupled_wedges;
+    uint16_t candidate_budget, search_ortho, search_perspective, audit_ortho, audit_perspective;
+    uint32_t search_seed, audit_seed;
+    double pixels_per_meter, meters_per_unit, base_pixels, last_pixels, max_lod0_delta_px;
+    double normal_weight, color_weight, material_weight;
+    double max_changed_area;
+    const blitz_curve_point* transition;
+    size_t transition_count;
+    const blitz_curve_point* normal_importance;
+    size_t normal_importance_count;
+    const blitz_curve_point* attribute_importance;
+    size_t attribute_importance_count;
+    int (*cancelled)(void*);
+    void* user_data;
+} blitz_settings;
+typedef struct blitz_lod_info {
+    uint32_t struct_size;
+    blitz_mesh mesh;
+    double screen_pixels, transition_limit, source_limit, transition_error, source_error;
+    uint32_t transition_worst_view, source_worst_view;
+    uint8_t shared_vertices, passed;
+    uint32_t reference_triangles;
+    double transition_changed_area, source_changed_area;
+    uint32_t transition_changed_area_worst_view, source_changed_area_worst_view;
+} blitz_lod_info;
+typedef struct blitz_result blitz_result;
+typedef struct blitz_storage_info {
+    uint32_t struct_size;
+    uint64_t source_vertex_bytes, added_vertex_bytes, index_bytes, total_bytes;
+    uint64_t added_vertex_budget_bytes;
+    uint32_t max_added_vertex_bytes_bps;
+} blitz_storage_info;
+blitz_status blitz_result_storage(const blitz_result*, blitz_storage_info*);
+typedef struct blitz_runtime_lod_storage_info {
+    uint32_t struct_size;
+    uint8_t scheduled_index;
+    uint64_t added_vertex_bytes, index_bytes, cumulative_added_vertex_bytes;
+} blitz_runtime_lod_storage_info;
+blitz_status blitz_result_runtime_lod_storage(const blitz_result*, size_t, blitz_runtime_lod_storage_info*);
+/* c_api.cpp:82-122 — defaults of blitz::Settings (remesher.hpp:31-56). */
+blitz_status blitz_settings_init(blitz_settings*, size_t);
+/* The classical reducer is not part of this engine: BLITZ_UNAVAILABLE. */
+blitz_status blitz_generate(const blitz_mesh*, const blitz_settings*, blitz_result**, char* error,
+                            size_t error_capacity);
+size_t blitz_result_lod_count(const blitz_result*);
+size_t blitz_result_runtime_lod_count(const blitz_result*);
+size_t blitz_result_runtime_lod_index(const blitz_result*, size_t);
+blitz_status blitz_result_lod(const blitz_result*, size_t, blitz_lod_info*);
+void blitz_result_destroy(blitz_result*);
+typedef struct blitz_neural_model blitz_neural_model;
+typedef struct blitz_neural_options {
+    uint32_t struct_size, version;
+    int32_t device;
+    uint32_t memory_mib;
+    uint8_t overdraw_tiebreak;
+    uint8_t reserved[3];
+} blitz_neural_options;
+typedef enum blitz_neural_origin {
+    BLITZ_NEURAL_SOURCE = 0,
+    BLITZ_NEURAL_PREVIOUS = 1,
+    BLITZ_NEURAL_BOTH = 2
+} blitz_neural_origin;
+typedef enum blitz_neural_action_stop {
+    BLITZ_NEURAL_TARGET_REACHED = 0,
+    BLITZ_NEURAL_TRIAL_BUDGET = 1,
+    BLITZ_NEURAL_NO_LEGAL_ACTIONS = 2,
+    BLITZ_NEURAL_NO_ACCEPTED_ACTION = 3,
+    BLITZ_NEURAL_ACTION_CANCELLED = 4,
+    BLITZ_NEURAL_ACTION_RESOURCE = 5,
+    BLITZ_NEURAL_INFEASIBLE_SEED = 6
+} blitz_neural_action_stop;
+typedef struct blitz_neural_action_proposal {
+    uint32_t struct_size, version;
+    uint32_t start_triangles, target_triangles, final_triangles, trial_budget, trials, accepted_batches;
+    double screen_pixels;
+    uint8_t origin, output, stop_reason;
+    uint8_t reserved[5];
+} blitz_neural_action_proposal;
+/* c_api.cpp:208-213 */
+blitz_status blitz_neural_options_init(blitz_neural_options*, size_t);
+/* BLZNET01/02/03 policy files (model_io.cpp:59-107: header, provenance,
+ * FP32 weights, SHA-256 checksum of the payload). The policy's weights are
+ * loaded and checked; rankings here are ShortestEdge, CurrentPlane and
+ * Constant (options v2 `ranking` 3, 4, 1); Learned and Shuffled, which score
+ * edits with the policy network, return BLITZ_UNAVAILABLE at generation. */
+blitz_status blitz_neural_model_load(const char* path, const blitz_neural_options*, blitz_neural_model**,
+                                     char* error, size_t error_capacity);
+blitz_status blitz_neural_model_load_v2(const char* path, const blitz_neural_options_v2*,
+                                        blitz_neural_model**, char* error, size_t error_capacity);
+void blitz_neural_model_destroy(blitz_neural_model*);
+/* Borrowed lowercase hex SHA-256 of the model file, valid until destruction. */
+const char* blitz_neural_model_sha256(const blitz_neural_model*);
+blitz_status blitz_generate_neural(const blitz_mesh*, const blitz_settings*, const blitz_neural_model*,
+                                   blitz_result**, char* error, size_t error_capacity);
+blitz_status blitz_result_neural_info(const blitz_result*, blitz_neural_info*);
+size_t blitz_result_neural_action_proposal_count(const blitz_result*);
+blitz_status blitz_result_neural_action_proposal(const blitz_result*, size_t, blitz_neural_action_proposal*);
 #endif
 
 /* POD mirror of blitz::EvalSettings for the coverage profile
@@ -463,6 +580,11 @@ blitz_status blitz_audit_state(blitz_audit_session*, uint32_t* indices, size_t i
  * argument when the session's mesh has no uv. */
 blitz_status blitz_audit_state_uv(blitz_audit_session*, float* uv, size_t uv_capacity, char* error,
                                   size_t error_capacity);
+/* Current state's per-face materials (compacted like the indices; the
+ * state keeps each surviving face's material). Invalid argument when the
+ * session's mesh has no materials. */
+blitz_status blitz_audit_state_materials(blitz_audit_session*, uint16_t* materials, size_t capacity,
+                                         uint32_t* face_count, char* error, size_t error_capacity);
 /* Restores the state to the source (GpuActionState::reset, action_gpu.cu:1884-1906). */
 blitz_status blitz_audit_reset(blitz_audit_session*, char* error, size_t error_capacity);
 

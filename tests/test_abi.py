@@ -55,6 +55,15 @@ int main(void) {
   O(blitz_mesh, indices) O(blitz_mesh, double_sided_count)
   O(blitz_neural_options_v2, exact_position_bps) O(blitz_neural_options_v2, reserved)
   O(blitz_neural_info, fallback_levels)
+  S(blitz_settings) S(blitz_lod_info) S(blitz_storage_info) S(blitz_runtime_lod_storage_info)
+  S(blitz_neural_options) S(blitz_neural_action_proposal) S(blitz_curve_point) S(blitz_color_rgba8)
+  O(blitz_settings, max_supersample) O(blitz_settings, search_seed) O(blitz_settings, max_changed_area)
+  O(blitz_settings, attribute_importance_count) O(blitz_settings, user_data)
+  O(blitz_lod_info, screen_pixels) O(blitz_lod_info, reference_triangles)
+  O(blitz_lod_info, source_changed_area_worst_view)
+  O(blitz_storage_info, max_added_vertex_bytes_bps) O(blitz_runtime_lod_storage_info, cumulative_added_vertex_bytes)
+  O(blitz_neural_options, reserved) O(blitz_neural_action_proposal, screen_pixels)
+  O(blitz_neural_action_proposal, reserved)
   %s
   return 0;
 }
