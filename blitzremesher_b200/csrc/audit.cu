@@ -643,13 +643,19 @@ __device__ void audit_unit(const CandidateRecord* __restrict__ rec, const PlanDe
         // bounds every search: a sample whose nearest covered sample is
         // closer cannot raise it.
         best = uint32_t(max(max(far1, far2), 0));
+        // Verdict-only calls (threshold predicate, evaluate.cu:1034-1169):
+        // a sample nearer than `floor` cannot change any gate's verdict, so
+        // its search may stop at any covered sample within it; once the
+        // maximum exceeds `ceiling` every gate of the plan fails this view
+        // and the search stops. Exact calls: floor 0, ceiling UINT32_MAX.
+        const uint32_t floor_d2 = plan.d2_floor, ceiling_d2 = plan.d2_ceiling;
         // Reference-only samples of the affected tiles outside the region.
-        for (uint32_t base = 0; base < qn; base += 32) {
+        for (uint32_t base = 0; base < qn && best <= ceiling_d2; base += 32) {
             const uint32_t k = base + lane;
             if (k < qn) {
                 const uint32_t e = ws.queue[k];
                 const uint32_t x = e & 0x7fffu, y = (e >> 15) & 0x7fffu;
-                const uint32_t d = nearest_d2(cmask, x, y, best);
+                const uint32_t d = nearest_d2(cmask, x, y, max(best, floor_d2));
                 best = d > best ? d : best;
             }
             for (int o = 16; o; o >>= 1) {
@@ -663,14 +669,15 @@ __device__ void audit_unit(const CandidateRecord* __restrict__ rec, const PlanDe
             // The region's changed samples are its flips, queued in phase 2.
             // Candidate-only samples measure to the reference (resident field
             // or search), reference-only samples search the candidate.
-            for (uint32_t base = 0; base < queued; base += 32) {
+            for (uint32_t base = 0; base < queued && best <= ceiling_d2; base += 32) {
                 const uint32_t k = base + lane;
                 if (k < queued) {
                     const uint32_t e = ws.queue[k];
                     const uint32_t x = uint32_t(wx0) + (e & 0x7fffu), y = uint32_t(ry0) + ((e >> 15) & 0x7fffu);
+                    const uint32_t enough = max(best, floor_d2);
                     uint32_t d;
-                    if (e >> 31) d = pv.ref_field ? pv.ref_field[size_t(y) * size + x] : nearest_d2(rmask, x, y, best);
-                    else d = nearest_d2(cmask, x, y, best);
+                    if (e >> 31) d = pv.ref_field ? pv.ref_field[size_t(y) * size + x] : nearest_d2(rmask, x, y, enough);
+                    else d = nearest_d2(cmask, x, y, enough);
                     best = d > best ? d : best;
                 }
                 for (int o = 16; o; o >>= 1) {
@@ -686,7 +693,7 @@ __device__ void audit_unit(const CandidateRecord* __restrict__ rec, const PlanDe
             uint32_t* rmask_s = ws.queue;       // 32 xor masks (the queue is consumed)
             uint32_t* cmask_s = ws.queue + 32;  // 32 candidate words
             uint32_t* pre = ws.work;            // 33 prefix counts
-            for (int base = 0; base < region_words; base += 32) {
+            for (int base = 0; base < region_words && best <= ceiling_d2; base += 32) {
                 const int k = base + int(lane);
                 uint32_t xm = 0, Cw = 0;
                 if (k < region_words) {
@@ -717,10 +724,11 @@ __device__ void audit_unit(const CandidateRecord* __restrict__ rec, const PlanDe
                     const int kw = base + int(w);
                     const uint32_t ry = uint32_t(ry0 + kw / words), cw = uint32_t(kw % words);
                     const uint32_t x = uint32_t(wx0) + 32 * cw + bit;
+                    const uint32_t enough = max(best, floor_d2);
                     uint32_t d;
                     if ((cmask_s[w] >> bit) & 1u)
-                        d = pv.ref_field ? pv.ref_field[size_t(ry) * size + x] : nearest_d2(rmask, x, ry, best);
-                    else d = nearest_d2(cmask, x, ry, best);
+                        d = pv.ref_field ? pv.ref_field[size_t(ry) * size + x] : nearest_d2(rmask, x, ry, enough);
+                    else d = nearest_d2(cmask, x, ry, enough);
                     best = d > best ? d : best;
                 }
                 for (int o = 16; o; o >>= 1) {

@@ -98,6 +98,10 @@ struct PlanDev {
     uint32_t nviews, ss, size;
     uint32_t force_two;
     uint32_t state_is_ref; // state masks equal the reference masks
+    // Verdict-only bounds on the squared distance (see audit_unit): samples
+    // nearer than d2_floor need no exact value, a view whose maximum exceeds
+    // d2_ceiling fails every gate of the plan. Exact: 0 and UINT32_MAX.
+    uint32_t d2_floor, d2_ceiling;
 };
 
 // ---- launchers (kernels.cu) ----

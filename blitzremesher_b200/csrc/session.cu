@@ -729,6 +729,7 @@ static Plan& plan_for(Session& S, const PlanKey& key) {
     p.dev.views = p.dviews.p;
     for (int k = 0; k < 3; ++k) p.dev.center[k] = S.bounds.center[k];
     p.dev.nviews = p.views, p.dev.ss = key.ss, p.dev.size = p.size, p.dev.force_two = key.force_two;
+    p.dev.d2_floor = 0, p.dev.d2_ceiling = 0xffffffffu;
     refresh_state(S, p);
     return *(S.plans[key] = std::move(plan));
 }
@@ -997,7 +998,35 @@ struct AuditSetup {
     uint32_t plan_of[4];
     std::vector<Plan*> plans;
 };
-static void setup_audit(Session& S, const blitz_eval_settings gates_in[4], AuditSetup& a) {
+// The largest squared distance at which a view still passes gate g on
+// coverage (finish_view's error <= limit, evaluate.cpp:271-298), or -1 when
+// no distance does: the error is non-decreasing in the distance, so a binary
+// search over the integers with the same FP64 expressions finds it.
+static int64_t pass_threshold(const GateSettings& g, uint32_t ss) {
+    auto passes = [&](uint64_t d2) {
+        ViewRecord r{};
+        r.changed = r.total = 1;
+        r.ca = r.cb = 1;
+        Measurement cur = default_measurement();
+        finish_view(cur, r, g, ss, double(d2));
+        return cur.error <= g.limit;
+    };
+    if (!passes(0)) return -1;
+    uint64_t lo = 0, hi = 0xffffffffull;
+    if (passes(hi)) return int64_t(hi);
+    while (lo + 1 < hi) {
+        const uint64_t mid = lo + (hi - lo) / 2;
+        if (passes(mid)) lo = mid;
+        else hi = mid;
+    }
+    return int64_t(lo);
+}
+
+// verdict_only: the caller takes verdicts only (no Measurements), so each
+// plan's audit may stop measuring a view once its verdicts are certain
+// (PlanDev d2_floor / d2_ceiling); else the audit measures exactly.
+static void setup_audit(Session& S, const blitz_eval_settings gates_in[4], AuditSetup& a,
+                        bool verdict_only = false) {
     a.keys.clear();
     a.plans.clear();
     for (int g = 0; g < 4; ++g) {
@@ -1015,6 +1044,19 @@ static void setup_audit(Session& S, const blitz_eval_settings gates_in[4], Audit
         Plan& p = plan_for(S, k);
         if (p.resource_limited) throw Failure(BLITZ_BUDGET_LIMITED, "raster exceeds per-view sample budget");
         a.plans.push_back(&p);
+    }
+    for (size_t i = 0; i < a.plans.size(); ++i) {
+        Plan& p = *a.plans[i];
+        p.dev.d2_floor = 0, p.dev.d2_ceiling = 0xffffffffu;
+        if (!verdict_only) continue;
+        int64_t lo = INT64_MAX, hi = -1;
+        for (int g = 0; g < 4; ++g) {
+            if (a.plan_of[g] != i) continue;
+            const int64_t t = pass_threshold(a.gates[g].g, p.key.ss);
+            lo = std::min(lo, t), hi = std::max(hi, t);
+        }
+        p.dev.d2_floor = uint32_t(std::max<int64_t>(lo, 0));
+        p.dev.d2_ceiling = uint32_t(std::max<int64_t>(hi, 0));
     }
 }
 // Per-plan record tables of k_verdicts for n candidates (records sized here).
@@ -1079,7 +1121,7 @@ static void audit_candidates(Session& S, const blitz_collapse* cands_dev, const 
     if (n > UINT32_MAX / 2) throw Failure(BLITZ_INVALID_ARGUMENT, "too many candidates");
     (void)cands_host;
     AuditSetup a;
-    setup_audit(S, gates_in, a);
+    setup_audit(S, gates_in, a, meas_dev == nullptr);
     const uint32_t nn = uint32_t(n);
     Topology& t = S.topo;
     S.records.ensure(S.pool, nn);
@@ -2426,7 +2468,7 @@ static void batch_candidates(blitz_audit_batch* b, const blitz_collapse* cands, 
         bool big = false, giant = false;
         for (size_t i = 0; i < ns; ++i) {
             Session& S = b->sessions[i]->s;
-            setup_audit(S, gates_in, setup[i]);
+            setup_audit(S, gates_in, setup[i], true);
             upload_verdict_tables(S, setup[i], uint32_t(counts[i]), S.stream);
             B200_CUDA(cudaStreamSynchronize(S.stream));
             slots = std::max(slots, setup[i].plans.size());

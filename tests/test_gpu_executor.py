@@ -233,3 +233,25 @@ def test_learned_ranking_passes_the_exact_audit(gpu_lib):
         for g in gates:
             m = br.evaluate(mesh, syn.Mesh(pos, idx), g, session=s)
             assert m.passed == 1
+
+
+@pytest.mark.parametrize("level,screen,limits", [(3, 24.0, (1.0, 0.5)), (1, 64.0, (2.0, 1.0)), (2, 96.0, (3.0, 1.5))])
+def test_verdict_only_audit_gives_the_exact_verdicts(gpu_lib, level, screen, limits):
+    """Without a Measurement buffer the audit stops measuring a view once its
+    verdicts are certain (the threshold predicate of evaluate.cu:1034-1169):
+    the verdicts and failed gates equal those of the exactly measured audit,
+    rejections included, at LOD0 and after commits."""
+    mesh = syn.noisy_icosphere(level, 31)
+    views = (6, 2, 97)
+    gates = [br.eval_settings(screen, limits[0], views, 8, 8, 1.0), br.eval_settings(screen, limits[1], views, 8, 8, 1.0),
+             br.eval_settings(screen, limits[0], views, 8, 8, 0.5), br.eval_settings(screen, limits[1], views, 8, 8, 0.5)]
+    with br.AuditSession(mesh) as s:
+        for commit in (False, True):
+            if commit:
+                s.execute(mesh.face_count - 8, 40, [br.eval_settings(screen, 6.0, views, 8, 8, 1.0)] * 4, batch=4)
+            cands = br.midpoint_collapses(s.actions())
+            exact, _ = s.candidates(cands, gates, measurements=True)
+            quick = s.candidates(cands, gates)
+            assert np.array_equal(exact["accepted"], quick["accepted"])
+            assert np.array_equal(exact["failed_gate"], quick["failed_gate"])
+            assert 0 < int(exact["accepted"].sum()) < cands.size
