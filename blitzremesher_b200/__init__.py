@@ -236,6 +236,11 @@ EXPORTS = {
     "blitz_result_neural_action_proposal": ([C.c_void_p, C.c_size_t, C.POINTER(ActionProposal)], C.c_int),
     "blitz_audit_state_materials": ([C.c_void_p, C.c_void_p, C.c_size_t, C.POINTER(C.c_uint32), C.c_char_p,
                                      C.c_size_t], C.c_int),
+    "blitz_mesh_file_load": ([C.c_char_p, C.POINTER(C.c_void_p), C.POINTER(BlitzMesh), C.c_char_p, C.c_size_t],
+                             C.c_int),
+    "blitz_mesh_file_destroy": ([C.c_void_p], None),
+    "blitz_mesh_save_ply": ([C.POINTER(BlitzMesh), C.c_char_p, C.c_char_p, C.c_size_t], C.c_int),
+    "blitz_result_save_chain": ([C.c_void_p, C.c_char_p, C.c_char_p, C.c_size_t], C.c_int),
     "blitz_audit_state": ([C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p, C.c_size_t, C.POINTER(C.c_uint32),
                            C.c_char_p, C.c_size_t], C.c_int),
     "blitz_mesh_bounds": ([C.c_void_p, C.c_void_p, C.POINTER(C.c_double), C.c_char_p, C.c_size_t], C.c_int),
@@ -857,16 +862,19 @@ class NeuralModel:
             pass
 
 
-def generate_neural(mesh, config: Settings, model: NeuralModel) -> dict:
+def generate_neural(mesh, config: Settings, model: NeuralModel, save_to=None) -> dict:
     """blitz_generate_neural: every scheduled level (0 = the source) with its
     lod info, indices and positions; runtime levels, storage, diagnostics and
-    per-level action proposals."""
+    per-level action proposals. With `save_to`, the chain is also exported
+    there (blitz_result_save_chain: chain.gltf, chain.bin, lods.json)."""
     lib = load()
     hold = _MeshHold(mesh)
     res = C.c_void_p()
     err = C.create_string_buffer(512)
     _check(lib.blitz_generate_neural(C.byref(hold.c), C.byref(config), model.handle, C.byref(res), err, 512), err)
     try:
+        if save_to is not None:
+            _check(lib.blitz_result_save_chain(res, str(save_to).encode(), err, 512), err)
         lods = []
         for i in range(lib.blitz_result_lod_count(res)):
             info = LodInfo()
@@ -897,3 +905,39 @@ def generate_neural(mesh, config: Settings, model: NeuralModel) -> dict:
                 "info": {k: getattr(ni, k) for k, _ in ni._fields_ if k != "struct_size"}, "proposals": props}
     finally:
         lib.blitz_result_destroy(res)
+
+
+def _stream_array(stream, dtype, width):
+    if not stream.data or not stream.count:
+        return None
+    n = stream.count * stream.stride // np.dtype(dtype).itemsize
+    raw = np.ctypeslib.as_array(C.cast(stream.data, C.POINTER(np.ctypeslib.as_ctypes_type(dtype))), shape=(n,))
+    return raw.reshape(stream.count, stream.stride // np.dtype(dtype).itemsize)[:, :width].copy()
+
+
+def load_mesh(path) -> dict:
+    """blitz_mesh_file_load: OBJ, PLY or STL as numpy arrays (positions,
+    indices, and normals / uv / colors / materials when the file has them)."""
+    lib = load()
+    handle = C.c_void_p()
+    d = BlitzMesh()
+    err = C.create_string_buffer(512)
+    _check(lib.blitz_mesh_file_load(str(path).encode(), C.byref(handle), C.byref(d), err, 512), err)
+    try:
+        out = {"positions": _stream_array(d.positions, np.float32, 3),
+               "indices": np.ctypeslib.as_array(C.cast(d.indices, C.POINTER(C.c_uint32)), shape=(d.index_count,)).copy(),
+               "normals": _stream_array(d.normals, np.float32, 3), "uv": _stream_array(d.uv, np.float32, 2),
+               "colors": _stream_array(d.colors, np.uint8, 4), "materials": None}
+        if d.materials:
+            out["materials"] = np.ctypeslib.as_array(C.cast(d.materials, C.POINTER(C.c_uint16)),
+                                                     shape=(d.material_count,)).copy()
+        return out
+    finally:
+        lib.blitz_mesh_file_destroy(handle)
+
+
+def save_ply(mesh, path) -> None:
+    """blitz_mesh_save_ply of a synthetic.Mesh-like object."""
+    hold = _MeshHold(mesh)
+    err = C.create_string_buffer(512)
+    _check(load().blitz_mesh_save_ply(C.byref(hold.c), str(path).encode(), err, 512), err)

@@ -14,7 +14,7 @@ from pathlib import Path
 HERE = Path(__file__).resolve().parent
 CSRC = HERE / "csrc"
 LIB = HERE / "libblitz_b200.so"
-SOURCES = ["topology.cu", "raster.cu", "audit.cu", "session.cu", "static_distance.cu", "surrogate.cu", "generate.cu"]
+SOURCES = ["topology.cu", "raster.cu", "audit.cu", "session.cu", "static_distance.cu", "surrogate.cu", "generate.cu", "mesh_io.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
 FLAGS = [

@@ -126,34 +126,34 @@ __device__ __forceinline__ void record_write(ViewRecord* out, const ViewRecord& 
 
 // Rows of interval ends kept per pass of the word-row region phase.
 constexpr int kPassRows = 8;
+// Shared memory of one warp of the global tiers: face setups, the pass's
+// interval ends and its two word-mask tables.
+constexpr size_t kGlobalTierWarpSmem = kMaxOk * sizeof(FaceSetup) + kPassRows * kMaxOk * 4 + 2 * kPassRows * 32 * 4;
 
-// Region phase over coverage words (the global tiers): lanes own 32-sample
-// words of the region's rows (several rows per pass when the region is
-// narrow). Per (face, row) the covered samples are one interval (exact
-// FP64 binary searches, face_interval), computed once per pass by the lanes
-// together and kept in `iv` (shared memory); each lane turns the intervals
-// crossing its word into masks: the union of the new faces' masks (B) and
-// a bit-sliced count of the old faces covering each sample (A). Because the
-// state's count pc includes every old face (pc >= A), the candidate's count
-// pc - A + B is positive wherever B > 0, and where B = 0 it is pc - A. So a
-// sample flips iff it is newly covered (B > 0 on a state-empty sample, from
-// the state's coverage word alone) or it loses its last faces (B = 0, A > 0
-// and pc == A: the only samples whose state count is read). Flipped samples
-// are written to the region words (candidate XOR state) and counted into the
-// popcount deltas against the reference.
+// Region phase over coverage words (the global tiers), kPassRows rows at a
+// time. Per (row, face) the covered samples are one interval (exact FP64
+// binary searches, face_interval), computed once per pass by the lanes
+// together and kept in `iv` (shared memory). Each interval is then OR-ed
+// into the pass's word masks in shared memory (`masks`): the union of the
+// new faces (B) and of the old faces (A). Because the state's count pc
+// includes every old face (pc >= A), the candidate's count pc - A + B is
+// positive wherever B > 0, and where B = 0 it is pc - A. So a sample flips
+// iff it is newly covered (B on a state-empty sample, from the state's
+// coverage word alone) or it loses its last faces (A without B, and pc
+// equal to the number of old faces covering it: the only samples whose
+// state count is read, and whose old faces are counted from the intervals).
+// Lanes own (row, word) items, up to eight each, whose coverage words are
+// all loaded before any is used. Flipped samples are written to the region
+// words (candidate XOR state) and counted into the popcount deltas against
+// the reference.
 __device__ void region_word_rows(const FaceSetup* faces, uint32_t nok, int wx0, int ry0, int ry1, int words,
                                  const PlanView& pv, uint32_t size, bool same_ref, uint32_t* region, short2* iv,
-                                 int& dchg, int& dtot, int& dcov, int& flips, bool& negative) {
+                                 uint32_t* masks, int& dchg, int& dtot, int& dcov, int& flips, bool& negative) {
     const uint32_t lane = lane_id();
-    // Lanes per row: the region's words rounded up to a power of two (at
-    // most 32); rows per pass: 32 / that, at most kPassRows.
-    uint32_t span = 1;
-    while (span < uint32_t(words) && span < 32) span <<= 1;
-    const uint32_t rows_per_pass = min(uint32_t(kPassRows), 32u / span);
-    const uint32_t my_row = lane / span, my_word = lane % span;
-    for (int ybase = ry0; ybase <= ry1; ybase += int(rows_per_pass)) {
-        const uint32_t pass_rows = min(rows_per_pass, uint32_t(ry1 - ybase + 1));
-        // Interval ends of every (row, face) of this pass.
+    uint32_t* const bn = masks;                  // [kPassRows][32] new-face union
+    uint32_t* const an = masks + kPassRows * 32; // [kPassRows][32] old-face union
+    for (int ybase = ry0; ybase <= ry1; ybase += kPassRows) {
+        const uint32_t pass_rows = min(uint32_t(kPassRows), uint32_t(ry1 - ybase + 1));
         const uint32_t items = pass_rows * nok;
         for (uint32_t t = lane; t < items; t += 32) {
             const uint32_t r = t / nok, f = t - r * nok;
@@ -163,62 +163,80 @@ __device__ void region_word_rows(const FaceSetup* faces, uint32_t nok, int wx0, 
             if (y >= fs.y0 && y <= fs.y1) face_interval(fs, double(y) + .5, lo, hi);
             iv[r * kMaxOk + f] = make_short2(short(lo), short(hi));
         }
-        __syncwarp();
-        const int y = ybase + int(my_row);
-        const bool row_ok = my_row < pass_rows;
-        for (uint32_t w = my_word; row_ok && w < uint32_t(words); w += span) {
-            const int xb = wx0 + 32 * int(w); // first sample of the word
-            uint32_t bnew = 0, a0 = 0, a1 = 0, a2 = 0, a3 = 0, a4 = 0, a5 = 0;
-            for (uint32_t f = 0; f < nok; ++f) {
-                const short2 e = iv[my_row * kMaxOk + f];
-                const int lo = max(int(e.x), xb), hi = min(int(e.y), xb + 31);
+        for (int c0 = 0; c0 < words; c0 += 32) { // 32-word windows of wide regions
+            const uint32_t cn = uint32_t(min(32, words - c0));
+            const int xc0 = wx0 + 32 * c0, xc1 = wx0 + 32 * (c0 + int(cn)) - 1;
+            for (uint32_t k = lane; k < 2 * kPassRows * 32; k += 32) masks[k] = 0;
+            __syncwarp();
+            for (uint32_t t = lane; t < items; t += 32) {
+                const uint32_t r = t / nok, f = t - r * nok;
+                const short2 e = iv[r * kMaxOk + f];
+                const int lo = max(int(e.x), xc0), hi = min(int(e.y), xc1);
                 if (lo > hi) continue;
-                const uint32_t m = (hi - xb == 31 ? 0xffffffffu : ((2u << (hi - xb)) - 1u)) & ~((1u << (lo - xb)) - 1u);
-                if (faces[f].pad > 0) {
-                    bnew |= m;
-                } else { // bit-sliced count of the old faces (at most 48 < 64)
-                    uint32_t c = m, t;
-                    t = a0 & c, a0 ^= c, c = t;
-                    t = a1 & c, a1 ^= c, c = t;
-                    t = a2 & c, a2 ^= c, c = t;
-                    t = a3 & c, a3 ^= c, c = t;
-                    t = a4 & c, a4 ^= c, c = t;
-                    a5 ^= c;
+                uint32_t* dst = (faces[f].pad > 0 ? bn : an) + r * 32;
+                for (int w = (lo - xc0) >> 5; w <= (hi - xc0) >> 5; ++w) {
+                    const int xb = xc0 + 32 * w, a = max(lo, xb) - xb, z = min(hi, xb + 31) - xb;
+                    const uint32_t m = (z == 31 ? 0xffffffffu : ((2u << z) - 1u)) & ~((1u << a) - 1u);
+                    atomicOr(dst + w, m);
                 }
             }
-            const uint32_t aany = a0 | a1 | a2 | a3 | a4 | a5;
-            if (!(bnew | aany)) {
-                region[uint32_t(y - ry0) * uint32_t(words) + w] = 0;
-                continue;
+            __syncwarp();
+            const uint32_t cells = pass_rows * cn;
+            uint32_t S[8], R[8];
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                const uint32_t t = lane + 32u * uint32_t(k);
+                S[k] = R[k] = 0;
+                if (t < cells) {
+                    const uint32_t r = t / cn, w = t - r * cn;
+                    if (bn[r * 32 + w] | an[r * 32 + w]) {
+                        const uint32_t y = uint32_t(ybase) + r, cw = (uint32_t(xc0) >> 5) + w;
+                        S[k] = chunk_global(pv.state_bits, size, y, cw);
+                        R[k] = same_ref ? S[k] : chunk_global(pv.ref_bits, size, y, cw);
+                    }
+                }
             }
-            const uint32_t cw = uint32_t(xb) >> 5;
-            const uint32_t S = chunk_global(pv.state_bits, size, uint32_t(y), cw);
-            const uint32_t R = same_ref ? S : chunk_global(pv.ref_bits, size, uint32_t(y), cw);
-            const uint32_t grown = bnew & ~S;   // newly covered
-            uint32_t lost_cand = aany & ~bnew;  // covered only if other faces cover it
-            negative |= (lost_cand & ~S) != 0;  // pc >= A > 0 must hold
-            lost_cand &= S;
-            uint32_t lost = 0;
-            const size_t row_at = size_t(y) * size;
-            while (lost_cand) {
-                const int i = __ffs(lost_cand) - 1;
-                lost_cand &= lost_cand - 1;
-                const uint32_t A = ((a0 >> i) & 1u) | (((a1 >> i) & 1u) << 1) | (((a2 >> i) & 1u) << 2) |
-                                   (((a3 >> i) & 1u) << 3) | (((a4 >> i) & 1u) << 4) | (((a5 >> i) & 1u) << 5);
-                const uint32_t pc = pv.state_count[row_at + size_t(xb + i)];
-                negative |= pc < A;
-                if (pc == A) lost |= 1u << i;
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                const uint32_t t = lane + 32u * uint32_t(k);
+                if (t >= cells) break;
+                const uint32_t r = t / cn, w = t - r * cn;
+                const uint32_t bnew = bn[r * 32 + w], aany = an[r * 32 + w];
+                uint32_t* out = region + (uint32_t(ybase) + r - uint32_t(ry0)) * uint32_t(words) + uint32_t(c0) + w;
+                if (!(bnew | aany)) {
+                    *out = 0;
+                    continue;
+                }
+                const int y = ybase + int(r), xb = xc0 + 32 * int(w);
+                const uint32_t grown = bnew & ~S[k];   // newly covered
+                uint32_t lost_cand = aany & ~bnew;     // covered only if other faces cover it
+                negative |= (lost_cand & ~S[k]) != 0;  // pc >= A > 0 must hold
+                lost_cand &= S[k];
+                uint32_t lost = 0;
+                while (lost_cand) {
+                    const int i = __ffs(lost_cand) - 1;
+                    lost_cand &= lost_cand - 1;
+                    const int x = xb + i;
+                    uint32_t A = 0; // old faces covering (x, y)
+                    for (uint32_t f = 0; f < nok; ++f) {
+                        const short2 e = iv[r * kMaxOk + f];
+                        A += faces[f].pad < 0 && int(e.x) <= x && x <= int(e.y);
+                    }
+                    const uint32_t pc = pv.state_count[size_t(y) * size + size_t(x)];
+                    negative |= pc < A;
+                    if (pc == A) lost |= 1u << i;
+                }
+                const uint32_t fl = grown | lost;
+                *out = fl;
+                if (!fl) continue;
+                flips += __popc(fl);
+                dcov += __popc(grown) - __popc(lost);
+                const uint32_t X = S[k] ^ R[k];
+                dchg += __popc(fl & ~X) - __popc(fl & X);
+                dtot += __popc(fl & ~R[k] & ~S[k]) - __popc(fl & ~R[k] & S[k]);
             }
-            const uint32_t fl = grown | lost;
-            region[uint32_t(y - ry0) * uint32_t(words) + w] = fl;
-            if (!fl) continue;
-            flips += __popc(fl);
-            dcov += __popc(grown) - __popc(lost);
-            const uint32_t X = S ^ R;
-            dchg += __popc(fl & ~X) - __popc(fl & X);
-            dtot += __popc(fl & ~R & ~S) - __popc(fl & ~R & S);
+            __syncwarp();
         }
-        __syncwarp();
     }
 }
 
@@ -228,13 +246,14 @@ template <class L>
 __device__ void audit_unit(const CandidateRecord* __restrict__ rec, const PlanDev& plan, uint32_t v,
                            WarpScratch<L>& ws, ViewRecord* out, unsigned long long* stats, uint32_t u,
                            uint32_t* spill, uint32_t heavy = 0xffffffffu, FaceSetup* face_table = nullptr,
-                           short2* iv_table = nullptr) {
+                           short2* iv_table = nullptr, uint32_t* mask_table = nullptr) {
     // The face setups: in the warp's scratch, or in shared memory for the
     // tiers whose scratch is global (the row sweep reads them every row).
     FaceSetup* const faces = face_table ? face_table : ws.faces;
-    // With an interval table the region phase runs over coverage words
-    // (region_word_rows) and the distance phase walks the region words.
-    const bool word_rows = iv_table != nullptr;
+    // The global tiers (regions taller than 256 rows) run the region phase
+    // over coverage words (region_word_rows, with the interval and mask
+    // tables in shared memory) and the distance phase walks the region words.
+    constexpr bool word_rows = L::kRegionRows > 256;
     constexpr int kRegionWords = L::kRegionWords, kRegionRows = L::kRegionRows;
     constexpr int kDeltaSamples = L::kDeltaSamples, kQueue = L::kQueue, kAffected = L::kAffected;
     const uint32_t lane = lane_id();
@@ -414,9 +433,9 @@ __device__ void audit_unit(const CandidateRecord* __restrict__ rec, const PlanDe
                     if (pos < uint32_t(kQueue)) ws.queue[pos] = xr | (yr << 15) | (C ? 0x80000000u : 0u);
                 }
             };
-            if (word_rows) {
-                region_word_rows(faces, nok, wx0, ry0, ry1, words, pv, size, same_ref, ws.region, iv_table, dchg, dtot,
-                                 dcov, flips, negative);
+            if constexpr (word_rows) {
+                region_word_rows(faces, nok, wx0, ry0, ry1, words, pv, size, same_ref, ws.region, iv_table, mask_table,
+                                 dchg, dtot, dcov, flips, negative);
             } else if (direct) {
                 const uint32_t delta_words = uint32_t(bws * bh) >> 2;
                 for (uint32_t k = lane; k < delta_words; k += 32) ws.delta[k] = 0x80808080u;
@@ -861,8 +880,13 @@ template <class L, int kWarps>
 __global__ void __launch_bounds__(kWarps * 32, 2)
     k_audit_global(const __grid_constant__ AuditJob job, unsigned long long* stats, const uint32_t* spill,
                    uint32_t* cursor, unsigned char* scratch, uint32_t* spill_next) {
-    __shared__ FaceSetup face_table[kWarps][kMaxOk];
-    __shared__ short2 iv_table[kWarps][kPassRows * kMaxOk];
+    // Dynamic shared memory, per warp: face setups, pass intervals, pass masks.
+    extern __shared__ __align__(16) unsigned char global_tier_smem[];
+    const uint32_t wslot = threadIdx.x >> 5;
+    unsigned char* mine = global_tier_smem + size_t(wslot) * kGlobalTierWarpSmem;
+    FaceSetup* face_table = reinterpret_cast<FaceSetup*>(mine);
+    short2* iv_table = reinterpret_cast<short2*>(mine + kMaxOk * sizeof(FaceSetup));
+    uint32_t* mask_table = reinterpret_cast<uint32_t*>(mine + kMaxOk * sizeof(FaceSetup) + kPassRows * kMaxOk * 4);
     const uint32_t lane = lane_id();
     const uint32_t slot = blockIdx.x * kWarps + (threadIdx.x >> 5);
     WarpScratch<L>& ws = reinterpret_cast<WarpScratch<L>*>(scratch)[slot];
@@ -880,7 +904,7 @@ __global__ void __launch_bounds__(kWarps * 32, 2)
         resolve_unit(job, u, plan, recs, out, lu);
         const uint32_t c = lu / plan->nviews, v = lu - c * plan->nviews;
         audit_unit(recs + c, *plan, v, ws, out + lu, stats, u, spill_next, 0xffffffffu,
-                   face_table[threadIdx.x >> 5], iv_table[threadIdx.x >> 5]);
+                   face_table, iv_table, mask_table);
     }
 }
 
@@ -978,6 +1002,8 @@ void launch_audit(const AuditJob& job, unsigned long long* stats, uint32_t* queu
         for (int v = 0; v < 2; ++v)
             for (int m = 0; m < 2; ++m) set_smem(warp_tier(v, m != 0), warp_tier_smem(v));
         set_smem(k_audit_large, large);
+        set_smem(k_audit_global<LimitsHuge, kHugeWarps>, kHugeWarps * kGlobalTierWarpSmem);
+        set_smem(k_audit_global<LimitsGiant, kGiantWarps>, kGiantWarps * kGlobalTierWarpSmem);
         configured = true;
     }
     const int tier = variant & 1;
@@ -1004,18 +1030,22 @@ void launch_audit(const AuditJob& job, unsigned long long* stats, uint32_t* queu
     if (huge && huge_blocks >= uint32_t(sms)) {
         // enough huge-tier warps: units the warp tier spills go there directly
         k_audit_global<LimitsHuge, kHugeWarps>
-            <<<huge_blocks, kHugeWarps * 32, 0, s>>>(job, stats, spill, queue + 1, huge_scratch, next);
+            <<<huge_blocks, kHugeWarps * 32, kHugeWarps * kGlobalTierWarpSmem, s>>>(job, stats, spill, queue + 1,
+                                                                                   huge_scratch, next);
     } else {
         if (spill)
             k_audit_large<<<uint32_t(sms), kLargeWarps * 32, large, s>>>(job, stats, spill, queue + 1,
                                                                          huge ? spill_huge : nullptr);
         if (huge)
             k_audit_global<LimitsHuge, kHugeWarps>
-                <<<huge_blocks, kHugeWarps * 32, 0, s>>>(job, stats, spill_huge, queue + 2, huge_scratch, next);
+                <<<huge_blocks, kHugeWarps * 32, kHugeWarps * kGlobalTierWarpSmem, s>>>(job, stats, spill_huge,
+                                                                                       queue + 2, huge_scratch, next);
     }
     if (big)
         k_audit_global<LimitsGiant, kGiantWarps>
-            <<<giant->blocks, kGiantWarps * 32, 0, s>>>(job, stats, giant->spill, queue + 3, giant->scratch, nullptr);
+            <<<giant->blocks, kGiantWarps * 32, kGiantWarps * kGlobalTierWarpSmem, s>>>(job, stats, giant->spill,
+                                                                                       queue + 3, giant->scratch,
+                                                                                       nullptr);
 }
 
 void launch_verdicts(const ViewRecord* const* plan_records, const uint32_t* plan_views, const uint32_t* plan_ss,

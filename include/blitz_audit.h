@@ -197,6 +197,26 @@ size_t blitz_result_neural_action_proposal_count(const blitz_result*);
 blitz_status blitz_result_neural_action_proposal(const blitz_result*, size_t, blitz_neural_action_proposal*);
 #endif
 
+/* ---- Mesh files ----------------------------------------------------------
+ * Import (the rules of load_mesh, src/io.cpp:118-229): OBJ (corners
+ * deduplicated by position/normal/uv index, polygons fanned, material ids
+ * 1 + place in the material library, non-opaque materials refused), PLY
+ * (ascii, binary either endianness, triangles only) and STL (binary or ascii,
+ * corners welded on exact position bits); 1 GiB cap; the reference's mesh
+ * validation (mesh.cpp:27-41). glTF import returns BLITZ_UNAVAILABLE. The
+ * descriptor borrows the file object's streams until it is destroyed. */
+typedef struct blitz_mesh_file blitz_mesh_file;
+blitz_status blitz_mesh_file_load(const char* path, blitz_mesh_file** out, blitz_mesh* mesh, char* error,
+                                  size_t error_capacity);
+void blitz_mesh_file_destroy(blitz_mesh_file*);
+/* Binary little-endian PLY of a mesh (save_ply, io.cpp:236-249). */
+blitz_status blitz_mesh_save_ply(const blitz_mesh* mesh, const char* path, char* error, size_t error_capacity);
+/* A generated chain as one glTF 2.0 scene (chain.gltf, chain.bin: one mesh
+ * per runtime level, one primitive per material, one node per scheduled
+ * level) and the lods.json manifest (save_chain, io.cpp:298-359). */
+blitz_status blitz_result_save_chain(const blitz_result* result, const char* directory, char* error,
+                                     size_t error_capacity);
+
 /* POD mirror of blitz::EvalSettings for the coverage profile
  * (include/blitz/evaluate.hpp:24-33; ViewSet evaluate.hpp:8). */
 typedef struct blitz_eval_settings {

@@ -4,6 +4,8 @@ loaded by blitz_neural_model_load_v2. Every emitted level equals the oracle's
 chain (schedule, four gates against the source and the previous level,
 batched midpoint executor), level 0 is the source itself, and the lod info,
 runtime levels, storage and proposals are consistent with the levels."""
+import json
+
 import numpy as np
 import pytest
 
@@ -28,7 +30,7 @@ def test_generate_neural_matches_oracle_chain(gpu_lib, oracle, tmp_path, batch):
                          transition=curve, search_ortho=search[0], search_perspective=search[1],
                          search_seed=search[2], audit_ortho=audit[0], audit_perspective=audit[1], audit_seed=audit[2],
                          search_supersample=4, audit_supersample=4, max_supersample=4, max_changed_area=1.0)
-    out = br.generate_neural(mesh, config, model)
+    out = br.generate_neural(mesh, config, model, save_to=tmp_path / "chain")
     lods = out["lods"]
     assert len(lods) == 4
     assert np.array_equal(lods[0]["indices"], mesh.indices) and lods[0]["shared_vertices"] == 1
@@ -50,6 +52,13 @@ def test_generate_neural_matches_oracle_chain(gpu_lib, oracle, tmp_path, batch):
     assert st["index_bytes"] == sum(lods[i]["indices"].size * 4 for i in out["runtime"])
     assert st["source_vertex_bytes"] == mesh.vertex_count * 12
     assert out["info"]["legal_collapses"] == sum(len(w["commits"]) for w in want)
+    # the exported chain: one node per level, one mesh per runtime level
+    gltf = json.loads((tmp_path / "chain" / "chain.gltf").read_text())
+    manifest = json.loads((tmp_path / "chain" / "lods.json").read_text())
+    assert len(gltf["nodes"]) == 4 and len(gltf["meshes"]) == len(out["runtime"])
+    assert gltf["buffers"][0]["byteLength"] == (tmp_path / "chain" / "chain.bin").stat().st_size
+    assert [l["triangles"] for l in manifest["lods"]] == [lv["indices"].size // 3 for lv in lods]
+    assert manifest["runtime_levels"] == out["runtime"]
     model.close()
 
 
