@@ -28,6 +28,7 @@ constexpr uint32_t kHeavyUnit = 512;    // changed samples above which a warp-ti
 // scratch small so that many warps stay resident; units that overflow it are
 // spilled to the large tier (few warps per SM, 256 x 256-sample regions).
 struct LimitsSmall {
+    static constexpr bool kWordRows = false; // region phase over coverage words
     static constexpr int kRegionWords = 4;     // region width <= 128 samples after 32-alignment
     static constexpr int kRegionRows = 64;     // region height
     static constexpr int kDeltaSamples = 2048; // region samples (unaligned bbox) with a count delta
@@ -37,6 +38,7 @@ struct LimitsSmall {
 // A wider warp tier for workloads whose units often overflow the small one
 // (one block of 8 warps per SM instead of three).
 struct LimitsMedium {
+    static constexpr bool kWordRows = true; // region phase over coverage words
     static constexpr int kRegionWords = 8;
     static constexpr int kRegionRows = 128;
     static constexpr int kDeltaSamples = 8192;
@@ -44,6 +46,7 @@ struct LimitsMedium {
     static constexpr int kAffected = 16;
 };
 struct LimitsLarge {
+    static constexpr bool kWordRows = true; // region phase over coverage words
     static constexpr int kRegionWords = 8;
     static constexpr int kRegionRows = 256;
     static constexpr int kDeltaSamples = 32768;
@@ -54,6 +57,7 @@ constexpr int kLargeWarps = 3; // warps per block of the large tier
 // The huge tier keeps its per-warp scratch in global memory (L2-resident
 // working set per unit): regions up to 1024 x 1024 samples.
 struct LimitsHuge {
+    static constexpr bool kWordRows = true; // region phase over coverage words
     static constexpr int kRegionWords = 32;
     static constexpr int kRegionRows = 1024;
     static constexpr int kDeltaSamples = 16384; // direct-test units only
@@ -64,6 +68,7 @@ constexpr int kHugeWarps = 8;
 // The giant tier: any region of a raster up to 4160 x 4160 (512 px x ss 8),
 // for the rare units beyond the huge tier; few warps, global scratch.
 struct LimitsGiant {
+    static constexpr bool kWordRows = true; // region phase over coverage words
     static constexpr int kRegionWords = 136;
     static constexpr int kRegionRows = 4160;
     static constexpr int kDeltaSamples = 16384;
@@ -250,10 +255,15 @@ __device__ void audit_unit(const CandidateRecord* __restrict__ rec, const PlanDe
     // The face setups: in the warp's scratch, or in shared memory for the
     // tiers whose scratch is global (the row sweep reads them every row).
     FaceSetup* const faces = face_table ? face_table : ws.faces;
-    // The global tiers (regions taller than 256 rows) run the region phase
-    // over coverage words (region_word_rows, with the interval and mask
-    // tables in shared memory) and the distance phase walks the region words.
-    constexpr bool word_rows = L::kRegionRows > 256;
+    // Every tier but the small one runs the region phase over coverage words
+    // (region_word_rows; its interval and mask tables in the warp's shared
+    // memory: given by the global tiers, else the delta map's space) and the
+    // distance phase walks the region words.
+    constexpr bool word_rows = L::kWordRows;
+    static_assert(!L::kWordRows || L::kDeltaSamples * sizeof(uint8_t) >= kPassRows * kMaxOk * 4 + 2 * kPassRows * 32 * 4,
+                  "the delta map's space holds the word-row tables");
+    short2* const iv_rows = iv_table ? iv_table : reinterpret_cast<short2*>(ws.delta);
+    uint32_t* const mask_rows = mask_table ? mask_table : ws.delta + kPassRows * kMaxOk;
     constexpr int kRegionWords = L::kRegionWords, kRegionRows = L::kRegionRows;
     constexpr int kDeltaSamples = L::kDeltaSamples, kQueue = L::kQueue, kAffected = L::kAffected;
     const uint32_t lane = lane_id();
@@ -434,7 +444,7 @@ __device__ void audit_unit(const CandidateRecord* __restrict__ rec, const PlanDe
                 }
             };
             if constexpr (word_rows) {
-                region_word_rows(faces, nok, wx0, ry0, ry1, words, pv, size, same_ref, ws.region, iv_table, mask_table,
+                region_word_rows(faces, nok, wx0, ry0, ry1, words, pv, size, same_ref, ws.region, iv_rows, mask_rows,
                                  dchg, dtot, dcov, flips, negative);
             } else if (direct) {
                 const uint32_t delta_words = uint32_t(bws * bh) >> 2;

@@ -440,6 +440,7 @@ struct Session {
     size_t sort_bytes = 0;
     blitz_neural_info info{};
     uint64_t internal_errors = 0;
+    std::vector<uint8_t> table_signature; // last uploaded verdict tables
     // profiling: device times of candidate calls; work counters as well
     // (per-unit clock and counter atomics in the audit kernels) when counting
     bool profiling = false, counting = false;
@@ -1060,7 +1061,9 @@ static void setup_audit(Session& S, const blitz_eval_settings gates_in[4], Audit
     }
 }
 // Per-plan record tables of k_verdicts for n candidates (records sized here).
-static void upload_verdict_tables(Session& S, const AuditSetup& a, uint32_t n, cudaStream_t st) {
+// Returns whether anything was uploaded: tables equal to the last upload's
+// (same plans, record buffers, gates) are not sent again.
+static bool upload_verdict_tables(Session& S, const AuditSetup& a, uint32_t n, cudaStream_t st) {
     std::vector<const ViewRecord*> table(a.plans.size());
     std::vector<uint32_t> pviews(a.plans.size()), pss(a.plans.size());
     for (size_t i = 0; i < a.plans.size(); ++i) {
@@ -1076,11 +1079,22 @@ static void upload_verdict_tables(Session& S, const AuditSetup& a, uint32_t n, c
     S.gate_table.ensure(S.pool, 4);
     S.exact_count.ensure(S.pool, 1);
     GateDev gd[4];
+    std::memset(gd, 0, sizeof gd);
     for (int g = 0; g < 4; ++g) gd[g] = GateDev{a.gates[g].g, a.plan_of[g]};
+    std::vector<uint8_t> sig;
+    auto put = [&](const void* q, size_t k) {
+        const uint8_t* c = static_cast<const uint8_t*>(q);
+        sig.insert(sig.end(), c, c + k);
+    };
+    put(table.data(), table.size() * sizeof(void*)), put(pviews.data(), pviews.size() * 4);
+    put(pss.data(), pss.size() * 4), put(gd, sizeof gd), put(&S.record_table.p, sizeof(void*));
+    if (sig == S.table_signature) return false;
     B200_CUDA(cudaMemcpyAsync(S.record_table.p, table.data(), table.size() * sizeof(void*), cudaMemcpyHostToDevice, st));
     B200_CUDA(cudaMemcpyAsync(S.plan_views.p, pviews.data(), pviews.size() * 4, cudaMemcpyHostToDevice, st));
     B200_CUDA(cudaMemcpyAsync(S.plan_ss.p, pss.data(), pss.size() * 4, cudaMemcpyHostToDevice, st));
     B200_CUDA(cudaMemcpyAsync(S.gate_table.p, gd, sizeof(gd), cudaMemcpyHostToDevice, st));
+    S.table_signature = std::move(sig);
+    return true;
 }
 // Candidates whose verdict needs the full-raster path (k_verdicts flagged
 // them): resolved one by one from their resume gate.
@@ -2469,8 +2483,8 @@ static void batch_candidates(blitz_audit_batch* b, const blitz_collapse* cands, 
         for (size_t i = 0; i < ns; ++i) {
             Session& S = b->sessions[i]->s;
             setup_audit(S, gates_in, setup[i], true);
-            upload_verdict_tables(S, setup[i], uint32_t(counts[i]), S.stream);
-            B200_CUDA(cudaStreamSynchronize(S.stream));
+            if (upload_verdict_tables(S, setup[i], uint32_t(counts[i]), S.stream))
+                B200_CUDA(cudaStreamSynchronize(S.stream));
             slots = std::max(slots, setup[i].plans.size());
             for (Plan* p : setup[i].plans) big |= p->size > 256, giant |= p->size > 1024;
         }

@@ -7,7 +7,7 @@ import numpy as np
 import pytest
 
 from blitzremesher_b200 import synthetic as syn
-from oracle.oracle import BoBounds, BoCamera, BoMeasurement, settings
+from oracle.oracle import BoBounds, BoCamera, BoEdit, BoMeasurement, settings
 
 from conftest import GOLDEN
 
@@ -194,3 +194,51 @@ def test_endpoint_walk_matches_reference_executor(oracle, reference, level, seed
     assert mine["stop"] == ref["stop"]
     assert np.array_equal(mine["indices"], ref["indices"])
     assert ref["accepted"] > 0
+
+
+PLACEMENT_GOLDEN = GOLDEN / "placement_ref.npz"
+
+
+@pytest.mark.skipif(not PLACEMENT_GOLDEN.exists(), reason="reference placement fixture absent")
+def test_midpoint_trials_match_reference_gpu_placement(oracle):
+    """The oracle's midpoint trial (placement, uv transport, validate_placement)
+    equals the reference's own GPU path (GpuActionState::trial,
+    action_gpu.cu:962-1156, run on a B200 by tests/golden/make_placement_golden.py)
+    trial for trial: validity, indices, and every moved slot's position and uv
+    bit for bit, on seamed meshes, a rock with 8 uv charts and ribbon cards,
+    with and without preserve_uv."""
+    import hashlib
+    import importlib.util
+
+    spec = importlib.util.spec_from_file_location("make_placement_golden", GOLDEN / "make_placement_golden.py")
+    maker = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(maker)
+    cases = maker.cases
+
+    g = np.load(PLACEMENT_GOLDEN)
+    checked = invalid = 0
+    for name, mesh, preserve in cases():
+        key = f"{name}_uv{preserve}"
+        at = 0
+        for row, (frm, to) in enumerate(g[f"{key}_from_to"]):
+            e = BoEdit()
+            e.from_, e.to = int(frm), int(to)
+            idx, pos, uv, valid = oracle.trial_midpoint(mesh, e, preserve_uv=bool(preserve))
+            assert int(valid) == int(g[f"{key}_valid"][row]), (key, frm, to)
+            if not valid:
+                invalid += 1
+                continue
+            n = int(g[f"{key}_count"][row])
+            slots = g[f"{key}_slots"][at:at + n]
+            assert idx.size // 3 == g[f"{key}_faces"][row]
+            assert hashlib.sha256(idx.astype(np.uint32).tobytes()).hexdigest()[:32] == g[f"{key}_sha"][row]
+            moved = np.any(pos.view(np.uint32) != mesh.positions.view(np.uint32), axis=1)
+            if mesh.uv is not None:
+                moved |= np.any(uv.view(np.uint32) != mesh.uv.view(np.uint32), axis=1)
+            assert np.array_equal(np.nonzero(moved)[0], slots), (key, frm, to)
+            assert np.array_equal(pos[slots].view(np.uint32), g[f"{key}_positions"][at:at + n].view(np.uint32))
+            if mesh.uv is not None:
+                assert np.array_equal(uv[slots].view(np.uint32), g[f"{key}_uv"][at:at + n].view(np.uint32))
+            at += n
+            checked += 1
+    assert checked > 200 and invalid > 0
