@@ -49,6 +49,10 @@ GATE_ARGS = [(SCREEN, SOURCE_LIMIT, VIEWS, SS, SS, 1.0), (SCREEN, TRANSITION_LIM
 # working set is L2-resident, the kernel is issue-bound.
 K_AUDIT_TRAFFIC = 45_381_120
 K_AUDIT_ISSUE_PCT = 65.6
+# DRAM bytes (read + write) of the batched workload's audit kernels per
+# batch: not yet captured (None).
+K_BATCH_TRAFFIC = None
+K_BATCH_TRAFFIC_NOTE = "not captured"
 
 
 BATCH_WORKLOAD = ("batched plain audit: 64 meshes (noisy spheres, R/r=3 tori, value-noise heightfields; "
@@ -558,14 +562,22 @@ def _shares(values) -> list:
 
 def _region_split(r) -> dict:
     """Region-phase sub-phases of a profiled batch (SM cycles, per unit)."""
-    zero, dcyc, dunits, scyc, sunits, sev, spc, srows = [float(x) for x in r]
-    units = dunits + sunits
-    return {"zeroing_cycles_per_unit": zero / units if units else 0.0,
-            "direct": {"units": int(dunits), "cycles_per_unit": dcyc / dunits if dunits else 0.0},
-            "sweep": {"units": int(sunits), "cycles_per_unit": scyc / sunits if sunits else 0.0,
-                      "event_cycles_per_unit": sev / sunits if sunits else 0.0,
-                      "piece_cycles_per_unit": spc / sunits if sunits else 0.0,
-                      "rows_per_unit": srows / sunits if sunits else 0.0}}
+    zero, dcyc, dunits, scyc, sunits, sev, spc, srows, wcyc, wunits, wiv, wmask, wwords, wlost, wrows = \
+        [float(x) for x in r]
+    units = dunits + sunits + wunits
+
+    def per(x, n):
+        return x / n if n else 0.0
+
+    return {"zeroing_cycles_per_unit": per(zero, units),
+            "direct": {"units": int(dunits), "cycles_per_unit": per(dcyc, dunits)},
+            "sweep": {"units": int(sunits), "cycles_per_unit": per(scyc, sunits),
+                      "event_cycles_per_unit": per(sev, sunits), "piece_cycles_per_unit": per(spc, sunits),
+                      "rows_per_unit": per(srows, sunits)},
+            "word_rows": {"units": int(wunits), "cycles_per_unit": per(wcyc, wunits),
+                          "interval_cycles_per_unit": per(wiv, wunits), "mask_cycles_per_unit": per(wmask, wunits),
+                          "word_cycles_per_unit": per(wwords, wunits), "lost_cycles_per_unit": per(wlost, wunits),
+                          "rows_per_unit": per(wrows, wunits)}}
 
 
 def _barrier(world: int) -> None:
@@ -648,6 +660,15 @@ def run_batched(args, rank: int, world: int, local: int) -> dict:
     alg_bytes = n * 624 * 1 + info["region_samples"] * (1 + 1 / 8) + info["units"] * 16
     achieved_gbs = alg_bytes / (audit_ms * 1e-3) / 1e9
     pk = peaks()
+    # The integer-pipe bound of the audit: per launch, 2 ops for each of the 3
+    # edge tests of every (face, bbox sample) pair a per-sample raster makes,
+    # plus 2 ops per region sample (XOR / OR popcounts), over the SMs' INT32
+    # lanes (128 per SM) at the SM clock sampled during the timed steps.
+    int_ops = 2 * 3 * info["face_samples"] + 2 * info["region_samples"]
+    sms = torch.cuda.get_device_properties(device).multi_processor_count
+    sm_mhz = clocks.summary().get("sm_mhz") or 1965.0
+    int_peak = sms * 128 * sm_mhz * 1e6 / 1e12
+    int_achieved = int_ops / (audit_ms * 1e-3) / 1e12
     # End to end through the host C ABI (blitz_audit_batch_candidates_host):
     # pinned host candidates in, host verdicts out, copies inside every step.
     pinned = torch.empty(n * br.COLLAPSE_DTYPE.itemsize, dtype=torch.uint8, pin_memory=True)
@@ -685,7 +706,12 @@ def run_batched(args, rank: int, world: int, local: int) -> dict:
                        "l2": "inputs larger than L2 (about 1.2 GB of state counts and masks per mesh)",
                        "parallelism": f"dp{world} (64 meshes per rank)"},
             "roofline": {"bound": "hbm", "achieved": achieved_gbs, "peak": pk["hbm_gbs"], "unit": "GB/s",
-                         "frac": achieved_gbs / pk["hbm_gbs"], "traffic": None,
+                         "frac": achieved_gbs / pk["hbm_gbs"], "traffic": K_BATCH_TRAFFIC,
+                         "traffic_note": K_BATCH_TRAFFIC_NOTE,
+                         "int32": {"achieved": int_achieved, "peak": int_peak, "unit": "Tops/s",
+                                   "frac": int_achieved / int_peak, "ops_per_launch": int_ops,
+                                   "face_bbox_samples": info["face_samples"],
+                                   "peak_source": f"{sms} SMs x 128 INT32 lanes x {sm_mhz:.0f} MHz (sampled)"},
                          "kernel": "k_audit (+ large and huge tiers)", "kernel_ms": audit_ms,
                          "kernel_ms_counting": info["audit_ms"],
                          "algorithmic_bytes": alg_bytes, "units_per_launch": info["units"],
@@ -738,11 +764,11 @@ ROCK_CHAIN = {"levels": 6, "base": 240.0, "last": 7.5, "curve": ((0.0, 1.0), (1.
 # 32 px (audits at 512 ... 32 px x ss 8), transition 1 px at LOD1 rising to
 # 3 px, LOD0 bound 2 px, 128 search and 128 audit views, uv preserved.
 ROCK_1M_CHAIN = {"levels": 6, "base": 1024.0, "last": 32.0, "curve": ((0.0, 1.0), (1.0, 3.0)), "lod0": 2.0,
-                 "views": 128, "ss": 8, "batch": 64, "budget": 40}
+                 "views": 128, "ss": 8, "batch": 64, "budget": 40, "memory_mib": 160_000}
 # The thin-structure workload: 2,000 ribbon cards (400k faces), 256 views at
 # 512 px, 6-level chain (512 -> 16 px, the same 32:1 ratio).
 RIBBON_CHAIN = {"levels": 6, "base": 512.0, "last": 16.0, "curve": ((0.0, 1.0), (1.0, 3.0)), "lod0": 2.0,
-                "views": 256, "ss": 8, "batch": 64, "budget": 40}
+                "views": 256, "ss": 8, "batch": 64, "budget": 40, "memory_mib": 160_000}
 
 
 def run_chain(args, local: int, mesh, c: dict, preserve_uv: int = 0, label: str = "") -> dict:
@@ -753,7 +779,10 @@ def run_chain(args, local: int, mesh, c: dict, preserve_uv: int = 0, label: str 
 
     import blitzremesher_b200 as br
 
-    session = br.AuditSession(mesh, br.neural_options(device=local, preserve_uv=preserve_uv))
+    # the plans of 128-256 views at 4160 x 4160 samples need more than the
+    # default 6 GiB workspace
+    session = br.AuditSession(mesh, br.neural_options(device=local, preserve_uv=preserve_uv,
+                                                      memory_mib=c.get("memory_mib", 6144)))
     settings = br.chain_settings(c["levels"], c["base"], c["last"], c["curve"], c["lod0"], (c["views"], 0, 0xB1172024),
                                  (c["views"], 0, 0xB1172026), c["ss"], c["ss"], c["ss"], 1.0, c["batch"], 0,
                                  c["budget"], 1)

@@ -353,7 +353,7 @@ class BatchInfo(C.Structure):
                 ("exact_candidates", C.c_uint64), ("audit_ms", C.c_float), ("units", C.c_uint64),
                 ("region_samples", C.c_uint64), ("changed_samples", C.c_uint64),
                 ("tier_units", C.c_uint64 * 4), ("tier_cycles", C.c_uint64 * 4), ("phase_cycles", C.c_uint64 * 3),
-                ("flipped_samples", C.c_uint64), ("region_split", C.c_uint64 * 8)]
+                ("flipped_samples", C.c_uint64), ("region_split", C.c_uint64 * 15), ("face_samples", C.c_uint64)]
 
 
 BATCH_GRAPH, BATCH_AUTOTUNE, BATCH_PROFILE, BATCH_TIMING = 1, 2, 4, 8

@@ -41,7 +41,7 @@ def build(force: bool = False, verbose: bool = False) -> Path:
     obj_dir.mkdir(exist_ok=True)
     for src in SOURCES:
         obj = obj_dir / (Path(src).stem + ".o")
-        cmd = [NVCC, *FLAGS, "-dc" if False else "-c", str(CSRC / src), "-o", str(obj)]
+        cmd = [NVCC, *FLAGS, "-c", str(CSRC / src), "-o", str(obj)]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode:
             sys.stderr.write(r.stdout + r.stderr)

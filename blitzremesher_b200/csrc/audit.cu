@@ -135,26 +135,30 @@ constexpr int kPassRows = 8;
 // interval ends and its two word-mask tables.
 constexpr size_t kGlobalTierWarpSmem = kMaxOk * sizeof(FaceSetup) + kPassRows * kMaxOk * 4 + 2 * kPassRows * 32 * 4;
 
-// Region phase over coverage words (the global tiers), kPassRows rows at a
-// time. Per (row, face) the covered samples are one interval (exact FP64
-// binary searches, face_interval), computed once per pass by the lanes
-// together and kept in `iv` (shared memory). Each interval is then OR-ed
-// into the pass's word masks in shared memory (`masks`): the union of the
-// new faces (B) and of the old faces (A). Because the state's count pc
-// includes every old face (pc >= A), the candidate's count pc - A + B is
-// positive wherever B > 0, and where B = 0 it is pc - A. So a sample flips
-// iff it is newly covered (B on a state-empty sample, from the state's
-// coverage word alone) or it loses its last faces (A without B, and pc
-// equal to the number of old faces covering it: the only samples whose
-// state count is read, and whose old faces are counted from the intervals).
-// Lanes own (row, word) items, up to eight each, whose coverage words are
-// all loaded before any is used. Flipped samples are written to the region
-// words (candidate XOR state) and counted into the popcount deltas against
-// the reference.
+// Region phase over coverage words (every tier but the small one),
+// kPassRows rows at a time. Per (row, face) the covered samples are one
+// interval (exact FP64 searches from the edges' crossings,
+// face_interval_guess), computed once per pass by the lanes together and
+// kept in `iv` (shared memory). Each interval is then OR-ed into the pass's
+// word masks in shared memory (`masks`): the union of the new faces (B) and
+// of the old faces (A). Because the state's count pc includes every old face
+// (pc >= A), the candidate's count pc - A + B is positive wherever B > 0,
+// and where B = 0 it is pc - A. So a sample flips iff it is newly covered (B
+// on a state-empty sample, from the state's coverage word alone) or it loses
+// its last faces (A without B, and pc equal to the number of old faces
+// covering it: the only samples whose state count is read, and whose old
+// faces are counted from the intervals). Lanes own (row, word) items, up to
+// eight each, whose coverage words are all loaded before any is used.
+// Flipped samples are written to the region words (candidate XOR state) and
+// counted into the popcount deltas against the reference. `clk` (profiling
+// only) accumulates SM cycles of the interval, mask and word steps and of
+// the lane's lost-sample counts.
 __device__ void region_word_rows(const FaceSetup* faces, uint32_t nok, int wx0, int ry0, int ry1, int words,
                                  const PlanView& pv, uint32_t size, bool same_ref, uint32_t* region, short2* iv,
-                                 uint32_t* masks, int& dchg, int& dtot, int& dcov, int& flips, bool& negative) {
+                                 uint32_t* masks, int& dchg, int& dtot, int& dcov, int& flips, bool& negative,
+                                 long long* clk) {
     const uint32_t lane = lane_id();
+    long long t0 = clk ? clock64() : 0;
     uint32_t* const bn = masks;                  // [kPassRows][32] new-face union
     uint32_t* const an = masks + kPassRows * 32; // [kPassRows][32] old-face union
     for (int ybase = ry0; ybase <= ry1; ybase += kPassRows) {
@@ -165,8 +169,12 @@ __device__ void region_word_rows(const FaceSetup* faces, uint32_t nok, int wx0, 
             const int y = ybase + int(r);
             const FaceSetup& fs = faces[f];
             int lo = 1, hi = 0;
-            if (y >= fs.y0 && y <= fs.y1) face_interval(fs, double(y) + .5, lo, hi);
+            if (y >= fs.y0 && y <= fs.y1) face_interval_guess(fs, double(y) + .5, lo, hi);
             iv[r * kMaxOk + f] = make_short2(short(lo), short(hi));
+        }
+        if (clk) {
+            const long long t = clock64();
+            clk[0] += t - t0, t0 = t;
         }
         for (int c0 = 0; c0 < words; c0 += 32) { // 32-word windows of wide regions
             const uint32_t cn = uint32_t(min(32, words - c0));
@@ -186,6 +194,10 @@ __device__ void region_word_rows(const FaceSetup* faces, uint32_t nok, int wx0, 
                 }
             }
             __syncwarp();
+            if (clk) {
+                const long long t = clock64();
+                clk[1] += t - t0, t0 = t;
+            }
             const uint32_t cells = pass_rows * cn;
             uint32_t S[8], R[8];
 #pragma unroll
@@ -218,6 +230,7 @@ __device__ void region_word_rows(const FaceSetup* faces, uint32_t nok, int wx0, 
                 negative |= (lost_cand & ~S[k]) != 0;  // pc >= A > 0 must hold
                 lost_cand &= S[k];
                 uint32_t lost = 0;
+                const long long l0 = clk && lost_cand ? clock64() : 0;
                 while (lost_cand) {
                     const int i = __ffs(lost_cand) - 1;
                     lost_cand &= lost_cand - 1;
@@ -231,6 +244,7 @@ __device__ void region_word_rows(const FaceSetup* faces, uint32_t nok, int wx0, 
                     negative |= pc < A;
                     if (pc == A) lost |= 1u << i;
                 }
+                if (l0) clk[3] += clock64() - l0;
                 const uint32_t fl = grown | lost;
                 *out = fl;
                 if (!fl) continue;
@@ -241,6 +255,10 @@ __device__ void region_word_rows(const FaceSetup* faces, uint32_t nok, int wx0, 
                 dtot += __popc(fl & ~R[k] & ~S[k]) - __popc(fl & ~R[k] & S[k]);
             }
             __syncwarp();
+            if (clk) {
+                const long long t = clock64();
+                clk[2] += t - t0, t0 = t;
+            }
         }
     }
 }
@@ -366,6 +384,7 @@ __device__ void audit_unit(const CandidateRecord* __restrict__ rec, const PlanDe
     // the sweep's per-lane event and piece cycles, max over lanes)
     long long st_zero = 0, st_path = 0, st_events = 0, st_pieces = 0;
     int st_kind = -1, st_rows = 0;
+    long long st_words = 0, st_lost = 0;
     int dchg = 0, dtot = 0, dcov = 0;
     uint32_t qn = 0, region_changed = 0, nflips = 0;
     int region_words = 0;
@@ -374,7 +393,7 @@ __device__ void audit_unit(const CandidateRecord* __restrict__ rec, const PlanDe
     cmask.state = pv.state_bits;
     cmask.region = ws.region;
     cmask.size = size;
-    uint64_t samples = 0;
+    uint64_t samples = 0, face_samples = 0;
     // The processed region: the changed faces' bbox widened to whole coverage
     // words; when the state differs from the reference, widened to whole
     // 32x32 tiles so every tile is either fully processed or fully outside.
@@ -395,6 +414,7 @@ __device__ void audit_unit(const CandidateRecord* __restrict__ rec, const PlanDe
             area += uint32_t(faces[lane + 32].x1 - faces[lane + 32].x0 + 1) *
                     uint32_t(faces[lane + 32].y1 - faces[lane + 32].y0 + 1);
         for (int o = 16; o; o >>= 1) area += __shfl_xor_sync(0xffffffffu, area, o);
+        face_samples = area;
         // The small tier (regions of at most 128 x 64 samples) always tests
         // every sample; a unit whose delta map does not fit goes on to the
         // next tier.
@@ -416,6 +436,7 @@ __device__ void audit_unit(const CandidateRecord* __restrict__ rec, const PlanDe
             __syncwarp();
             const long long t_zero = stats ? clock64() : 0;
             long long c_events = 0, c_pieces = 0;
+            long long wr_clk[4] = {0, 0, 0, 0}; // word rows: intervals, masks, words, lost samples
             bool negative = false;
             int flips = 0;
             // A sample whose count changes by dv (state count pc): it flips
@@ -445,7 +466,7 @@ __device__ void audit_unit(const CandidateRecord* __restrict__ rec, const PlanDe
             };
             if constexpr (word_rows) {
                 region_word_rows(faces, nok, wx0, ry0, ry1, words, pv, size, same_ref, ws.region, iv_rows, mask_rows,
-                                 dchg, dtot, dcov, flips, negative);
+                                 dchg, dtot, dcov, flips, negative, stats ? wr_clk : nullptr);
             } else if (direct) {
                 const uint32_t delta_words = uint32_t(bws * bh) >> 2;
                 for (uint32_t k = lane; k < delta_words; k += 32) ws.delta[k] = 0x80808080u;
@@ -572,8 +593,12 @@ __device__ void audit_unit(const CandidateRecord* __restrict__ rec, const PlanDe
             if (stats) {
                 st_zero = t_zero - t_setup;
                 st_path = clock64() - t_zero;
-                st_kind = direct && !word_rows ? 0 : 1;
+                st_kind = word_rows ? 2 : direct ? 0 : 1;
                 st_rows = bh;
+            }
+            if (stats && word_rows) {
+                for (int o = 16; o; o >>= 1) wr_clk[3] = max(wr_clk[3], __shfl_xor_sync(0xffffffffu, wr_clk[3], o));
+                c_events = wr_clk[0], c_pieces = wr_clk[1], st_words = wr_clk[2], st_lost = wr_clk[3];
             }
             if (__any_sync(0xffffffffu, negative)) fallback = true;
             for (int o = 16; o; o >>= 1) {
@@ -779,7 +804,10 @@ __device__ void audit_unit(const CandidateRecord* __restrict__ rec, const PlanDe
             // searched samples; per tier units and SM cycles; SM cycles of the
             // face setup, the region phases and the distance phase; flips;
             // region sub-phases (zeroing; direct path cycles and units; row
-            // sweep cycles and units, its event and piece cycles, rows)
+            // sweep cycles and units, its event and piece cycles, rows; word
+            // rows cycles and units, their interval, mask, word and
+            // lost-sample cycles, rows); samples of the faces' bboxes (the
+            // (face, sample) pairs a per-sample raster tests)
             const long long t_end = clock64();
             constexpr int tier = L::kRegionRows <= 128 ? 0 : L::kRegionRows <= 256 ? 1 : L::kRegionRows <= 1024 ? 2 : 3;
             atomicAdd(stats, 1ull);
@@ -801,7 +829,16 @@ __device__ void audit_unit(const CandidateRecord* __restrict__ rec, const PlanDe
                 atomicAdd(stats + 20, (unsigned long long)st_events);
                 atomicAdd(stats + 21, (unsigned long long)st_pieces);
                 atomicAdd(stats + 22, (unsigned long long)st_rows);
+            } else if (st_kind == 2) {
+                atomicAdd(stats + 23, (unsigned long long)st_path);
+                atomicAdd(stats + 24, 1ull);
+                atomicAdd(stats + 25, (unsigned long long)st_events);
+                atomicAdd(stats + 26, (unsigned long long)st_pieces);
+                atomicAdd(stats + 27, (unsigned long long)st_words);
+                atomicAdd(stats + 28, (unsigned long long)st_lost);
+                atomicAdd(stats + 29, (unsigned long long)st_rows);
             }
+            atomicAdd(stats + 30, (unsigned long long)face_samples);
         }
     }
     __syncwarp();

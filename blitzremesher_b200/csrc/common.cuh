@@ -169,6 +169,75 @@ BH void face_interval(const FaceSetup& s, double py, int& lo, int& hi) {
     }
 }
 
+// The same interval from a computed guess: per edge of face_covers the
+// covered samples of a row are a prefix (c >= 0: up to the last covered x,
+// x0 - 1 when none) or a suffix (c < 0: from the first covered x, x1 + 1
+// when none) of the face's bbox columns. The edge's crossing
+// x* = (t1 + r) / c + ax - 1/2 is within a rounding of that boundary, so an
+// exponential search from floor / ceil(x*) brackets it in one or two tests
+// and a binary search over the same FP64 edge expressions settles it
+// exactly: [max of suffix starts, min of prefix ends] equals face_interval's
+// interval (lo > hi: none) whatever the guess.
+BH void face_interval_guess(const FaceSetup& s, double py, int& lo, int& hi) {
+    const double ax3[3] = {s.dx, s.ex, s.ax}, ay3[3] = {s.dy, s.ey, s.ay};
+    const double bx3[3] = {s.ex, s.ax, s.dx}, by3[3] = {s.ey, s.ay, s.dy};
+    const double r3[3] = {s.r0, s.r1, s.r2};
+    lo = s.x0, hi = s.x1;
+#pragma unroll
+    for (int e = 0; e < 3; ++e) {
+        const double ax = ax3[e], ay = ay3[e], r = r3[e];
+        const double t1 = (bx3[e] - ax) * (py - ay), c = by3[e] - ay;
+        const bool prefix = c >= 0; // c == 0: every column or none
+        // One column's test, the out-of-range columns as sentinels: left of
+        // the bbox a prefix is covered and a suffix is not, right of it the
+        // other way round.
+        auto ok = [&](int x) {
+            if (x < s.x0) return prefix;
+            if (x > s.x1) return !prefix;
+            return !((t1 - c * ((double(x) + .5) - ax)) + r < 0);
+        };
+        int g = s.x0;
+        if (c != 0) {
+            double xs = (t1 + r) / c + ax - .5; // NaN or out of range: clamped
+            xs = xs > double(s.x0 - 1) ? xs : double(s.x0 - 1);
+            xs = xs < double(s.x1 + 1) ? xs : double(s.x1 + 1);
+            g = prefix ? int(floor(xs)) : int(ceil(xs));
+        }
+        // Bracket [a, b] with ok(a) == prefix and ok(b) != prefix, then bisect.
+        int a, b;
+        if (ok(g) == prefix) {
+            a = g;
+            for (int step = 1;; step *= 2) {
+                b = a + step;
+                if (b >= s.x1 + 1) {
+                    b = s.x1 + 1;
+                    break;
+                }
+                if (ok(b) != prefix) break;
+                a = b;
+            }
+        } else {
+            b = g;
+            for (int step = 1;; step *= 2) {
+                a = b - step;
+                if (a <= s.x0 - 1) {
+                    a = s.x0 - 1;
+                    break;
+                }
+                if (ok(a) == prefix) break;
+                b = a;
+            }
+        }
+        while (b - a > 1) {
+            const int m = a + (b - a) / 2;
+            if (ok(m) == prefix) a = m;
+            else b = m;
+        }
+        if (prefix) hi = a < hi ? a : hi; // last covered
+        else lo = b > lo ? b : lo;        // first covered
+    }
+}
+
 // CPU float value of the field where the exact distance reaches 2^24: the
 // row pass rounds g^2 to float, the column pass rounds (dy^2 + f) to float;
 // the lower envelope of the reference picks the smallest such value. `g`:

@@ -52,7 +52,7 @@ struct UvSource {
 };
 
 // Slots of the audit kernels' profiling counters (launch_audit `stats`).
-constexpr int kAuditStats = 24;
+constexpr int kAuditStats = 31;
 
 constexpr int kMaxAffected = 32; // faces in faces(from) U faces(to) handled on the fast path
 constexpr int kMaxLocal = 31;    // distinct vertex slots of those faces; local index 31 = placement

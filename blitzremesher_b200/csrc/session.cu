@@ -9,6 +9,7 @@
 #include "surrogate.cuh"
 
 #include <algorithm>
+#include <type_traits>
 #include <chrono>
 #include <cstdio>
 #include <map>
@@ -94,7 +95,7 @@ template <class T> struct Buf {
 // ---------------------------------------------------------------------------
 // Host mesh copied out of a borrowed blitz_mesh (streams may be strided).
 struct HostMesh {
-    std::vector<float> pos, normals, uv;
+    std::vector<float> pos, normals, uv, tangents;
     std::vector<uint8_t> colors;
     std::vector<uint32_t> idx;
     std::vector<uint16_t> mat;
@@ -125,6 +126,7 @@ static HostMesh import_mesh(const blitz_mesh* m) {
     copy_stream<float>(m->normals, n, 3, h.normals, "normal");
     copy_stream<float>(m->uv, n, 2, h.uv, "uv");
     copy_stream<uint8_t>(m->colors, n, 4, h.colors, "color");
+    copy_stream<float>(m->tangents, n, 4, h.tangents, "tangent");
     h.idx.assign(m->indices, m->indices + m->index_count);
     size_t nf = m->index_count / 3;
     if (m->material_count) {
@@ -145,6 +147,40 @@ static HostMesh import_mesh(const blitz_mesh* m) {
     for (float f : h.uv)
         if (!std::isfinite(f)) throw Failure(BLITZ_INVALID_ARGUMENT, "nonfinite UV");
     return h;
+}
+
+// Attribute classes of the GPU state (action_gpu.cu:57-60 same_attributes,
+// 178-211 insert/lookup_vertices with attributes): slots with bitwise equal
+// positions, normals and colours, and with `with_uv` also uv and tangents,
+// share a class named by its smallest slot.
+static std::vector<uint32_t> attribute_roots(const HostMesh& h, bool with_uv) {
+    const uint32_t n = h.nv();
+    auto key = [&](uint32_t i) {
+        std::vector<uint32_t> k;
+        auto add = [&](const auto& v, size_t comps) {
+            if (v.empty()) return;
+            using T = typename std::decay_t<decltype(v)>::value_type;
+            for (size_t c = 0; c < comps; ++c) {
+                uint32_t b = 0;
+                std::memcpy(&b, &v[i * comps + c], sizeof(T));
+                k.push_back(b);
+            }
+        };
+        add(h.pos, 3);
+        add(h.normals, 3);
+        add(h.colors, 4);
+        if (with_uv) add(h.uv, 2), add(h.tangents, 4);
+        return k;
+    };
+    std::vector<std::vector<uint32_t>> keys(n);
+    for (uint32_t i = 0; i < n; ++i) keys[i] = key(i);
+    std::vector<uint32_t> order(n), root(n);
+    for (uint32_t i = 0; i < n; ++i) order[i] = i;
+    std::sort(order.begin(), order.end(),
+              [&](uint32_t a, uint32_t b) { return keys[a] != keys[b] ? keys[a] < keys[b] : a < b; });
+    for (uint32_t k = 0; k < n; ++k)
+        root[order[k]] = k && keys[order[k]] == keys[order[k - 1]] ? root[order[k - 1]] : order[k];
+    return root;
 }
 
 struct Bounds {
@@ -497,19 +533,16 @@ static void init_topology(Session& S) {
     t.flat = Buf<uint32_t>(P, 1);
     t.pos_cap = pow2_at_least(4ull * n);
     t.positions = Buf<uint32_t>(P, t.pos_cap);
-    const uint32_t* canonical = t.geometry.p;
+    // Attribute classes (action_gpu.cu:1518-1525), with uv and tangents only
+    // under preserve_uv (without it the indices were welded to these classes
+    // at creation); then each class's source faces in ascending order for
+    // place_vertices.
+    const std::vector<uint32_t> cls = attribute_roots(S.source_h, S.options.preserve_uv != 0);
+    t.canonical = Buf<uint32_t>(P, n);
+    B200_CUDA(cudaMemcpyAsync(t.canonical.p, cls.data(), size_t(n) * 4, cudaMemcpyHostToDevice, S.stream));
+    const uint32_t* canonical = t.canonical.p;
     if (m.uv) {
-        // Attribute charts (action_gpu.cu:1520-1525): with preserve_uv the
-        // position + uv weld, else the geometric classes; then each class's
-        // source faces in ascending order for place_vertices.
-        if (S.options.preserve_uv) {
-            t.canonical = Buf<uint32_t>(P, n);
-            launch_weld(m, t.table.p, t.table_cap, true, t.canonical.p, S.stream);
-            canonical = t.canonical.p;
-        }
-        std::vector<uint32_t> cls(n), offsets(size_t(n) + 1, 0), faces;
-        B200_CUDA(cudaMemcpyAsync(cls.data(), canonical, size_t(n) * 4, cudaMemcpyDeviceToHost, S.stream));
-        B200_CUDA(cudaStreamSynchronize(S.stream));
+        std::vector<uint32_t> offsets(size_t(n) + 1, 0), faces;
         const std::vector<uint32_t>& idx = S.source_h.idx;
         auto corners = [&](uint32_t f, uint32_t* c) {
             for (int j = 0; j < 3; ++j) c[j] = cls[idx[3 * f + j]];
@@ -1822,6 +1855,14 @@ blitz_status blitz_audit_session_create(const blitz_mesh* source, const blitz_ne
         Bounds b = bounds_of(h);
         if (!(b.radius > 0) || !std::isfinite(b.radius))
             throw Failure(BLITZ_INVALID_ARGUMENT, "zero or invalid source extent");
+        if (!o.preserve_uv) {
+            // Without preserve_uv the GPU state welds every corner to its
+            // attribute class ignoring uv and tangents (action_gpu.cu:1527-1532
+            // weld_uv_indices), so uv seams are no wedges; the welded indices
+            // are the session's source and state (the same triangles).
+            const std::vector<uint32_t> root = attribute_roots(h, false);
+            for (uint32_t& i : h.idx) i = root[i];
+        }
         auto session = std::make_unique<blitz_audit_session>();
         Session& S = session->s;
         S.device = o.device;
@@ -2693,7 +2734,8 @@ blitz_status blitz_audit_batch_read_info(const blitz_audit_batch* b, blitz_audit
     for (int k = 0; k < 4; ++k) out->tier_units[k] = b->prof[3 + k], out->tier_cycles[k] = b->prof[7 + k];
     for (int k = 0; k < 3; ++k) out->phase_cycles[k] = b->prof[11 + k];
     out->flipped_samples = b->prof[14];
-    for (int k = 0; k < 8; ++k) out->region_split[k] = b->prof[15 + k];
+    for (int k = 0; k < 15; ++k) out->region_split[k] = b->prof[15 + k];
+    out->face_samples = b->prof[30];
     return BLITZ_OK;
 }
 

@@ -507,8 +507,13 @@ typedef struct blitz_audit_batch_info {
     /* region phases split: SM cycles zeroing the region words; direct-test
      * path cycles and units; row-sweep path cycles and units; the sweep's
      * cycles building sorted interval ends and visiting pieces (each the max
-     * over a warp's lanes); rows swept */
-    uint64_t region_split[8];
+     * over a warp's lanes); rows swept; word-row path cycles and units, its
+     * cycles computing intervals, OR-ing word masks, testing words and (the
+     * max over a warp's lanes) counting old faces of losing samples; rows */
+    uint64_t region_split[15];
+    /* the same call: samples of the rasterized faces' bounding boxes summed
+     * over units (the (face, sample) pairs a per-sample raster would test) */
+    uint64_t face_samples;
 } blitz_audit_batch_info;
 blitz_status blitz_audit_batch_create(blitz_audit_session* const* sessions, size_t count, blitz_audit_batch** out,
                                       char* error, size_t error_capacity);

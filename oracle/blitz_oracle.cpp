@@ -501,6 +501,32 @@ Topology build_topology(const bo_mesh& m, bool preserve_uv, const Topology* clas
     return t;
 }
 
+// Without preserve_uv the reference's GPU state welds every corner to its
+// attribute class ignoring uv (action_gpu.cu:1518-1532: insert/lookup_vertices
+// with attributes, then weld_uv_indices), so uv seams stop being wedges. This
+// mesh record has no normals or colours, so the class is the bitwise position
+// class. `welded.m` views `*m` with the welded indices.
+struct UvWelded {
+    std::vector<uint32_t> indices;
+    bo_mesh m;
+};
+UvWelded weld_uv_indices(const bo_mesh& m) {
+    UvWelded w;
+    const std::vector<uint32_t> root = weld(m, false);
+    w.indices.resize(size_t(m.face_count) * 3);
+    for (size_t i = 0; i < w.indices.size(); ++i) w.indices[i] = root[m.indices[i]];
+    w.m = m;
+    w.m.indices = w.indices.data();
+    return w;
+}
+// The mesh the GPU state works on for `preserve_uv`: `m` itself, or its
+// uv-welded copy held in `hold`.
+const bo_mesh& state_mesh(const bo_mesh& m, bool preserve_uv, UvWelded& hold) {
+    if (preserve_uv) return m;
+    hold = weld_uv_indices(m);
+    return hold.m;
+}
+
 bool has_neighbor(const Topology& t, uint32_t u, uint32_t v) {
     return std::binary_search(t.neighbors.begin() + t.offsets[u], t.neighbors.begin() + t.offsets[u + 1], v);
 }
@@ -1104,8 +1130,10 @@ int bo_schedule(double first, double last, uint32_t levels, const float* curve_x
 int64_t bo_actions(const bo_mesh* m, int placement, int preserve_uv, bo_edit* out, uint64_t capacity) {
     int64_t count = -1;
     int status = guarded([&] {
-        auto t = build_topology(*m, preserve_uv != 0);
-        auto edits = enumerate(*m, t, placement != 0, preserve_uv != 0);
+        UvWelded hold;
+        const bo_mesh& sm = state_mesh(*m, preserve_uv != 0, hold);
+        auto t = build_topology(sm, preserve_uv != 0);
+        auto edits = enumerate(sm, t, placement != 0, preserve_uv != 0);
         for (size_t i = 0; i < edits.size() && i < capacity; ++i) out[i] = edits[i];
         count = int64_t(edits.size());
     });
@@ -1125,13 +1153,15 @@ int64_t bo_trial_midpoint(const bo_mesh* m, const bo_edit* e, int preserve_uv, u
                           float* positions, float* uv, uint8_t* valid) {
     int64_t faces = -1;
     int status = guarded([&] {
-        auto t = build_topology(*m, preserve_uv != 0);
+        UvWelded hold;
+        const bo_mesh& sm = state_mesh(*m, preserve_uv != 0, hold);
+        auto t = build_topology(sm, preserve_uv != 0);
         bo_edit edit{};
         edit.from = e->from, edit.to = e->to;
-        if (edit.from >= m->vertex_count || edit.to >= m->vertex_count || edit.from == edit.to ||
-            !has_neighbor(t, edit.from, edit.to) || !legal(*m, t, edit, true, preserve_uv != 0))
+        if (edit.from >= sm.vertex_count || edit.to >= sm.vertex_count || edit.from == edit.to ||
+            !has_neighbor(t, edit.from, edit.to) || !legal(sm, t, edit, true, preserve_uv != 0))
             throw std::invalid_argument("illegal collapse");
-        Trial tr = make_trial(*m, t, *m, t, edit, preserve_uv != 0);
+        Trial tr = make_trial(sm, t, sm, t, edit, preserve_uv != 0);
         std::copy(tr.indices.begin(), tr.indices.end(), indices);
         std::copy(tr.positions.begin(), tr.positions.end(), positions);
         if (uv && m->uv) std::copy(tr.uv.begin(), tr.uv.end(), uv);
@@ -1216,6 +1246,14 @@ int execute_walk(const bo_mesh* source, const bo_mesh* previous, const bo_mesh* 
         const bo_mesh& from = start ? *start : *source;
         st.pos.assign(from.positions, from.positions + size_t(from.vertex_count) * 3);
         st.idx.assign(from.indices, from.indices + size_t(from.face_count) * 3);
+        // The state's classes and uv-transport source: the source, uv-welded
+        // without preserve_uv like the state itself (once, at construction).
+        UvWelded hold;
+        const bo_mesh& welded_source = endpoint ? *source : state_mesh(*source, preserve_uv != 0, hold);
+        if (!endpoint && !preserve_uv) {
+            const std::vector<uint32_t> root = weld(*source, false);
+            for (uint32_t& i : st.idx) i = root[i];
+        }
         if (from.materials) st.mat.assign(from.materials, from.materials + from.face_count);
         if (source->double_sided) st.sided.assign(source->double_sided, source->double_sided + source->double_sided_count);
         if (from.uv) st.uv.assign(from.uv, from.uv + size_t(from.vertex_count) * 2);
@@ -1223,8 +1261,8 @@ int execute_walk(const bo_mesh* source, const bo_mesh* previous, const bo_mesh* 
         bo_bounds_of(source, &b);
         const double diameter = std::max(1e-20, b.radius * 2);
         const bo_mesh& prev = previous ? *previous : *source;
-        const Topology classes = build_topology(*source, preserve_uv != 0);
-        const bo_mesh original = *source;
+        const Topology classes = build_topology(welded_source, preserve_uv != 0);
+        const bo_mesh original = welded_source;
         target = std::max<uint32_t>(1, target);
         uint32_t n_commits = 0, n_trials = 0;
         uint8_t reason = 3;
@@ -1324,6 +1362,8 @@ int bo_audit_candidate(const bo_mesh* parent, const bo_edit* e, const bo_mesh* s
                        int preserve_uv, bo_verdict* out) {
     return guarded([&] {
         *out = bo_verdict{};
+        UvWelded hold;
+        parent = &state_mesh(*parent, preserve_uv != 0, hold);
         auto t = build_topology(*parent, preserve_uv != 0);
         // The edit's wedges come from legality (action_gpu.cu:487-643), as in
         // the reference executor; only from/to are taken from the caller.

@@ -4,7 +4,8 @@ Measurements for a fixed sample of the batched workload's candidates.
 Workload: the 64 seeded meshes of `synthetic.batched_set(64, seed=2)` (noisy
 spheres, R/r = 3 tori, value-noise heightfields; FP32 UVs with chart seams),
 audited at 512 px x ss 8 (4160 x 4160 samples per view) with a 2 px LOD0 and
-a 1 px transition limit, midpoint placement, uv not preserved. Sample: the
+a 1 px transition limit, midpoint placement, uv not preserved (so uv seams
+are welded, as the reference's GPU state does without preserve_uv). Sample: the
 smallest mesh, the median one and the three largest (sphere, torus and
 heightfield among them); per mesh 4 of the 64 evenly spaced legal collapses
 the benchmark audits (positions 0, 21, 42 and 63 of its list), on the first

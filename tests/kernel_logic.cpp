@@ -53,6 +53,12 @@ int main() {
         Proj p[3];
         for (auto& q : p) q = Proj{cx + uni(-span, span), cy + uni(-span, span), 1.0};
         if (t % 7 == 0) p[2] = Proj{p[0].x + (p[1].x - p[0].x) * 0.5, p[0].y + (p[1].y - p[0].y) * 0.5 + 1e-7, 1.0};
+        // edges through sample centres (ties of the edge test), horizontal and
+        // vertical edges
+        if (t % 11 == 1)
+            for (auto& q : p) q.x = std::floor(q.x) + .5, q.y = std::floor(q.y) + .5;
+        if (t % 13 == 2) p[1].y = p[0].y;
+        if (t % 17 == 3) p[2].x = p[1].x;
         const FaceSetup s = setup_face(p[0], p[1], p[2], false, t % 2 == 0, size);
         if (s.status != kFaceOk) continue;
         const int step = s.y1 - s.y0 > 400 ? 37 : 1;
@@ -61,6 +67,12 @@ int main() {
             face_interval(s, double(y) + .5, lo, hi);
             bool ok = true;
             for (int x = s.x0; x <= s.x1 && ok; ++x) ok = face_covers(s, x, y) == (x >= lo && x <= hi);
+            // the interval searched from the edges' computed crossings is the
+            // same set
+            int glo, ghi;
+            face_interval_guess(s, double(y) + .5, glo, ghi);
+            const bool empty = lo > hi, gempty = glo > ghi;
+            ok = ok && empty == gempty && (empty || (glo == lo && ghi == hi));
             ++rows;
             bad_rows += !ok;
         }
