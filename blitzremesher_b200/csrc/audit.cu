@@ -133,13 +133,18 @@ __device__ __forceinline__ void record_write(ViewRecord* out, const ViewRecord& 
 constexpr int kPassRows = 8;
 // Shared memory of one warp of the global tiers: face setups, the pass's
 // interval ends and its two word-mask tables.
-constexpr size_t kGlobalTierWarpSmem = kMaxOk * sizeof(FaceSetup) + kPassRows * kMaxOk * 4 + 2 * kPassRows * 32 * 4;
+// The two word-mask tables of a pass are followed by the per-face item
+// prefixes (kMaxOk u16) of region_word_rows.
+constexpr size_t kPassMaskBytes = 2 * kPassRows * 32 * 4 + kMaxOk * 2;
+constexpr size_t kGlobalTierWarpSmem = kMaxOk * sizeof(FaceSetup) + kPassRows * kMaxOk * 4 + kPassMaskBytes;
 
 // Region phase over coverage words (every tier but the small one),
 // kPassRows rows at a time. Per (row, face) the covered samples are one
-// interval (exact FP64 searches from the edges' crossings,
-// face_interval_guess), computed once per pass by the lanes together and
-// kept in `iv` (shared memory). Each interval is then OR-ed into the pass's
+// interval (exact FP64 searches from the edges' guessed crossings,
+// face_interval_guess). A pass computes them for the (row, face) pairs whose
+// row the face spans, spread evenly over the lanes (per-face prefixes of
+// those pairs in `masks`' tail), and keeps them in `iv` (shared memory;
+// empty for the other pairs). Each interval is then OR-ed into the pass's
 // word masks in shared memory (`masks`): the union of the new faces (B) and
 // of the old faces (A). Because the state's count pc includes every old face
 // (pc >= A), the candidate's count pc - A + B is positive wherever B > 0,
@@ -161,17 +166,49 @@ __device__ void region_word_rows(const FaceSetup* faces, uint32_t nok, int wx0, 
     long long t0 = clk ? clock64() : 0;
     uint32_t* const bn = masks;                  // [kPassRows][32] new-face union
     uint32_t* const an = masks + kPassRows * 32; // [kPassRows][32] old-face union
+    uint16_t* const first = reinterpret_cast<uint16_t*>(masks + 2 * kPassRows * 32); // [kMaxOk]
     for (int ybase = ry0; ybase <= ry1; ybase += kPassRows) {
-        const uint32_t pass_rows = min(uint32_t(kPassRows), uint32_t(ry1 - ybase + 1));
-        const uint32_t items = pass_rows * nok;
+        const int ylast = min(ry1, ybase + kPassRows - 1);
+        const uint32_t pass_rows = uint32_t(ylast - ybase + 1);
+        // Rows of the pass that faces lane and lane + 32 span; their
+        // exclusive prefix over faces numbers the pass's (row, face) items.
+        auto first_row = [&](uint32_t f) { return max(faces[f].y0, ybase); };
+        auto span = [&](uint32_t f) {
+            const int lo = first_row(f), hi = min(faces[f].y1, ylast);
+            return lo <= hi ? uint32_t(hi - lo + 1) : 0u;
+        };
+        const uint32_t n0 = lane < nok ? span(lane) : 0u, n1 = lane + 32 < nok ? span(lane + 32) : 0u;
+        uint32_t s0 = n0, s1 = n1;
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t a = __shfl_up_sync(0xffffffffu, s0, o), b = __shfl_up_sync(0xffffffffu, s1, o);
+            if (lane >= uint32_t(o)) s0 += a, s1 += b;
+        }
+        const uint32_t tot0 = __shfl_sync(0xffffffffu, s0, 31);
+        const uint32_t items = tot0 + __shfl_sync(0xffffffffu, s1, 31);
+        for (uint32_t f = lane; f < nok; f += 32) {
+            first[f] = uint16_t(f < 32 ? s0 - n0 : tot0 + s1 - n1);
+            for (uint32_t r = 0; r < pass_rows; ++r) iv[r * kMaxOk + f] = make_short2(1, 0);
+        }
+        __syncwarp();
+        // Item t -> its face (the last with first <= t) and row.
+        auto item = [&](uint32_t t, uint32_t& f, uint32_t& r) {
+            uint32_t lo = 0, hi = nok - 1;
+            while (lo < hi) {
+                const uint32_t mid = (lo + hi + 1) >> 1;
+                if (first[mid] <= t) lo = mid;
+                else hi = mid - 1;
+            }
+            f = lo;
+            r = uint32_t(first_row(lo) - ybase) + (t - first[lo]);
+        };
         for (uint32_t t = lane; t < items; t += 32) {
-            const uint32_t r = t / nok, f = t - r * nok;
-            const int y = ybase + int(r);
-            const FaceSetup& fs = faces[f];
-            int lo = 1, hi = 0;
-            if (y >= fs.y0 && y <= fs.y1) face_interval_guess(fs, double(y) + .5, lo, hi);
+            uint32_t f, r;
+            item(t, f, r);
+            int lo, hi;
+            face_interval_guess(faces[f], double(ybase + int(r)) + .5, lo, hi);
             iv[r * kMaxOk + f] = make_short2(short(lo), short(hi));
         }
+        __syncwarp();
         if (clk) {
             const long long t = clock64();
             clk[0] += t - t0, t0 = t;
@@ -182,7 +219,8 @@ __device__ void region_word_rows(const FaceSetup* faces, uint32_t nok, int wx0, 
             for (uint32_t k = lane; k < 2 * kPassRows * 32; k += 32) masks[k] = 0;
             __syncwarp();
             for (uint32_t t = lane; t < items; t += 32) {
-                const uint32_t r = t / nok, f = t - r * nok;
+                uint32_t f, r;
+                item(t, f, r);
                 const short2 e = iv[r * kMaxOk + f];
                 const int lo = max(int(e.x), xc0), hi = min(int(e.y), xc1);
                 if (lo > hi) continue;
@@ -278,7 +316,7 @@ __device__ void audit_unit(const CandidateRecord* __restrict__ rec, const PlanDe
     // memory: given by the global tiers, else the delta map's space) and the
     // distance phase walks the region words.
     constexpr bool word_rows = L::kWordRows;
-    static_assert(!L::kWordRows || L::kDeltaSamples * sizeof(uint8_t) >= kPassRows * kMaxOk * 4 + 2 * kPassRows * 32 * 4,
+    static_assert(!L::kWordRows || L::kDeltaSamples * sizeof(uint8_t) >= kPassRows * kMaxOk * 4 + kPassMaskBytes,
                   "the delta map's space holds the word-row tables");
     short2* const iv_rows = iv_table ? iv_table : reinterpret_cast<short2*>(ws.delta);
     uint32_t* const mask_rows = mask_table ? mask_table : ws.delta + kPassRows * kMaxOk;

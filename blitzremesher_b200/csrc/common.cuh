@@ -169,16 +169,15 @@ BH void face_interval(const FaceSetup& s, double py, int& lo, int& hi) {
     }
 }
 
-// The same interval from a computed guess: per edge of face_covers the
-// covered samples of a row are a prefix (c >= 0: up to the last covered x,
-// x0 - 1 when none) or a suffix (c < 0: from the first covered x, x1 + 1
-// when none) of the face's bbox columns. The edge's crossing
-// x* = (t1 + r) / c + ax - 1/2 is within a rounding of that boundary, so an
-// exponential search from floor / ceil(x*) brackets it in one or two tests
-// and a binary search over the same FP64 edge expressions settles it
-// exactly: [max of suffix starts, min of prefix ends] equals face_interval's
-// interval (lo > hi: none) whatever the guess.
-BH void face_interval_guess(const FaceSetup& s, double py, int& lo, int& hi) {
+// The same interval from guessed edge boundaries: per edge of face_covers
+// the covered samples of a row are a prefix (c >= 0: up to the last covered
+// x, x0 - 1 when none) or a suffix (c < 0: from the first covered x, x1 + 1
+// when none) of the face's bbox columns. From any guess, an exponential
+// search brackets the boundary and a binary search over the same FP64 edge
+// expressions settles it exactly, so [max of suffix starts, min of prefix
+// ends] equals face_interval's interval (lo > hi: none) whatever `guess`
+// holds; a good guess takes one or two tests per edge.
+BH void face_interval_at(const FaceSetup& s, double py, const int guess[3], int& lo, int& hi) {
     const double ax3[3] = {s.dx, s.ex, s.ax}, ay3[3] = {s.dy, s.ey, s.ay};
     const double bx3[3] = {s.ex, s.ax, s.dx}, by3[3] = {s.ey, s.ay, s.dy};
     const double r3[3] = {s.r0, s.r1, s.r2};
@@ -196,13 +195,7 @@ BH void face_interval_guess(const FaceSetup& s, double py, int& lo, int& hi) {
             if (x > s.x1) return !prefix;
             return !((t1 - c * ((double(x) + .5) - ax)) + r < 0);
         };
-        int g = s.x0;
-        if (c != 0) {
-            double xs = (t1 + r) / c + ax - .5; // NaN or out of range: clamped
-            xs = xs > double(s.x0 - 1) ? xs : double(s.x0 - 1);
-            xs = xs < double(s.x1 + 1) ? xs : double(s.x1 + 1);
-            g = prefix ? int(floor(xs)) : int(ceil(xs));
-        }
+        const int g = guess[e] < s.x0 - 1 ? s.x0 - 1 : (guess[e] > s.x1 + 1 ? s.x1 + 1 : guess[e]);
         // Bracket [a, b] with ok(a) == prefix and ok(b) != prefix, then bisect.
         int a, b;
         if (ok(g) == prefix) {
@@ -236,6 +229,31 @@ BH void face_interval_guess(const FaceSetup& s, double py, int& lo, int& hi) {
         if (prefix) hi = a < hi ? a : hi; // last covered
         else lo = b > lo ? b : lo;        // first covered
     }
+}
+
+// face_interval_at with each edge's boundary guessed from its crossing
+// x* = (t1 + r) / c + ax - 1/2 in single precision (within a small fraction
+// of a sample of the exact one; the searches settle it).
+BH void face_interval_guess(const FaceSetup& s, double py, int& lo, int& hi) {
+    const double ax3[3] = {s.dx, s.ex, s.ax}, ay3[3] = {s.dy, s.ey, s.ay};
+    const double bx3[3] = {s.ex, s.ax, s.dx}, by3[3] = {s.ey, s.ay, s.dy};
+    const double r3[3] = {s.r0, s.r1, s.r2};
+    int guess[3];
+#pragma unroll
+    for (int e = 0; e < 3; ++e) {
+        const double c = by3[e] - ay3[e];
+        const float num = float((bx3[e] - ax3[e]) * (py - ay3[e]) + r3[e]), den = float(c);
+#ifdef __CUDA_ARCH__
+        float xs = __fdividef(num, den) + float(ax3[e]) - .5f;
+#else
+        float xs = num / den + float(ax3[e]) - .5f;
+#endif
+        // NaN, infinities and far crossings clamp to the sentinels
+        xs = fmaxf(xs, float(s.x0 - 1));
+        xs = fminf(xs, float(s.x1 + 1));
+        guess[e] = c == 0 ? s.x0 : (c > 0 ? int(floorf(xs)) : int(ceilf(xs)));
+    }
+    face_interval_at(s, py, guess, lo, hi);
 }
 
 // CPU float value of the field where the exact distance reaches 2^24: the

@@ -149,7 +149,8 @@ void launch_refresh_views(const DevMesh& m, const Camera* cams_dev, uint32_t nvi
                           uint32_t size, bool force_two, uint8_t* counts, size_t cstride, uint32_t* state,
                           uint32_t* state_bits, const uint32_t* ref_bits, uint32_t wstride,
                           unsigned long long* pop, const uint32_t* ref_field, uint32_t* state_field, uint32_t* g,
-                          int32_t* sv, long long* sn, long long* sd, int32_t* t1, int32_t* t2, cudaStream_t s);
+                          int32_t* sv, long long* sn, long long* sd, int32_t* t1, int32_t* t2, bool saturate,
+                          cudaStream_t s);
 // Per view, the max of t1 and of t2 over its tiles: out[2v], out[2v+1].
 void launch_view_maxima(const int32_t* t1, const int32_t* t2, uint32_t tiles, uint32_t nviews, int32_t* out,
                         cudaStream_t s);

@@ -58,6 +58,19 @@ __device__ __forceinline__ void count_sample(uint8_t* counts, size_t i, uint32_t
     uint32_t old = atomicAdd(w, 1u << shift);
     if (((old >> shift) & 0xffu) == 0xffu) state[3] = 1;
 }
+// The same count held at 255 ("255 or more"): exact for the audits, which
+// compare a count with at most kMaxOk (< 255) changed faces, and for the
+// coverage bits (count > 0); counts are always rebuilt from scratch.
+__device__ __forceinline__ void count_sample_saturating(uint8_t* counts, size_t i) {
+    uint32_t* w = reinterpret_cast<uint32_t*>(counts) + (i >> 2);
+    const uint32_t shift = 8 * uint32_t(i & 3);
+    uint32_t old = *w, seen;
+    do {
+        seen = old;
+        if (((seen >> shift) & 0xffu) == 0xffu) return;
+        old = atomicCAS(w, seen, seen + (1u << shift));
+    } while (old != seen);
+}
 
 // One thread per face over its bounding box. bits: coverage (u64 LE layout as
 // u32 words); counts: covering faces per sample (u8, packed in u32 words).
@@ -302,7 +315,9 @@ __device__ FaceSetup face_setup_view(const ViewsArgs& a, const Camera& cam, uint
     return setup_face(p[0], p[1], p[2], cam.perspective != 0, two, a.size);
 }
 
-// Face counts of every view: state[4v+2] clipped faces, state[4v+3] overflow.
+// Face counts of every view: state[4v+2] clipped faces, state[4v+3] overflow
+// (kSaturate: counts held at 255 instead, no overflow).
+template <bool kSaturate>
 __global__ void k_count_views(ViewsArgs a, uint8_t* counts, size_t stride, uint32_t* state) {
     const uint32_t f = blockIdx.x * blockDim.x + threadIdx.x, v = blockIdx.y;
     if (f >= a.m.nf) return;
@@ -317,7 +332,10 @@ __global__ void k_count_views(ViewsArgs a, uint8_t* counts, size_t stride, uint3
     uint8_t* c = counts + stride * v;
     for (int y = s.y0; y <= s.y1; ++y)
         for (int x = s.x0; x <= s.x1; ++x)
-            if (face_covers(s, x, y)) count_sample(c, size_t(y) * a.size + x, st);
+            if (face_covers(s, x, y)) {
+                if constexpr (kSaturate) count_sample_saturating(c, size_t(y) * a.size + x);
+                else count_sample(c, size_t(y) * a.size + x, st);
+            }
 }
 __global__ void k_counts_to_bits_views(const uint8_t* counts, size_t cstride, size_t samples, uint32_t* bits,
                                        uint32_t wstride, uint32_t words) {
@@ -390,7 +408,8 @@ void launch_refresh_views(const DevMesh& m, const Camera* cams_dev, uint32_t nvi
                           uint32_t size, bool force_two, uint8_t* counts, size_t cstride, uint32_t* state,
                           uint32_t* state_bits, const uint32_t* ref_bits, uint32_t wstride,
                           unsigned long long* pop, const uint32_t* ref_field, uint32_t* state_field, uint32_t* g,
-                          int32_t* sv, long long* sn, long long* sd, int32_t* t1, int32_t* t2, cudaStream_t s) {
+                          int32_t* sv, long long* sn, long long* sd, int32_t* t1, int32_t* t2, bool saturate,
+                          cudaStream_t s) {
     ViewsArgs a;
     a.m = m;
     a.cams = cams_dev;
@@ -399,7 +418,11 @@ void launch_refresh_views(const DevMesh& m, const Camera* cams_dev, uint32_t nvi
     const size_t samples = size_t(size) * size;
     cudaMemsetAsync(counts, 0, cstride * nviews, s);
     cudaMemsetAsync(state, 0, 16 * size_t(nviews), s);
-    if (m.nf) k_count_views<<<dim3(blocks_for(m.nf, 128), nviews), 128, 0, s>>>(a, counts, cstride, state);
+    if (m.nf) {
+        const dim3 grid(blocks_for(m.nf, 128), nviews);
+        if (saturate) k_count_views<true><<<grid, 128, 0, s>>>(a, counts, cstride, state);
+        else k_count_views<false><<<grid, 128, 0, s>>>(a, counts, cstride, state);
+    }
     const uint32_t words = uint32_t((samples + 63) / 64) * 2;
     if (state_bits) {
         k_counts_to_bits_views<<<dim3(blocks_for(words), nviews), kThreads, 0, s>>>(counts, cstride, samples,

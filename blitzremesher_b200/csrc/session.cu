@@ -682,24 +682,31 @@ static void refresh_state(Session& S, Plan& p) {
     if (fields) ensure_tile_data(S, p);
     // Views per launch: the field scratch of one chunk stays within 256 MiB.
     const uint32_t chunk = fields ? field_chunk(S, p) : p.views;
-    for (uint32_t v0 = 0; v0 < p.views; v0 += chunk) {
-        const uint32_t n = std::min(chunk, p.views - v0);
-        const size_t w0 = size_t(p.words) * v0, s0 = samples * v0, t0 = size_t(tiles) * v0;
-        launch_refresh_views(live, p.cameras.p + v0, n, S.bounds.center, key.ss, p.size, key.force_two,
-                             p.state_count.p + cstride * v0, cstride, p.raster_state.p + 4 * v0,
-                             own_bits ? p.state_bits.p + w0 : nullptr, p.ref_bits.p + w0, p.words, p.pop.p + 4 * v0,
-                             fields ? p.ref_field.p + s0 : nullptr, fields ? S.scratch.vfield.p : nullptr,
-                             S.scratch.vg.p, S.scratch.vsv.p, S.scratch.vsn.p, S.scratch.vsd.p,
-                             fields ? p.t1.p + t0 : nullptr, fields ? p.t2.p + t0 : nullptr, st);
-    }
     std::vector<unsigned long long>& hpop = p.hpop;
     std::vector<uint32_t>& hstate = p.hstate;
-    B200_CUDA(cudaMemcpyAsync(hpop.data(), p.pop.p, hpop.size() * 8, cudaMemcpyDeviceToHost, st));
-    B200_CUDA(cudaMemcpyAsync(hstate.data(), p.raster_state.p, hstate.size() * 4, cudaMemcpyDeviceToHost, st));
-    B200_CUDA(cudaStreamSynchronize(st));
-    B200_CUDA(cudaGetLastError());
+    // Counts of up to 255 faces per sample; a plan with more is rebuilt with
+    // counts held at 255 (exact for the audits).
+    for (bool saturate : {false, true}) {
+        for (uint32_t v0 = 0; v0 < p.views; v0 += chunk) {
+            const uint32_t n = std::min(chunk, p.views - v0);
+            const size_t w0 = size_t(p.words) * v0, s0 = samples * v0, t0 = size_t(tiles) * v0;
+            launch_refresh_views(live, p.cameras.p + v0, n, S.bounds.center, key.ss, p.size, key.force_two,
+                                 p.state_count.p + cstride * v0, cstride, p.raster_state.p + 4 * v0,
+                                 own_bits ? p.state_bits.p + w0 : nullptr, p.ref_bits.p + w0, p.words,
+                                 p.pop.p + 4 * v0, fields ? p.ref_field.p + s0 : nullptr,
+                                 fields ? S.scratch.vfield.p : nullptr, S.scratch.vg.p, S.scratch.vsv.p,
+                                 S.scratch.vsn.p, S.scratch.vsd.p, fields ? p.t1.p + t0 : nullptr,
+                                 fields ? p.t2.p + t0 : nullptr, saturate, st);
+        }
+        B200_CUDA(cudaMemcpyAsync(hpop.data(), p.pop.p, hpop.size() * 8, cudaMemcpyDeviceToHost, st));
+        B200_CUDA(cudaMemcpyAsync(hstate.data(), p.raster_state.p, hstate.size() * 4, cudaMemcpyDeviceToHost, st));
+        B200_CUDA(cudaStreamSynchronize(st));
+        B200_CUDA(cudaGetLastError());
+        bool overflow = false;
+        for (uint32_t v = 0; v < p.views; ++v) overflow |= hstate[4 * v + 3] != 0;
+        if (!overflow) break;
+    }
     for (uint32_t v = 0; v < p.views; ++v) {
-        if (hstate[4 * v + 3]) throw Failure(BLITZ_OUT_OF_MEMORY, "more than 255 faces cover one sample");
         PlanView& pv = p.hviews[v];
         pv.state_bits = sbits + size_t(v) * p.words;
         pv.state_count = p.state_count.p + cstride * v;
@@ -1325,24 +1332,29 @@ static void trial_views(Session& S, Plan& p, const DevMesh& cand, uint64_t tag) 
     ensure_tile_data(S, p);
     const uint32_t chunk = field_chunk(S, p);
     Scratch& x = S.scratch;
-    for (uint32_t v0 = 0; v0 < p.views; v0 += chunk) {
-        const uint32_t n = std::min(chunk, p.views - v0);
-        const size_t w0 = size_t(p.words) * v0, s0 = samples * v0, t0 = size_t(tiles) * v0;
-        launch_refresh_views(cand, p.cameras.p + v0, n, S.bounds.center, p.key.ss, p.size, p.key.force_two,
-                             p.trial_count.p + cstride * v0, cstride, p.trial_state.p + 4 * v0, p.trial_bits.p + w0,
-                             p.ref_bits.p + w0, p.words, p.trial_pop.p + 4 * v0, p.ref_field.p + s0,
-                             x.vfield.p, x.vg.p, x.vsv.p, x.vsn.p, x.vsd.p, p.trial_t1.p + t0,
-                             p.trial_t2.p + t0, st);
+    for (bool saturate : {false, true}) { // as in refresh_state: counts held at 255 on overflow
+        for (uint32_t v0 = 0; v0 < p.views; v0 += chunk) {
+            const uint32_t n = std::min(chunk, p.views - v0);
+            const size_t w0 = size_t(p.words) * v0, s0 = samples * v0, t0 = size_t(tiles) * v0;
+            launch_refresh_views(cand, p.cameras.p + v0, n, S.bounds.center, p.key.ss, p.size, p.key.force_two,
+                                 p.trial_count.p + cstride * v0, cstride, p.trial_state.p + 4 * v0,
+                                 p.trial_bits.p + w0, p.ref_bits.p + w0, p.words, p.trial_pop.p + 4 * v0,
+                                 p.ref_field.p + s0, x.vfield.p, x.vg.p, x.vsv.p, x.vsn.p, x.vsd.p,
+                                 p.trial_t1.p + t0, p.trial_t2.p + t0, saturate, st);
+        }
+        launch_view_maxima(p.trial_t1.p, p.trial_t2.p, tiles, p.views, p.trial_max.p, st);
+        B200_CUDA(cudaMemcpyAsync(p.trial_hpop.data(), p.trial_pop.p, p.trial_hpop.size() * 8, cudaMemcpyDeviceToHost,
+                                  st));
+        B200_CUDA(cudaMemcpyAsync(p.trial_hstate.data(), p.trial_state.p, p.trial_hstate.size() * 4,
+                                  cudaMemcpyDeviceToHost, st));
+        B200_CUDA(cudaMemcpyAsync(p.trial_hmax.data(), p.trial_max.p, p.trial_hmax.size() * 4, cudaMemcpyDeviceToHost,
+                                  st));
+        B200_CUDA(cudaStreamSynchronize(st));
+        B200_CUDA(cudaGetLastError());
+        bool overflow = false;
+        for (uint32_t v = 0; v < p.views; ++v) overflow |= p.trial_hstate[4 * v + 3] != 0;
+        if (!overflow) break;
     }
-    launch_view_maxima(p.trial_t1.p, p.trial_t2.p, tiles, p.views, p.trial_max.p, st);
-    B200_CUDA(cudaMemcpyAsync(p.trial_hpop.data(), p.trial_pop.p, p.trial_hpop.size() * 8, cudaMemcpyDeviceToHost, st));
-    B200_CUDA(cudaMemcpyAsync(p.trial_hstate.data(), p.trial_state.p, p.trial_hstate.size() * 4,
-                              cudaMemcpyDeviceToHost, st));
-    B200_CUDA(cudaMemcpyAsync(p.trial_hmax.data(), p.trial_max.p, p.trial_hmax.size() * 4, cudaMemcpyDeviceToHost, st));
-    B200_CUDA(cudaStreamSynchronize(st));
-    B200_CUDA(cudaGetLastError());
-    for (uint32_t v = 0; v < p.views; ++v)
-        if (p.trial_hstate[4 * v + 3]) throw Failure(BLITZ_OUT_OF_MEMORY, "more than 255 faces cover one sample");
     p.trial_tag = tag;
     S.profile.launches += 8;
 }
@@ -2456,9 +2468,42 @@ struct blitz_audit_batch {
     cudaEvent_t ev[2] = {nullptr, nullptr};
     float audit_ms = 0;
     unsigned long long prof[kAuditStats] = {};
+    // Side streams that run the sessions' small per-candidate launches
+    // (records, verdicts) side by side, forked from and joined to the
+    // batch's stream by events (captured into the graph as parallel
+    // branches).
+    std::vector<cudaStream_t> side;
+    std::vector<cudaEvent_t> side_done;
+    cudaEvent_t fork = nullptr;
+    void ensure_side(size_t n) {
+        if (!fork) B200_CUDA(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
+        while (side.size() < n) {
+            cudaStream_t s;
+            cudaEvent_t e;
+            B200_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+            side.push_back(s);
+            B200_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+            side_done.push_back(e);
+        }
+    }
+    // Runs launch(i, stream) for i < n spread over the side streams; `st`
+    // waits for all of them.
+    template <class F> void side_by_side(size_t n, cudaStream_t st, F&& launch) {
+        const size_t k = std::min(side.size(), n);
+        B200_CUDA(cudaEventRecord(fork, st));
+        for (size_t j = 0; j < k; ++j) B200_CUDA(cudaStreamWaitEvent(side[j], fork, 0));
+        for (size_t i = 0; i < n; ++i) launch(i, side[i % k]);
+        for (size_t j = 0; j < k; ++j) {
+            B200_CUDA(cudaEventRecord(side_done[j], side[j]));
+            B200_CUDA(cudaStreamWaitEvent(st, side_done[j], 0));
+        }
+    }
     ~blitz_audit_batch() {
         for (auto e : ev)
             if (e) cudaEventDestroy(e);
+        for (auto e : side_done) cudaEventDestroy(e);
+        for (auto s_ : side) cudaStreamDestroy(s_);
+        if (fork) cudaEventDestroy(fork);
         stats.release();
         if (exec) cudaGraphExecDestroy(exec);
         if (graph) cudaGraphDestroy(graph);
@@ -2573,15 +2618,16 @@ static void batch_candidates(blitz_audit_batch* b, const blitz_collapse* cands, 
             B200_CUDA(cudaEventCreate(&b->ev[0]));
             B200_CUDA(cudaEventCreate(&b->ev[1]));
         }
+        b->ensure_side(std::min<size_t>(ns, 16));
         auto body = [&](int variant) {
-            for (size_t i = 0; i < ns; ++i) {
-                if (!counts[i]) continue;
+            b->side_by_side(ns, st, [&](size_t i, cudaStream_t ss) {
+                if (!counts[i]) return;
                 Session& S = b->sessions[i]->s;
                 Topology& t = S.topo;
                 launch_prepare(S.state.view, t.view, S.state.view, t.view, cands + off[i], uint32_t(counts[i]),
                                t.positions.p, t.pos_cap, t.flat.p, S.options.preserve_uv != 0, b->records.p + off[i],
-                               st, t.uv());
-            }
+                               ss, t.uv());
+            });
             if (profile) {
                 cudaMemsetAsync(b->stats.p, 0, kAuditStats * 8, st);
                 cudaEventRecord(b->ev[0], st);
@@ -2596,12 +2642,12 @@ static void batch_candidates(blitz_audit_batch* b, const blitz_collapse* cands, 
             }
             if (profile) cudaEventRecord(b->ev[1], st);
             cudaMemsetAsync(b->exact.p, 0, 4 * ns, st);
-            for (size_t i = 0; i < ns; ++i) {
-                if (!counts[i]) continue;
+            b->side_by_side(ns, st, [&](size_t i, cudaStream_t ss) {
+                if (!counts[i]) return;
                 Session& S = b->sessions[i]->s;
                 launch_verdicts(S.record_table.p, S.plan_views.p, S.plan_ss.p, S.gate_table.p, b->records.p + off[i],
-                                uint32_t(counts[i]), out + off[i], nullptr, b->exact.p + i, st);
-            }
+                                uint32_t(counts[i]), out + off[i], nullptr, b->exact.p + i, ss);
+            });
         };
         // Autotune: time both warp-tier variants on this call, keep the faster.
         if ((flags & 2u) && off[ns]) {

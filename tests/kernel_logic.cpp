@@ -67,12 +67,18 @@ int main() {
             face_interval(s, double(y) + .5, lo, hi);
             bool ok = true;
             for (int x = s.x0; x <= s.x1 && ok; ++x) ok = face_covers(s, x, y) == (x >= lo && x <= hi);
-            // the interval searched from the edges' computed crossings is the
-            // same set
+            // the interval searched from the edges' guessed crossings, and
+            // from arbitrary guesses, is the same set
             int glo, ghi;
             face_interval_guess(s, double(y) + .5, glo, ghi);
-            const bool empty = lo > hi, gempty = glo > ghi;
-            ok = ok && empty == gempty && (empty || (glo == lo && ghi == hi));
+            const bool empty = lo > hi;
+            ok = ok && (empty ? glo > ghi : (glo == lo && ghi == hi));
+            int guess[3];
+            const int span_x = s.x1 - s.x0 + 3;
+            for (int e = 0; e < 3; ++e)
+                guess[e] = t % 3 == 0 ? int(rng() % 20000) - 10000 : s.x0 - 1 + int(rng() % uint64_t(span_x));
+            face_interval_at(s, double(y) + .5, guess, glo, ghi);
+            ok = ok && (empty ? glo > ghi : (glo == lo && ghi == hi));
             ++rows;
             bad_rows += !ok;
         }

@@ -86,6 +86,56 @@ def test_candidates_of_committed_state_match_oracle(gpu_lib, oracle):
             assert measurement_fields(meas[i, g]) == measurement_fields(want.gates[g]), (i, g)
 
 
+def _stacked_sheets(layers: int, seed: int):
+    """`layers` parallel 2 x 2-quad sheets facing +z, 0.0005 apart, each with
+    its centre vertex jittered: front views see every layer over most samples,
+    so more than 255 faces cover a sample."""
+    rng = np.random.default_rng(seed)
+    g = np.linspace(-1.0, 1.0, 3)
+    xs, ys = np.meshgrid(g, g)
+    pos, idx = [], []
+    for k in range(layers):
+        p = np.stack([xs.ravel(), ys.ravel(), np.full(9, 0.0005 * k)], 1)
+        p[4, :2] += rng.uniform(-0.3, 0.3, 2)
+        pos.append(p)
+        for i in range(2):
+            for j in range(2):
+                a = 9 * k + 3 * i + j
+                idx += [a, a + 1, a + 4, a, a + 4, a + 3]
+    return syn.Mesh(np.concatenate(pos).astype(np.float32), np.array(idx, np.uint32))
+
+
+def test_deep_overlap_matches_oracle(gpu_lib, oracle):
+    """Samples covered by more than 255 faces: the state counts are held at
+    255, which leaves every verdict, Measurement and commit exact (a collapse
+    changes at most 48 faces)."""
+    mesh = _stacked_sheets(320, 4)
+    views = (6, 2, 5)
+    args = _gates(16.0, views, 4)
+    gates_o = [oracle_settings(*a) for a in args]
+    gates_g = [br.eval_settings(*a) for a in args]
+    b = oracle.bounds(mesh)
+    with br.AuditSession(mesh) as s:
+        cands = br.midpoint_collapses(s.actions())
+        picks = cands[:: max(1, cands.size // 24)]
+        verdicts, meas = s.candidates(picks, gates_g, measurements=True)
+        got = s.execute(mesh.face_count - 200, 40, gates_g, batch=8)
+        idx, pos = s.state()
+    for i, c in enumerate(picks):
+        e = BoEdit()
+        e.from_, e.to = int(c["from"]), int(c["to"])
+        want = oracle.audit_candidate(mesh, e, mesh, mesh, b, gates_o)
+        assert verdicts[i]["accepted"] == want.accepted and verdicts[i]["failed_gate"] == want.failed_gate, i
+        stop = 4 if want.failed_gate == 0 else (want.failed_gate if want.failed_gate <= 4 else 0)
+        for g in range(stop):
+            assert measurement_fields(meas[i, g]) == measurement_fields(want.gates[g]), (i, g)
+    want = oracle.execute(mesh, mesh.face_count - 200, 40, gates_o, batch=8)
+    assert len(want["commits"]) > 0
+    assert np.array_equal(got["commits"], want["commits"])
+    assert got["trials"] == want["trials"] and got["stop"] == want["stop"]
+    assert np.array_equal(idx, want["indices"]) and np.array_equal(pos, want["positions"])
+
+
 @pytest.mark.parametrize("commit", [False, True])
 def test_large_regions_match_oracle(gpu_lib, oracle, commit):
     """Coarse triangles at 64 px x ss 8: most (candidate, view) regions
