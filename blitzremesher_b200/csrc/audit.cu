@@ -130,21 +130,21 @@ __device__ __forceinline__ void record_write(ViewRecord* out, const ViewRecord& 
 }
 
 // Rows of interval ends kept per pass of the word-row region phase.
-constexpr int kPassRows = 8;
+constexpr int kPassRows = 8; // a pass's row fits 3 bits of the (row, face) item table
 // Shared memory of one warp of the global tiers: face setups, the pass's
 // interval ends and its two word-mask tables.
-// The two word-mask tables of a pass are followed by the per-face item
-// prefixes (kMaxOk u16) of region_word_rows.
-constexpr size_t kPassMaskBytes = 2 * kPassRows * 32 * 4 + kMaxOk * 2;
+// The two word-mask tables of a pass are followed by its (row, face) item
+// table (kPassRows * kMaxOk u16) of region_word_rows.
+constexpr size_t kPassMaskBytes = 2 * kPassRows * 32 * 4 + kPassRows * kMaxOk * 2;
 constexpr size_t kGlobalTierWarpSmem = kMaxOk * sizeof(FaceSetup) + kPassRows * kMaxOk * 4 + kPassMaskBytes;
 
 // Region phase over coverage words (every tier but the small one),
 // kPassRows rows at a time. Per (row, face) the covered samples are one
 // interval (exact FP64 searches from the edges' guessed crossings,
 // face_interval_guess). A pass computes them for the (row, face) pairs whose
-// row the face spans, spread evenly over the lanes (per-face prefixes of
-// those pairs in `masks`' tail), and keeps them in `iv` (shared memory;
-// empty for the other pairs). Each interval is then OR-ed into the pass's
+// row the face spans, spread evenly over the lanes (the pairs listed in
+// `masks`' tail, face-major), and keeps them in `iv` (shared memory; empty
+// for the other pairs). Each interval is then OR-ed into the pass's
 // word masks in shared memory (`masks`): the union of the new faces (B) and
 // of the old faces (A). Because the state's count pc includes every old face
 // (pc >= A), the candidate's count pc - A + B is positive wherever B > 0,
@@ -166,7 +166,8 @@ __device__ void region_word_rows(const FaceSetup* faces, uint32_t nok, int wx0, 
     long long t0 = clk ? clock64() : 0;
     uint32_t* const bn = masks;                  // [kPassRows][32] new-face union
     uint32_t* const an = masks + kPassRows * 32; // [kPassRows][32] old-face union
-    uint16_t* const first = reinterpret_cast<uint16_t*>(masks + 2 * kPassRows * 32); // [kMaxOk]
+    static_assert(kPassRows == 8 && kMaxOk < 8192, "item = face << 3 | row");
+    uint16_t* const pairs = reinterpret_cast<uint16_t*>(masks + 2 * kPassRows * 32); // face << 3 | row
     for (int ybase = ry0; ybase <= ry1; ybase += kPassRows) {
         const int ylast = min(ry1, ybase + kPassRows - 1);
         const uint32_t pass_rows = uint32_t(ylast - ybase + 1);
@@ -186,20 +187,15 @@ __device__ void region_word_rows(const FaceSetup* faces, uint32_t nok, int wx0, 
         const uint32_t tot0 = __shfl_sync(0xffffffffu, s0, 31);
         const uint32_t items = tot0 + __shfl_sync(0xffffffffu, s1, 31);
         for (uint32_t f = lane; f < nok; f += 32) {
-            first[f] = uint16_t(f < 32 ? s0 - n0 : tot0 + s1 - n1);
+            const uint32_t at = f < 32 ? s0 - n0 : tot0 + s1 - n1, n = f < 32 ? n0 : n1;
+            const uint32_t r0 = uint32_t(first_row(f) - ybase);
+            for (uint32_t j = 0; j < n; ++j) pairs[at + j] = uint16_t(f << 3 | (r0 + j));
             for (uint32_t r = 0; r < pass_rows; ++r) iv[r * kMaxOk + f] = make_short2(1, 0);
         }
         __syncwarp();
-        // Item t -> its face (the last with first <= t) and row.
         auto item = [&](uint32_t t, uint32_t& f, uint32_t& r) {
-            uint32_t lo = 0, hi = nok - 1;
-            while (lo < hi) {
-                const uint32_t mid = (lo + hi + 1) >> 1;
-                if (first[mid] <= t) lo = mid;
-                else hi = mid - 1;
-            }
-            f = lo;
-            r = uint32_t(first_row(lo) - ybase) + (t - first[lo]);
+            const uint32_t p = pairs[t];
+            f = p >> 3, r = p & 7u;
         };
         for (uint32_t t = lane; t < items; t += 32) {
             uint32_t f, r;
