@@ -714,6 +714,7 @@ def run_batched(args, rank: int, world: int, local: int) -> dict:
                                    "peak_source": f"{sms} SMs x 128 INT32 lanes x {sm_mhz:.0f} MHz (sampled)"},
                          "kernel": "k_audit (+ large and huge tiers)", "kernel_ms": audit_ms,
                          "kernel_ms_counting": info["audit_ms"],
+                         "tier_ms": dict(zip(("warp", "huge", "giant"), batch.info()["tier_ms"])),
                          "algorithmic_bytes": alg_bytes, "units_per_launch": info["units"],
                          "samples_per_launch": info["region_samples"],
                          "peak_source": pk["source"] + " hbm_gbs (burst)",
@@ -723,6 +724,8 @@ def run_batched(args, rank: int, world: int, local: int) -> dict:
                                    "cycles_per_unit": dict(zip(("warp", "large", "huge", "giant"),
                                                                [c / u if u else 0.0 for c, u in
                                                                 zip(info["tier_cycles"], info["tier_units"])])),
+                                   "max_cycles_per_unit": dict(zip(("warp", "large", "huge", "giant"),
+                                                                   info["tier_max_cycles"])),
                                    "phase_share": dict(zip(("setup", "region", "distance"),
                                                            _shares(info["phase_cycles"]))),
                                    "flipped_samples": info["flipped_samples"],

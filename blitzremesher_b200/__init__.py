@@ -353,7 +353,7 @@ class BatchInfo(C.Structure):
                 ("exact_candidates", C.c_uint64), ("audit_ms", C.c_float), ("units", C.c_uint64),
                 ("region_samples", C.c_uint64), ("changed_samples", C.c_uint64),
                 ("tier_units", C.c_uint64 * 4), ("tier_cycles", C.c_uint64 * 4), ("phase_cycles", C.c_uint64 * 3),
-                ("flipped_samples", C.c_uint64), ("region_split", C.c_uint64 * 15), ("face_samples", C.c_uint64)]
+                ("flipped_samples", C.c_uint64), ("region_split", C.c_uint64 * 15), ("face_samples", C.c_uint64), ("tier_max_cycles", C.c_uint64 * 4), ("tier_ms", C.c_float * 3)]
 
 
 BATCH_GRAPH, BATCH_AUTOTUNE, BATCH_PROFILE, BATCH_TIMING = 1, 2, 4, 8
@@ -711,7 +711,7 @@ class AuditBatch:
         i.struct_size = C.sizeof(BatchInfo)
         assert self.lib.blitz_audit_batch_read_info(self.handle, C.byref(i)) == BLITZ_OK
         d = {k: getattr(i, k) for k, _ in i._fields_ if k != "struct_size"}
-        for k in ("tune_ms", "tier_units", "tier_cycles", "phase_cycles", "region_split"):
+        for k in ("tune_ms", "tier_units", "tier_cycles", "phase_cycles", "region_split", "tier_max_cycles", "tier_ms"):
             d[k] = list(getattr(i, k))
         return d
 

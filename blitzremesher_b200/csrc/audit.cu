@@ -841,7 +841,8 @@ __device__ void audit_unit(const CandidateRecord* __restrict__ rec, const PlanDe
             // sweep cycles and units, its event and piece cycles, rows; word
             // rows cycles and units, their interval, mask, word and
             // lost-sample cycles, rows); samples of the faces' bboxes (the
-            // (face, sample) pairs a per-sample raster tests)
+            // (face, sample) pairs a per-sample raster tests); per tier the
+            // longest unit's SM cycles)
             const long long t_end = clock64();
             constexpr int tier = L::kRegionRows <= 128 ? 0 : L::kRegionRows <= 256 ? 1 : L::kRegionRows <= 1024 ? 2 : 3;
             atomicAdd(stats, 1ull);
@@ -849,6 +850,7 @@ __device__ void audit_unit(const CandidateRecord* __restrict__ rec, const PlanDe
             atomicAdd(stats + 2, (unsigned long long)(qn + region_changed));
             atomicAdd(stats + 3 + tier, 1ull);
             atomicAdd(stats + 7 + tier, (unsigned long long)(t_end - t_start));
+            atomicMax(stats + 31 + tier, (unsigned long long)(t_end - t_start));
             atomicAdd(stats + 11, (unsigned long long)(t_setup - t_start));
             atomicAdd(stats + 12, (unsigned long long)(t_region - t_setup));
             atomicAdd(stats + 13, (unsigned long long)(t_end - t_region));
@@ -1075,7 +1077,7 @@ size_t warp_tier_smem(int variant) {
 
 void launch_audit(const AuditJob& job, unsigned long long* stats, uint32_t* queue, uint32_t* spill,
                   uint32_t* spill_huge, unsigned char* huge_scratch, uint32_t huge_blocks, cudaStream_t s,
-                  int variant, const GiantTier* giant) {
+                  int variant, const GiantTier* giant, cudaEvent_t* marks) {
     if (!job.total) return;
     static bool configured = false;
     const size_t large = audit_large_smem_bytes();
@@ -1107,7 +1109,9 @@ void launch_audit(const AuditJob& job, unsigned long long* stats, uint32_t* queu
     if (huge) cudaMemsetAsync(spill_huge, 0, 4, s);
     if (big) cudaMemsetAsync(giant->spill, 0, 4, s);
     uint32_t* next = big ? giant->spill : nullptr;
+    if (marks) cudaEventRecord(marks[0], s);
     kernel<<<uint32_t(grid), kAuditWarps * 32, smem, s>>>(tuned, stats, queue, spill);
+    if (marks) cudaEventRecord(marks[1], s);
     if (huge && huge_blocks >= uint32_t(sms)) {
         // enough huge-tier warps: units the warp tier spills go there directly
         k_audit_global<LimitsHuge, kHugeWarps>
@@ -1122,11 +1126,13 @@ void launch_audit(const AuditJob& job, unsigned long long* stats, uint32_t* queu
                 <<<huge_blocks, kHugeWarps * 32, kHugeWarps * kGlobalTierWarpSmem, s>>>(job, stats, spill_huge,
                                                                                        queue + 2, huge_scratch, next);
     }
+    if (marks) cudaEventRecord(marks[2], s);
     if (big)
         k_audit_global<LimitsGiant, kGiantWarps>
             <<<giant->blocks, kGiantWarps * 32, kGiantWarps * kGlobalTierWarpSmem, s>>>(job, stats, giant->spill,
                                                                                        queue + 3, giant->scratch,
                                                                                        nullptr);
+    if (marks) cudaEventRecord(marks[3], s);
 }
 
 void launch_verdicts(const ViewRecord* const* plan_records, const uint32_t* plan_views, const uint32_t* plan_ss,

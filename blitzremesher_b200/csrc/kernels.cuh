@@ -52,7 +52,7 @@ struct UvSource {
 };
 
 // Slots of the audit kernels' profiling counters (launch_audit `stats`).
-constexpr int kAuditStats = 31;
+constexpr int kAuditStats = 35;
 
 constexpr int kMaxAffected = 32; // faces in faces(from) U faces(to) handled on the fast path
 constexpr int kMaxLocal = 31;    // distinct vertex slots of those faces; local index 31 = placement
@@ -215,10 +215,12 @@ struct GiantTier {
     unsigned char* scratch;
     uint32_t blocks;
 };
-// queue: 4 words (work cursors).
+// queue: 4 words (work cursors). marks (profiling, may be null): 4 events
+// recorded before the warp tier, after it, after the large / huge tier and
+// after the giant tier.
 void launch_audit(const AuditJob& job, unsigned long long* stats, uint32_t* queue, uint32_t* spill,
                   uint32_t* spill_huge, unsigned char* huge_scratch, uint32_t huge_blocks, cudaStream_t s,
-                  int variant = kAuditTierSmall, const GiantTier* giant = nullptr);
+                  int variant = kAuditTierSmall, const GiantTier* giant = nullptr, cudaEvent_t* marks = nullptr);
 size_t audit_huge_scratch_bytes(uint32_t blocks);
 size_t audit_giant_scratch_bytes(uint32_t blocks);
 struct GateDev {

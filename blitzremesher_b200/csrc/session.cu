@@ -2466,7 +2466,8 @@ struct blitz_audit_batch {
     // profile of the last call with BLITZ_BATCH_PROFILE
     Buf<unsigned long long> stats;
     cudaEvent_t ev[2] = {nullptr, nullptr};
-    float audit_ms = 0;
+    std::vector<cudaEvent_t> marks; // per plan slot, 4 (launch_audit)
+    float audit_ms = 0, tier_ms[3] = {0, 0, 0};
     unsigned long long prof[kAuditStats] = {};
     // Side streams that run the sessions' small per-candidate launches
     // (records, verdicts) side by side, forked from and joined to the
@@ -2502,6 +2503,7 @@ struct blitz_audit_batch {
         for (auto e : ev)
             if (e) cudaEventDestroy(e);
         for (auto e : side_done) cudaEventDestroy(e);
+        for (auto e : marks) cudaEventDestroy(e);
         for (auto s_ : side) cudaStreamDestroy(s_);
         if (fork) cudaEventDestroy(fork);
         stats.release();
@@ -2618,6 +2620,11 @@ static void batch_candidates(blitz_audit_batch* b, const blitz_collapse* cands, 
             B200_CUDA(cudaEventCreate(&b->ev[0]));
             B200_CUDA(cudaEventCreate(&b->ev[1]));
         }
+        while (profile && b->marks.size() < 4 * slots) {
+            cudaEvent_t e;
+            B200_CUDA(cudaEventCreate(&e));
+            b->marks.push_back(e);
+        }
         b->ensure_side(std::min<size_t>(ns, 16));
         auto body = [&](int variant) {
             b->side_by_side(ns, st, [&](size_t i, cudaStream_t ss) {
@@ -2638,7 +2645,7 @@ static void batch_candidates(blitz_audit_batch* b, const blitz_collapse* cands, 
                 job.entries = b->entries[j].p, job.nentries = b->nentries[j], job.total = b->units[j];
                 launch_audit(job, counting ? b->stats.p : nullptr, b->queue.p, b->spill.p,
                              big ? b->spill_huge.p : nullptr, big ? b->huge.p : nullptr, big ? b->huge_blocks : 0,
-                             st, variant, giant ? &giant_tier : nullptr);
+                             st, variant, giant ? &giant_tier : nullptr, profile ? b->marks.data() + 4 * j : nullptr);
             }
             if (profile) cudaEventRecord(b->ev[1], st);
             cudaMemsetAsync(b->exact.p, 0, 4 * ns, st);
@@ -2718,6 +2725,15 @@ static void batch_candidates(blitz_audit_batch* b, const blitz_collapse* cands, 
         if (profile && off[ns]) {
             B200_CUDA(cudaEventElapsedTime(&b->audit_ms, b->ev[0], b->ev[1]));
             if (counting) B200_CUDA(cudaMemcpy(b->prof, b->stats.p, sizeof(b->prof), cudaMemcpyDeviceToHost));
+            for (float& t : b->tier_ms) t = 0;
+            for (size_t j = 0; j < slots; ++j) {
+                if (!b->units[j]) continue;
+                for (int k = 0; k < 3; ++k) {
+                    float ms = 0;
+                    B200_CUDA(cudaEventElapsedTime(&ms, b->marks[4 * j + k], b->marks[4 * j + k + 1]));
+                    b->tier_ms[k] += ms;
+                }
+            }
         }
         for (size_t i = 0; i < ns; ++i) {
             if (!exact[i]) continue;
@@ -2774,6 +2790,7 @@ blitz_status blitz_audit_batch_read_info(const blitz_audit_batch* b, blitz_audit
     out->graph_launches = b->graph_launches;
     out->exact_candidates = b->exact_candidates;
     out->audit_ms = b->audit_ms;
+    for (int k = 0; k < 3; ++k) out->tier_ms[k] = b->tier_ms[k];
     out->units = b->prof[0];
     out->region_samples = b->prof[1];
     out->changed_samples = b->prof[2];
@@ -2782,6 +2799,7 @@ blitz_status blitz_audit_batch_read_info(const blitz_audit_batch* b, blitz_audit
     out->flipped_samples = b->prof[14];
     for (int k = 0; k < 15; ++k) out->region_split[k] = b->prof[15 + k];
     out->face_samples = b->prof[30];
+    for (int k = 0; k < 4; ++k) out->tier_max_cycles[k] = b->prof[31 + k];
     return BLITZ_OK;
 }
 

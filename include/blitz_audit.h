@@ -514,6 +514,12 @@ typedef struct blitz_audit_batch_info {
     /* the same call: samples of the rasterized faces' bounding boxes summed
      * over units (the (face, sample) pairs a per-sample raster would test) */
     uint64_t face_samples;
+    /* the same call, per tier: SM cycles of its longest unit */
+    uint64_t tier_max_cycles[4];
+    /* last BLITZ_BATCH_PROFILE or BLITZ_BATCH_TIMING call: device time of the
+     * warp tier's launches, of the large / huge tier's and of the giant
+     * tier's */
+    float tier_ms[3];
 } blitz_audit_batch_info;
 blitz_status blitz_audit_batch_create(blitz_audit_session* const* sessions, size_t count, blitz_audit_batch** out,
                                       char* error, size_t error_capacity);
