@@ -733,9 +733,11 @@ __device__ void audit_unit(const CandidateRecord* __restrict__ rec, const PlanDe
         best = uint32_t(max(max(far1, far2), 0));
         // Verdict-only calls (threshold predicate, evaluate.cu:1034-1169):
         // a sample nearer than `floor` cannot change any gate's verdict, so
-        // its search may stop at any covered sample within it; once the
-        // maximum exceeds `ceiling` every gate of the plan fails this view
-        // and the search stops. Exact calls: floor 0, ceiling UINT32_MAX.
+        // its search may stop at any covered sample within it; a search
+        // stops at `ceiling` (a farther nearest sample counts as ceiling + 1),
+        // and once the maximum exceeds it every gate of the plan fails this
+        // view and the view's searches stop. Exact calls: floor 0, ceiling
+        // UINT32_MAX.
         const uint32_t floor_d2 = plan.d2_floor, ceiling_d2 = plan.d2_ceiling;
         // Reference-only samples of the affected tiles outside the region.
         for (uint32_t base = 0; base < qn && best <= ceiling_d2; base += 32) {
@@ -743,7 +745,7 @@ __device__ void audit_unit(const CandidateRecord* __restrict__ rec, const PlanDe
             if (k < qn) {
                 const uint32_t e = ws.queue[k];
                 const uint32_t x = e & 0x7fffu, y = (e >> 15) & 0x7fffu;
-                const uint32_t d = nearest_d2(cmask, x, y, max(best, floor_d2));
+                const uint32_t d = nearest_d2(cmask, x, y, max(best, floor_d2), ceiling_d2);
                 best = d > best ? d : best;
             }
             for (int o = 16; o; o >>= 1) {
@@ -764,8 +766,10 @@ __device__ void audit_unit(const CandidateRecord* __restrict__ rec, const PlanDe
                     const uint32_t x = uint32_t(wx0) + (e & 0x7fffu), y = uint32_t(ry0) + ((e >> 15) & 0x7fffu);
                     const uint32_t enough = max(best, floor_d2);
                     uint32_t d;
-                    if (e >> 31) d = pv.ref_field ? pv.ref_field[size_t(y) * size + x] : nearest_d2(rmask, x, y, enough);
-                    else d = nearest_d2(cmask, x, y, enough);
+                    if (e >> 31)
+                        d = pv.ref_field ? pv.ref_field[size_t(y) * size + x]
+                                         : nearest_d2(rmask, x, y, enough, ceiling_d2);
+                    else d = nearest_d2(cmask, x, y, enough, ceiling_d2);
                     best = d > best ? d : best;
                 }
                 for (int o = 16; o; o >>= 1) {
@@ -815,8 +819,9 @@ __device__ void audit_unit(const CandidateRecord* __restrict__ rec, const PlanDe
                     const uint32_t enough = max(best, floor_d2);
                     uint32_t d;
                     if ((cmask_s[w] >> bit) & 1u)
-                        d = pv.ref_field ? pv.ref_field[size_t(ry) * size + x] : nearest_d2(rmask, x, ry, enough);
-                    else d = nearest_d2(cmask, x, ry, enough);
+                        d = pv.ref_field ? pv.ref_field[size_t(ry) * size + x]
+                                         : nearest_d2(rmask, x, ry, enough, ceiling_d2);
+                    else d = nearest_d2(cmask, x, ry, enough, ceiling_d2);
                     best = d > best ? d : best;
                 }
                 for (int o = 16; o; o >>= 1) {

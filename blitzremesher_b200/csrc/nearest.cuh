@@ -92,27 +92,41 @@ template <class M> NEAREST_HD inline uint32_t nearest_in_row(const M& mask, uint
 // Exact squared Euclidean distance from (x, y) to the nearest covered sample
 // (kNone: none), or any value <= `enough` once a covered sample that close is
 // found (the caller only needs distances above `enough`: the running
-// maximum). The search runs in boxes of half-width R = 32, 128, ...: rows
-// are scanned up to R columns until a covered sample is found, and then
-// within its distance; a result <= R^2 (or <= enough) is final, since every
-// sample left out of the box is farther than R.
+// maximum), or cap + 1 when no covered sample lies within squared distance
+// `cap` (the caller only needs to know that it is farther; cap = UINT32_MAX:
+// no cap). The search runs in boxes of half-width R = 32, 128, ...: rows are
+// scanned up to R columns until a covered sample is found, and then within
+// its distance; a result <= R^2 (or <= enough) is final, since every sample
+// left out of the box is farther than R. With a cap the last box reaches
+// floor(sqrt(cap)) + 1, beyond which every sample is farther than the cap.
 NEAREST_HD_PRAGMA
-template <class M> NEAREST_HD inline uint32_t nearest_d2(const M& mask, uint32_t x, uint32_t y, uint32_t enough = 0) {
+template <class M>
+NEAREST_HD inline uint32_t nearest_d2(const M& mask, uint32_t x, uint32_t y, uint32_t enough = 0,
+                                      uint32_t cap = 0xffffffffu) {
     const uint32_t size = mask.size;
+    const bool capped = cap != 0xffffffffu;
+    uint32_t reach = size;
+    if (capped) {
+        uint64_t r = uint64_t(sqrt(double(cap)));
+        while (r * r > cap) --r;
+        while ((r + 1) * (r + 1) <= cap) ++r;
+        reach = r + 1 < size ? uint32_t(r + 1) : size;
+    }
     for (uint32_t R = 32;; R *= 4) {
-        const bool last = R >= size;
+        const bool last = R >= reach;
+        const uint32_t box = last ? reach : R;
         uint32_t best = kNone;
         for (uint32_t dy = 0;; ++dy) {
             const uint64_t dy2 = uint64_t(dy) * dy;
             if (best != kNone && (dy2 >= best || best <= enough)) break;
-            if (best == kNone && !last && dy > R) break;
+            if (dy > box && (best == kNone || last)) break;
             bool any = false;
             for (int side = 0; side < (dy ? 2 : 1); ++side) {
                 const int64_t row = side ? int64_t(y) + dy : int64_t(y) - dy;
                 if (row < 0 || row >= int64_t(size)) continue;
                 any = true;
-                const uint32_t maxdx =
-                    best == kNone ? (last ? size : R) : uint32_t(sqrtf(float(best - dy2))) + 1;
+                uint32_t maxdx = best == kNone ? box : uint32_t(sqrtf(float(best - dy2))) + 1;
+                if (last && maxdx > box) maxdx = box;
                 const uint32_t dx = nearest_in_row(mask, uint32_t(row), x, maxdx);
                 if (dx != kNone) {
                     const uint64_t d = uint64_t(dx) * dx + dy2;
@@ -121,7 +135,8 @@ template <class M> NEAREST_HD inline uint32_t nearest_d2(const M& mask, uint32_t
             }
             if (!any) break;
         }
-        if (last || (best != kNone && (best <= enough || uint64_t(best) <= uint64_t(R) * R))) return best;
+        if (last) return capped && (best == kNone || best > cap) ? cap + 1 : best;
+        if (best != kNone && (best <= enough || uint64_t(best) <= uint64_t(R) * R)) return best;
     }
 }
 

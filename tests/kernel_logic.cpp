@@ -111,6 +111,13 @@ int main() {
             if (want == kNone) ok = got == kNone;
             else if (enough && want <= enough) ok = got >= want && got <= enough;
             else ok = got == want;
+            // with a cap: the same answer when the nearest is within it, else
+            // cap + 1 (also for an empty mask)
+            const uint32_t cap = q % 2 ? uint32_t(rng() % (4ull * m.size * m.size)) : uint32_t(rng() % 50);
+            const uint32_t capped = nearest_d2(m, x, y, enough, cap);
+            if (want == kNone || want > cap) ok = ok && capped == cap + 1;
+            else if (enough && want <= enough) ok = ok && capped >= want && capped <= enough;
+            else ok = ok && capped == want;
             ++queries;
             bad_queries += !ok;
         }
