@@ -132,10 +132,9 @@ __device__ __forceinline__ void record_write(ViewRecord* out, const ViewRecord& 
 // Rows of interval ends kept per pass of the word-row region phase.
 constexpr int kPassRows = 8; // a pass's row fits 3 bits of the (row, face) item table
 // Shared memory of one warp of the global tiers: face setups, the pass's
-// interval ends and its two word-mask tables.
-// The two word-mask tables of a pass are followed by its (row, face) item
-// table (kPassRows * kMaxOk u16) of region_word_rows.
-constexpr size_t kPassMaskBytes = 2 * kPassRows * 32 * 4 + kPassRows * kMaxOk * 2;
+// interval ends (kPassRows * kMaxOk short2) and its (row, face) item table
+// (kPassRows * kMaxOk u16) of region_word_rows.
+constexpr size_t kPassMaskBytes = kPassRows * kMaxOk * 2;
 constexpr size_t kGlobalTierWarpSmem = kMaxOk * sizeof(FaceSetup) + kPassRows * kMaxOk * 4 + kPassMaskBytes;
 
 // Region phase over coverage words (every tier but the small one),
@@ -143,34 +142,49 @@ constexpr size_t kGlobalTierWarpSmem = kMaxOk * sizeof(FaceSetup) + kPassRows * 
 // interval (exact FP64 searches from the edges' guessed crossings,
 // face_interval_guess). A pass computes them for the (row, face) pairs whose
 // row the face spans, spread evenly over the lanes (the pairs listed in
-// `masks`' tail, face-major), and keeps them in `iv` (shared memory; empty
-// for the other pairs). Each interval is then OR-ed into the pass's
-// word masks in shared memory (`masks`): the union of the new faces (B) and
-// of the old faces (A). Because the state's count pc includes every old face
-// (pc >= A), the candidate's count pc - A + B is positive wherever B > 0,
-// and where B = 0 it is pc - A. So a sample flips iff it is newly covered (B
-// on a state-empty sample, from the state's coverage word alone) or it loses
-// its last faces (A without B, and pc equal to the number of old faces
-// covering it: the only samples whose state count is read, and whose old
-// faces are counted from the intervals). Lanes own (row, word) items, up to
-// eight each, whose coverage words are all loaded before any is used.
-// Flipped samples are written to the region words (candidate XOR state) and
-// counted into the popcount deltas against the reference. `clk` (profiling
-// only) accumulates SM cycles of the interval, mask and word steps and of
-// the lane's lost-sample counts.
+// `pairs`, face-major), and keeps them in `iv` (shared memory; empty for the
+// other pairs). Lanes then own (row, word) cells, up to eight each: a cell's
+// masks of the new faces (B) and of the old faces (A) are the OR of those
+// faces' intervals in its row. Because the state's count pc includes every
+// old face (pc >= A), the candidate's count pc - A + B is positive wherever
+// B > 0, and where B = 0 it is pc - A. So a sample flips iff it is newly
+// covered (B on a state-empty sample, from the state's coverage word alone)
+// or it loses its last faces (A without B, and pc equal to the number of old
+// faces covering it: the only samples whose state count is read, and whose
+// old faces are counted from the intervals). The cells' coverage words are
+// all loaded before any is used, and the next pass's rows are prefetched
+// into L2 while this one runs. Flipped samples are written to the region
+// words (candidate XOR state) and counted into the popcount deltas against
+// the reference. `clk` (profiling only) accumulates SM cycles of the
+// interval, mask and word steps and of the lane's lost-sample counts.
 __device__ void region_word_rows(const FaceSetup* faces, uint32_t nok, int wx0, int ry0, int ry1, int words,
                                  const PlanView& pv, uint32_t size, bool same_ref, uint32_t* region, short2* iv,
-                                 uint32_t* masks, int& dchg, int& dtot, int& dcov, int& flips, bool& negative,
+                                 uint16_t* pairs, int& dchg, int& dtot, int& dcov, int& flips, bool& negative,
                                  long long* clk) {
     const uint32_t lane = lane_id();
     long long t0 = clk ? clock64() : 0;
-    uint32_t* const bn = masks;                  // [kPassRows][32] new-face union
-    uint32_t* const an = masks + kPassRows * 32; // [kPassRows][32] old-face union
     static_assert(kPassRows == 8 && kMaxOk < 8192, "item = face << 3 | row");
-    uint16_t* const pairs = reinterpret_cast<uint16_t*>(masks + 2 * kPassRows * 32); // face << 3 | row
+    // bit f: face f is a new face (pad > 0), else an old one
+    const uint64_t new_faces = uint64_t(__ballot_sync(0xffffffffu, lane < nok && faces[lane].pad > 0)) |
+                               uint64_t(__ballot_sync(0xffffffffu, lane + 32 < nok && faces[lane + 32].pad > 0))
+                                   << 32;
+    // Prefetch (to L2) of the state and reference words of rows [y, y + 8):
+    // lanes 0-15 the state's, 16-31 the reference's, two per row (the lines
+    // of the region's first and last word in the row).
+    auto prefetch_rows = [&](int y) {
+        const int row = y + int((lane >> 1) & 7u);
+        const bool ref = lane >= 16;
+        if (row > ry1 || (ref && same_ref)) return;
+        const uint32_t* bits = ref ? pv.ref_bits : pv.state_bits;
+        const size_t first = (size_t(row) * size + size_t(wx0)) >> 5;
+        const uint32_t* at = bits + first + ((lane & 1u) ? size_t(words - 1) : 0);
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(at));
+    };
+    prefetch_rows(ry0);
     for (int ybase = ry0; ybase <= ry1; ybase += kPassRows) {
         const int ylast = min(ry1, ybase + kPassRows - 1);
         const uint32_t pass_rows = uint32_t(ylast - ybase + 1);
+        if (ybase + kPassRows <= ry1) prefetch_rows(ybase + kPassRows);
         // Rows of the pass that faces lane and lane + 32 span; their
         // exclusive prefix over faces numbers the pass's (row, face) items.
         auto first_row = [&](uint32_t f) { return max(faces[f].y0, ybase); };
@@ -211,40 +225,51 @@ __device__ void region_word_rows(const FaceSetup* faces, uint32_t nok, int wx0, 
         }
         for (int c0 = 0; c0 < words; c0 += 32) { // 32-word windows of wide regions
             const uint32_t cn = uint32_t(min(32, words - c0));
-            const int xc0 = wx0 + 32 * c0, xc1 = wx0 + 32 * (c0 + int(cn)) - 1;
-            for (uint32_t k = lane; k < 2 * kPassRows * 32; k += 32) masks[k] = 0;
-            __syncwarp();
-            for (uint32_t t = lane; t < items; t += 32) {
-                uint32_t f, r;
-                item(t, f, r);
-                const short2 e = iv[r * kMaxOk + f];
-                const int lo = max(int(e.x), xc0), hi = min(int(e.y), xc1);
-                if (lo > hi) continue;
-                uint32_t* dst = (faces[f].pad > 0 ? bn : an) + r * 32;
-                for (int w = (lo - xc0) >> 5; w <= (hi - xc0) >> 5; ++w) {
-                    const int xb = xc0 + 32 * w, a = max(lo, xb) - xb, z = min(hi, xb + 31) - xb;
-                    const uint32_t m = (z == 31 ? 0xffffffffu : ((2u << z) - 1u)) & ~((1u << a) - 1u);
-                    atomicOr(dst + w, m);
+            const int xc0 = wx0 + 32 * c0;
+            const uint32_t cells = pass_rows * cn;
+            // Each lane's cells (row r, word w): t = lane + 32k, up to eight.
+            // Their new-face (B) and old-face (A) masks come from the faces
+            // that span the rows of the cells of the same k (a ballot per
+            // k), each lane testing its own cell's word against the face's
+            // interval in its row.
+            uint32_t S[8], R[8], B[8], A[8];
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                B[k] = A[k] = 0;
+                if (32u * uint32_t(k) >= cells) continue;
+                const uint32_t t = lane + 32u * uint32_t(k);
+                const uint32_t r = t / cn, w = t - r * cn;
+                const int y_lo = ybase + int((32u * uint32_t(k)) / cn);
+                const int y_hi = min(ylast, ybase + int((32u * uint32_t(k) + 31u) / cn));
+                auto spans = [&](uint32_t f) { return f < nok && faces[f].y0 <= y_hi && faces[f].y1 >= y_lo; };
+                uint64_t act = uint64_t(__ballot_sync(0xffffffffu, spans(lane))) |
+                               uint64_t(__ballot_sync(0xffffffffu, spans(lane + 32))) << 32;
+                const int xb = xc0 + 32 * int(w);
+                while (act) {
+                    const uint32_t f = uint32_t(__ffsll((long long)act) - 1);
+                    act &= act - 1;
+                    if (t >= cells) continue;
+                    const short2 e = iv[r * kMaxOk + f];
+                    const int lo = max(int(e.x), xb) - xb, hi = min(int(e.y), xb + 31) - xb;
+                    if (lo > hi) continue;
+                    const uint32_t m = (hi == 31 ? 0xffffffffu : ((2u << hi) - 1u)) & ~((1u << lo) - 1u);
+                    if ((new_faces >> f) & 1u) B[k] |= m;
+                    else A[k] |= m;
                 }
             }
-            __syncwarp();
             if (clk) {
                 const long long t = clock64();
                 clk[1] += t - t0, t0 = t;
             }
-            const uint32_t cells = pass_rows * cn;
-            uint32_t S[8], R[8];
 #pragma unroll
             for (int k = 0; k < 8; ++k) {
                 const uint32_t t = lane + 32u * uint32_t(k);
                 S[k] = R[k] = 0;
-                if (t < cells) {
+                if (t < cells && (B[k] | A[k])) {
                     const uint32_t r = t / cn, w = t - r * cn;
-                    if (bn[r * 32 + w] | an[r * 32 + w]) {
-                        const uint32_t y = uint32_t(ybase) + r, cw = (uint32_t(xc0) >> 5) + w;
-                        S[k] = chunk_global(pv.state_bits, size, y, cw);
-                        R[k] = same_ref ? S[k] : chunk_global(pv.ref_bits, size, y, cw);
-                    }
+                    const uint32_t y = uint32_t(ybase) + r, cw = (uint32_t(xc0) >> 5) + w;
+                    S[k] = chunk_global(pv.state_bits, size, y, cw);
+                    R[k] = same_ref ? S[k] : chunk_global(pv.ref_bits, size, y, cw);
                 }
             }
 #pragma unroll
@@ -252,7 +277,7 @@ __device__ void region_word_rows(const FaceSetup* faces, uint32_t nok, int wx0, 
                 const uint32_t t = lane + 32u * uint32_t(k);
                 if (t >= cells) break;
                 const uint32_t r = t / cn, w = t - r * cn;
-                const uint32_t bnew = bn[r * 32 + w], aany = an[r * 32 + w];
+                const uint32_t bnew = B[k], aany = A[k];
                 uint32_t* out = region + (uint32_t(ybase) + r - uint32_t(ry0)) * uint32_t(words) + uint32_t(c0) + w;
                 if (!(bnew | aany)) {
                     *out = 0;
@@ -269,14 +294,14 @@ __device__ void region_word_rows(const FaceSetup* faces, uint32_t nok, int wx0, 
                     const int i = __ffs(lost_cand) - 1;
                     lost_cand &= lost_cand - 1;
                     const int x = xb + i;
-                    uint32_t A = 0; // old faces covering (x, y)
+                    uint32_t n_old = 0; // old faces covering (x, y)
                     for (uint32_t f = 0; f < nok; ++f) {
                         const short2 e = iv[r * kMaxOk + f];
-                        A += faces[f].pad < 0 && int(e.x) <= x && x <= int(e.y);
+                        n_old += !((new_faces >> f) & 1u) && int(e.x) <= x && x <= int(e.y);
                     }
                     const uint32_t pc = pv.state_count[size_t(y) * size + size_t(x)];
-                    negative |= pc < A;
-                    if (pc == A) lost |= 1u << i;
+                    negative |= pc < n_old;
+                    if (pc == n_old) lost |= 1u << i;
                 }
                 if (l0) clk[3] += clock64() - l0;
                 const uint32_t fl = grown | lost;
@@ -303,19 +328,19 @@ template <class L>
 __device__ void audit_unit(const CandidateRecord* __restrict__ rec, const PlanDev& plan, uint32_t v,
                            WarpScratch<L>& ws, ViewRecord* out, unsigned long long* stats, uint32_t u,
                            uint32_t* spill, uint32_t heavy = 0xffffffffu, FaceSetup* face_table = nullptr,
-                           short2* iv_table = nullptr, uint32_t* mask_table = nullptr) {
+                           short2* iv_table = nullptr, uint16_t* pair_table = nullptr) {
     // The face setups: in the warp's scratch, or in shared memory for the
     // tiers whose scratch is global (the row sweep reads them every row).
     FaceSetup* const faces = face_table ? face_table : ws.faces;
     // Every tier but the small one runs the region phase over coverage words
-    // (region_word_rows; its interval and mask tables in the warp's shared
+    // (region_word_rows; its interval and item tables in the warp's shared
     // memory: given by the global tiers, else the delta map's space) and the
     // distance phase walks the region words.
     constexpr bool word_rows = L::kWordRows;
     static_assert(!L::kWordRows || L::kDeltaSamples * sizeof(uint8_t) >= kPassRows * kMaxOk * 4 + kPassMaskBytes,
                   "the delta map's space holds the word-row tables");
     short2* const iv_rows = iv_table ? iv_table : reinterpret_cast<short2*>(ws.delta);
-    uint32_t* const mask_rows = mask_table ? mask_table : ws.delta + kPassRows * kMaxOk;
+    uint16_t* const pair_rows = pair_table ? pair_table : reinterpret_cast<uint16_t*>(ws.delta + kPassRows * kMaxOk);
     constexpr int kRegionWords = L::kRegionWords, kRegionRows = L::kRegionRows;
     constexpr int kDeltaSamples = L::kDeltaSamples, kQueue = L::kQueue, kAffected = L::kAffected;
     const uint32_t lane = lane_id();
@@ -499,7 +524,7 @@ __device__ void audit_unit(const CandidateRecord* __restrict__ rec, const PlanDe
                 }
             };
             if constexpr (word_rows) {
-                region_word_rows(faces, nok, wx0, ry0, ry1, words, pv, size, same_ref, ws.region, iv_rows, mask_rows,
+                region_word_rows(faces, nok, wx0, ry0, ry1, words, pv, size, same_ref, ws.region, iv_rows, pair_rows,
                                  dchg, dtot, dcov, flips, negative, stats ? wr_clk : nullptr);
             } else if (direct) {
                 const uint32_t delta_words = uint32_t(bws * bh) >> 2;
@@ -968,13 +993,13 @@ template <class L, int kWarps>
 __global__ void __launch_bounds__(kWarps * 32, 2)
     k_audit_global(const __grid_constant__ AuditJob job, unsigned long long* stats, const uint32_t* spill,
                    uint32_t* cursor, unsigned char* scratch, uint32_t* spill_next) {
-    // Dynamic shared memory, per warp: face setups, pass intervals, pass masks.
+    // Dynamic shared memory, per warp: face setups, pass intervals, pass items.
     extern __shared__ __align__(16) unsigned char global_tier_smem[];
     const uint32_t wslot = threadIdx.x >> 5;
     unsigned char* mine = global_tier_smem + size_t(wslot) * kGlobalTierWarpSmem;
     FaceSetup* face_table = reinterpret_cast<FaceSetup*>(mine);
     short2* iv_table = reinterpret_cast<short2*>(mine + kMaxOk * sizeof(FaceSetup));
-    uint32_t* mask_table = reinterpret_cast<uint32_t*>(mine + kMaxOk * sizeof(FaceSetup) + kPassRows * kMaxOk * 4);
+    uint16_t* pair_table = reinterpret_cast<uint16_t*>(mine + kMaxOk * sizeof(FaceSetup) + kPassRows * kMaxOk * 4);
     const uint32_t lane = lane_id();
     const uint32_t slot = blockIdx.x * kWarps + (threadIdx.x >> 5);
     WarpScratch<L>& ws = reinterpret_cast<WarpScratch<L>*>(scratch)[slot];
@@ -992,7 +1017,7 @@ __global__ void __launch_bounds__(kWarps * 32, 2)
         resolve_unit(job, u, plan, recs, out, lu);
         const uint32_t c = lu / plan->nviews, v = lu - c * plan->nviews;
         audit_unit(recs + c, *plan, v, ws, out + lu, stats, u, spill_next, 0xffffffffu,
-                   face_table, iv_table, mask_table);
+                   face_table, iv_table, pair_table);
     }
 }
 

@@ -181,24 +181,36 @@ BH void face_interval_at(const FaceSetup& s, double py, const int guess[3], int&
     const double ax3[3] = {s.dx, s.ex, s.ax}, ay3[3] = {s.dy, s.ey, s.ay};
     const double bx3[3] = {s.ex, s.ax, s.dx}, by3[3] = {s.ey, s.ay, s.dy};
     const double r3[3] = {s.r0, s.r1, s.r2};
-    lo = s.x0, hi = s.x1;
+    double t1[3], c[3];
+    bool prefix[3];
+    int last[3]; // per edge the last column whose test equals `prefix`: the boundary
+    bool settled[3];
+    // One column's test, the out-of-range columns as sentinels: left of the
+    // bbox a prefix is covered and a suffix is not, right of it the other
+    // way round.
+    auto ok = [&](int e, int x) {
+        const bool covered = !((t1[e] - c[e] * ((double(x) + .5) - ax3[e])) + r3[e] < 0);
+        return x < s.x0 ? prefix[e] : (x > s.x1 ? !prefix[e] : covered);
+    };
+    // The three columns around each guess, for all edges at once (no
+    // branches: independent tests); most boundaries are settled there.
 #pragma unroll
     for (int e = 0; e < 3; ++e) {
-        const double ax = ax3[e], ay = ay3[e], r = r3[e];
-        const double t1 = (bx3[e] - ax) * (py - ay), c = by3[e] - ay;
-        const bool prefix = c >= 0; // c == 0: every column or none
-        // One column's test, the out-of-range columns as sentinels: left of
-        // the bbox a prefix is covered and a suffix is not, right of it the
-        // other way round.
-        auto ok = [&](int x) {
-            if (x < s.x0) return prefix;
-            if (x > s.x1) return !prefix;
-            return !((t1 - c * ((double(x) + .5) - ax)) + r < 0);
-        };
+        t1[e] = (bx3[e] - ax3[e]) * (py - ay3[e]);
+        c[e] = by3[e] - ay3[e];
+        prefix[e] = c[e] >= 0; // c == 0: every column or none
+        const int g = guess[e] < s.x0 - 1 ? s.x0 - 1 : (guess[e] > s.x1 + 1 ? s.x1 + 1 : guess[e]);
+        const bool before = ok(e, g - 1) == prefix[e], at = ok(e, g) == prefix[e], after = ok(e, g + 1) == prefix[e];
+        settled[e] = (at && !after) || (!at && before);
+        last[e] = at ? g : g - 1;
+    }
+#pragma unroll
+    for (int e = 0; e < 3; ++e) {
+        if (settled[e]) continue;
         const int g = guess[e] < s.x0 - 1 ? s.x0 - 1 : (guess[e] > s.x1 + 1 ? s.x1 + 1 : guess[e]);
         // Bracket [a, b] with ok(a) == prefix and ok(b) != prefix, then bisect.
         int a, b;
-        if (ok(g) == prefix) {
+        if (ok(e, g) == prefix[e]) {
             a = g;
             for (int step = 1;; step *= 2) {
                 b = a + step;
@@ -206,7 +218,7 @@ BH void face_interval_at(const FaceSetup& s, double py, const int guess[3], int&
                     b = s.x1 + 1;
                     break;
                 }
-                if (ok(b) != prefix) break;
+                if (ok(e, b) != prefix[e]) break;
                 a = b;
             }
         } else {
@@ -217,17 +229,22 @@ BH void face_interval_at(const FaceSetup& s, double py, const int guess[3], int&
                     a = s.x0 - 1;
                     break;
                 }
-                if (ok(a) == prefix) break;
+                if (ok(e, a) == prefix[e]) break;
                 b = a;
             }
         }
         while (b - a > 1) {
             const int m = a + (b - a) / 2;
-            if (ok(m) == prefix) a = m;
+            if (ok(e, m) == prefix[e]) a = m;
             else b = m;
         }
-        if (prefix) hi = a < hi ? a : hi; // last covered
-        else lo = b > lo ? b : lo;        // first covered
+        last[e] = a;
+    }
+    lo = s.x0, hi = s.x1;
+#pragma unroll
+    for (int e = 0; e < 3; ++e) {
+        if (prefix[e]) hi = last[e] < hi ? last[e] : hi; // last covered
+        else lo = last[e] + 1 > lo ? last[e] + 1 : lo;   // first covered
     }
 }
 
