@@ -774,7 +774,8 @@ RIBBON_CHAIN = {"levels": 6, "base": 512.0, "last": 16.0, "curve": ((0.0, 1.0), 
                 "views": 256, "ss": 8, "batch": 64, "budget": 40, "memory_mib": 160_000}
 
 
-def run_chain(args, local: int, mesh, c: dict, preserve_uv: int = 0, label: str = "") -> dict:
+def run_chain(args, local: int, mesh, c: dict, preserve_uv: int = 0, label: str = "", model=None,
+              keep_permille: int = 0) -> dict:
     """One LOD chain (blitz_audit_chain: schedule, four gates per level,
     previous-level binding, batched executor, confirmation of every emitted
     level) of `mesh` under the chain settings `c`; wall clock around it."""
@@ -786,9 +787,11 @@ def run_chain(args, local: int, mesh, c: dict, preserve_uv: int = 0, label: str 
     # default 6 GiB workspace
     session = br.AuditSession(mesh, br.neural_options(device=local, preserve_uv=preserve_uv,
                                                       memory_mib=c.get("memory_mib", 6144)))
+    if model is not None:
+        session.attach_surrogate(model)
     settings = br.chain_settings(c["levels"], c["base"], c["last"], c["curve"], c["lod0"], (c["views"], 0, 0xB1172024),
-                                 (c["views"], 0, 0xB1172026), c["ss"], c["ss"], c["ss"], 1.0, c["batch"], 0,
-                                 c["budget"], 1)
+                                 (c["views"], 0, 0xB1172026), c["ss"], c["ss"], c["ss"], 1.0, c["batch"],
+                                 keep_permille, c["budget"], 1)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     levels, _ = session.chain(settings, meshes=False)
@@ -834,14 +837,97 @@ def run_rock_1m(args, local: int) -> dict:
     return out
 
 
+def ribbon_first_level_gates(c: dict):
+    """The four gates of the chain's first level: its screen (the schedule's
+    second size), 1 px LOD0 and transition bounds, the chain's search and
+    audit views."""
+    import blitzremesher_b200 as br
+
+    px = c["base"] * (c["last"] / c["base"]) ** (1.0 / (c["levels"] - 1))
+    search, audit = (c["views"], 0, 0xB1172024), (c["views"], 0, 0xB1172026)
+    return px, [br.eval_settings(px, 1.0, search, c["ss"], c["ss"], 1.0),
+                br.eval_settings(px, 1.0, search, c["ss"], c["ss"], 1.0),
+                br.eval_settings(px, 1.0, audit, c["ss"], c["ss"], 1.0),
+                br.eval_settings(px, 1.0, audit, c["ss"], c["ss"], 1.0)]
+
+
+def ribbon_surrogate(args, local: int, mesh, c: dict, sample: int = 8192):
+    """The thin-structure figures beyond the plain chain: the share of the
+    source's legal collapses that the exact audit rejects at the first
+    level's gates (an evenly spaced sample), and a surrogate trained on exact
+    verdicts of four smaller ribbon meshes (250 cards each, other seeds) at
+    the same gates: its false-reject rate when it keeps the top 25% of the
+    sample. Returns (figures, model)."""
+    import torch
+
+    import blitzremesher_b200 as br
+    from blitzremesher_b200 import surrogate_train as st
+    from blitzremesher_b200 import synthetic as syn
+
+    px, gates = ribbon_first_level_gates(c)
+    opts = br.neural_options(device=local, preserve_uv=0, memory_mib=c.get("memory_mib", 6144))
+
+    def labelled(m):
+        with br.AuditSession(m, opts) as s:
+            feats, cols = s.surrogate_features(px, px)
+            v = s.candidates(cols, gates)
+        lab = np.zeros((cols.size, 2), np.float32)
+        lab[:, 0] = v["accepted"]
+        lab[:, 1] = np.where(v["accepted"] == 1, 0.0, st.ERROR_CAP)  # verdict-only labels
+        return feats, torch.from_numpy(lab).cuda(), v
+
+    t0 = time.perf_counter()
+    parts = [labelled(syn.ribbons(250, seed=100 + k)) for k in range(4)]
+    label_s = time.perf_counter() - t0
+    train = st.LabelSet(torch.cat([p[0] for p in parts]), torch.cat([p[1] for p in parts]),
+                        np.concatenate([np.full(p[1].shape[0], k, np.int32) for k, p in enumerate(parts)]),
+                        [{} for _ in parts])
+    model = br.Surrogate(seed=1, device=local)
+    t0 = time.perf_counter()
+    history = st.fit(model, train)
+    fit_s = time.perf_counter() - t0
+    # the workload mesh: an evenly spaced sample of its legal collapses
+    with br.AuditSession(mesh, opts) as s:
+        f_all, cols = s.surrogate_features(px, px)
+        pick = np.linspace(0, cols.size - 1, min(sample, cols.size)).astype(np.int64)
+        t0 = time.perf_counter()
+        v = s.candidates(cols[pick], gates)
+        audit_s = time.perf_counter() - t0
+        feats = f_all[torch.from_numpy(pick).cuda()].contiguous()
+    lab = np.zeros((pick.size, 2), np.float32)
+    lab[:, 0] = v["accepted"]
+    held = st.LabelSet(feats, torch.from_numpy(lab).cuda(), np.zeros(pick.size, np.int32), [{}])
+    return {"level_gates": f"{px:g} px, LOD0 and transition bounds 1 px, {c['views']} search and {c['views']} audit "
+                           f"views, ss {c['ss']}",
+            "legal_collapses": int(cols.size), "sample": int(pick.size),
+            "exact_reject_share": float(1.0 - v["accepted"].mean()), "sample_audit_s": audit_s,
+            "surrogate": {"train": "exact verdicts of every legal collapse of 4 ribbon meshes of 250 cards "
+                                   "(seeds 100-103) at the same gates",
+                          "train_rows": int(train.features.shape[0]), "label_s": label_s, "fit_s": fit_s,
+                          "loss": history, "keep": 0.25, "pruning": st.pruning_stats(model, held)}}, model
+
+
 def run_ribbons(args, local: int) -> dict:
     """The thin-structure workload: 2,000 two-sided ribbon cards (400k faces),
-    256 views at 512 px, 6-level chain."""
+    256 views at 512 px, 6-level chain; with the share of collapses the exact
+    audit rejects, the surrogate's false-reject rate, and the chain with the
+    surrogate keeping the top 25% of each ranking (its triangle-count gap to
+    the plain chain)."""
     from blitzremesher_b200 import synthetic as syn
 
     mesh = syn.ribbons(2000, seed=5)
-    out = run_chain(args, local, mesh, RIBBON_CHAIN, 0, f"2,000 ribbon cards ({mesh.face_count} faces), two-sided")
+    label = f"2,000 ribbon cards ({mesh.face_count} faces), two-sided"
+    out = run_chain(args, local, mesh, RIBBON_CHAIN, 0, label)
     out["note"] = f"trial budget {RIBBON_CHAIN['budget']} batches of up to 64 collapses per level"
+    if not args.no_surrogate:
+        stress, model = ribbon_surrogate(args, local, mesh, RIBBON_CHAIN)
+        pruned = run_chain(args, local, mesh, RIBBON_CHAIN, 0, label, model=model, keep_permille=250)
+        plain_faces, pruned_faces = out["levels"][-1]["faces"], pruned["levels"][-1]["faces"]
+        stress["chain_with_surrogate"] = {"seconds": pruned["seconds"], "all_confirmed": pruned["all_confirmed"],
+                                          "faces_per_level": [l["faces"] for l in pruned["levels"]],
+                                          "triangle_gap": (pruned_faces - plain_faces) / plain_faces,
+                                          "speedup_vs_plain": out["seconds"] / pruned["seconds"]}
+        out["stress"] = stress
     return out
 
 

@@ -634,16 +634,23 @@ static void ensure_tile_data(Session& S, Plan& p) {
                      S.scratch.sv.p, S.scratch.sn.p, S.scratch.sd.p, st);
 }
 
-// Views per refresh launch so that the chunk's field scratch (row distances,
-// envelope stacks, the field itself: 28 bytes a sample) stays within 256 MiB;
-// sizes the scratch for it.
+// Views per refresh launch whose field scratch (row distances, envelope
+// stacks, the field itself: 28 bytes a sample) fits the budget below; sizes
+// the scratch for it.
 static uint32_t field_chunk(Session& S, const Plan& p) {
     const size_t samples = size_t(p.size) * p.size;
-    const uint32_t chunk =
-        uint32_t(std::max<size_t>(1, std::min<size_t>(p.views, (size_t(256) << 20) / (samples * 28))));
     Scratch& x = S.scratch;
+    // An eighth of the workspace (at least 256 MiB), at most half of what is
+    // free (counting the scratch held now): at 4160 x 4160 samples a view
+    // needs 485 MB, and one view per launch leaves most SMs idle.
+    const size_t floor_bytes = size_t(256) << 20;
+    const size_t room = S.pool.limit - S.pool.used + x.view_entries * 28;
+    const size_t budget = std::max(floor_bytes, std::min(S.pool.limit / 8, room / 2));
+    const uint32_t chunk = uint32_t(std::max<size_t>(1, std::min<size_t>(p.views, budget / (samples * 28))));
     const size_t entries = samples * chunk;
     if (x.view_entries < entries) {
+        x.vg.release(), x.vfield.release(), x.vsv.release(), x.vsn.release(), x.vsd.release();
+        x.view_entries = 0;
         x.vg = Buf<uint32_t>(S.pool, entries);
         x.vfield = Buf<uint32_t>(S.pool, entries);
         x.vsv = Buf<int32_t>(S.pool, entries);
