@@ -830,10 +830,15 @@ def run_rock_1m(args, local: int) -> dict:
     6-octave ridged noise, 8 UV charts, uv preserved), 128 views, 1024 -> 32 px."""
     from blitzremesher_b200 import synthetic as syn
 
-    mesh = syn.rock(8, 3)
-    label = f"rock: icosphere level 8 ({mesh.face_count} faces), 6-octave ridged noise, 8 UV charts, preserve_uv"
-    out = run_chain(args, local, mesh, ROCK_1M_CHAIN, 1, label)
-    out["note"] = f"trial budget {ROCK_1M_CHAIN['budget']} batches of up to 64 collapses per level"
+    level = args.rock_level
+    mesh = syn.rock(level, 3)
+    c = dict(ROCK_1M_CHAIN)
+    if args.chain_budget:
+        c["budget"] = args.chain_budget
+    label = (f"rock: icosphere level {level} ({mesh.face_count} faces), 6-octave ridged noise, 8 UV charts, "
+             f"preserve_uv" + ("" if level == 8 and not args.chain_budget else " (not the workload: smaller case)"))
+    out = run_chain(args, local, mesh, c, 1, label)
+    out["note"] = f"trial budget {c['budget']} batches of up to 64 collapses per level"
     return out
 
 
@@ -985,6 +990,10 @@ def main() -> None:
     ap.add_argument("--no-icosphere", action="store_true")
     ap.add_argument("--no-rock", action="store_true")
     ap.add_argument("--meshes", type=int, default=BATCH_MESHES, help="meshes of the batched set (64 = the workload)")
+    ap.add_argument("--rock-level", type=int, default=8,
+                    help="icosphere level of the rock1m chain's mesh (8 = the workload, 1.31 M faces)")
+    ap.add_argument("--chain-budget", type=int, default=0,
+                    help="trials per level of the rock1m chain (0 = the workload's 40)")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

@@ -151,6 +151,11 @@ void launch_refresh_views(const DevMesh& m, const Camera* cams_dev, uint32_t nvi
                           unsigned long long* pop, const uint32_t* ref_field, uint32_t* state_field, uint32_t* g,
                           int32_t* sv, long long* sn, long long* sd, int32_t* t1, int32_t* t2, bool saturate,
                           cudaStream_t s);
+// Tile maxima and popcounts of already computed state views against another
+// reference (the last stages of launch_refresh_views).
+void launch_compare_views(uint32_t nviews, uint32_t size, const uint32_t* state_bits, const uint32_t* ref_bits,
+                          uint32_t wstride, const uint32_t* ref_field, const uint32_t* state_field, int32_t* t1,
+                          int32_t* t2, unsigned long long* pop, cudaStream_t s);
 // Per view, the max of t1 and of t2 over its tiles: out[2v], out[2v+1].
 void launch_view_maxima(const int32_t* t1, const int32_t* t2, uint32_t tiles, uint32_t nviews, int32_t* out,
                         cudaStream_t s);

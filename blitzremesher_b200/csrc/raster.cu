@@ -444,6 +444,23 @@ void launch_refresh_views(const DevMesh& m, const Camera* cams_dev, uint32_t nvi
                                                                words, pop);
 }
 
+// The last stages of launch_refresh_views against another reference, for
+// views whose state coverage (state_bits) and field (state_field) are
+// already computed: tile maxima and popcounts.
+void launch_compare_views(uint32_t nviews, uint32_t size, const uint32_t* state_bits, const uint32_t* ref_bits,
+                          uint32_t wstride, const uint32_t* ref_field, const uint32_t* state_field, int32_t* t1,
+                          int32_t* t2, unsigned long long* pop, cudaStream_t s) {
+    const size_t samples = size_t(size) * size;
+    const uint32_t words = uint32_t((samples + 63) / 64) * 2;
+    const uint32_t tiles = ((size + 31) / 32) * ((size + 31) / 32);
+    k_tile_maxima_views<<<dim3(tiles, nviews), 32, 0, s>>>(ref_bits, state_bits, wstride, ref_field, state_field, size,
+                                                           t1, t2);
+    cudaMemsetAsync(pop, 0, 32 * size_t(nviews), s);
+    uint32_t grid = blocks_for(words);
+    if (grid > 64) grid = 64;
+    k_popcounts_views<<<dim3(grid, nviews), kThreads, 0, s>>>(ref_bits, state_bits, wstride, words, pop);
+}
+
 namespace {
 // Per view: max over its 32x32 tiles of t1 and t2 (-1 when no tile has a sample).
 __global__ void k_view_maxima(const int32_t* t1, const int32_t* t2, uint32_t tiles, int32_t* out) {

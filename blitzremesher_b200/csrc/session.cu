@@ -1323,22 +1323,49 @@ static void trial_views(Session& S, Plan& p, const DevMesh& cand, uint64_t tag) 
     cudaStream_t st = S.stream;
     const size_t samples = size_t(p.size) * p.size, cstride = count_stride(samples);
     const uint32_t tiles = ((p.size + 31) / 32) * ((p.size + 31) / 32);
-    if (!p.trial_count.p) {
-        p.trial_count = Buf<uint8_t>(S.pool, cstride * p.views);
-        p.trial_bits = Buf<uint32_t>(S.pool, size_t(p.words) * p.views);
-        B200_CUDA(cudaMemsetAsync(p.trial_bits.p, 0, size_t(p.words) * p.views * 4, st));
-        p.trial_state = Buf<uint32_t>(S.pool, 4 * size_t(p.views));
-        p.trial_t1 = Buf<int32_t>(S.pool, size_t(tiles) * p.views);
-        p.trial_t2 = Buf<int32_t>(S.pool, size_t(tiles) * p.views);
-        p.trial_max = Buf<int32_t>(S.pool, 2 * size_t(p.views));
-        p.trial_pop = Buf<unsigned long long>(S.pool, 4 * size_t(p.views));
-        p.trial_hstate.assign(4 * size_t(p.views), 0);
-        p.trial_hpop.assign(4 * size_t(p.views), 0);
-        p.trial_hmax.assign(2 * size_t(p.views), 0);
-    }
+    auto ensure_trial = [&](Plan& q) {
+        if (q.trial_count.p) return;
+        q.trial_count = Buf<uint8_t>(S.pool, cstride * q.views);
+        q.trial_bits = Buf<uint32_t>(S.pool, size_t(q.words) * q.views);
+        B200_CUDA(cudaMemsetAsync(q.trial_bits.p, 0, size_t(q.words) * q.views * 4, st));
+        q.trial_state = Buf<uint32_t>(S.pool, 4 * size_t(q.views));
+        q.trial_t1 = Buf<int32_t>(S.pool, size_t(tiles) * q.views);
+        q.trial_t2 = Buf<int32_t>(S.pool, size_t(tiles) * q.views);
+        q.trial_max = Buf<int32_t>(S.pool, 2 * size_t(q.views));
+        q.trial_pop = Buf<unsigned long long>(S.pool, 4 * size_t(q.views));
+        q.trial_hstate.assign(4 * size_t(q.views), 0);
+        q.trial_hpop.assign(4 * size_t(q.views), 0);
+        q.trial_hmax.assign(2 * size_t(q.views), 0);
+    };
+    ensure_trial(p);
     ensure_tile_data(S, p);
+    // Plans of the same views (cameras, screen, supersample, sides) against
+    // the other reference: the trial's counts, coverage and field are the
+    // same, so they take copies and only their tile maxima and popcounts
+    // against their own reference are computed.
+    std::vector<Plan*> same_views;
+    for (auto& kv : S.plans) {
+        Plan& q = *kv.second;
+        const PlanKey &a = q.key, &b = p.key;
+        if (&q == &p || q.resource_limited || !q.tiled || q.trial_tag == tag || a.reference == b.reference ||
+            a.ortho != b.ortho || a.persp != b.persp || a.seed != b.seed || a.screen != b.screen || a.ss != b.ss ||
+            a.force_two != b.force_two || q.size != p.size || q.views != p.views)
+            continue;
+        ensure_trial(q);
+        ensure_tile_data(S, q);
+        same_views.push_back(&q);
+    }
     const uint32_t chunk = field_chunk(S, p);
     Scratch& x = S.scratch;
+    auto read_back = [&](Plan& q) {
+        launch_view_maxima(q.trial_t1.p, q.trial_t2.p, tiles, q.views, q.trial_max.p, st);
+        B200_CUDA(cudaMemcpyAsync(q.trial_hpop.data(), q.trial_pop.p, q.trial_hpop.size() * 8, cudaMemcpyDeviceToHost,
+                                  st));
+        B200_CUDA(cudaMemcpyAsync(q.trial_hstate.data(), q.trial_state.p, q.trial_hstate.size() * 4,
+                                  cudaMemcpyDeviceToHost, st));
+        B200_CUDA(cudaMemcpyAsync(q.trial_hmax.data(), q.trial_max.p, q.trial_hmax.size() * 4, cudaMemcpyDeviceToHost,
+                                  st));
+    };
     for (bool saturate : {false, true}) { // as in refresh_state: counts held at 255 on overflow
         for (uint32_t v0 = 0; v0 < p.views; v0 += chunk) {
             const uint32_t n = std::min(chunk, p.views - v0);
@@ -1348,14 +1375,20 @@ static void trial_views(Session& S, Plan& p, const DevMesh& cand, uint64_t tag) 
                                  p.trial_bits.p + w0, p.ref_bits.p + w0, p.words, p.trial_pop.p + 4 * v0,
                                  p.ref_field.p + s0, x.vfield.p, x.vg.p, x.vsv.p, x.vsn.p, x.vsd.p,
                                  p.trial_t1.p + t0, p.trial_t2.p + t0, saturate, st);
+            for (Plan* q : same_views) {
+                B200_CUDA(cudaMemcpyAsync(q->trial_count.p + cstride * v0, p.trial_count.p + cstride * v0,
+                                          cstride * n, cudaMemcpyDeviceToDevice, st));
+                B200_CUDA(cudaMemcpyAsync(q->trial_bits.p + w0, p.trial_bits.p + w0, size_t(p.words) * n * 4,
+                                          cudaMemcpyDeviceToDevice, st));
+                B200_CUDA(cudaMemcpyAsync(q->trial_state.p + 4 * v0, p.trial_state.p + 4 * v0, 16 * size_t(n),
+                                          cudaMemcpyDeviceToDevice, st));
+                launch_compare_views(n, p.size, p.trial_bits.p + w0, q->ref_bits.p + w0, p.words, q->ref_field.p + s0,
+                                     x.vfield.p, q->trial_t1.p + t0, q->trial_t2.p + t0, q->trial_pop.p + 4 * v0,
+                                     st);
+            }
         }
-        launch_view_maxima(p.trial_t1.p, p.trial_t2.p, tiles, p.views, p.trial_max.p, st);
-        B200_CUDA(cudaMemcpyAsync(p.trial_hpop.data(), p.trial_pop.p, p.trial_hpop.size() * 8, cudaMemcpyDeviceToHost,
-                                  st));
-        B200_CUDA(cudaMemcpyAsync(p.trial_hstate.data(), p.trial_state.p, p.trial_hstate.size() * 4,
-                                  cudaMemcpyDeviceToHost, st));
-        B200_CUDA(cudaMemcpyAsync(p.trial_hmax.data(), p.trial_max.p, p.trial_hmax.size() * 4, cudaMemcpyDeviceToHost,
-                                  st));
+        read_back(p);
+        for (Plan* q : same_views) read_back(*q);
         B200_CUDA(cudaStreamSynchronize(st));
         B200_CUDA(cudaGetLastError());
         bool overflow = false;
@@ -1363,7 +1396,8 @@ static void trial_views(Session& S, Plan& p, const DevMesh& cand, uint64_t tag) 
         if (!overflow) break;
     }
     p.trial_tag = tag;
-    S.profile.launches += 8;
+    for (Plan* q : same_views) q->trial_tag = tag;
+    S.profile.launches += 8 + 6 * same_views.size();
 }
 
 // evaluate_impl (evaluate.cpp:312-352) over the per-view data of trial_views.
