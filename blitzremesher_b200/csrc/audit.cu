@@ -131,19 +131,21 @@ __device__ __forceinline__ void record_write(ViewRecord* out, const ViewRecord& 
 
 // Rows of interval ends kept per pass of the word-row region phase.
 constexpr int kPassRows = 8; // a pass's row fits 3 bits of the (row, face) item table
-// Shared memory of one warp of the global tiers: face setups, the pass's
-// interval ends (kPassRows * kMaxOk short2) and its (row, face) item table
-// (kPassRows * kMaxOk u16) of region_word_rows.
-constexpr size_t kPassMaskBytes = kPassRows * kMaxOk * 2;
-constexpr size_t kGlobalTierWarpSmem = kMaxOk * sizeof(FaceSetup) + kPassRows * kMaxOk * 4 + kPassMaskBytes;
+// Tables of region_word_rows after its interval ends (kPassRows * kMaxOk
+// short2): the pass's (row, face) items (kPassRows * kMaxOk u16) and the
+// faces' edge crossing lines (kMaxOk * 6 floats).
+constexpr size_t kPassTableBytes = kPassRows * kMaxOk * 2 + kMaxOk * 6 * 4;
+// Shared memory of one warp of the global tiers: face setups, interval ends
+// and the tables above.
+constexpr size_t kGlobalTierWarpSmem = kMaxOk * sizeof(FaceSetup) + kPassRows * kMaxOk * 4 + kPassTableBytes;
 
 // Region phase over coverage words (every tier but the small one),
 // kPassRows rows at a time. Per (row, face) the covered samples are one
-// interval (exact FP64 searches from the edges' guessed crossings,
-// face_interval_guess). A pass computes them for the (row, face) pairs whose
-// row the face spans, spread evenly over the lanes (the pairs listed in
-// `pairs`, face-major), and keeps them in `iv` (shared memory; empty for the
-// other pairs). Lanes then own (row, word) cells, up to eight each: a cell's
+// interval (exact FP64 searches from guesses on each edge's crossing line,
+// face_interval_lines; the lines in `pairs`' tail). A pass computes them for
+// the (row, face) pairs whose row the face spans, spread evenly over the
+// lanes (the pairs listed in `pairs`, face-major), and keeps them in `iv`
+// (shared memory; empty for the other pairs). Lanes then own (row, word) cells, up to eight each: a cell's
 // masks of the new faces (B) and of the old faces (A) are the OR of those
 // faces' intervals in its row. Because the state's count pc includes every
 // old face (pc >= A), the candidate's count pc - A + B is positive wherever
@@ -164,6 +166,8 @@ __device__ void region_word_rows(const FaceSetup* faces, uint32_t nok, int wx0, 
     const uint32_t lane = lane_id();
     long long t0 = clk ? clock64() : 0;
     static_assert(kPassRows == 8 && kMaxOk < 8192, "item = face << 3 | row");
+    float* const lines = reinterpret_cast<float*>(pairs + kPassRows * kMaxOk); // [kMaxOk][6]: k[3], m[3]
+    for (uint32_t f = lane; f < nok; f += 32) face_crossing_lines(faces[f], lines + 6 * f, lines + 6 * f + 3);
     // bit f: face f is a new face (pad > 0), else an old one
     const uint64_t new_faces = uint64_t(__ballot_sync(0xffffffffu, lane < nok && faces[lane].pad > 0)) |
                                uint64_t(__ballot_sync(0xffffffffu, lane + 32 < nok && faces[lane + 32].pad > 0))
@@ -215,7 +219,7 @@ __device__ void region_word_rows(const FaceSetup* faces, uint32_t nok, int wx0, 
             uint32_t f, r;
             item(t, f, r);
             int lo, hi;
-            face_interval_guess(faces[f], double(ybase + int(r)) + .5, lo, hi);
+            face_interval_lines(faces[f], double(ybase + int(r)) + .5, lines + 6 * f, lines + 6 * f + 3, lo, hi);
             iv[r * kMaxOk + f] = make_short2(short(lo), short(hi));
         }
         __syncwarp();
@@ -337,7 +341,7 @@ __device__ void audit_unit(const CandidateRecord* __restrict__ rec, const PlanDe
     // memory: given by the global tiers, else the delta map's space) and the
     // distance phase walks the region words.
     constexpr bool word_rows = L::kWordRows;
-    static_assert(!L::kWordRows || L::kDeltaSamples * sizeof(uint8_t) >= kPassRows * kMaxOk * 4 + kPassMaskBytes,
+    static_assert(!L::kWordRows || L::kDeltaSamples * sizeof(uint8_t) >= kPassRows * kMaxOk * 4 + kPassTableBytes,
                   "the delta map's space holds the word-row tables");
     short2* const iv_rows = iv_table ? iv_table : reinterpret_cast<short2*>(ws.delta);
     uint16_t* const pair_rows = pair_table ? pair_table : reinterpret_cast<uint16_t*>(ws.delta + kPassRows * kMaxOk);

@@ -188,10 +188,12 @@ BH void face_interval_at(const FaceSetup& s, double py, const int guess[3], int&
     // One column's test, the out-of-range columns as sentinels: left of the
     // bbox a prefix is covered and a suffix is not, right of it the other
     // way round.
-    auto ok = [&](int e, int x) {
-        const bool covered = !((t1[e] - c[e] * ((double(x) + .5) - ax3[e])) + r3[e] < 0);
+    // (px = double(x) + 1/2, exact, as evaluate.cpp's sample centre)
+    auto ok_at = [&](int e, int x, double px) {
+        const bool covered = !((t1[e] - c[e] * (px - ax3[e])) + r3[e] < 0);
         return x < s.x0 ? prefix[e] : (x > s.x1 ? !prefix[e] : covered);
     };
+    auto ok = [&](int e, int x) { return ok_at(e, x, double(x) + .5); };
     // The three columns around each guess, for all edges at once (no
     // branches: independent tests); most boundaries are settled there.
 #pragma unroll
@@ -200,7 +202,9 @@ BH void face_interval_at(const FaceSetup& s, double py, const int guess[3], int&
         c[e] = by3[e] - ay3[e];
         prefix[e] = c[e] >= 0; // c == 0: every column or none
         const int g = guess[e] < s.x0 - 1 ? s.x0 - 1 : (guess[e] > s.x1 + 1 ? s.x1 + 1 : guess[e]);
-        const bool before = ok(e, g - 1) == prefix[e], at = ok(e, g) == prefix[e], after = ok(e, g + 1) == prefix[e];
+        const double pg = double(g) + .5; // g - 1 and g + 1 are pg -/+ 1, exactly
+        const bool before = ok_at(e, g - 1, pg - 1.0) == prefix[e], at = ok_at(e, g, pg) == prefix[e],
+                   after = ok_at(e, g + 1, pg + 1.0) == prefix[e];
         settled[e] = (at && !after) || (!at && before);
         last[e] = at ? g : g - 1;
     }
@@ -269,6 +273,38 @@ BH void face_interval_guess(const FaceSetup& s, double py, int& lo, int& hi) {
         xs = fmaxf(xs, float(s.x0 - 1));
         xs = fminf(xs, float(s.x1 + 1));
         guess[e] = c == 0 ? s.x0 : (c > 0 ? int(floorf(xs)) : int(ceilf(xs)));
+    }
+    face_interval_at(s, py, guess, lo, hi);
+}
+
+// The crossing of each edge as a line in the row centre py:
+// x* = k py + m with k = (bx - ax) / c and m = (r - (bx - ax) ay) / c + ax -
+// 1/2, in single precision, once per face (k = 0, m = NaN for c = 0).
+BH void face_crossing_lines(const FaceSetup& s, float k[3], float m[3]) {
+    const double ax3[3] = {s.dx, s.ex, s.ax}, ay3[3] = {s.dy, s.ey, s.ay};
+    const double bx3[3] = {s.ex, s.ax, s.dx}, by3[3] = {s.ey, s.ay, s.dy};
+    const double r3[3] = {s.r0, s.r1, s.r2};
+#pragma unroll
+    for (int e = 0; e < 3; ++e) {
+        const double c = by3[e] - ay3[e], dx = bx3[e] - ax3[e];
+        k[e] = c == 0 ? 0.f : float(dx / c);
+        m[e] = c == 0 ? NAN : float((r3[e] - dx * ay3[e]) / c + ax3[e] - .5);
+    }
+}
+
+// face_interval_at with the guesses read off the crossing lines of
+// face_crossing_lines: one multiply-add per edge and row.
+BH void face_interval_lines(const FaceSetup& s, double py, const float k[3], const float m[3], int& lo, int& hi) {
+    const double ay3[3] = {s.dy, s.ey, s.ay}, by3[3] = {s.ey, s.ay, s.dy};
+    const float pyf = float(py);
+    int guess[3];
+#pragma unroll
+    for (int e = 0; e < 3; ++e) {
+        const double c = by3[e] - ay3[e];
+        float xs = k[e] * pyf + m[e];
+        xs = fmaxf(xs, float(s.x0 - 1)); // NaN clamps to the left sentinel
+        xs = fminf(xs, float(s.x1 + 1));
+        guess[e] = c > 0 ? int(floorf(xs)) : int(ceilf(xs));
     }
     face_interval_at(s, py, guess, lo, hi);
 }
