@@ -132,9 +132,10 @@ __device__ __forceinline__ void record_write(ViewRecord* out, const ViewRecord& 
 // Rows of interval ends kept per pass of the word-row region phase.
 constexpr int kPassRows = 8; // a pass's row fits 3 bits of the (row, face) item table
 // Tables of region_word_rows after its interval ends (kPassRows * kMaxOk
-// short2): the pass's (row, face) items (kPassRows * kMaxOk u16) and the
-// faces' edge crossing lines (kMaxOk * 6 floats).
-constexpr size_t kPassTableBytes = kPassRows * kMaxOk * 2 + kMaxOk * 6 * 4;
+// short2): the pass's (row, face) items (kPassRows * kMaxOk u16), the
+// faces' edge crossing lines (kMaxOk * 6 floats) and the pass's word masks
+// of the new and of the old faces (2 * kPassRows * 32 u32).
+constexpr size_t kPassTableBytes = kPassRows * kMaxOk * 2 + kMaxOk * 6 * 4 + 2 * kPassRows * 32 * 4;
 // Shared memory of one warp of the global tiers: face setups, interval ends
 // and the tables above.
 constexpr size_t kGlobalTierWarpSmem = kMaxOk * sizeof(FaceSetup) + kPassRows * kMaxOk * 4 + kPassTableBytes;
@@ -145,20 +146,21 @@ constexpr size_t kGlobalTierWarpSmem = kMaxOk * sizeof(FaceSetup) + kPassRows * 
 // face_interval_lines; the lines in `pairs`' tail). A pass computes them for
 // the (row, face) pairs whose row the face spans, spread evenly over the
 // lanes (the pairs listed in `pairs`, face-major), and keeps them in `iv`
-// (shared memory; empty for the other pairs). Lanes then own (row, word) cells, up to eight each: a cell's
-// masks of the new faces (B) and of the old faces (A) are the OR of those
-// faces' intervals in its row. Because the state's count pc includes every
-// old face (pc >= A), the candidate's count pc - A + B is positive wherever
-// B > 0, and where B = 0 it is pc - A. So a sample flips iff it is newly
-// covered (B on a state-empty sample, from the state's coverage word alone)
-// or it loses its last faces (A without B, and pc equal to the number of old
-// faces covering it: the only samples whose state count is read, and whose
-// old faces are counted from the intervals). The cells' coverage words are
-// all loaded before any is used, and the next pass's rows are prefetched
-// into L2 while this one runs. Flipped samples are written to the region
-// words (candidate XOR state) and counted into the popcount deltas against
-// the reference. `clk` (profiling only) accumulates SM cycles of the
-// interval, mask and word steps and of the lane's lost-sample counts.
+// (shared memory; empty for the other pairs). Each interval is then OR-ed
+// into the pass's word masks in shared memory: the union of the new faces
+// (B) and of the old faces (A); lanes own (row, word) cells, up to eight
+// each. Because the state's count pc includes every old face (pc >= A), the
+// candidate's count pc - A + B is positive wherever B > 0, and where B = 0
+// it is pc - A. So a sample flips iff it is newly covered (B on a
+// state-empty sample, from the state's coverage word alone) or it loses its
+// last faces (A without B, and pc equal to the number of old faces covering
+// it: the only samples whose state count is read, and whose old faces are
+// counted from the intervals). The cells' coverage words are all loaded
+// before any is used, and the next pass's rows are prefetched into L2 while
+// this one runs. Flipped samples are written to the region words (candidate
+// XOR state) and counted into the popcount deltas against the reference.
+// `clk` (profiling only) accumulates SM cycles of the interval, mask and
+// word steps and of the lane's lost-sample counts.
 __device__ void region_word_rows(const FaceSetup* faces, uint32_t nok, int wx0, int ry0, int ry1, int words,
                                  const PlanView& pv, uint32_t size, bool same_ref, uint32_t* region, short2* iv,
                                  uint16_t* pairs, int& dchg, int& dtot, int& dcov, int& flips, bool& negative,
@@ -167,6 +169,8 @@ __device__ void region_word_rows(const FaceSetup* faces, uint32_t nok, int wx0, 
     long long t0 = clk ? clock64() : 0;
     static_assert(kPassRows == 8 && kMaxOk < 8192, "item = face << 3 | row");
     float* const lines = reinterpret_cast<float*>(pairs + kPassRows * kMaxOk); // [kMaxOk][6]: k[3], m[3]
+    uint32_t* const bn = reinterpret_cast<uint32_t*>(lines + 6 * kMaxOk); // [kPassRows][32] new-face union
+    uint32_t* const an = bn + kPassRows * 32;                             // [kPassRows][32] old-face union
     for (uint32_t f = lane; f < nok; f += 32) face_crossing_lines(faces[f], lines + 6 * f, lines + 6 * f + 3);
     // bit f: face f is a new face (pad > 0), else an old one
     const uint64_t new_faces = uint64_t(__ballot_sync(0xffffffffu, lane < nok && faces[lane].pad > 0)) |
@@ -231,34 +235,33 @@ __device__ void region_word_rows(const FaceSetup* faces, uint32_t nok, int wx0, 
             const uint32_t cn = uint32_t(min(32, words - c0));
             const int xc0 = wx0 + 32 * c0;
             const uint32_t cells = pass_rows * cn;
-            // Each lane's cells (row r, word w): t = lane + 32k, up to eight.
-            // Their new-face (B) and old-face (A) masks come from the faces
-            // that span the rows of the cells of the same k (a ballot per
-            // k), each lane testing its own cell's word against the face's
-            // interval in its row.
+            // The pass's word masks: every (row, face) interval OR-ed into
+            // the words it spans, then each lane's cells (row r, word w:
+            // t = lane + 32k, up to eight) read theirs.
+            const int xc1 = wx0 + 32 * (c0 + int(cn)) - 1;
+            for (uint32_t k = lane; k < 2 * kPassRows * 32; k += 32) bn[k] = 0;
+            __syncwarp();
+            for (uint32_t t = lane; t < items; t += 32) {
+                uint32_t f, r;
+                item(t, f, r);
+                const short2 e = iv[r * kMaxOk + f];
+                const int lo = max(int(e.x), xc0), hi = min(int(e.y), xc1);
+                if (lo > hi) continue;
+                uint32_t* dst = (((new_faces >> f) & 1u) ? bn : an) + r * 32;
+                for (int w = (lo - xc0) >> 5; w <= (hi - xc0) >> 5; ++w) {
+                    const int xb = xc0 + 32 * w, a = max(lo, xb) - xb, z = min(hi, xb + 31) - xb;
+                    atomicOr(dst + w, (z == 31 ? 0xffffffffu : ((2u << z) - 1u)) & ~((1u << a) - 1u));
+                }
+            }
+            __syncwarp();
             uint32_t S[8], R[8], B[8], A[8];
 #pragma unroll
             for (int k = 0; k < 8; ++k) {
-                B[k] = A[k] = 0;
-                if (32u * uint32_t(k) >= cells) continue;
                 const uint32_t t = lane + 32u * uint32_t(k);
-                const uint32_t r = t / cn, w = t - r * cn;
-                const int y_lo = ybase + int((32u * uint32_t(k)) / cn);
-                const int y_hi = min(ylast, ybase + int((32u * uint32_t(k) + 31u) / cn));
-                auto spans = [&](uint32_t f) { return f < nok && faces[f].y0 <= y_hi && faces[f].y1 >= y_lo; };
-                uint64_t act = uint64_t(__ballot_sync(0xffffffffu, spans(lane))) |
-                               uint64_t(__ballot_sync(0xffffffffu, spans(lane + 32))) << 32;
-                const int xb = xc0 + 32 * int(w);
-                while (act) {
-                    const uint32_t f = uint32_t(__ffsll((long long)act) - 1);
-                    act &= act - 1;
-                    if (t >= cells) continue;
-                    const short2 e = iv[r * kMaxOk + f];
-                    const int lo = max(int(e.x), xb) - xb, hi = min(int(e.y), xb + 31) - xb;
-                    if (lo > hi) continue;
-                    const uint32_t m = (hi == 31 ? 0xffffffffu : ((2u << hi) - 1u)) & ~((1u << lo) - 1u);
-                    if ((new_faces >> f) & 1u) B[k] |= m;
-                    else A[k] |= m;
+                B[k] = A[k] = 0;
+                if (t < cells) {
+                    const uint32_t r = t / cn, w = t - r * cn;
+                    B[k] = bn[r * 32 + w], A[k] = an[r * 32 + w];
                 }
             }
             if (clk) {
