@@ -172,10 +172,6 @@ __device__ void region_word_rows(const FaceSetup* faces, uint32_t nok, int wx0, 
     uint32_t* const bn = reinterpret_cast<uint32_t*>(lines + 6 * kMaxOk); // [kPassRows][32] new-face union
     uint32_t* const an = bn + kPassRows * 32;                             // [kPassRows][32] old-face union
     for (uint32_t f = lane; f < nok; f += 32) face_crossing_lines(faces[f], lines + 6 * f, lines + 6 * f + 3);
-    // bit f: face f is a new face (pad > 0), else an old one
-    const uint64_t new_faces = uint64_t(__ballot_sync(0xffffffffu, lane < nok && faces[lane].pad > 0)) |
-                               uint64_t(__ballot_sync(0xffffffffu, lane + 32 < nok && faces[lane + 32].pad > 0))
-                                   << 32;
     // Prefetch (to L2) of the state and reference words of rows [y, y + 8):
     // lanes 0-15 the state's, 16-31 the reference's, two per row (the lines
     // of the region's first and last word in the row).
@@ -236,8 +232,8 @@ __device__ void region_word_rows(const FaceSetup* faces, uint32_t nok, int wx0, 
             const int xc0 = wx0 + 32 * c0;
             const uint32_t cells = pass_rows * cn;
             // The pass's word masks: every (row, face) interval OR-ed into
-            // the words it spans, then each lane's cells (row r, word w:
-            // t = lane + 32k, up to eight) read theirs.
+            // the words it spans; lanes then own (row, word) cells:
+            // t = lane + 32k, up to eight.
             const int xc1 = wx0 + 32 * (c0 + int(cn)) - 1;
             for (uint32_t k = lane; k < 2 * kPassRows * 32; k += 32) bn[k] = 0;
             __syncwarp();
@@ -247,36 +243,29 @@ __device__ void region_word_rows(const FaceSetup* faces, uint32_t nok, int wx0, 
                 const short2 e = iv[r * kMaxOk + f];
                 const int lo = max(int(e.x), xc0), hi = min(int(e.y), xc1);
                 if (lo > hi) continue;
-                uint32_t* dst = (((new_faces >> f) & 1u) ? bn : an) + r * 32;
+                uint32_t* dst = (faces[f].pad > 0 ? bn : an) + r * 32;
                 for (int w = (lo - xc0) >> 5; w <= (hi - xc0) >> 5; ++w) {
                     const int xb = xc0 + 32 * w, a = max(lo, xb) - xb, z = min(hi, xb + 31) - xb;
                     atomicOr(dst + w, (z == 31 ? 0xffffffffu : ((2u << z) - 1u)) & ~((1u << a) - 1u));
                 }
             }
             __syncwarp();
-            uint32_t S[8], R[8], B[8], A[8];
-#pragma unroll
-            for (int k = 0; k < 8; ++k) {
-                const uint32_t t = lane + 32u * uint32_t(k);
-                B[k] = A[k] = 0;
-                if (t < cells) {
-                    const uint32_t r = t / cn, w = t - r * cn;
-                    B[k] = bn[r * 32 + w], A[k] = an[r * 32 + w];
-                }
-            }
             if (clk) {
                 const long long t = clock64();
                 clk[1] += t - t0, t0 = t;
             }
+            uint32_t S[8], R[8];
 #pragma unroll
             for (int k = 0; k < 8; ++k) {
                 const uint32_t t = lane + 32u * uint32_t(k);
                 S[k] = R[k] = 0;
-                if (t < cells && (B[k] | A[k])) {
+                if (t < cells) {
                     const uint32_t r = t / cn, w = t - r * cn;
-                    const uint32_t y = uint32_t(ybase) + r, cw = (uint32_t(xc0) >> 5) + w;
-                    S[k] = chunk_global(pv.state_bits, size, y, cw);
-                    R[k] = same_ref ? S[k] : chunk_global(pv.ref_bits, size, y, cw);
+                    if (bn[r * 32 + w] | an[r * 32 + w]) {
+                        const uint32_t y = uint32_t(ybase) + r, cw = (uint32_t(xc0) >> 5) + w;
+                        S[k] = chunk_global(pv.state_bits, size, y, cw);
+                        R[k] = same_ref ? S[k] : chunk_global(pv.ref_bits, size, y, cw);
+                    }
                 }
             }
 #pragma unroll
@@ -284,7 +273,7 @@ __device__ void region_word_rows(const FaceSetup* faces, uint32_t nok, int wx0, 
                 const uint32_t t = lane + 32u * uint32_t(k);
                 if (t >= cells) break;
                 const uint32_t r = t / cn, w = t - r * cn;
-                const uint32_t bnew = B[k], aany = A[k];
+                const uint32_t bnew = bn[r * 32 + w], aany = an[r * 32 + w];
                 uint32_t* out = region + (uint32_t(ybase) + r - uint32_t(ry0)) * uint32_t(words) + uint32_t(c0) + w;
                 if (!(bnew | aany)) {
                     *out = 0;
@@ -304,7 +293,7 @@ __device__ void region_word_rows(const FaceSetup* faces, uint32_t nok, int wx0, 
                     uint32_t n_old = 0; // old faces covering (x, y)
                     for (uint32_t f = 0; f < nok; ++f) {
                         const short2 e = iv[r * kMaxOk + f];
-                        n_old += !((new_faces >> f) & 1u) && int(e.x) <= x && x <= int(e.y);
+                        n_old += faces[f].pad < 0 && int(e.x) <= x && x <= int(e.y);
                     }
                     const uint32_t pc = pv.state_count[size_t(y) * size + size_t(x)];
                     negative |= pc < n_old;
