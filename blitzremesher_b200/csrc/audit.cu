@@ -132,18 +132,17 @@ __device__ __forceinline__ void record_write(ViewRecord* out, const ViewRecord& 
 // Rows of interval ends kept per pass of the word-row region phase.
 constexpr int kPassRows = 8; // a pass's row fits 3 bits of the (row, face) item table
 // Tables of region_word_rows after its interval ends (kPassRows * kMaxOk
-// short2): the pass's (row, face) items (kPassRows * kMaxOk u16), the
-// faces' edge crossing lines (kMaxOk * 6 floats) and the pass's word masks
-// of the new and of the old faces (2 * kPassRows * 32 u32).
-constexpr size_t kPassTableBytes = kPassRows * kMaxOk * 2 + kMaxOk * 6 * 4 + 2 * kPassRows * 32 * 4;
+// short2): the pass's (row, face) items (kPassRows * kMaxOk u16) and its
+// word masks of the new and of the old faces (2 * kPassRows * 32 u32).
+constexpr size_t kPassTableBytes = kPassRows * kMaxOk * 2 + 2 * kPassRows * 32 * 4;
 // Shared memory of one warp of the global tiers: face setups, interval ends
 // and the tables above.
 constexpr size_t kGlobalTierWarpSmem = kMaxOk * sizeof(FaceSetup) + kPassRows * kMaxOk * 4 + kPassTableBytes;
 
 // Region phase over coverage words (every tier but the small one),
 // kPassRows rows at a time. Per (row, face) the covered samples are one
-// interval (exact FP64 searches from guesses on each edge's crossing line,
-// face_interval_lines; the lines in `pairs`' tail). A pass computes them for
+// interval (exact FP64 searches from a single-precision guess of each
+// edge's crossing, face_interval_guess). A pass computes them for
 // the (row, face) pairs whose row the face spans, spread evenly over the
 // lanes (the pairs listed in `pairs`, face-major), and keeps them in `iv`
 // (shared memory; empty for the other pairs). Each interval is then OR-ed
@@ -168,10 +167,8 @@ __device__ void region_word_rows(const FaceSetup* faces, uint32_t nok, int wx0, 
     const uint32_t lane = lane_id();
     long long t0 = clk ? clock64() : 0;
     static_assert(kPassRows == 8 && kMaxOk < 8192, "item = face << 3 | row");
-    float* const lines = reinterpret_cast<float*>(pairs + kPassRows * kMaxOk); // [kMaxOk][6]: k[3], m[3]
-    uint32_t* const bn = reinterpret_cast<uint32_t*>(lines + 6 * kMaxOk); // [kPassRows][32] new-face union
-    uint32_t* const an = bn + kPassRows * 32;                             // [kPassRows][32] old-face union
-    for (uint32_t f = lane; f < nok; f += 32) face_crossing_lines(faces[f], lines + 6 * f, lines + 6 * f + 3);
+    uint32_t* const bn = reinterpret_cast<uint32_t*>(pairs + kPassRows * kMaxOk); // [kPassRows][32] new-face union
+    uint32_t* const an = bn + kPassRows * 32;                                      // [kPassRows][32] old-face union
     // Prefetch (to L2) of the state and reference words of rows [y, y + 8):
     // lanes 0-15 the state's, 16-31 the reference's, two per row (the lines
     // of the region's first and last word in the row).
@@ -219,7 +216,7 @@ __device__ void region_word_rows(const FaceSetup* faces, uint32_t nok, int wx0, 
             uint32_t f, r;
             item(t, f, r);
             int lo, hi;
-            face_interval_lines(faces[f], double(ybase + int(r)) + .5, lines + 6 * f, lines + 6 * f + 3, lo, hi);
+            face_interval_guess(faces[f], double(ybase + int(r)) + .5, lo, hi);
             iv[r * kMaxOk + f] = make_short2(short(lo), short(hi));
         }
         __syncwarp();
@@ -986,7 +983,7 @@ __global__ void __launch_bounds__(kLargeWarps * 32, 1)
 // own slot of global scratch (`scratch`, one WarpScratch<L> per resident
 // warp); what overflows goes to `spill_next` (may be null).
 template <class L, int kWarps>
-__global__ void __launch_bounds__(kWarps * 32, 2)
+__global__ void __launch_bounds__(kWarps * 32, 3)
     k_audit_global(const __grid_constant__ AuditJob job, unsigned long long* stats, const uint32_t* spill,
                    uint32_t* cursor, unsigned char* scratch, uint32_t* spill_next) {
     // Dynamic shared memory, per warp: face setups, pass intervals, pass items.

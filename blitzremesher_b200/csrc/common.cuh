@@ -277,38 +277,6 @@ BH void face_interval_guess(const FaceSetup& s, double py, int& lo, int& hi) {
     face_interval_at(s, py, guess, lo, hi);
 }
 
-// The crossing of each edge as a line in the row centre py:
-// x* = k py + m with k = (bx - ax) / c and m = (r - (bx - ax) ay) / c + ax -
-// 1/2, in single precision, once per face (k = 0, m = NaN for c = 0).
-BH void face_crossing_lines(const FaceSetup& s, float k[3], float m[3]) {
-    const double ax3[3] = {s.dx, s.ex, s.ax}, ay3[3] = {s.dy, s.ey, s.ay};
-    const double bx3[3] = {s.ex, s.ax, s.dx}, by3[3] = {s.ey, s.ay, s.dy};
-    const double r3[3] = {s.r0, s.r1, s.r2};
-#pragma unroll
-    for (int e = 0; e < 3; ++e) {
-        const double c = by3[e] - ay3[e], dx = bx3[e] - ax3[e];
-        k[e] = c == 0 ? 0.f : float(dx / c);
-        m[e] = c == 0 ? NAN : float((r3[e] - dx * ay3[e]) / c + ax3[e] - .5);
-    }
-}
-
-// face_interval_at with the guesses read off the crossing lines of
-// face_crossing_lines: one multiply-add per edge and row.
-BH void face_interval_lines(const FaceSetup& s, double py, const float k[3], const float m[3], int& lo, int& hi) {
-    const double ay3[3] = {s.dy, s.ey, s.ay}, by3[3] = {s.ey, s.ay, s.dy};
-    const float pyf = float(py);
-    int guess[3];
-#pragma unroll
-    for (int e = 0; e < 3; ++e) {
-        const double c = by3[e] - ay3[e];
-        float xs = k[e] * pyf + m[e];
-        xs = fmaxf(xs, float(s.x0 - 1)); // NaN clamps to the left sentinel
-        xs = fminf(xs, float(s.x1 + 1));
-        guess[e] = c > 0 ? int(floorf(xs)) : int(ceilf(xs));
-    }
-    face_interval_at(s, py, guess, lo, hi);
-}
-
 // CPU float value of the field where the exact distance reaches 2^24: the
 // row pass rounds g^2 to float, the column pass rounds (dy^2 + f) to float;
 // the lower envelope of the reference picks the smallest such value. `g`:

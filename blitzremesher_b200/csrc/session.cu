@@ -2646,7 +2646,7 @@ static void batch_candidates(blitz_audit_batch* b, const blitz_collapse* cands, 
         if (big && !b->huge.p) {
             int sms = 148;
             B200_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device));
-            b->huge_blocks = uint32_t(std::max(1, 2 * sms));
+            b->huge_blocks = uint32_t(std::max(1, 3 * sms));
             b->huge = Buf<unsigned char>(b->pool, audit_huge_scratch_bytes(b->huge_blocks));
         }
         if (big) b->spill_huge.ensure(b->pool, max_units + 1);

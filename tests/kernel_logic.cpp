@@ -73,10 +73,6 @@ int main() {
             face_interval_guess(s, double(y) + .5, glo, ghi);
             const bool empty = lo > hi;
             ok = ok && (empty ? glo > ghi : (glo == lo && ghi == hi));
-            float lk[3], lm[3];
-            face_crossing_lines(s, lk, lm);
-            face_interval_lines(s, double(y) + .5, lk, lm, glo, ghi);
-            ok = ok && (empty ? glo > ghi : (glo == lo && ghi == hi));
             int guess[3];
             const int span_x = s.x1 - s.x0 + 3;
             for (int e = 0; e < 3; ++e)
