@@ -151,6 +151,10 @@ void launch_refresh_views(const DevMesh& m, const Camera* cams_dev, uint32_t nvi
                           unsigned long long* pop, const uint32_t* ref_field, uint32_t* state_field, uint32_t* g,
                           int32_t* sv, long long* sn, long long* sd, int32_t* t1, int32_t* t2, bool saturate,
                           cudaStream_t s);
+// Exact squared distance fields of nviews masks at once (launch_field's row
+// pass and column envelope; scratch g, sv, sn, sd of size^2 * nviews).
+void launch_fields_views(const uint32_t* bits, uint32_t wstride, uint32_t nviews, uint32_t size, uint32_t* g,
+                         uint32_t* field, int32_t* sv, long long* sn, long long* sd, cudaStream_t s);
 // Tile maxima and popcounts of already computed state views against another
 // reference (the last stages of launch_refresh_views).
 void launch_compare_views(uint32_t nviews, uint32_t size, const uint32_t* state_bits, const uint32_t* ref_bits,

@@ -444,6 +444,15 @@ void launch_refresh_views(const DevMesh& m, const Camera* cams_dev, uint32_t nvi
                                                                words, pop);
 }
 
+// Exact squared distance fields of `nviews` masks (view v's coverage at
+// bits + wstride * v, its field at field + size^2 * v): the row pass and the
+// column envelope of launch_field for all of them in two launches.
+void launch_fields_views(const uint32_t* bits, uint32_t wstride, uint32_t nviews, uint32_t size, uint32_t* g,
+                         uint32_t* field, int32_t* sv, long long* sn, long long* sd, cudaStream_t s) {
+    k_row_nearest_views<<<dim3(blocks_for(uint64_t(size) * 32, 128), nviews), 128, 0, s>>>(bits, wstride, size, g);
+    k_column_envelope_views<<<dim3(blocks_for(size, 64), nviews), 64, 0, s>>>(g, size, field, sv, sn, sd);
+}
+
 // The last stages of launch_refresh_views against another reference, for
 // views whose state coverage (state_bits) and field (state_field) are
 // already computed: tile maxima and popcounts.

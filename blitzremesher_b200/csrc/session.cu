@@ -452,6 +452,7 @@ struct Session {
     Buf<const ViewRecord*> record_table;
     Buf<uint32_t> plan_views, plan_ss;
     Buf<GateDev> gate_table;
+    Buf<int32_t> view_maxima; // per view max t1 / t2 of a plan (chain confirmation)
     // exact path and commits
     DeviceMesh trial;
     Buf<uint32_t> trial_keep, trial_offsets;
@@ -616,6 +617,7 @@ static void ensure_scratch(Session& S, uint32_t size);
 
 static size_t count_stride(size_t samples) { return (samples + 3) & ~size_t(3); }
 
+static uint32_t field_chunk(Session& S, const Plan& p);
 // The reference's exact distance field and the tile-maxima arrays of a plan,
 // built the first time its state differs from the reference.
 static void ensure_tile_data(Session& S, Plan& p) {
@@ -629,9 +631,12 @@ static void ensure_tile_data(Session& S, Plan& p) {
     p.t2 = Buf<int32_t>(S.pool, size_t(tiles) * p.views);
     B200_CUDA(cudaMemsetAsync(p.t1.p, 0xff, size_t(tiles) * p.views * 4, st));
     B200_CUDA(cudaMemsetAsync(p.t2.p, 0xff, size_t(tiles) * p.views * 4, st));
-    for (uint32_t v = 0; v < p.views; ++v)
-        launch_field(p.ref_bits.p + size_t(p.words) * v, p.size, p.size, S.scratch.g.p, p.ref_field.p + samples * v,
-                     S.scratch.sv.p, S.scratch.sn.p, S.scratch.sd.p, st);
+    // many views per launch (the field chunk's scratch)
+    const uint32_t chunk = field_chunk(S, p);
+    Scratch& x = S.scratch;
+    for (uint32_t v0 = 0; v0 < p.views; v0 += chunk)
+        launch_fields_views(p.ref_bits.p + size_t(p.words) * v0, p.words, std::min(chunk, p.views - v0), p.size,
+                            x.vg.p, p.ref_field.p + samples * v0, x.vsv.p, x.vsn.p, x.vsd.p, st);
 }
 
 // Views per refresh launch whose field scratch (row distances, envelope
@@ -2844,6 +2849,37 @@ blitz_status blitz_audit_batch_read_info(const blitz_audit_batch* b, blitz_audit
     return BLITZ_OK;
 }
 
+// Per-view records of the session's state against a plan's reference, read
+// from the plan's resident state data (popcounts, clip counts, tile maxima;
+// the plan is refreshed first if the state moved on), for evaluate_full: the
+// confirmation of a level redraws no raster. Views with clipping or a
+// distance of 2^24 or more carry a flag, so evaluate_full redraws them.
+static std::vector<ViewRecord> plan_state_records(Session& S, Plan& p) {
+    std::vector<ViewRecord> recs(p.views);
+    std::vector<int32_t> maxima(2 * size_t(p.views), -1);
+    if (!p.state_is_ref && p.t1.p) {
+        const uint32_t tiles = ((p.size + 31) / 32) * ((p.size + 31) / 32);
+        S.view_maxima.ensure(S.pool, 2 * size_t(p.views));
+        launch_view_maxima(p.t1.p, p.t2.p, tiles, p.views, S.view_maxima.p, S.stream);
+        B200_CUDA(cudaMemcpyAsync(maxima.data(), S.view_maxima.p, maxima.size() * 4, cudaMemcpyDeviceToHost,
+                                  S.stream));
+        B200_CUDA(cudaStreamSynchronize(S.stream));
+    }
+    for (uint32_t v = 0; v < p.views; ++v) {
+        ViewRecord& r = recs[v];
+        r = ViewRecord{};
+        r.changed = uint32_t(p.hpop[4 * v]);
+        r.total = uint32_t(p.hpop[4 * v + 1]);
+        r.ca = p.hpop[4 * v + 2] > 0;
+        r.cb = p.hpop[4 * v + 3] > 0;
+        r.flags = uint8_t((p.hviews[v].clipped_ref ? kRecClippedRef : 0) | (p.hstate[4 * v + 2] ? kRecClippedCand : 0));
+        const int32_t m = std::max(std::max(maxima[2 * v], maxima[2 * v + 1]), 0);
+        if (r.changed && r.ca && r.cb) r.max_d2 = uint32_t(m);
+        if (r.max_d2 >= kExactLimit) r.flags |= kRecLarge;
+    }
+    return recs;
+}
+
 // ---------------------------------------------------------------------------
 // LOD chain: schedule, per-level executor and confirmation.
 namespace {
@@ -3048,8 +3084,15 @@ blitz_status blitz_audit_chain(blitz_audit_session* s, const blitz_chain_setting
             DevMesh state = S.state.view;
             state.nf = S.state_faces;
             const DevMesh& prev = S.previous_is_source ? S.source.view : S.previous.view;
-            const Measurement ms = evaluate_full(S, S.source.view, state, &gates[2], refs[2].g);
-            const Measurement mt = evaluate_full(S, prev, state, &gates[3], refs[3].g);
+            // the audit plans hold the state's data against both references
+            auto records = [&](int gi) {
+                Plan& p = plan_for(S, keys[gi]);
+                return p.resource_limited || !p.tiled ? std::vector<ViewRecord>() : plan_state_records(S, p);
+            };
+            const std::vector<ViewRecord> rs = records(2), rt = records(3);
+            const Measurement ms = evaluate_full(S, S.source.view, state, &gates[2], refs[2].g,
+                                                 rs.empty() ? nullptr : rs.data());
+            const Measurement mt = evaluate_full(S, prev, state, &gates[3], refs[3].g, rt.empty() ? nullptr : rt.data());
             B200_CUDA(cudaStreamSynchronize(S.stream));
             if (out) {
                 blitz_chain_level& l = out[level - 1];

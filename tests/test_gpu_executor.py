@@ -244,10 +244,21 @@ def test_chain_matches_oracle(gpu_lib, oracle, batch):
     with br.AuditSession(mesh) as s:
         levels, meshes = s.chain(settings)
     assert len(levels) == 3 and len(meshes) == 3
-    for lv, (idx, pos), w in zip(levels, meshes, want):
+    p, t, b = oracle.schedule(48.0, 12.0, 4, [v for xy in curve for v in xy], 2.0)
+    bounds = oracle.bounds(mesh)
+    prev = mesh
+    for i, (lv, (idx, pos), w) in enumerate(zip(levels, meshes, want), start=1):
         assert lv["trials"] == w["trials"] and lv["stop_reason"] == w["stop"]
         assert np.array_equal(idx, w["indices"]) and np.array_equal(pos, w["positions"])
         assert lv["confirmed"] == 1
+        # the confirmation's Measurements (from the audit plans' resident
+        # data) equal the oracle's full evaluation of the emitted level
+        level = syn.Mesh(pos, idx)
+        src = oracle.evaluate(mesh, level, bounds, oracle_settings(p[i], b[i], audit, 4, 4, 1.0))
+        trn = oracle.evaluate(prev, level, bounds, oracle_settings(p[i], t[i], audit, 4, 4, 1.0))
+        assert measurement_fields(lv["source_audit"]) == measurement_fields(src), i
+        assert measurement_fields(lv["transition_audit"]) == measurement_fields(trn), i
+        prev = level
     assert levels[-1]["faces"] < levels[0]["faces"] < mesh.face_count
 
 
