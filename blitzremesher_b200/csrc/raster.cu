@@ -8,6 +8,7 @@
 // equals the exact integer squared distance below 2^24; above it the float
 // rounding of the two separable passes is reproduced.
 #include "kernels.cuh"
+#include "nearest.cuh"
 
 namespace b200 {
 namespace {
@@ -293,6 +294,49 @@ __device__ void tile_maxima_body(const uint32_t* ref_bits, const uint32_t* state
     }
     if (lane == 0) t1[tile] = m1, t2[tile] = m2;
 }
+// A packed coverage mask (bit i = sample i = y * size + x of a linear bit
+// stream) read 32 columns at a time, for nearest_d2.
+struct StreamMask {
+    const uint32_t* bits;
+    uint32_t size;
+    __device__ uint32_t chunk(uint32_t row, uint32_t c) const {
+        const size_t b = size_t(row) * size + size_t(c) * 32;
+        const uint32_t sh = uint32_t(b & 31);
+        const size_t w = b >> 5;
+        uint32_t v = bits[w];
+        if (sh) v = (v >> sh) | (bits[w + 1] << (32 - sh)); // the mask's padding word keeps this in bounds
+        const uint32_t rem = size - c * 32;
+        return rem >= 32 ? v : v & ((1u << rem) - 1u);
+    }
+};
+// tile_maxima_body without the state's field: t2 takes each reference-only
+// sample's exact squared distance to the state's nearest covered sample by
+// the outward search (the value the field holds there; kNone, as the field's
+// empty value, clamps the same way).
+__device__ void tile_maxima_search_body(const uint32_t* ref_bits, const uint32_t* state_bits,
+                                        const uint32_t* ref_field, uint32_t size, uint32_t tile, int32_t* t1,
+                                        int32_t* t2) {
+    const uint32_t tiles_x = (size + 31) / 32;
+    const uint32_t lane = threadIdx.x;
+    const uint32_t tx = tile % tiles_x, ty = tile / tiles_x;
+    const uint32_t x = tx * 32 + lane;
+    const StreamMask state{state_bits, size};
+    int32_t m1 = -1, m2 = -1;
+    if (x < size)
+        for (uint32_t r = 0; r < 32; ++r) {
+            const uint32_t y = ty * 32 + r;
+            if (y >= size) break;
+            const size_t i = size_t(y) * size + x;
+            const bool p = bit_at(state_bits, i), q = bit_at(ref_bits, i);
+            if (p && !q) m1 = max(m1, int32_t(min(ref_field[i], 0x7fffffffu)));
+            if (q && !p) m2 = max(m2, int32_t(min(nearest_d2(state, x, y), 0x7fffffffu)));
+        }
+    for (int o = 16; o; o >>= 1) {
+        m1 = max(m1, __shfl_xor_sync(0xffffffffu, m1, o));
+        m2 = max(m2, __shfl_xor_sync(0xffffffffu, m2, o));
+    }
+    if (lane == 0) t1[tile] = m1, t2[tile] = m2;
+}
 // ---- all views of a plan in one launch (blockIdx.y = view) ----
 struct ViewsArgs {
     DevMesh m;
@@ -372,6 +416,13 @@ __global__ void k_tile_maxima_views(const uint32_t* ref_bits, const uint32_t* st
     tile_maxima_body(ref_bits + size_t(wstride) * v, state_bits + size_t(wstride) * v, ref_field + samples * v,
                      state_field + samples * v, size, blockIdx.x, t1 + size_t(tiles) * v, t2 + size_t(tiles) * v);
 }
+__global__ void k_tile_maxima_search_views(const uint32_t* ref_bits, const uint32_t* state_bits, uint32_t wstride,
+                                           const uint32_t* ref_field, uint32_t size, int32_t* t1, int32_t* t2) {
+    const uint32_t v = blockIdx.y, tiles_x = (size + 31) / 32, tiles = tiles_x * tiles_x;
+    const size_t samples = size_t(size) * size;
+    tile_maxima_search_body(ref_bits + size_t(wstride) * v, state_bits + size_t(wstride) * v, ref_field + samples * v,
+                            size, blockIdx.x, t1 + size_t(tiles) * v, t2 + size_t(tiles) * v);
+}
 __global__ void k_popcounts_views(const uint32_t* a, const uint32_t* b, uint32_t wstride, uint32_t words,
                                   unsigned long long* out) {
     const uint32_t v = blockIdx.y;
@@ -403,7 +454,9 @@ __global__ void k_popcounts_views(const uint32_t* a, const uint32_t* b, uint32_t
 
 // The state data of all views of a plan, refreshed in a handful of launches:
 // counts (and clipped/overflow counters), coverage words, popcounts against the
-// reference and, when fields are kept, the state field and tile maxima.
+// reference and, when fields are kept, the tile maxima: from the state field
+// when `state_field` is given, else (ref_field, t1, t2 given) by searches
+// from the reference-only samples.
 void launch_refresh_views(const DevMesh& m, const Camera* cams_dev, uint32_t nviews, const float* center, uint32_t ss,
                           uint32_t size, bool force_two, uint8_t* counts, size_t cstride, uint32_t* state,
                           uint32_t* state_bits, const uint32_t* ref_bits, uint32_t wstride,
@@ -435,6 +488,11 @@ void launch_refresh_views(const DevMesh& m, const Camera* cams_dev, uint32_t nvi
             const uint32_t tiles = ((size + 31) / 32) * ((size + 31) / 32);
             k_tile_maxima_views<<<dim3(tiles, nviews), 32, 0, s>>>(ref_bits, state_bits, wstride, ref_field,
                                                                    state_field, size, t1, t2);
+        } else if (ref_field && t1 && t2) {
+            // no state field: t2 by searches from the reference-only samples
+            const uint32_t tiles = ((size + 31) / 32) * ((size + 31) / 32);
+            k_tile_maxima_search_views<<<dim3(tiles, nviews), 32, 0, s>>>(ref_bits, state_bits, wstride, ref_field,
+                                                                          size, t1, t2);
         }
     }
     cudaMemsetAsync(pop, 0, 32 * size_t(nviews), s);
@@ -454,16 +512,21 @@ void launch_fields_views(const uint32_t* bits, uint32_t wstride, uint32_t nviews
 }
 
 // The last stages of launch_refresh_views against another reference, for
-// views whose state coverage (state_bits) and field (state_field) are
-// already computed: tile maxima and popcounts.
+// views whose state coverage (state_bits) and, optionally, field
+// (state_field; null: t2 by searches) are already computed: tile maxima and
+// popcounts.
 void launch_compare_views(uint32_t nviews, uint32_t size, const uint32_t* state_bits, const uint32_t* ref_bits,
                           uint32_t wstride, const uint32_t* ref_field, const uint32_t* state_field, int32_t* t1,
                           int32_t* t2, unsigned long long* pop, cudaStream_t s) {
     const size_t samples = size_t(size) * size;
     const uint32_t words = uint32_t((samples + 63) / 64) * 2;
     const uint32_t tiles = ((size + 31) / 32) * ((size + 31) / 32);
-    k_tile_maxima_views<<<dim3(tiles, nviews), 32, 0, s>>>(ref_bits, state_bits, wstride, ref_field, state_field, size,
-                                                           t1, t2);
+    if (state_field)
+        k_tile_maxima_views<<<dim3(tiles, nviews), 32, 0, s>>>(ref_bits, state_bits, wstride, ref_field, state_field,
+                                                               size, t1, t2);
+    else
+        k_tile_maxima_search_views<<<dim3(tiles, nviews), 32, 0, s>>>(ref_bits, state_bits, wstride, ref_field, size,
+                                                                      t1, t2);
     cudaMemsetAsync(pop, 0, 32 * size_t(nviews), s);
     uint32_t grid = blocks_for(words);
     if (grid > 64) grid = 64;

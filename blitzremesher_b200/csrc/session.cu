@@ -693,7 +693,9 @@ static void refresh_state(Session& S, Plan& p) {
     const uint32_t tiles = ((p.size + 31) / 32) * ((p.size + 31) / 32);
     if (fields) ensure_tile_data(S, p);
     // Views per launch: the field scratch of one chunk stays within 256 MiB.
-    const uint32_t chunk = fields ? field_chunk(S, p) : p.views;
+    // tile maxima by searches from the reference-only samples: no state
+    // field, all views in one launch
+    const uint32_t chunk = p.views;
     std::vector<unsigned long long>& hpop = p.hpop;
     std::vector<uint32_t>& hstate = p.hstate;
     // Counts of up to 255 faces per sample; a plan with more is rebuilt with
@@ -705,9 +707,8 @@ static void refresh_state(Session& S, Plan& p) {
             launch_refresh_views(live, p.cameras.p + v0, n, S.bounds.center, key.ss, p.size, key.force_two,
                                  p.state_count.p + cstride * v0, cstride, p.raster_state.p + 4 * v0,
                                  own_bits ? p.state_bits.p + w0 : nullptr, p.ref_bits.p + w0, p.words,
-                                 p.pop.p + 4 * v0, fields ? p.ref_field.p + s0 : nullptr,
-                                 fields ? S.scratch.vfield.p : nullptr, S.scratch.vg.p, S.scratch.vsv.p,
-                                 S.scratch.vsn.p, S.scratch.vsd.p, fields ? p.t1.p + t0 : nullptr,
+                                 p.pop.p + 4 * v0, fields ? p.ref_field.p + s0 : nullptr, nullptr, nullptr,
+                                 nullptr, nullptr, nullptr, fields ? p.t1.p + t0 : nullptr,
                                  fields ? p.t2.p + t0 : nullptr, saturate, st);
         }
         B200_CUDA(cudaMemcpyAsync(hpop.data(), p.pop.p, hpop.size() * 8, cudaMemcpyDeviceToHost, st));
@@ -1322,8 +1323,9 @@ static void resolve_gates(Session& S, const blitz_eval_settings gates_in[4], Gat
 }
 
 // Per-view data of a whole candidate mesh against the plan's reference, all
-// views in a handful of launches (counts, coverage, exact field, tile maxima,
-// popcounts, per-view maxima), left in the plan's trial buffers.
+// views in a handful of launches (counts, coverage, tile maxima from the
+// reference field and from searches, popcounts, per-view maxima), left in
+// the plan's trial buffers.
 static void trial_views(Session& S, Plan& p, const DevMesh& cand, uint64_t tag) {
     cudaStream_t st = S.stream;
     const size_t samples = size_t(p.size) * p.size, cstride = count_stride(samples);
@@ -1345,9 +1347,9 @@ static void trial_views(Session& S, Plan& p, const DevMesh& cand, uint64_t tag) 
     ensure_trial(p);
     ensure_tile_data(S, p);
     // Plans of the same views (cameras, screen, supersample, sides) against
-    // the other reference: the trial's counts, coverage and field are the
-    // same, so they take copies and only their tile maxima and popcounts
-    // against their own reference are computed.
+    // the other reference: the trial's counts and coverage are the same, so
+    // they take copies and only their tile maxima and popcounts against their
+    // own reference are computed.
     std::vector<Plan*> same_views;
     for (auto& kv : S.plans) {
         Plan& q = *kv.second;
@@ -1360,8 +1362,7 @@ static void trial_views(Session& S, Plan& p, const DevMesh& cand, uint64_t tag) 
         ensure_tile_data(S, q);
         same_views.push_back(&q);
     }
-    const uint32_t chunk = field_chunk(S, p);
-    Scratch& x = S.scratch;
+    const uint32_t chunk = p.views; // no state field (tile maxima by searches): all views at once
     auto read_back = [&](Plan& q) {
         launch_view_maxima(q.trial_t1.p, q.trial_t2.p, tiles, q.views, q.trial_max.p, st);
         B200_CUDA(cudaMemcpyAsync(q.trial_hpop.data(), q.trial_pop.p, q.trial_hpop.size() * 8, cudaMemcpyDeviceToHost,
@@ -1378,7 +1379,7 @@ static void trial_views(Session& S, Plan& p, const DevMesh& cand, uint64_t tag) 
             launch_refresh_views(cand, p.cameras.p + v0, n, S.bounds.center, p.key.ss, p.size, p.key.force_two,
                                  p.trial_count.p + cstride * v0, cstride, p.trial_state.p + 4 * v0,
                                  p.trial_bits.p + w0, p.ref_bits.p + w0, p.words, p.trial_pop.p + 4 * v0,
-                                 p.ref_field.p + s0, x.vfield.p, x.vg.p, x.vsv.p, x.vsn.p, x.vsd.p,
+                                 p.ref_field.p + s0, nullptr, nullptr, nullptr, nullptr, nullptr,
                                  p.trial_t1.p + t0, p.trial_t2.p + t0, saturate, st);
             for (Plan* q : same_views) {
                 B200_CUDA(cudaMemcpyAsync(q->trial_count.p + cstride * v0, p.trial_count.p + cstride * v0,
@@ -1388,8 +1389,7 @@ static void trial_views(Session& S, Plan& p, const DevMesh& cand, uint64_t tag) 
                 B200_CUDA(cudaMemcpyAsync(q->trial_state.p + 4 * v0, p.trial_state.p + 4 * v0, 16 * size_t(n),
                                           cudaMemcpyDeviceToDevice, st));
                 launch_compare_views(n, p.size, p.trial_bits.p + w0, q->ref_bits.p + w0, p.words, q->ref_field.p + s0,
-                                     x.vfield.p, q->trial_t1.p + t0, q->trial_t2.p + t0, q->trial_pop.p + 4 * v0,
-                                     st);
+                                     nullptr, q->trial_t1.p + t0, q->trial_t2.p + t0, q->trial_pop.p + 4 * v0, st);
             }
         }
         read_back(p);
