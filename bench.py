@@ -50,9 +50,12 @@ GATE_ARGS = [(SCREEN, SOURCE_LIMIT, VIEWS, SS, SS, 1.0), (SCREEN, TRANSITION_LIM
 K_AUDIT_TRAFFIC = 45_381_120
 K_AUDIT_ISSUE_PCT = 65.6
 # DRAM bytes (read + write) of the batched workload's audit kernels per
-# batch: not yet captured (None).
-K_BATCH_TRAFFIC = None
-K_BATCH_TRAFFIC_NOTE = "not captured"
+# batch, from one ncu capture of each tier on the 2-mesh case (huge tier
+# 22.6 KB a unit, warp tier 1.0 KB a unit) scaled to the 64-mesh batch's
+# units (126,277 huge-tier, 262,144 warp-tier).
+K_BATCH_TRAFFIC = 3_120_000_000
+K_BATCH_TRAFFIC_NOTE = ("ncu dram__bytes_read + dram__bytes_write on the 2-mesh case per tier, scaled by units "
+                        "to the full batch")
 
 
 BATCH_WORKLOAD = ("batched plain audit: 64 meshes (noisy spheres, R/r=3 tori, value-noise heightfields; "
