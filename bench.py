@@ -923,8 +923,10 @@ def run_ribbons(args, local: int) -> dict:
     the plain chain)."""
     from blitzremesher_b200 import synthetic as syn
 
-    mesh = syn.ribbons(2000, seed=5)
-    label = f"2,000 ribbon cards ({mesh.face_count} faces), two-sided"
+    cards = args.ribbon_cards
+    mesh = syn.ribbons(cards, seed=5)
+    label = f"{cards:,} ribbon cards ({mesh.face_count} faces), two-sided" + (
+        "" if cards == 2000 else " (not the workload: smaller case)")
     out = run_chain(args, local, mesh, RIBBON_CHAIN, 0, label)
     out["note"] = f"trial budget {RIBBON_CHAIN['budget']} batches of up to 64 collapses per level"
     if not args.no_surrogate:
@@ -995,6 +997,8 @@ def main() -> None:
     ap.add_argument("--meshes", type=int, default=BATCH_MESHES, help="meshes of the batched set (64 = the workload)")
     ap.add_argument("--rock-level", type=int, default=8,
                     help="icosphere level of the rock1m chain's mesh (8 = the workload, 1.31 M faces)")
+    ap.add_argument("--ribbon-cards", type=int, default=2000,
+                    help="cards of the ribbons chain's mesh (2000 = the workload, 400k faces)")
     ap.add_argument("--chain-budget", type=int, default=0,
                     help="trials per level of the rock1m chain (0 = the workload's 40)")
     args = ap.parse_args()

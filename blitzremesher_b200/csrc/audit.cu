@@ -316,12 +316,13 @@ __device__ void region_word_rows(const FaceSetup* faces, uint32_t nok, int wx0, 
 }
 
 // `spill` (small tier only): units that overflow the tier's limits append
-// their unit index `u` there for the large tier instead of falling back.
+// their unit index `u` there for the large tier instead of falling back, or
+// to `far` (may be null) when their region is beyond the huge tier's.
 template <class L>
 __device__ void audit_unit(const CandidateRecord* __restrict__ rec, const PlanDev& plan, uint32_t v,
                            WarpScratch<L>& ws, ViewRecord* out, unsigned long long* stats, uint32_t u,
                            uint32_t* spill, uint32_t heavy = 0xffffffffu, FaceSetup* face_table = nullptr,
-                           short2* iv_table = nullptr, uint16_t* pair_table = nullptr) {
+                           short2* iv_table = nullptr, uint16_t* pair_table = nullptr, uint32_t* far = nullptr) {
     // The face setups: in the warp's scratch, or in shared memory for the
     // tiers whose scratch is global (the row sweep reads them every row).
     FaceSetup* const faces = face_table ? face_table : ws.faces;
@@ -440,7 +441,7 @@ __device__ void audit_unit(const CandidateRecord* __restrict__ rec, const PlanDe
     int dchg = 0, dtot = 0, dcov = 0;
     uint32_t qn = 0, region_changed = 0, nflips = 0;
     int region_words = 0;
-    bool fallback = false;
+    bool fallback = false, beyond_huge = false;
     CandMask cmask;
     cmask.state = pv.state_bits;
     cmask.region = ws.region;
@@ -476,6 +477,7 @@ __device__ void audit_unit(const CandidateRecord* __restrict__ rec, const PlanDe
         if (words > kRegionWords || rows > kRegionRows ||
             (!kSweep && uint32_t(bws) * uint32_t(bh) > uint32_t(kDeltaSamples))) {
             fallback = true;
+            beyond_huge = words > LimitsHuge::kRegionWords || rows > LimitsHuge::kRegionRows;
         } else {
             samples = uint64_t(rows) * uint64_t(words) * 32;
             // ws.region holds the candidate's coverage words XOR the state's
@@ -854,7 +856,11 @@ __device__ void audit_unit(const CandidateRecord* __restrict__ rec, const PlanDe
     if (fallback) r.flags |= kRecFallback;
     if (best >= kExactLimit) r.flags |= kRecLarge;
     if (lane == 0) {
-        if (fallback && spill) spill[1 + atomicAdd(spill, 1u)] = u;
+        if (fallback && spill) {
+            // a region beyond the huge tier's goes straight to the giant tier
+            uint32_t* dst = far && beyond_huge ? far : spill;
+            dst[1 + atomicAdd(dst, 1u)] = u;
+        }
         *out = r;
         if (stats) {
             // profiling counters (kAuditStats slots): units, region samples,
@@ -950,7 +956,7 @@ __global__ void __launch_bounds__(kAuditWarps * 32, kMinBlocks)
             record_write(slot, r);
             continue;
         }
-        audit_unit(rec, *plan, v, ws, slot, stats, u, spill, job.heavy);
+        audit_unit(rec, *plan, v, ws, slot, stats, u, spill, job.heavy, nullptr, nullptr, nullptr, job.far);
     }
 }
 
@@ -1127,14 +1133,33 @@ void launch_audit(const AuditJob& job, unsigned long long* stats, uint32_t* queu
     const bool big = huge && giant && giant->spill && giant->scratch && giant->blocks;
     AuditJob tuned = job;
     tuned.heavy = (variant & kAuditSpillHeavy) && huge && huge_blocks >= uint32_t(sms) ? kHeavyUnit : 0xffffffffu;
-    cudaMemsetAsync(queue, 0, 16, s);
+    // units beyond the huge tier's regions go from the warp tier straight to
+    // the giant tier, which takes them while the huge tier runs
+    const bool far = big && giant->far;
+    tuned.far = far ? giant->far : nullptr;
+    cudaMemsetAsync(queue, 0, 20, s);
     if (spill) cudaMemsetAsync(spill, 0, 4, s);
     if (huge) cudaMemsetAsync(spill_huge, 0, 4, s);
     if (big) cudaMemsetAsync(giant->spill, 0, 4, s);
+    if (far) cudaMemsetAsync(giant->far, 0, 4, s);
     uint32_t* next = big ? giant->spill : nullptr;
     if (marks) cudaEventRecord(marks[0], s);
     kernel<<<uint32_t(grid), kAuditWarps * 32, smem, s>>>(tuned, stats, queue, spill);
     if (marks) cudaEventRecord(marks[1], s);
+    const bool beside = far && giant->side && giant->fork && giant->join;
+    if (far) {
+        cudaStream_t gs = s;
+        if (beside) {
+            cudaEventRecord(giant->fork, s);
+            cudaStreamWaitEvent(giant->side, giant->fork, 0);
+            gs = giant->side;
+        }
+        k_audit_global<LimitsGiant, kGiantWarps>
+            <<<giant->blocks, kGiantWarps * 32, kGiantWarps * kGlobalTierWarpSmem, gs>>>(job, stats, giant->far,
+                                                                                        queue + 4, giant->scratch,
+                                                                                        nullptr);
+        if (beside) cudaEventRecord(giant->join, giant->side);
+    }
     if (huge && huge_blocks >= uint32_t(sms)) {
         // enough huge-tier warps: units the warp tier spills go there directly
         k_audit_global<LimitsHuge, kHugeWarps>
@@ -1150,6 +1175,7 @@ void launch_audit(const AuditJob& job, unsigned long long* stats, uint32_t* queu
                                                                                        queue + 2, huge_scratch, next);
     }
     if (marks) cudaEventRecord(marks[2], s);
+    if (beside) cudaStreamWaitEvent(s, giant->join, 0); // the giant scratch is free again
     if (big)
         k_audit_global<LimitsGiant, kGiantWarps>
             <<<giant->blocks, kGiantWarps * 32, kGiantWarps * kGlobalTierWarpSmem, s>>>(job, stats, giant->spill,

@@ -209,6 +209,7 @@ struct AuditJob {
     uint32_t nentries;
     uint64_t total;            // units
     uint32_t heavy;            // set by launch_audit
+    uint32_t* far;             // set by launch_audit: units beyond the huge tier's regions (1 + units), or null
 };
 // variant: the warp tier's limits (kAuditTierSmall: regions up to 128 x 64
 // samples, 3 blocks per SM; kAuditTierMedium: 256 x 128, 1 block per SM).
@@ -223,8 +224,15 @@ struct GiantTier {
     uint32_t* spill;
     unsigned char* scratch;
     uint32_t blocks;
+    // Units whose region is beyond the huge tier's, listed by the warp tier
+    // (1 + units words, or null): the giant tier takes them while the huge
+    // tier runs, on `side` (forked from and joined to the launch stream by
+    // `fork` / `join`; null: after the warp tier on the same stream).
+    uint32_t* far = nullptr;
+    cudaStream_t side = nullptr;
+    cudaEvent_t fork = nullptr, join = nullptr;
 };
-// queue: 4 words (work cursors). marks (profiling, may be null): 4 events
+// queue: 5 words (work cursors). marks (profiling, may be null): 4 events
 // recorded before the warp tier, after it, after the large / huge tier and
 // after the giant tier.
 void launch_audit(const AuditJob& job, unsigned long long* stats, uint32_t* queue, uint32_t* spill,

@@ -938,7 +938,7 @@ static HugeScratch& huge_scratch(int device) {
 
 // Plans of rasters above 256 x 256 can hold regions beyond the large tier.
 static void run_audit(Session& S, Plan& p, uint32_t n, unsigned long long* stats, cudaStream_t st) {
-    S.work_queue.ensure(S.pool, 4);
+    S.work_queue.ensure(S.pool, 8);
     S.spill.ensure(S.pool, size_t(n) * p.views + 1);
     AuditJob job{};
     job.plan = p.dev, job.recs = S.records.p, job.out = p.records.p, job.total = uint64_t(n) * p.views;
@@ -2498,7 +2498,8 @@ struct blitz_audit_batch {
     std::vector<Buf<AuditEntry>> entries; // per plan slot
     std::vector<uint32_t> nentries;
     std::vector<uint64_t> units;
-    Buf<uint32_t> queue, spill, spill_huge, spill_giant, exact;
+    Buf<uint32_t> queue, spill, spill_huge, spill_giant, spill_far, exact;
+    cudaEvent_t giant_fork = nullptr, giant_join = nullptr;
     Buf<unsigned char> huge, giant;
     uint32_t huge_blocks = 0;
     int variant = kAuditTierSmall;
@@ -2550,6 +2551,8 @@ struct blitz_audit_batch {
             if (e) cudaEventDestroy(e);
         for (auto e : side_done) cudaEventDestroy(e);
         for (auto e : marks) cudaEventDestroy(e);
+        if (giant_fork) cudaEventDestroy(giant_fork);
+        if (giant_join) cudaEventDestroy(giant_join);
         for (auto s_ : side) cudaStreamDestroy(s_);
         if (fork) cudaEventDestroy(fork);
         stats.release();
@@ -2557,7 +2560,7 @@ struct blitz_audit_batch {
         if (graph) cudaGraphDestroy(graph);
         records.release(), queue.release(), spill.release(), spill_huge.release(), exact.release(), huge.release();
         host_cands.release(), host_out.release();
-        spill_giant.release(), giant.release();
+        spill_giant.release(), spill_far.release(), giant.release();
         entries.clear();
         if (stream) cudaStreamDestroy(stream);
     }
@@ -2645,7 +2648,7 @@ static void batch_candidates(blitz_audit_batch* b, const blitz_collapse* cands, 
             b->units[j] = first;
             max_units = std::max(max_units, first);
         }
-        b->queue.ensure(b->pool, 4);
+        b->queue.ensure(b->pool, 8);
         b->spill.ensure(b->pool, max_units + 1);
         b->exact.ensure(b->pool, ns);
         if (big && !b->huge.p) {
@@ -2656,8 +2659,8 @@ static void batch_candidates(blitz_audit_batch* b, const blitz_collapse* cands, 
         }
         if (big) b->spill_huge.ensure(b->pool, max_units + 1);
         if (giant && !b->giant.p) b->giant = Buf<unsigned char>(b->pool, audit_giant_scratch_bytes(kGiantBlocks));
-        if (giant) b->spill_giant.ensure(b->pool, max_units + 1);
-        const GiantTier giant_tier{b->spill_giant.p, b->giant.p, kGiantBlocks};
+        if (giant) b->spill_giant.ensure(b->pool, max_units + 1), b->spill_far.ensure(b->pool, max_units + 1);
+        GiantTier giant_tier{b->spill_giant.p, b->giant.p, kGiantBlocks};
         B200_CUDA(cudaStreamSynchronize(st));
         // The launch sequence: per-session records, one audit job per plan
         // slot over all sessions, per-session verdicts.
@@ -2672,6 +2675,17 @@ static void batch_candidates(blitz_audit_batch* b, const blitz_collapse* cands, 
             b->marks.push_back(e);
         }
         b->ensure_side(std::min<size_t>(ns, 16));
+        if (giant) {
+            // units beyond the huge tier's regions: the giant tier beside the
+            // huge tier, on the first side stream
+            if (!b->giant_fork) {
+                B200_CUDA(cudaEventCreateWithFlags(&b->giant_fork, cudaEventDisableTiming));
+                B200_CUDA(cudaEventCreateWithFlags(&b->giant_join, cudaEventDisableTiming));
+            }
+            giant_tier.far = b->spill_far.p;
+            giant_tier.side = b->side.empty() ? nullptr : b->side[0];
+            giant_tier.fork = b->giant_fork, giant_tier.join = b->giant_join;
+        }
         auto body = [&](int variant) {
             b->side_by_side(ns, st, [&](size_t i, cudaStream_t ss) {
                 if (!counts[i]) return;
@@ -2743,7 +2757,7 @@ static void batch_candidates(blitz_audit_batch* b, const blitz_collapse* cands, 
         for (auto& e : b->entries) put(&e.p, sizeof(void*));
         for (const void* q : {(const void*)b->records.p, (const void*)b->queue.p, (const void*)b->spill.p,
                               (const void*)b->spill_huge.p, (const void*)b->huge.p, (const void*)b->exact.p,
-                              (const void*)b->spill_giant.p, (const void*)b->giant.p})
+                              (const void*)b->spill_giant.p, (const void*)b->giant.p, (const void*)b->spill_far.p})
             put(&q, sizeof(q));
         if ((flags & 1u) && off[ns]) {
             if (b->exec && sig == b->signature) {
