@@ -150,7 +150,7 @@ void launch_refresh_views(const DevMesh& m, const Camera* cams_dev, uint32_t nvi
                           uint32_t* state_bits, const uint32_t* ref_bits, uint32_t wstride,
                           unsigned long long* pop, const uint32_t* ref_field, uint32_t* state_field, uint32_t* g,
                           int32_t* sv, long long* sn, long long* sd, int32_t* t1, int32_t* t2, bool saturate,
-                          cudaStream_t s);
+                          cudaStream_t s, uint32_t* wide = nullptr);
 // Exact squared distance fields of nviews masks at once (launch_field's row
 // pass and column envelope; scratch g, sv, sn, sd of size^2 * nviews).
 void launch_fields_views(const uint32_t* bits, uint32_t wstride, uint32_t nviews, uint32_t size, uint32_t* g,

@@ -381,6 +381,30 @@ __global__ void k_count_views(ViewsArgs a, uint8_t* counts, size_t stride, uint3
                 else count_sample(c, size_t(y) * a.size + x, st);
             }
 }
+// Face counts of every view into 32-bit counters (`wide`, samples per view;
+// no overflow, for the deep overlaps of small screens), then narrowed to
+// counts held at 255 by k_narrow_counts_views: far fewer retries than the
+// compare-and-swap counts where hundreds of faces cover a sample.
+__global__ void k_count_views_wide(ViewsArgs a, uint32_t* wide, uint32_t* state) {
+    const uint32_t f = blockIdx.x * blockDim.x + threadIdx.x, v = blockIdx.y;
+    if (f >= a.m.nf) return;
+    const Camera cam = a.cams[v];
+    FaceSetup s = face_setup_view(a, cam, f);
+    if (s.status == kFaceClipBox || s.status == kFaceClipZ) {
+        atomicAdd(state + 4 * v + 2, 1u);
+        return;
+    }
+    if (s.status != kFaceOk) return;
+    uint32_t* c = wide + size_t(a.size) * a.size * v;
+    for (int y = s.y0; y <= s.y1; ++y)
+        for (int x = s.x0; x <= s.x1; ++x)
+            if (face_covers(s, x, y)) atomicAdd(c + size_t(y) * a.size + x, 1u);
+}
+__global__ void k_narrow_counts_views(const uint32_t* wide, size_t samples, uint8_t* counts, size_t cstride) {
+    const size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    const uint32_t v = blockIdx.y;
+    if (i < samples) counts[cstride * v + i] = uint8_t(min(wide[samples * v + i], 255u));
+}
 __global__ void k_counts_to_bits_views(const uint8_t* counts, size_t cstride, size_t samples, uint32_t* bits,
                                        uint32_t wstride, uint32_t words) {
     const uint32_t w = blockIdx.x * blockDim.x + threadIdx.x, v = blockIdx.y;
@@ -456,13 +480,14 @@ __global__ void k_popcounts_views(const uint32_t* a, const uint32_t* b, uint32_t
 // counts (and clipped/overflow counters), coverage words, popcounts against the
 // reference and, when fields are kept, the tile maxima: from the state field
 // when `state_field` is given, else (ref_field, t1, t2 given) by searches
-// from the reference-only samples.
+// from the reference-only samples. `saturate`: counts held at 255, through
+// 32-bit counters in `wide` (samples * nviews) when given.
 void launch_refresh_views(const DevMesh& m, const Camera* cams_dev, uint32_t nviews, const float* center, uint32_t ss,
                           uint32_t size, bool force_two, uint8_t* counts, size_t cstride, uint32_t* state,
                           uint32_t* state_bits, const uint32_t* ref_bits, uint32_t wstride,
                           unsigned long long* pop, const uint32_t* ref_field, uint32_t* state_field, uint32_t* g,
                           int32_t* sv, long long* sn, long long* sd, int32_t* t1, int32_t* t2, bool saturate,
-                          cudaStream_t s) {
+                          cudaStream_t s, uint32_t* wide) {
     ViewsArgs a;
     a.m = m;
     a.cams = cams_dev;
@@ -473,8 +498,16 @@ void launch_refresh_views(const DevMesh& m, const Camera* cams_dev, uint32_t nvi
     cudaMemsetAsync(state, 0, 16 * size_t(nviews), s);
     if (m.nf) {
         const dim3 grid(blocks_for(m.nf, 128), nviews);
-        if (saturate) k_count_views<true><<<grid, 128, 0, s>>>(a, counts, cstride, state);
-        else k_count_views<false><<<grid, 128, 0, s>>>(a, counts, cstride, state);
+        if (saturate && wide) {
+            cudaMemsetAsync(wide, 0, samples * nviews * 4, s);
+            k_count_views_wide<<<grid, 128, 0, s>>>(a, wide, state);
+            k_narrow_counts_views<<<dim3(uint32_t((samples + 255) / 256), nviews), 256, 0, s>>>(wide, samples, counts,
+                                                                                                 cstride);
+        } else if (saturate) {
+            k_count_views<true><<<grid, 128, 0, s>>>(a, counts, cstride, state);
+        } else {
+            k_count_views<false><<<grid, 128, 0, s>>>(a, counts, cstride, state);
+        }
     }
     const uint32_t words = uint32_t((samples + 63) / 64) * 2;
     if (state_bits) {

@@ -358,6 +358,7 @@ struct Plan {
     Buf<PlanView> dviews;
     std::vector<PlanView> hviews;
     bool state_is_ref = true;
+    bool deep = false; // a raster of this plan had a sample under more than 255 faces
     uint64_t state_revision = ~0ull;
     Buf<ViewRecord> records;
     Buf<uint32_t> raster_state;      // 4 words per view
@@ -383,9 +384,11 @@ struct Scratch {
     Buf<long long> sn, sd;
     Buf<unsigned long long> pop;
     size_t samples = 0;
-    // per-view field scratch of the batched state refresh (vfield: the state
-    // or trial field of the chunk, only used to build the tile maxima)
+    // per-view field scratch of the batched reference fields (vfield unused
+    // by the state and trial refreshes, whose tile maxima come from searches)
     Buf<uint32_t> vg, vfield;
+    // 32-bit face counts of all views of a plan with deep overlaps
+    Buf<uint32_t> wide;
     Buf<int32_t> vsv;
     Buf<long long> vsn, vsd;
     size_t view_entries = 0;
@@ -618,6 +621,19 @@ static void ensure_scratch(Session& S, uint32_t size);
 static size_t count_stride(size_t samples) { return (samples + 3) & ~size_t(3); }
 
 static uint32_t field_chunk(Session& S, const Plan& p);
+// 32-bit counters for a saturated refresh of all views of `p` when they fit
+// a sixteenth of the workspace (at least 256 MiB) and half of what is free,
+// else null (compare-and-swap counts).
+static uint32_t* wide_counts(Session& S, const Plan& p) {
+    Scratch& x = S.scratch;
+    const size_t need = size_t(p.size) * p.size * p.views;
+    if (x.wide.n >= need) return x.wide.p;
+    const size_t room = S.pool.limit - S.pool.used + x.wide.n * 4;
+    if (need * 4 > std::max(size_t(256) << 20, S.pool.limit / 16) || need * 4 > room / 2) return nullptr;
+    x.wide.release();
+    x.wide = Buf<uint32_t>(S.pool, need);
+    return x.wide.p;
+}
 // The reference's exact distance field and the tile-maxima arrays of a plan,
 // built the first time its state differs from the reference.
 static void ensure_tile_data(Session& S, Plan& p) {
@@ -700,7 +716,9 @@ static void refresh_state(Session& S, Plan& p) {
     std::vector<uint32_t>& hstate = p.hstate;
     // Counts of up to 255 faces per sample; a plan with more is rebuilt with
     // counts held at 255 (exact for the audits).
-    for (bool saturate : {false, true}) {
+    for (int pass = p.deep ? 1 : 0; pass < 2; ++pass) {
+        const bool saturate = pass == 1;
+        uint32_t* const wide = saturate ? wide_counts(S, p) : nullptr;
         for (uint32_t v0 = 0; v0 < p.views; v0 += chunk) {
             const uint32_t n = std::min(chunk, p.views - v0);
             const size_t w0 = size_t(p.words) * v0, s0 = samples * v0, t0 = size_t(tiles) * v0;
@@ -709,7 +727,7 @@ static void refresh_state(Session& S, Plan& p) {
                                  own_bits ? p.state_bits.p + w0 : nullptr, p.ref_bits.p + w0, p.words,
                                  p.pop.p + 4 * v0, fields ? p.ref_field.p + s0 : nullptr, nullptr, nullptr,
                                  nullptr, nullptr, nullptr, fields ? p.t1.p + t0 : nullptr,
-                                 fields ? p.t2.p + t0 : nullptr, saturate, st);
+                                 fields ? p.t2.p + t0 : nullptr, saturate, st, wide);
         }
         B200_CUDA(cudaMemcpyAsync(hpop.data(), p.pop.p, hpop.size() * 8, cudaMemcpyDeviceToHost, st));
         B200_CUDA(cudaMemcpyAsync(hstate.data(), p.raster_state.p, hstate.size() * 4, cudaMemcpyDeviceToHost, st));
@@ -718,6 +736,7 @@ static void refresh_state(Session& S, Plan& p) {
         bool overflow = false;
         for (uint32_t v = 0; v < p.views; ++v) overflow |= hstate[4 * v + 3] != 0;
         if (!overflow) break;
+        p.deep = true;
     }
     for (uint32_t v = 0; v < p.views; ++v) {
         PlanView& pv = p.hviews[v];
@@ -1372,7 +1391,9 @@ static void trial_views(Session& S, Plan& p, const DevMesh& cand, uint64_t tag) 
         B200_CUDA(cudaMemcpyAsync(q.trial_hmax.data(), q.trial_max.p, q.trial_hmax.size() * 4, cudaMemcpyDeviceToHost,
                                   st));
     };
-    for (bool saturate : {false, true}) { // as in refresh_state: counts held at 255 on overflow
+    for (int pass = p.deep ? 1 : 0; pass < 2; ++pass) { // as in refresh_state
+        const bool saturate = pass == 1;
+        uint32_t* const wide = saturate ? wide_counts(S, p) : nullptr;
         for (uint32_t v0 = 0; v0 < p.views; v0 += chunk) {
             const uint32_t n = std::min(chunk, p.views - v0);
             const size_t w0 = size_t(p.words) * v0, s0 = samples * v0, t0 = size_t(tiles) * v0;
@@ -1380,7 +1401,7 @@ static void trial_views(Session& S, Plan& p, const DevMesh& cand, uint64_t tag) 
                                  p.trial_count.p + cstride * v0, cstride, p.trial_state.p + 4 * v0,
                                  p.trial_bits.p + w0, p.ref_bits.p + w0, p.words, p.trial_pop.p + 4 * v0,
                                  p.ref_field.p + s0, nullptr, nullptr, nullptr, nullptr, nullptr,
-                                 p.trial_t1.p + t0, p.trial_t2.p + t0, saturate, st);
+                                 p.trial_t1.p + t0, p.trial_t2.p + t0, saturate, st, wide);
             for (Plan* q : same_views) {
                 B200_CUDA(cudaMemcpyAsync(q->trial_count.p + cstride * v0, p.trial_count.p + cstride * v0,
                                           cstride * n, cudaMemcpyDeviceToDevice, st));
@@ -1399,6 +1420,7 @@ static void trial_views(Session& S, Plan& p, const DevMesh& cand, uint64_t tag) 
         bool overflow = false;
         for (uint32_t v = 0; v < p.views; ++v) overflow |= p.trial_hstate[4 * v + 3] != 0;
         if (!overflow) break;
+        p.deep = true;
     }
     p.trial_tag = tag;
     for (Plan* q : same_views) q->trial_tag = tag;
