@@ -384,9 +384,9 @@ struct Scratch {
     Buf<long long> sn, sd;
     Buf<unsigned long long> pop;
     size_t samples = 0;
-    // per-view field scratch of the batched reference fields (vfield unused
-    // by the state and trial refreshes, whose tile maxima come from searches)
-    Buf<uint32_t> vg, vfield;
+    // per-view scratch of the batched reference fields (row distances,
+    // envelope stacks)
+    Buf<uint32_t> vg;
     // 32-bit face counts of all views of a plan with deep overlaps
     Buf<uint32_t> wide;
     Buf<int32_t> vsv;
@@ -655,25 +655,24 @@ static void ensure_tile_data(Session& S, Plan& p) {
                             x.vg.p, p.ref_field.p + samples * v0, x.vsv.p, x.vsn.p, x.vsd.p, st);
 }
 
-// Views per refresh launch whose field scratch (row distances, envelope
-// stacks, the field itself: 28 bytes a sample) fits the budget below; sizes
-// the scratch for it.
+// Views per reference-field launch whose scratch (row distances and
+// envelope stacks: 24 bytes a sample) fits the budget below; sizes the
+// scratch for it.
 static uint32_t field_chunk(Session& S, const Plan& p) {
     const size_t samples = size_t(p.size) * p.size;
     Scratch& x = S.scratch;
     // An eighth of the workspace (at least 256 MiB), at most half of what is
     // free (counting the scratch held now): at 4160 x 4160 samples a view
-    // needs 485 MB, and one view per launch leaves most SMs idle.
+    // needs 415 MB, and one view per launch leaves most SMs idle.
     const size_t floor_bytes = size_t(256) << 20;
-    const size_t room = S.pool.limit - S.pool.used + x.view_entries * 28;
+    const size_t room = S.pool.limit - S.pool.used + x.view_entries * 24;
     const size_t budget = std::max(floor_bytes, std::min(S.pool.limit / 8, room / 2));
-    const uint32_t chunk = uint32_t(std::max<size_t>(1, std::min<size_t>(p.views, budget / (samples * 28))));
+    const uint32_t chunk = uint32_t(std::max<size_t>(1, std::min<size_t>(p.views, budget / (samples * 24))));
     const size_t entries = samples * chunk;
     if (x.view_entries < entries) {
-        x.vg.release(), x.vfield.release(), x.vsv.release(), x.vsn.release(), x.vsd.release();
+        x.vg.release(), x.vsv.release(), x.vsn.release(), x.vsd.release();
         x.view_entries = 0;
         x.vg = Buf<uint32_t>(S.pool, entries);
-        x.vfield = Buf<uint32_t>(S.pool, entries);
         x.vsv = Buf<int32_t>(S.pool, entries);
         x.vsn = Buf<long long>(S.pool, entries);
         x.vsd = Buf<long long>(S.pool, entries);
@@ -708,9 +707,8 @@ static void refresh_state(Session& S, Plan& p) {
     const bool fields = p.tiled && !p.state_is_ref;
     const uint32_t tiles = ((p.size + 31) / 32) * ((p.size + 31) / 32);
     if (fields) ensure_tile_data(S, p);
-    // Views per launch: the field scratch of one chunk stays within 256 MiB.
-    // tile maxima by searches from the reference-only samples: no state
-    // field, all views in one launch
+    // Tile maxima by searches from the reference-only samples: no state
+    // field, all views in one launch.
     const uint32_t chunk = p.views;
     std::vector<unsigned long long>& hpop = p.hpop;
     std::vector<uint32_t>& hstate = p.hstate;
