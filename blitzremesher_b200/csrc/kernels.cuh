@@ -150,7 +150,26 @@ void launch_refresh_views(const DevMesh& m, const Camera* cams_dev, uint32_t nvi
                           uint32_t* state_bits, const uint32_t* ref_bits, uint32_t wstride,
                           unsigned long long* pop, const uint32_t* ref_field, uint32_t* state_field, uint32_t* g,
                           int32_t* sv, long long* sn, long long* sd, int32_t* t1, int32_t* t2, bool saturate,
-                          cudaStream_t s, uint32_t* wide = nullptr);
+                          cudaStream_t s, uint32_t* wide = nullptr,
+                          bool recount = true);
+// A combined trial as changes of the state: which state faces the batch
+// changes (a corner remapped by `remap`, or in a class that `owner` moves to
+// a placement), whether each survives (`keep`) and where (`offsets` into the
+// trial mesh `trial`).
+struct TrialDelta {
+    const uint32_t* geometry;
+    const uint32_t* remap;
+    const uint32_t* owner;
+    const uint32_t* keep;
+    const uint32_t* offsets;
+    DevMesh trial;
+};
+// The trial's face counts of all views from the state's (already copied into
+// `counts`, clip counters into `state`): each changed state face's samples
+// -1, its surviving trial face's +1 (overflow past 255 sets state[4v+3]).
+void launch_count_delta_views(const DevMesh& m, const TrialDelta& d, const Camera* cams_dev, uint32_t nviews,
+                              const float* center, uint32_t ss, uint32_t size, bool force_two, uint8_t* counts,
+                              size_t cstride, uint32_t* state, cudaStream_t s);
 // Exact squared distance fields of nviews masks at once (launch_field's row
 // pass and column envelope; scratch g, sv, sn, sd of size^2 * nviews).
 void launch_fields_views(const uint32_t* bits, uint32_t wstride, uint32_t nviews, uint32_t size, uint32_t* g,

@@ -381,6 +381,46 @@ __global__ void k_count_views(ViewsArgs a, uint8_t* counts, size_t stride, uint3
                 else count_sample(c, size_t(y) * a.size + x, st);
             }
 }
+// Changed faces of a combined trial, all views: the state's face leaves its
+// samples (-1; every covered sample counts it, so no count goes below zero),
+// the trial's face, when it survives, enters (+1; passing 255 sets the view's
+// overflow flag, and the caller counts afresh).
+__global__ void k_count_delta_views(ViewsArgs a, TrialDelta d, uint8_t* counts, size_t stride, uint32_t* state) {
+    const uint32_t f = blockIdx.x * blockDim.x + threadIdx.x, v = blockIdx.y;
+    if (f >= a.m.nf) return;
+    bool changed = false;
+    for (int j = 0; j < 3; ++j) {
+        const uint32_t id = a.m.idx[3 * f + j];
+        changed |= d.remap[id] != kNone || d.owner[d.geometry[id]] != kNone;
+    }
+    if (!changed) return;
+    const Camera cam = a.cams[v];
+    uint32_t* st = state + 4 * v;
+    uint8_t* c = counts + stride * v;
+    const FaceSetup s = face_setup_view(a, cam, f);
+    if (s.status == kFaceClipBox || s.status == kFaceClipZ) {
+        atomicSub(st + 2, 1u);
+    } else if (s.status == kFaceOk) {
+        for (int y = s.y0; y <= s.y1; ++y)
+            for (int x = s.x0; x <= s.x1; ++x)
+                if (face_covers(s, x, y)) {
+                    const size_t i = size_t(y) * a.size + x;
+                    atomicSub(reinterpret_cast<uint32_t*>(c) + (i >> 2), 1u << (8 * uint32_t(i & 3)));
+                }
+    }
+    if (!d.keep[f]) return;
+    ViewsArgs b = a;
+    b.m = d.trial;
+    const FaceSetup t = face_setup_view(b, cam, d.offsets[f]);
+    if (t.status == kFaceClipBox || t.status == kFaceClipZ) {
+        atomicAdd(st + 2, 1u);
+        return;
+    }
+    if (t.status != kFaceOk) return;
+    for (int y = t.y0; y <= t.y1; ++y)
+        for (int x = t.x0; x <= t.x1; ++x)
+            if (face_covers(t, x, y)) count_sample(c, size_t(y) * a.size + x, st);
+}
 // Face counts of every view into 32-bit counters (`wide`, samples per view;
 // no overflow, for the deep overlaps of small screens), then narrowed to
 // counts held at 255 by k_narrow_counts_views: far fewer retries than the
@@ -481,22 +521,23 @@ __global__ void k_popcounts_views(const uint32_t* a, const uint32_t* b, uint32_t
 // reference and, when fields are kept, the tile maxima: from the state field
 // when `state_field` is given, else (ref_field, t1, t2 given) by searches
 // from the reference-only samples. `saturate`: counts held at 255, through
-// 32-bit counters in `wide` (samples * nviews) when given.
+// 32-bit counters in `wide` (samples * nviews) when given. `recount` false:
+// `counts` and `state` already hold the views' counts (launch_count_delta_views).
 void launch_refresh_views(const DevMesh& m, const Camera* cams_dev, uint32_t nviews, const float* center, uint32_t ss,
                           uint32_t size, bool force_two, uint8_t* counts, size_t cstride, uint32_t* state,
                           uint32_t* state_bits, const uint32_t* ref_bits, uint32_t wstride,
                           unsigned long long* pop, const uint32_t* ref_field, uint32_t* state_field, uint32_t* g,
                           int32_t* sv, long long* sn, long long* sd, int32_t* t1, int32_t* t2, bool saturate,
-                          cudaStream_t s, uint32_t* wide) {
+                          cudaStream_t s, uint32_t* wide, bool recount) {
     ViewsArgs a;
     a.m = m;
     a.cams = cams_dev;
     a.center[0] = center[0], a.center[1] = center[1], a.center[2] = center[2];
     a.ss = ss, a.size = size, a.force_two = force_two, a.pad = 0;
     const size_t samples = size_t(size) * size;
-    cudaMemsetAsync(counts, 0, cstride * nviews, s);
-    cudaMemsetAsync(state, 0, 16 * size_t(nviews), s);
-    if (m.nf) {
+    if (recount) cudaMemsetAsync(counts, 0, cstride * nviews, s);
+    if (recount) cudaMemsetAsync(state, 0, 16 * size_t(nviews), s);
+    if (m.nf && recount) {
         const dim3 grid(blocks_for(m.nf, 128), nviews);
         if (saturate && wide) {
             cudaMemsetAsync(wide, 0, samples * nviews * 4, s);
@@ -533,6 +574,18 @@ void launch_refresh_views(const DevMesh& m, const Camera* cams_dev, uint32_t nvi
     if (grid > 64) grid = 64;
     k_popcounts_views<<<dim3(grid, nviews), kThreads, 0, s>>>(ref_bits, state_bits ? state_bits : ref_bits, wstride,
                                                                words, pop);
+}
+
+void launch_count_delta_views(const DevMesh& m, const TrialDelta& d, const Camera* cams_dev, uint32_t nviews,
+                              const float* center, uint32_t ss, uint32_t size, bool force_two, uint8_t* counts,
+                              size_t cstride, uint32_t* state, cudaStream_t s) {
+    if (!m.nf) return;
+    ViewsArgs a;
+    a.m = m;
+    a.cams = cams_dev;
+    a.center[0] = center[0], a.center[1] = center[1], a.center[2] = center[2];
+    a.ss = ss, a.size = size, a.force_two = force_two, a.pad = 0;
+    k_count_delta_views<<<dim3(blocks_for(m.nf, 128), nviews), 128, 0, s>>>(a, d, counts, cstride, state);
 }
 
 // Exact squared distance fields of `nviews` masks (view v's coverage at

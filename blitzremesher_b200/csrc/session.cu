@@ -932,7 +932,7 @@ static void ensure_trial_buffers(Session& S) {
     S.trial_collapse = Buf<blitz_collapse>(S.pool, 1);
 }
 
-static void trial_views(Session& S, Plan& p, const DevMesh& cand, uint64_t tag);
+static void trial_views(Session& S, Plan& p, const DevMesh& cand, uint64_t tag, const TrialDelta* delta = nullptr);
 static bool gate_from_trial(const Plan& p, const GateSettings& g, Measurement& result);
 
 // Global-memory scratch of the huge audit tier, one per device and shared by
@@ -1012,11 +1012,11 @@ static PlanKey plan_key_of(const Session& S, int gi, const blitz_eval_settings& 
 // fields when the plan keeps them and no view clips or refines, else the
 // per-view full-raster path.
 static Measurement gate_of_trial(Session& S, const DevMesh& cand, const GateRef& gate, int gi, uint64_t tag,
-                                 const ViewRecord* recs_dev = nullptr) {
+                                 const ViewRecord* recs_dev = nullptr, const TrialDelta* delta = nullptr) {
     Plan& p = plan_for(S, plan_key_of(S, gi, *gate.es));
     Measurement r;
     if (!p.resource_limited && p.tiled) {
-        if (p.trial_tag != tag) trial_views(S, p, cand, tag);
+        if (p.trial_tag != tag) trial_views(S, p, cand, tag, delta);
         if (gate_from_trial(p, gate.g, r)) return r;
     }
     std::vector<ViewRecord> recs;
@@ -1343,7 +1343,7 @@ static void resolve_gates(Session& S, const blitz_eval_settings gates_in[4], Gat
 // views in a handful of launches (counts, coverage, tile maxima from the
 // reference field and from searches, popcounts, per-view maxima), left in
 // the plan's trial buffers.
-static void trial_views(Session& S, Plan& p, const DevMesh& cand, uint64_t tag) {
+static void trial_views(Session& S, Plan& p, const DevMesh& cand, uint64_t tag, const TrialDelta* delta) {
     cudaStream_t st = S.stream;
     const size_t samples = size_t(p.size) * p.size, cstride = count_stride(samples);
     const uint32_t tiles = ((p.size + 31) / 32) * ((p.size + 31) / 32);
@@ -1392,6 +1392,20 @@ static void trial_views(Session& S, Plan& p, const DevMesh& cand, uint64_t tag) 
     for (int pass = p.deep ? 1 : 0; pass < 2; ++pass) { // as in refresh_state
         const bool saturate = pass == 1;
         uint32_t* const wide = saturate ? wide_counts(S, p) : nullptr;
+        // Exact (not held) state counts of the current state: the trial's are
+        // those plus the changed faces' deltas, instead of a full count.
+        const bool incremental = !saturate && delta && !p.deep && p.state_count.p &&
+                                 p.state_revision == S.state_revision;
+        if (incremental) {
+            B200_CUDA(cudaMemcpyAsync(p.trial_count.p, p.state_count.p, cstride * p.views, cudaMemcpyDeviceToDevice,
+                                      st));
+            B200_CUDA(cudaMemcpyAsync(p.trial_state.p, p.raster_state.p, 16 * size_t(p.views),
+                                      cudaMemcpyDeviceToDevice, st));
+            DevMesh state = S.state.view;
+            state.nf = S.state_faces;
+            launch_count_delta_views(state, *delta, p.cameras.p, p.views, S.bounds.center, p.key.ss, p.size,
+                                     p.key.force_two, p.trial_count.p, cstride, p.trial_state.p, st);
+        }
         for (uint32_t v0 = 0; v0 < p.views; v0 += chunk) {
             const uint32_t n = std::min(chunk, p.views - v0);
             const size_t w0 = size_t(p.words) * v0, s0 = samples * v0, t0 = size_t(tiles) * v0;
@@ -1399,7 +1413,7 @@ static void trial_views(Session& S, Plan& p, const DevMesh& cand, uint64_t tag) 
                                  p.trial_count.p + cstride * v0, cstride, p.trial_state.p + 4 * v0,
                                  p.trial_bits.p + w0, p.ref_bits.p + w0, p.words, p.trial_pop.p + 4 * v0,
                                  p.ref_field.p + s0, nullptr, nullptr, nullptr, nullptr, nullptr,
-                                 p.trial_t1.p + t0, p.trial_t2.p + t0, saturate, st, wide);
+                                 p.trial_t1.p + t0, p.trial_t2.p + t0, saturate, st, wide, !incremental);
             for (Plan* q : same_views) {
                 B200_CUDA(cudaMemcpyAsync(q->trial_count.p + cstride * v0, p.trial_count.p + cstride * v0,
                                           cstride * n, cudaMemcpyDeviceToDevice, st));
@@ -1457,10 +1471,10 @@ static bool gate_from_trial(const Plan& p, const GateSettings& g, Measurement& r
 // The four gates of the combined trial in the session's trial buffers.
 // Returns the failed gate (1..4) or 0 when accepted.
 static int gates_of_trial(Session& S, const DevMesh& cand, const GateRef gates[4], const PlanKey keys[4],
-                          uint64_t tag) {
+                          uint64_t tag, const TrialDelta* delta = nullptr) {
     (void)keys;
     for (int gi = 0; gi < 4; ++gi)
-        if (!measurement_accepted(gate_of_trial(S, cand, gates[gi], gi, tag))) return gi + 1;
+        if (!measurement_accepted(gate_of_trial(S, cand, gates[gi], gi, tag, nullptr, delta))) return gi + 1;
     return 0;
 }
 
@@ -1670,7 +1684,10 @@ static void execute_batched(Session& S, uint32_t target, uint32_t budget, const 
                 cand.idx = S.trial.idx.p;
                 cand.mat = S.state.view.mat ? S.trial.mat.p : nullptr;
                 cand.nf = trial_faces;
-                if (!invalid && trial_faces && gates_of_trial(S, cand, gates, keys, tag) == 0) {
+                // the trial as changes of the state (incremental face counts)
+                const TrialDelta delta{t.geometry.p, S.batch_remap.p, S.batch_owner.p, S.trial_keep.p,
+                                       S.trial_offsets.p, cand};
+                if (!invalid && trial_faces && gates_of_trial(S, cand, gates, keys, tag, &delta) == 0) {
                     S.collapse_dev.ensure(S.pool, 64);
                     launch_gather_window(t.edits.p, S.batch_selected.p, 0, count, S.collapse_dev.p, st);
                     B200_CUDA(cudaMemcpyAsync(chosen.data(), S.collapse_dev.p, count * sizeof(blitz_collapse),
