@@ -517,8 +517,9 @@ typedef struct blitz_audit_batch_info {
     /* the same call, per tier: SM cycles of its longest unit */
     uint64_t tier_max_cycles[4];
     /* last BLITZ_BATCH_PROFILE or BLITZ_BATCH_TIMING call: device time of the
-     * warp tier's launches, of the large / huge tier's and of the giant
-     * tier's */
+     * warp tier's launches, of the large / huge tier's (units whose regions
+     * are beyond the huge tier's run in the giant tier beside it) and of the
+     * giant tier's launches after it */
     float tier_ms[3];
 } blitz_audit_batch_info;
 blitz_status blitz_audit_batch_create(blitz_audit_session* const* sessions, size_t count, blitz_audit_batch** out,
